@@ -1,0 +1,417 @@
+"""Python mirror of the reference's hot-path routines, backed by the B200
+library.  Names, argument meaning and layouts follow the reference
+(flat FP64 row-major arrays, int32 lists); each function cites the routine it
+replaces.  Every call runs CUDA kernels; nothing here computes on the CPU.
+
+Citations: LJ = src/fuller_LJ_npt_md_serial_omp_acc.cpp,
+AI = src/fuller_airebo_npt_md_serial_omp_acc.cpp,
+MM = src/fuller_LJ_npt_mmmd_serial_omp_acc.cpp.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from ._lib import FmdError, NPT, MMTopology, RunParams, Obs, Avg
+
+MAX_NEIGH_RIGID = 80      # LJ:108
+MAX_LJ_NEIGH = 400        # AI:127, MM:119
+MAX_REBO_NEIGH = 12       # AI:126
+LJ_LIST_RC_AIREBO = 3.0 * 3.40 + 2.0    # AI:265 (LJ_RCUT + 2)
+LJ_LIST_RC_MM = 3.0 * 3.431 + 2.0       # MM:339 (RCUT + 2)
+REBO_LIST_RC = 2.0 + 0.3                # AI:116, AI:253
+
+
+def _d(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _i(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _i32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def npt_from_array(a) -> NPT:
+    """{xi, Q, Vg[9], W, Pe, Tt, Nf} -> fmd_npt."""
+    s = NPT()
+    s.xi, s.Q = float(a[0]), float(a[1])
+    for k in range(9):
+        s.Vg[k] = float(a[2 + k])
+    s.W, s.Pe, s.Tt, s.Nf = float(a[11]), float(a[12]), float(a[13]), int(a[14])
+    return s
+
+
+def npt_to_array(s: NPT) -> np.ndarray:
+    return np.array([s.xi, s.Q, *list(s.Vg), s.W, s.Pe, s.Tt, float(s.Nf)], dtype=np.float64)
+
+
+class Context:
+    """One device, one stream (fmd_ctx)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = _lib.load()
+        h = ctypes.c_void_p()
+        rc = self.lib.fmd_ctx_create(ctypes.byref(h), device)
+        if rc != 0:
+            raise FmdError(rc, f"fmd_ctx_create(device={device}) failed: "
+                           f"{self.lib.fmd_status_string(rc).decode()}")
+        self.h = h
+
+    def check(self, rc: int, what: str) -> None:
+        if rc != 0:
+            msg = self.lib.fmd_ctx_last_error(self.h).decode()
+            raise FmdError(rc, f"{what}: {msg}")
+
+    def set_stream(self, stream_ptr: int) -> None:
+        self.check(self.lib.fmd_ctx_set_stream(self.h, ctypes.c_void_p(stream_ptr)), "set_stream")
+
+    def stream(self) -> int:
+        return int(self.lib.fmd_ctx_get_stream(self.h) or 0)
+
+    def synchronize(self) -> None:
+        self.check(self.lib.fmd_ctx_synchronize(self.h), "synchronize")
+
+    def close(self) -> None:
+        if self.h:
+            self.lib.fmd_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- geometry (LJ:113-151) -------------------------------------------
+    def mat_inv9(self, h) -> np.ndarray:
+        h = _f64(h)
+        hi = np.zeros(9)
+        self.check(self.lib.fmd_mat_inv9(self.h, _d(h), _d(hi)), "mat_inv9")
+        return hi
+
+    def apply_pbc(self, pos, h, hi) -> np.ndarray:
+        pos = _f64(pos).copy()
+        n = pos.size // 3
+        self.check(self.lib.fmd_apply_pbc(self.h, _d(pos), _d(_f64(h)), _d(_f64(hi)), n), "apply_pbc")
+        return pos
+
+    # ---- neighbour lists (a1-a3) -------------------------------------------
+    def nlist_build_sym(self, pos, h, hi, n: int, rmcut: float, max_neigh: int = MAX_NEIGH_RIGID):
+        """nlist_build_sym (LJ:257-268) -> (nl_count, nl_list, dropped)."""
+        cnt = np.zeros(n, np.int32)
+        lst = np.zeros(n * max_neigh, np.int32)
+        drop = ctypes.c_int(0)
+        self.check(self.lib.fmd_nlist_rigid(self.h, _d(_f64(pos)), _d(_f64(h)), _d(_f64(hi)), n, float(rmcut),
+                                            max_neigh, _i(cnt), _i(lst), ctypes.byref(drop)), "nlist_build_sym")
+        return cnt, lst, drop.value
+
+    def build_nlist_lj(self, pos, h, hi, na: int, mol_id, rc_list: float = LJ_LIST_RC_AIREBO,
+                       max_neigh: int = MAX_LJ_NEIGH):
+        """build_nlist_lj (AI:263-272, MM:337-346) -> (nlc, nll, dropped)."""
+        cnt = np.zeros(na, np.int32)
+        lst = np.zeros(na * max_neigh, np.int32)
+        drop = ctypes.c_int(0)
+        self.check(self.lib.fmd_nlist_lj_half(self.h, _d(_f64(pos)), _d(_f64(h)), _d(_f64(hi)), na,
+                                              _i(_i32(mol_id)), float(rc_list), max_neigh, _i(cnt), _i(lst),
+                                              ctypes.byref(drop)), "build_nlist_lj")
+        return cnt, lst, drop.value
+
+    def build_nlist_rebo(self, pos, h, hi, na: int, mol_id, rc: float = REBO_LIST_RC,
+                         max_neigh: int = MAX_REBO_NEIGH):
+        """build_nlist_rebo (AI:251-261) -> (nlc, nll, dropped)."""
+        cnt = np.zeros(na, np.int32)
+        lst = np.zeros(na * max_neigh, np.int32)
+        drop = ctypes.c_int(0)
+        self.check(self.lib.fmd_nlist_rebo(self.h, _d(_f64(pos)), _d(_f64(h)), _d(_f64(hi)), na,
+                                           _i(_i32(mol_id)), float(rc), max_neigh, _i(cnt), _i(lst),
+                                           ctypes.byref(drop)), "build_nlist_rebo")
+        return cnt, lst, drop.value
+
+    # ---- forces ---------------------------------------------------------------
+    def forces(self, pos, qv, body, h, hi, nl_count, nl_list, n: int, natom: int, rmcut2: float,
+               max_neigh: int = MAX_NEIGH_RIGID, precision: int = _lib.FMD_PREC_FP64):
+        """forces (LJ:271-400) -> (Ep, Fv, Tv, Wm9)."""
+        F = np.zeros(3 * n)
+        T = np.zeros(3 * n)
+        W = np.zeros(9)
+        Ep = ctypes.c_double(0)
+        self.check(self.lib.fmd_lj_rigid_forces(self.h, _d(_f64(pos)), _d(_f64(qv)), _d(_f64(body)),
+                                                _d(_f64(h)), _d(_f64(hi)), _i(_i32(nl_count)), _i(_i32(nl_list)),
+                                                max_neigh, n, natom, float(rmcut2), precision, _d(F), _d(T),
+                                                _d(W), ctypes.byref(Ep)), "forces")
+        return Ep.value, F, T, W
+
+    def compute_rebo(self, F: np.ndarray, vir9: np.ndarray, pos, h, hi, nlc, nll, na: int,
+                     max_neigh: int = MAX_REBO_NEIGH) -> float:
+        """compute_rebo (AI:275-421): adds into F and vir9 in place; returns Ep."""
+        E = ctypes.c_double(0)
+        self.check(self.lib.fmd_rebo_forces(self.h, _d(_f64(pos)), _d(_f64(h)), _d(_f64(hi)), _i(_i32(nlc)),
+                                            _i(_i32(nll)), max_neigh, na, _d(F), _d(vir9), ctypes.byref(E)),
+                   "compute_rebo")
+        return E.value
+
+    def compute_lj(self, F: np.ndarray, vir9: np.ndarray, pos, h, hi, nlc, nll, na: int,
+                   ff: int = _lib.FMD_FF_AIREBO, max_neigh: int = MAX_LJ_NEIGH) -> float:
+        """compute_lj (AI:424-473) / MM LJ block (MM:711-764): adds in place; returns Ep."""
+        E = ctypes.c_double(0)
+        self.check(self.lib.fmd_lj_half_forces(self.h, ff, _d(_f64(pos)), _d(_f64(h)), _d(_f64(hi)),
+                                               _i(_i32(nlc)), _i(_i32(nll)), max_neigh, na, _d(F), _d(vir9),
+                                               ctypes.byref(E)), "compute_lj")
+        return E.value
+
+    def compute_forces_airebo(self, pos, h, hi, nlc_r, nll_r, nlc_l, nll_l, na: int):
+        """compute_forces (AI:477-495) -> (E3, F, vir9), E3 = (Ep, Ep_rebo, Ep_lj)."""
+        F = np.zeros(3 * na)
+        W = np.zeros(9)
+        E = np.zeros(3)
+        self.check(self.lib.fmd_airebo_forces(self.h, _d(_f64(pos)), _d(_f64(h)), _d(_f64(hi)), _i(_i32(nlc_r)),
+                                              _i(_i32(nll_r)), _i(_i32(nlc_l)), _i(_i32(nll_l)), na, _d(F),
+                                              _d(W), _d(E)), "compute_forces")
+        return E, F, W
+
+    def compute_forces_mm(self, topo: "Topology", pos, h, hi, nlc, nll, na: int, charge=None, mol_id=None):
+        """compute_forces (MM:351-788) -> (E7, F, vir9)."""
+        F = np.zeros(3 * na)
+        W = np.zeros(9)
+        E = np.zeros(7)
+        has_q = 0
+        q = np.zeros(1)
+        m = np.zeros(1, np.int32)
+        if charge is not None:
+            q = _f64(charge)
+            m = _i32(mol_id)
+            has_q = int(np.any(np.abs(q) > 1e-10))
+        self.check(self.lib.fmd_mm_forces(self.h, ctypes.byref(topo.c), _d(_f64(pos)), _d(_f64(h)), _d(_f64(hi)),
+                                          _i(_i32(nlc)), _i(_i32(nll)), _d(q), _i(m), has_q, na, _d(F), _d(W),
+                                          _d(E)), "compute_forces")
+        return E, F, W
+
+    # ---- one NPT step on host state -----------------------------------------
+    def step_npt_rigid(self, st: dict, body, I0: float, Mmol: float, natom: int, rmcut2: float, dt: float,
+                       nl_count, nl_list, max_neigh: int = MAX_NEIGH_RIGID, precision: int = _lib.FMD_PREC_FP64):
+        """step_npt (LJ:434-538) on a state dict with pos, vel, qv, omg, F, T, W9, h, hi, npt
+        (arrays updated in place); returns (Ep, KE)."""
+        npt = npt_from_array(st["npt"])
+        out = np.zeros(2)
+        n = st["pos"].size // 3
+        self.check(self.lib.fmd_rigid_step(self.h, _d(st["pos"]), _d(st["vel"]), _d(st["qv"]), _d(st["omg"]),
+                                           _d(st["F"]), _d(st["T"]), _d(st["W9"]), _d(st["h"]), _d(st["hi"]),
+                                           _d(_f64(body)), float(I0), float(Mmol), n, natom, float(rmcut2),
+                                           float(dt), ctypes.byref(npt), _i(_i32(nl_count)), _i(_i32(nl_list)),
+                                           max_neigh, precision, _d(out)), "step_npt")
+        st["npt"][:] = npt_to_array(npt)
+        return out[0], out[1]
+
+    def step_npt_airebo(self, st: dict, dt: float, nlc_r, nll_r, nlc_l, nll_l):
+        """step_npt (AI:518-590) on a state dict with pos, vel, F, vir9, h, hi, mass, npt;
+        returns (Ep, Ep_rebo, Ep_lj, KE)."""
+        npt = npt_from_array(st["npt"])
+        out = np.zeros(4)
+        na = st["pos"].size // 3
+        self.check(self.lib.fmd_airebo_step(self.h, _d(st["pos"]), _d(st["vel"]), _d(st["F"]), _d(st["vir9"]),
+                                            _d(st["h"]), _d(st["hi"]), _d(_f64(st["mass"])), na, float(dt),
+                                            ctypes.byref(npt), _i(_i32(nlc_r)), _i(_i32(nll_r)), _i(_i32(nlc_l)),
+                                            _i(_i32(nll_l)), _d(out)), "step_npt")
+        st["npt"][:] = npt_to_array(npt)
+        return tuple(out)
+
+    def step_npt_mm(self, st: dict, dt: float, topo: "Topology", nlc, nll, charge=None, mol_id=None):
+        """step_npt (MM:811-890); returns (Eb, Ea, Ed, Ei, Elj, Ecoul, Etot, KE)."""
+        npt = npt_from_array(st["npt"])
+        out = np.zeros(8)
+        na = st["pos"].size // 3
+        has_q = 0
+        q = np.zeros(1)
+        m = np.zeros(1, np.int32)
+        if charge is not None:
+            q = _f64(charge)
+            m = _i32(mol_id)
+            has_q = int(np.any(np.abs(q) > 1e-10))
+        self.check(self.lib.fmd_mm_step(self.h, _d(st["pos"]), _d(st["vel"]), _d(st["F"]), _d(st["vir9"]),
+                                        _d(st["h"]), _d(st["hi"]), na, float(dt), ctypes.byref(npt),
+                                        ctypes.byref(topo.c), _i(_i32(nlc)), _i(_i32(nll)), _d(q), _i(m), has_q,
+                                        _d(out)), "step_npt")
+        st["npt"][:] = npt_to_array(npt)
+        return tuple(out)
+
+
+class Topology:
+    """Owns the arrays behind an fmd_mm_topology (FlatTopology, MM:226-237).
+    Index arrays are given as (n, k) int arrays, k = 2/3/4 atoms per term."""
+
+    def __init__(self, bonds, kb, r0, angles, kth, th0, dihedrals, vn, mult, gamma, impropers, ki, igamma):
+        self._keep = []
+
+        def col(a, k):
+            c = np.ascontiguousarray(a[:, k], dtype=np.int32)
+            if c.size == 0:
+                c = np.zeros(1, np.int32)
+            self._keep.append(c)
+            return _i(c)
+
+        def dv(a):
+            c = _f64(a)
+            self._keep.append(c)
+            return _d(c)
+
+        def iv(a):
+            c = _i32(a)
+            self._keep.append(c)
+            return _i(c)
+
+        bonds = np.asarray(bonds, np.int32).reshape(-1, 2)
+        angles = np.asarray(angles, np.int32).reshape(-1, 3)
+        dihedrals = np.asarray(dihedrals, np.int32).reshape(-1, 4)
+        impropers = np.asarray(impropers, np.int32).reshape(-1, 4)
+        t = MMTopology()
+        t.nb = len(bonds)
+        t.b_i0, t.b_i1, t.b_kb, t.b_r0 = col(bonds, 0), col(bonds, 1), dv(kb), dv(r0)
+        t.nang = len(angles)
+        t.ang_i0, t.ang_i1, t.ang_i2 = col(angles, 0), col(angles, 1), col(angles, 2)
+        t.ang_kth, t.ang_th0 = dv(kth), dv(th0)
+        t.ndih = len(dihedrals)
+        t.dih_i0, t.dih_i1, t.dih_i2, t.dih_i3 = (col(dihedrals, k) for k in range(4))
+        t.dih_vn, t.dih_mult, t.dih_gamma = dv(vn), iv(mult), dv(gamma)
+        t.nimp = len(impropers)
+        t.imp_i0, t.imp_i1, t.imp_i2, t.imp_i3 = (col(impropers, k) for k in range(4))
+        t.imp_ki, t.imp_gamma = dv(ki), dv(igamma)
+        self.c = t
+
+
+@dataclass
+class RunConfig:
+    dt: float
+    T: float
+    Pe: float
+    T_cold: float = 4.0
+    coldstart: int = 0
+    warmup: int = 0
+    nsteps: int = 0
+    nlup: int = 20
+    gavg_from: int = 1
+    gavg_to: int = 0
+    nc: int = 1
+    nmol: int = 1
+    precision: int = _lib.FMD_PREC_FP64
+    use_graphs: int = 1
+
+    def c(self) -> RunParams:
+        p = RunParams()
+        for k in RunParams._fields_:
+            setattr(p, k[0], getattr(self, k[0]))
+        return p
+
+
+class System:
+    """A device-resident system (fmd_system): state stays in HBM across steps."""
+
+    def __init__(self, ctx: Context, handle: ctypes.c_void_p, n: int, kind: int):
+        self.ctx, self.h, self.n, self.kind = ctx, handle, n, kind
+
+    @classmethod
+    def airebo(cls, ctx: Context, cfg: RunConfig, pos, vel, mass, mol_id, h, npt) -> "System":
+        na = np.asarray(pos).size // 3
+        out = ctypes.c_void_p()
+        n = npt_from_array(npt)
+        ctx.check(ctx.lib.fmd_system_create_airebo(ctx.h, ctypes.byref(cfg.c()), na, _d(_f64(pos)), _d(_f64(vel)),
+                                                   _d(_f64(mass)), _i(_i32(mol_id)), _d(_f64(h)), ctypes.byref(n),
+                                                   ctypes.byref(out)), "fmd_system_create_airebo")
+        return cls(ctx, out, na, _lib.FMD_SYS_AIREBO)
+
+    @classmethod
+    def rigid(cls, ctx: Context, cfg: RunConfig, natom: int, body, I0: float, Mmol: float, rmcut: float,
+              pos, vel, qv, omg, h, npt, max_neigh: int = MAX_NEIGH_RIGID) -> "System":
+        n = np.asarray(pos).size // 3
+        out = ctypes.c_void_p()
+        s = npt_from_array(npt)
+        ctx.check(ctx.lib.fmd_system_create_rigid(ctx.h, ctypes.byref(cfg.c()), n, natom, _d(_f64(body)), float(I0),
+                                                  float(Mmol), float(rmcut), max_neigh, _d(_f64(pos)), _d(_f64(vel)),
+                                                  _d(_f64(qv)), _d(_f64(omg)), _d(_f64(h)), ctypes.byref(s),
+                                                  ctypes.byref(out)), "fmd_system_create_rigid")
+        return cls(ctx, out, n, _lib.FMD_SYS_RIGID)
+
+    @classmethod
+    def mm(cls, ctx: Context, cfg: RunConfig, pos, vel, mol_id, topo: Topology, h, npt, charge=None) -> "System":
+        na = np.asarray(pos).size // 3
+        out = ctypes.c_void_p()
+        s = npt_from_array(npt)
+        q = _f64(charge) if charge is not None else None
+        ctx.check(ctx.lib.fmd_system_create_mm(ctx.h, ctypes.byref(cfg.c()), na, _d(_f64(pos)), _d(_f64(vel)),
+                                               _i(_i32(mol_id)), ctypes.byref(topo.c),
+                                               _d(q) if q is not None else None, _d(_f64(h)), ctypes.byref(s),
+                                               ctypes.byref(out)), "fmd_system_create_mm")
+        sysm = cls(ctx, out, na, _lib.FMD_SYS_MM)
+        sysm._topo = topo
+        return sysm
+
+    def init(self) -> None:
+        self.ctx.check(self.ctx.lib.fmd_system_init(self.h), "fmd_system_init")
+
+    def run(self, first: int, last: int) -> Obs:
+        o = Obs()
+        self.ctx.check(self.ctx.lib.fmd_system_run(self.h, first, last, ctypes.byref(o)), "fmd_system_run")
+        return o
+
+    def enqueue(self, first: int, last: int) -> None:
+        """Enqueues steps first..last without synchronising."""
+        self.ctx.check(self.ctx.lib.fmd_system_enqueue(self.h, first, last), "fmd_system_enqueue")
+
+    def averages(self) -> Avg:
+        a = Avg()
+        self.ctx.check(self.ctx.lib.fmd_system_averages(self.h, ctypes.byref(a)), "fmd_system_averages")
+        return a
+
+    def download(self):
+        n = self.n
+        pos, vel = np.zeros(3 * n), np.zeros(3 * n)
+        qv = np.zeros(4 * n) if self.kind == _lib.FMD_SYS_RIGID else None
+        omg = np.zeros(3 * n) if self.kind == _lib.FMD_SYS_RIGID else None
+        h = np.zeros(9)
+        npt = NPT()
+        self.ctx.check(self.ctx.lib.fmd_system_download(self.h, _d(pos), _d(vel), _d(qv) if qv is not None else None,
+                                                        _d(omg) if omg is not None else None, _d(h),
+                                                        ctypes.byref(npt)), "fmd_system_download")
+        return {"pos": pos, "vel": vel, "qv": qv, "omg": omg, "h": h, "npt": npt_to_array(npt)}
+
+    def lists(self, cap_a: int, cap_b: int = 0):
+        n = self.n
+        ca, la = np.zeros(n, np.int32), np.zeros(n * cap_a, np.int32)
+        cb = np.zeros(n, np.int32) if cap_b else None
+        lb = np.zeros(n * cap_b, np.int32) if cap_b else None
+        self.ctx.check(self.ctx.lib.fmd_system_lists(self.h, _i(ca), _i(la), _i(cb) if cb is not None else None,
+                                                     _i(lb) if lb is not None else None), "fmd_system_lists")
+        return ca, la, cb, lb
+
+    def kernel_ms(self, stage: int, reps: int = 20) -> float:
+        """Mean duration (ms) of one launch of a stage, CUDA events on the context stream."""
+        ms = ctypes.c_double(0)
+        self.ctx.check(self.ctx.lib.fmd_system_kernel_ms(self.h, stage, reps, ctypes.byref(ms)), "kernel_ms")
+        return ms.value
+
+    def step_kernels(self, rebuild: bool, phase: bool = False) -> int:
+        k = ctypes.c_int(0)
+        self.ctx.check(self.ctx.lib.fmd_system_step_kernels(self.h, int(rebuild), int(phase), ctypes.byref(k)),
+                       "step_kernels")
+        return k.value
+
+    def close(self) -> None:
+        if self.h:
+            self.ctx.lib.fmd_system_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,95 @@
+// kernels.h -- host-side launch interface of the device kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include "fmd_internal.h"
+
+namespace fmd {
+
+// ---------------------------------------------------------------- cells ----
+// Cell grid in fractional space, computed on the device from the current
+// cell matrix so a list rebuild needs no host round trip.
+struct GridDev {
+    int n[3];        // cells per axis
+    int ncell;
+    int lo[3];       // first stencil offset per axis
+    int span[3];     // stencil width per axis (1..3, never repeats a cell)
+    int prefilter;   // 1 if the FP32 pre-filter is exact-safe for this box
+    float hf[9];     // cell matrix in FP32 for the pre-filter
+    float rc2_hi;    // conservative FP32 rejection threshold
+};
+
+struct CellList {
+    GridDev* grid = nullptr;    // device
+    int* cell_count = nullptr;  // [cap_cells]
+    int* cell_start = nullptr;  // [cap_cells + 1]
+    int* cell_atoms = nullptr;  // [n]
+    int* slot_of = nullptr;     // [n]
+    int* cell_of = nullptr;     // [n]
+    float4* s4 = nullptr;       // [n] fractional coordinates (FP32)
+    int cap_n[3] = {1, 1, 1};
+    int cap_cells = 1;
+    int n = 0;
+};
+
+// Host helper: cells per axis for a cell matrix and list radius.
+void grid_dims_host(const double* h, double rc, int* n);
+cudaError_t cells_alloc(CellList& cl, int n, const double* h_host, double rc);
+void cells_free(CellList& cl);
+// hh = device pointer to {h[9], hi[9]}.  Bins pos[3*n] into cells.
+cudaError_t cells_build(CellList& cl, const double* pos, int n, const double* hh, double rc,
+                        DevErr* err, cudaStream_t st);
+
+// -------------------------------------------------------- neighbour lists ----
+enum ListMode { LIST_SYM = 0, LIST_INTRA = 1, LIST_HALF = 2 };
+// Reference-exact list into cnt[n], list[n*cap]; *dropped (device int) += overflow.
+cudaError_t nlist_build(const CellList& cl, int mode, const double* pos, const int* mol_id, int n,
+                        const double* hh, double rc2, int cap, int* cnt, int* list, int* dropped,
+                        DevErr* err, cudaStream_t st);
+// Incoming (transposed) entries of a half list, sorted ascending per row.
+cudaError_t nlist_transpose(const int* cnt, const int* list, int cap, int n, int* in_cnt,
+                            int* in_list, int in_cap, DevErr* err, cudaStream_t st);
+size_t nlist_bitmap_smem(int n, int* warps_per_block);
+
+// ---------------------------------------------------------------- forces ----
+constexpr int kForceBlocks = kSMs * 4;     // grid of the reduction-producing kernels
+constexpr int kNV = 10;                    // {E, W[9]} per block partial
+
+// REBO (a7): atomics into F, per-block {E, W9} partials in part[grid*kNV].
+cudaError_t rebo_launch(const double* pos, const double* hh, const int* cnt, const int* list,
+                        int cap, int na, double* F, double* part, cudaStream_t st);
+// Half-list LJ gather (a8, a14): F[i] = Facc[i] + LJ(i); Facc[i] zeroed
+// (Facc may alias F only if zero_acc == 0).  ff: FMD_FF_AIREBO / FMD_FF_MM.
+cudaError_t lj_gather_launch(int ff, const double* pos, const double* hh, const int* cnt,
+                             const int* list, int cap, const int* in_cnt, const int* in_list,
+                             int in_cap, int na, double* F, double* Facc, double* part,
+                             cudaStream_t st);
+// Rigid site-site LJ (a5-a6): writes F, T; per-block {E, W9} partials (grid n).
+cudaError_t rigid_launch(int precision, const double* pos, const double* qv, const double* body,
+                         const double* hh, const int* cnt, const int* list, int cap, int n,
+                         int natom, double rmcut2, double* F, double* T, double* part,
+                         cudaStream_t st);
+int rigid_grid(int n);
+
+// MM bonded terms (a10-a13): atomics into Facc; partials {E_b,E_a,E_d,E_i, W00,W11,W22}
+struct MMTopoDev {
+    int nb, nang, ndih, nimp;
+    const int *b_i0, *b_i1; const double *b_kb, *b_r0;
+    const int *a_i0, *a_i1, *a_i2; const double *a_kth, *a_th0;
+    const int *d_i0, *d_i1, *d_i2, *d_i3; const double *d_vn; const int *d_mult; const double *d_gamma;
+    const int *m_i0, *m_i1, *m_i2, *m_i3; const double *m_ki, *m_gamma;
+};
+constexpr int kMMNV = 7;
+cudaError_t mm_bonded_launch(const MMTopoDev& t, const double* pos, const double* hh, double* Facc,
+                             double* part, cudaStream_t st);
+// Cut Coulomb (a15), all pairs of different molecules: adds into Facc; {Ecoul} partials.
+cudaError_t mm_coulomb_launch(const double* pos, const double* hh, const double* charge,
+                              const int* mol_id, int na, double* Facc, double* part, cudaStream_t st);
+
+// Sums `nblk` partial records of width nv into out[nv] (deterministic).
+cudaError_t reduce_partials(const double* part, int nblk, int nv, double* out, cudaStream_t st);
+
+// Geometry helpers on device data.
+cudaError_t apply_pbc_launch(double* pos, int n, const double* hh, cudaStream_t st);
+cudaError_t inv9_launch(double* hh, cudaStream_t st);   // hh[9..17] = inv(hh[0..8])
+
+}  // namespace fmd

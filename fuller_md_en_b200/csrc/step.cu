@@ -1,0 +1,400 @@
+// step.cu -- NPT velocity-Verlet on the device (a17 rigid LJ:434-538,
+// a18 atomistic AI:518-590 / MM:811-890) and the driver's per-step schedule
+// (a19: LJ:847-897, AI:871-912, MM:1192-1236).
+//
+// The reference keeps xi, Vg and h on the host and synchronises several
+// times per step.  Here they live in a device struct (SysScal) updated by
+// single-thread "scalar" kernels, so a whole step -- and a list rebuild -- is
+// a fixed sequence of launches with no host round trip, which is what lets
+// the step be replayed as a CUDA graph:
+//
+//   k_begin     schedule (Tt ramp, cold resets), thermostat/barostat first
+//               half, scaling factors, cell update and its inverse
+//   k_kick      first half-kick, drift in fractional coordinates, wrap,
+//               back to Cartesian with the new cell (+ quaternion update)
+//   forces      (airebo.cu / rigid.cu / mm.cu)
+//   k_kick2     second half-kick, per-block kinetic partials
+//   k_end       force/kinetic reductions (fixed order), thermostat/barostat
+//               second half, observables, rescale decision, averages
+//   k_rescale / k_rescale_end   cold/warm phases only
+//
+// Scalar arithmetic follows the reference expressions; this file is built
+// with -fmad=false so they round like the reference's host code.
+#include <cmath>
+#include "step.h"
+#include "geom.cuh"
+
+namespace fmd {
+namespace {
+
+constexpr int kPB = 256;   // threads of per-particle kernels
+constexpr double kMC = 12.011;
+
+__device__ __forceinline__ double clampd(double x, double lo, double hi) {
+    return x < lo ? lo : (x > hi ? hi : x);
+}
+__device__ __forceinline__ double inst_T(double ke, int nf) { return 2 * ke / (nf * kKB); }
+__device__ __forceinline__ double inst_P(const double* W, double ke, double V) {
+    return (2 * ke + W[0] + W[4] + W[8]) / (3 * V) * kEV2GPa;
+}
+
+// Thermostat + barostat half update (LJ:448-455, AI:524-530).
+__device__ void npt_half(fmd_npt& s, double hdt, double ke, double ke_p, const double* W, double V,
+                         double xi_lim, double vg_lim) {
+    s.xi += hdt * (2 * ke - s.Nf * kKB * s.Tt) / s.Q;
+    s.xi = clampd(s.xi, -xi_lim, xi_lim);
+    const double dP = inst_P(W, ke_p, V) - s.Pe;
+    for (int a = 0; a < 3; a++) s.Vg[a * 4] += hdt * V * dP / (s.W * kEV2GPa);
+    for (int a = 0; a < 3; a++) s.Vg[a * 4] = clampd(s.Vg[a * 4], -vg_lim, vg_lim);
+}
+
+__global__ void k_begin(SysScal* S, int kind, StepParams p) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    fmd_npt& npt = S->npt;
+    if (p.schedule) {
+        const int g = ++S->gstep;
+        // Tt schedule and resets (LJ:851-857)
+        if (g <= p.coldstart) npt.Tt = p.T_cold;
+        else if (g <= p.coldstart + p.warmup)
+            npt.Tt = p.T_cold + (p.T - p.T_cold) * double(g - p.coldstart) / double(p.warmup);
+        else npt.Tt = p.T;
+        if (p.coldstart > 0 && g == p.coldstart + 1) {
+            npt.xi = 0;
+            for (int k = 0; k < 9; k++) npt.Vg[k] = 0;
+        }
+        if (g <= p.coldstart)
+            for (int k = 0; k < 9; k++) npt.Vg[k] = 0;
+    }
+    const double hdt = 0.5 * p.dt;
+    const bool rigid = kind == FMD_SYS_RIGID;
+    if (rigid) inv9(S->h, S->hi);                                  // LJ:442
+    const double V = fabs(det9(S->h));
+    if (rigid) npt_half(npt, hdt, S->kt + S->kr, S->kt, S->W9, V, 0.1, 0.01);
+    else npt_half(npt, hdt, S->KE, S->KE, S->W9, V, 0.05, 0.005);
+    const double eps = npt.Vg[0] * S->hi[0] + npt.Vg[4] * S->hi[4] + npt.Vg[8] * S->hi[8];
+    const double sc_nh = exp(-hdt * npt.xi), sc_pr = exp(-hdt * eps / 3.0);
+    S->sc_nh = sc_nh;
+    S->sc_v = sc_nh * sc_pr;
+    for (int k = 0; k < 9; k++) S->hi_old[k] = S->hi[k];
+    for (int k = 0; k < 9; k++) S->h[k] += p.dt * npt.Vg[k];          // LJ:484
+    inv9(S->h, S->hi);                                                // LJ:509, AI:555
+    const double eps2 = npt.Vg[0] * S->hi[0] + npt.Vg[4] * S->hi[4] + npt.Vg[8] * S->hi[8];
+    S->sc_v2 = sc_nh * exp(-hdt * eps2 / 3.0);
+}
+
+// LJ:166-174.
+__device__ __forceinline__ void quat_step(double* q, double wx, double wy, double wz, double dt) {
+    double dq[4];
+    const double wm = sqrt(wx * wx + wy * wy + wz * wz), th = wm * dt * 0.5;
+    if (th < 1e-14) { dq[0] = 1.0; dq[1] = 0.5 * dt * wx; dq[2] = 0.5 * dt * wy; dq[3] = 0.5 * dt * wz; }
+    else { const double s = sin(th) / wm; dq[0] = cos(th); dq[1] = s * wx; dq[2] = s * wy; dq[3] = s * wz; }
+    double o[4];
+    o[0] = q[0] * dq[0] - q[1] * dq[1] - q[2] * dq[2] - q[3] * dq[3];
+    o[1] = q[0] * dq[1] + q[1] * dq[0] + q[2] * dq[3] - q[3] * dq[2];
+    o[2] = q[0] * dq[2] - q[1] * dq[3] + q[2] * dq[0] + q[3] * dq[1];
+    o[3] = q[0] * dq[3] + q[1] * dq[2] - q[2] * dq[1] + q[3] * dq[0];
+    const double nrm = sqrt(o[0] * o[0] + o[1] * o[1] + o[2] * o[2] + o[3] * o[3]), inv = 1.0 / nrm;
+    for (int k = 0; k < 4; k++) q[k] = o[k] * inv;
+}
+
+__global__ void __launch_bounds__(kPB) k_kick(StepArrays a, double dt) {
+    const SysScal* S = a.S;
+    const double hdt = 0.5 * dt, sc_v = S->sc_v, sc_nh = S->sc_nh;
+    const double* hi = S->hi_old;
+    const double* h = S->h;
+    const bool rigid = a.kind == FMD_SYS_RIGID;
+    const double cF = rigid ? kConv / a.Mmol : kConv / kMC, cT = rigid ? kConv / a.I0 : 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+        const double mi = (a.mass != nullptr) ? kConv / a.mass[i] : cF;
+        double v[3], p[3];
+        for (int c = 0; c < 3; c++) {
+            v[c] = a.vel[3 * i + c] * sc_v + hdt * a.F[3 * i + c] * mi;
+            a.vel[3 * i + c] = v[c];
+            p[c] = a.pos[3 * i + c];
+        }
+        double sx = hi[0] * p[0] + hi[1] * p[1] + hi[2] * p[2];
+        double sy = hi[3] * p[0] + hi[4] * p[1] + hi[5] * p[2];
+        double sz = hi[6] * p[0] + hi[7] * p[1] + hi[8] * p[2];
+        const double vx = hi[0] * v[0] + hi[1] * v[1] + hi[2] * v[2];
+        const double vy = hi[3] * v[0] + hi[4] * v[1] + hi[5] * v[2];
+        const double vz = hi[6] * v[0] + hi[7] * v[1] + hi[8] * v[2];
+        sx += dt * vx; sy += dt * vy; sz += dt * vz;
+        sx -= floor(sx); sy -= floor(sy); sz -= floor(sz);
+        a.pos[3 * i] = h[0] * sx + h[1] * sy + h[2] * sz;
+        a.pos[3 * i + 1] = h[3] * sx + h[4] * sy + h[5] * sz;
+        a.pos[3 * i + 2] = h[6] * sx + h[7] * sy + h[8] * sz;
+        if (rigid) {
+            double w[3];
+            for (int c = 0; c < 3; c++) {
+                w[c] = a.omg[3 * i + c] * sc_nh + hdt * a.T[3 * i + c] * cT;
+                a.omg[3 * i + c] = w[c];
+            }
+            quat_step(a.qv + 4 * i, w[0], w[1], w[2], dt);               // LJ:503-508
+        }
+    }
+}
+
+// Second half-kick with per-block sums of m v^2 (atomistic) or v^2 and w^2 (rigid).
+__global__ void __launch_bounds__(kPB) k_kick2(StepArrays a, double dt) {
+    __shared__ double sm[32 * 2];
+    const SysScal* S = a.S;
+    const double hdt = 0.5 * dt, sc_v2 = S->sc_v2, sc_nh = S->sc_nh;
+    const bool rigid = a.kind == FMD_SYS_RIGID;
+    const double cF = rigid ? kConv / a.Mmol : kConv / kMC, cT = rigid ? kConv / a.I0 : 0.0;
+    double acc[2] = {0.0, 0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+        const double mi = (a.mass != nullptr) ? kConv / a.mass[i] : cF;
+        double vv = 0;
+        for (int c = 0; c < 3; c++) {
+            const double v = (a.vel[3 * i + c] + hdt * a.F[3 * i + c] * mi) * sc_v2;
+            a.vel[3 * i + c] = v;
+            vv += v * v;
+        }
+        if (rigid) {
+            double ww = 0;
+            for (int c = 0; c < 3; c++) {
+                const double w = (a.omg[3 * i + c] + hdt * a.T[3 * i + c] * cT) * sc_nh;
+                a.omg[3 * i + c] = w;
+                ww += w * w;
+            }
+            acc[0] += vv;
+            acc[1] += ww;
+        } else {
+            acc[0] += (a.mass != nullptr ? a.mass[i] : kMC) * vv;
+        }
+    }
+    block_sum_store<2>(acc, sm, a.part_ke + 2 * blockIdx.x);
+}
+
+__global__ void __launch_bounds__(kPB) k_ke_partial(StepArrays a) {
+    __shared__ double sm[32 * 2];
+    const bool rigid = a.kind == FMD_SYS_RIGID;
+    double acc[2] = {0.0, 0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+        const double vv = a.vel[3 * i] * a.vel[3 * i] + a.vel[3 * i + 1] * a.vel[3 * i + 1] +
+                          a.vel[3 * i + 2] * a.vel[3 * i + 2];
+        if (rigid) {
+            acc[0] += vv;
+            acc[1] += a.omg[3 * i] * a.omg[3 * i] + a.omg[3 * i + 1] * a.omg[3 * i + 1] +
+                      a.omg[3 * i + 2] * a.omg[3 * i + 2];
+        } else {
+            acc[0] += (a.mass != nullptr ? a.mass[i] : kMC) * vv;
+        }
+    }
+    block_sum_store<2>(acc, sm, a.part_ke + 2 * blockIdx.x);
+}
+
+__global__ void __launch_bounds__(kPB) k_rescale(StepArrays a) {
+    __shared__ double sm[32 * 2];
+    const SysScal* S = a.S;
+    const bool rigid = a.kind == FMD_SYS_RIGID;
+    const bool doit = S->do_rescale != 0;
+    const double sc = S->scale;
+    double acc[2] = {0.0, 0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+        double vv = 0, ww = 0;
+        for (int c = 0; c < 3; c++) {
+            double v = a.vel[3 * i + c];
+            if (doit) { v *= sc; a.vel[3 * i + c] = v; }
+            vv += v * v;
+            if (rigid) {
+                double w = a.omg[3 * i + c];
+                if (doit) { w *= sc; a.omg[3 * i + c] = w; }
+                ww += w * w;
+            }
+        }
+        if (rigid) { acc[0] += vv; acc[1] += ww; }
+        else acc[0] += (a.mass != nullptr ? a.mass[i] : kMC) * vv;
+    }
+    block_sum_store<2>(acc, sm, a.part_ke + 2 * blockIdx.x);
+}
+
+// Fixed-order sum of nblk records of width nv, field k, by a 256-thread block.
+__device__ double block_reduce_field(const double* part, int nblk, int nv, int k, double* sm) {
+    double v[1] = {0.0};
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x) v[0] += part[(size_t)b * nv + k];
+    double out[1];
+    block_sum_store<1>(v, sm, out);
+    __shared__ double bc;
+    if (threadIdx.x == 0) bc = out[0];
+    __syncthreads();
+    const double r = bc;
+    __syncthreads();
+    return r;
+}
+
+// Writes the kinetic energies from the kinetic partials into S.
+__device__ void kinetic_from_partials(const StepArrays& a, int nblk, double* sm) {
+    const double s0 = block_reduce_field(a.part_ke, nblk, 2, 0, sm);
+    const double s1 = block_reduce_field(a.part_ke, nblk, 2, 1, sm);
+    if (threadIdx.x == 0) {
+        SysScal* S = a.S;
+        if (a.kind == FMD_SYS_RIGID) {
+            S->kt = 0.5 * a.Mmol * s0 / kConv;     // LJ:411
+            S->kr = 0.5 * a.I0 * s1 / kConv;       // LJ:420
+            S->KE = S->kt + S->kr;
+        } else {
+            S->KE = 0.5 * s0 / kConv;              // AI:506, MM:799
+        }
+    }
+}
+
+// Force partials -> S->W9, S->E.
+__device__ void forces_from_partials(const StepArrays& a, int nblk_f1, double* sm) {
+    SysScal* S = a.S;
+    double e[8] = {0, 0, 0, 0, 0, 0, 0, 0}, w[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (a.kind == FMD_SYS_RIGID) {
+        e[0] = block_reduce_field(a.part_f1, nblk_f1, kNV, 0, sm);
+        for (int q = 0; q < 9; q++) w[q] = block_reduce_field(a.part_f1, nblk_f1, kNV, 1 + q, sm);
+    } else if (a.kind == FMD_SYS_AIREBO) {
+        const double er = block_reduce_field(a.part_f1, kForceBlocks, kNV, 0, sm);
+        const double el = block_reduce_field(a.part_f2, kForceBlocks, kNV, 0, sm);
+        for (int q = 0; q < 9; q++)
+            w[q] = block_reduce_field(a.part_f1, kForceBlocks, kNV, 1 + q, sm) +
+                   block_reduce_field(a.part_f2, kForceBlocks, kNV, 1 + q, sm);
+        e[0] = er + el; e[1] = er; e[2] = el;
+    } else {
+        for (int q = 0; q < 4; q++) e[q] = block_reduce_field(a.part_f1, kForceBlocks, kMMNV, q, sm);
+        e[4] = block_reduce_field(a.part_f2, kForceBlocks, kNV, 0, sm);
+        e[5] = a.has_charge ? block_reduce_field(a.part_f3, kForceBlocks, 1, 0, sm) : 0.0;
+        e[6] = e[0] + e[1] + e[2] + e[3] + e[4] + e[5];
+        const int d[3] = {0, 4, 8};
+        for (int q = 0; q < 3; q++)
+            w[d[q]] = block_reduce_field(a.part_f1, kForceBlocks, kMMNV, 4 + q, sm) +
+                      block_reduce_field(a.part_f2, kForceBlocks, kNV, 1 + d[q], sm);
+    }
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < 9; q++) S->W9[q] = w[q];
+        for (int q = 0; q < 8; q++) S->E[q] = e[q];
+    }
+    __syncthreads();
+}
+
+// Observables, averages and the monitor record (LJ:874-897, AI:896-912, MM:1215-1236).
+__device__ void record(SysScal* S, int kind, const StepParams& p) {
+    const int g = S->gstep;
+    const double an = S->h[0] / p.nc;
+    S->an = an;
+    if (g >= p.gavg_from && g <= p.gavg_to) {
+        fmd_avg& A = S->avg;
+        A.sT += S->Tn; A.sP += S->Pn; A.sa += an;
+        if (kind == FMD_SYS_RIGID) {
+            A.sE[0] += S->E[0] / p.nmol;
+        } else if (kind == FMD_SYS_AIREBO) {
+            A.sE[0] += S->E[1] / p.nmol; A.sE[1] += S->E[2] / p.nmol; A.sE[2] += S->E[0] / p.nmol;
+        } else {
+            A.sE[0] += S->E[0] / p.nmol; A.sE[1] += S->E[1] / p.nmol;
+            A.sE[2] += (S->E[2] + S->E[3]) / p.nmol; A.sE[3] += S->E[4] / p.nmol;
+            A.sE[4] += S->E[6] / p.nmol;
+        }
+        A.n++;
+    }
+    fmd_obs& o = S->obs;
+    o.step = g; o.T = S->Tn; o.P = S->Pn; o.a = an; o.KE = S->KE;
+    for (int q = 0; q < 8; q++) o.E[q] = S->E[q];
+}
+
+__global__ void __launch_bounds__(256) k_end(StepArrays a, StepParams p, int nblk_f1, int nblk_ke) {
+    __shared__ double sm[32];
+    forces_from_partials(a, nblk_f1, sm);
+    kinetic_from_partials(a, nblk_ke, sm);
+    if (threadIdx.x != 0) return;
+    SysScal* S = a.S;
+    const double hdt = 0.5 * p.dt;
+    const bool rigid = a.kind == FMD_SYS_RIGID;
+    const double V2 = fabs(det9(S->h));
+    if (rigid) npt_half(S->npt, hdt, S->KE, S->kt, S->W9, V2, 0.1, 0.01);
+    else npt_half(S->npt, hdt, S->KE, S->KE, S->W9, V2, 0.05, 0.005);
+    if (!p.schedule) return;
+    // Driver observables after step_npt (LJ:874-876, AI:896, MM:1215-1219).
+    const double V = fabs(det9(S->h));
+    S->Tn = inst_T(S->KE, S->npt.Nf);
+    S->Pn = inst_P(S->W9, rigid ? S->kt : S->KE, V);
+    const int g = S->gstep;
+    const bool phase = (g <= p.coldstart || g <= p.coldstart + p.warmup);
+    S->do_rescale = 0;
+    if (phase && S->Tn > 0.1) {                                      // LJ:879-894
+        const double tgt = (g <= p.coldstart) ? p.T_cold : S->npt.Tt;
+        S->scale = sqrt(fmax(tgt, 0.1) / S->Tn);
+        S->do_rescale = 1;
+    }
+    if (!phase) record(S, a.kind, p);
+}
+
+__global__ void __launch_bounds__(256) k_rescale_end(StepArrays a, StepParams p, int nblk_ke) {
+    __shared__ double sm[32];
+    SysScal* S = a.S;
+    const bool doit = S->do_rescale != 0;
+    if (doit) kinetic_from_partials(a, nblk_ke, sm);
+    if (threadIdx.x != 0) return;
+    if (doit) {
+        S->Tn = inst_T(S->KE, S->npt.Nf);
+        S->npt.xi = 0;
+        if (S->gstep <= p.coldstart)
+            for (int k = 0; k < 9; k++) S->npt.Vg[k] = 0;
+    }
+    record(S, a.kind, p);
+}
+
+__global__ void __launch_bounds__(256) k_ke_final(StepArrays a, int nblk_ke) {
+    __shared__ double sm[32];
+    kinetic_from_partials(a, nblk_ke, sm);
+}
+
+__global__ void __launch_bounds__(256) k_force_final(StepArrays a, int nblk_f1) {
+    __shared__ double sm[32];
+    forces_from_partials(a, nblk_f1, sm);
+}
+
+}  // namespace
+
+int force_partial_blocks(const StepArrays& a) {
+    return a.kind == FMD_SYS_RIGID ? rigid_grid(a.n) : kForceBlocks;
+}
+
+cudaError_t enqueue_forces(const StepArrays& a, cudaStream_t st) {
+    cudaError_t e = cudaSuccess;
+    const double* hh = a.S->h;
+    if (a.kind == FMD_SYS_RIGID) {
+        e = rigid_launch(a.precision, a.pos, a.qv, a.body, hh, a.cnt_a, a.list_a, a.cap_a, a.n, a.natom,
+                         a.rmcut2, a.F, a.T, a.part_f1, st);
+    } else if (a.kind == FMD_SYS_AIREBO) {
+        if ((e = rebo_launch(a.pos, hh, a.cnt_b, a.list_b, a.cap_b, a.n, a.Facc, a.part_f1, st)) != cudaSuccess) return e;
+        e = lj_gather_launch(FMD_FF_AIREBO, a.pos, hh, a.cnt_a, a.list_a, a.cap_a, a.in_cnt, a.in_list, a.in_cap,
+                             a.n, a.F, a.Facc, a.part_f2, st);
+    } else {
+        if ((e = mm_bonded_launch(a.topo, a.pos, hh, a.Facc, a.part_f1, st)) != cudaSuccess) return e;
+        if (a.has_charge)
+            if ((e = mm_coulomb_launch(a.pos, hh, a.charge, a.mol_id, a.n, a.Facc, a.part_f3, st)) != cudaSuccess) return e;
+        e = lj_gather_launch(FMD_FF_MM, a.pos, hh, a.cnt_a, a.list_a, a.cap_a, a.in_cnt, a.in_list, a.in_cap,
+                             a.n, a.F, a.Facc, a.part_f2, st);
+    }
+    return e;
+}
+
+cudaError_t enqueue_force_reduce(const StepArrays& a, cudaStream_t st) {
+    k_force_final<<<1, 256, 0, st>>>(a, force_partial_blocks(a));
+    return cudaGetLastError();
+}
+
+cudaError_t enqueue_ke(const StepArrays& a, cudaStream_t st) {
+    k_ke_partial<<<kForceBlocks, kPB, 0, st>>>(a);
+    k_ke_final<<<1, 256, 0, st>>>(a, kForceBlocks);
+    return cudaGetLastError();
+}
+
+cudaError_t enqueue_step(const StepArrays& a, const StepParams& p, bool rescale_phase, cudaStream_t st) {
+    cudaError_t e;
+    k_begin<<<1, 32, 0, st>>>(a.S, a.kind, p);
+    k_kick<<<kForceBlocks, kPB, 0, st>>>(a, p.dt);
+    if ((e = enqueue_forces(a, st)) != cudaSuccess) return e;
+    k_kick2<<<kForceBlocks, kPB, 0, st>>>(a, p.dt);
+    k_end<<<1, 256, 0, st>>>(a, p, force_partial_blocks(a), kForceBlocks);
+    if (rescale_phase && p.schedule) {
+        k_rescale<<<kForceBlocks, kPB, 0, st>>>(a);
+        k_rescale_end<<<1, 256, 0, st>>>(a, p, kForceBlocks);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace fmd

@@ -1,0 +1,68 @@
+// step.h -- the velocity-Verlet NPT step as a sequence of device kernels.
+#pragma once
+#include "kernels.h"
+
+namespace fmd {
+
+// Device-resident scalars of one system.  h[9] and hi[9] are adjacent so
+// &h[0] is the {h, hi} block every force and list kernel reads.
+struct SysScal {
+    double h[9], hi[9];
+    double hi_old[9];        // inverse cell used by the drift (before the cell update)
+    fmd_npt npt;
+    double sc_v, sc_nh, sc_v2;
+    double KE, kt, kr;       // current kinetic energies (kt, kr: rigid only)
+    double W9[9];            // virial of the last force call
+    double E[8];             // energies of the last force call (program grouping)
+    double Tn, Pn, an;
+    double scale;
+    int do_rescale;
+    int gstep;
+    fmd_obs obs;
+    fmd_avg avg;
+};
+
+// Device pointers and sizes of one step.
+struct StepArrays {
+    int kind = FMD_SYS_AIREBO;
+    int n = 0;               // particles: molecules (rigid) or atoms
+    int natom = 0;           // sites per rigid molecule
+    double* pos = nullptr; double* vel = nullptr; double* F = nullptr; double* Facc = nullptr;
+    double* omg = nullptr; double* qv = nullptr; double* T = nullptr;
+    const double* mass = nullptr;     // AIREBO per-atom masses; nullptr: constant carbon mass
+    const double* body = nullptr;
+    const int* mol_id = nullptr;
+    const double* charge = nullptr;
+    int has_charge = 0;
+    SysScal* S = nullptr;
+    const int* cnt_a = nullptr; const int* list_a = nullptr; int cap_a = 0;     // LJ half / rigid
+    const int* in_cnt = nullptr; const int* in_list = nullptr; int in_cap = 0;  // LJ incoming
+    const int* cnt_b = nullptr; const int* list_b = nullptr; int cap_b = 0;     // REBO
+    double* part_f1 = nullptr;  // REBO / rigid / bonded partials
+    double* part_f2 = nullptr;  // LJ partials
+    double* part_f3 = nullptr;  // Coulomb partials
+    double* part_ke = nullptr;  // kinetic partials
+    MMTopoDev topo{};
+    double rmcut2 = 0, Mmol = 0, I0 = 0;
+    int precision = FMD_PREC_FP64;
+};
+
+struct StepParams {
+    double dt = 1.0, T = 300.0, T_cold = 4.0;
+    int coldstart = 0, warmup = 0, gavg_from = 1, gavg_to = 0, nc = 1, nmol = 1;
+    int schedule = 0;        // 1: driver schedule, observables and averages (system runs)
+};
+
+// Force evaluation of the step's kind; fills partials and F (and T).
+cudaError_t enqueue_forces(const StepArrays& a, cudaStream_t st);
+// Reduces the force partials into S->W9 / S->E (one small kernel).
+cudaError_t enqueue_force_reduce(const StepArrays& a, cudaStream_t st);
+// Recomputes S->KE (and kt, kr) from the velocities.
+cudaError_t enqueue_ke(const StepArrays& a, cudaStream_t st);
+// One step_npt (+ driver schedule if p.schedule); rescale_phase selects the
+// cold/warm velocity rescale kernels.
+cudaError_t enqueue_step(const StepArrays& a, const StepParams& p, bool rescale_phase, cudaStream_t st);
+// Observables / averages for the pre-loop state (not a step).
+int force_partial_blocks(const StepArrays& a);
+
+}  // namespace fmd

@@ -1,0 +1,473 @@
+// system.cu -- device-resident systems: state in HBM for the whole run, list
+// rebuilds on the device every nlup steps, each step replayed as a CUDA graph
+// (one graph per {rebuild, cold/warm} variant, captured on first use).
+// The host only sees observables at the steps it asks for.
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include "step.h"
+#include "system.h"
+
+using namespace fmd;
+
+namespace fmd {
+
+namespace {
+template <class T>
+cudaError_t dalloc(T** p, size_t count) {
+    return cudaMalloc((void**)p, sizeof(T) * (count > 0 ? count : 1));
+}
+template <class T>
+cudaError_t dupload(T** p, const T* src, size_t count, cudaStream_t st) {
+    cudaError_t e = dalloc(p, count);
+    if (e != cudaSuccess || src == nullptr || count == 0) return e;
+    return cudaMemcpyAsync(*p, src, sizeof(T) * count, cudaMemcpyHostToDevice, st);
+}
+}  // namespace
+
+void System::release() {
+    for (auto& row : graphs)
+        for (auto& g : row)
+            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    for (void* p : owned) cudaFree(p);
+    owned.clear();
+    cells_free(cells_a);
+    cells_free(cells_b);
+}
+
+template <class T>
+cudaError_t System::alloc(T** p, size_t count, const T* src) {
+    cudaError_t e = dupload(p, src, count, ctx->stream);
+    if (e == cudaSuccess) owned.push_back((void*)*p);
+    return e;
+}
+
+int System::alloc_common(const double* pos_h, const double* vel_h, const double* h_h, const fmd_npt* npt_h) {
+    cudaStream_t st = ctx->stream;
+    const int n = arr.n;
+    if (alloc(&arr.pos, 3 * (size_t)n, pos_h) || alloc(&arr.vel, 3 * (size_t)n, vel_h) ||
+        alloc(&arr.F, 3 * (size_t)n, (const double*)nullptr) || alloc(&arr.Facc, 3 * (size_t)n, (const double*)nullptr) ||
+        alloc(&arr.part_f1, (size_t)std::max(kForceBlocks, n) * kNV, (const double*)nullptr) ||
+        alloc(&arr.part_f2, (size_t)kForceBlocks * kNV, (const double*)nullptr) ||
+        alloc(&arr.part_f3, (size_t)kForceBlocks, (const double*)nullptr) ||
+        alloc(&arr.part_ke, (size_t)kForceBlocks * 2, (const double*)nullptr) ||
+        alloc(&dropped, 2, (const int*)nullptr) || alloc(&arr.S, 1, (const SysScal*)nullptr))
+        return ctx->fail(FMD_ERR_CUDA, "device allocation failed");
+    cudaMemsetAsync(arr.F, 0, sizeof(double) * 3 * n, st);
+    cudaMemsetAsync(arr.Facc, 0, sizeof(double) * 3 * n, st);
+    cudaMemsetAsync(dropped, 0, sizeof(int) * 2, st);
+    SysScal s;
+    std::memset(&s, 0, sizeof(s));
+    for (int k = 0; k < 9; k++) s.h[k] = h_h[k];
+    s.npt = *npt_h;
+    s.gstep = 0;
+    cudaMemcpyAsync(arr.S, &s, sizeof(s), cudaMemcpyHostToDevice, st);
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, cudaGetErrorString(e));
+    std::memcpy(h0, h_h, sizeof(h0));
+    return FMD_OK;
+}
+
+int System::alloc_lists(double rc_list_a, int cap_a_, double rc_list_b, int cap_b_, bool transpose) {
+    const int n = arr.n;
+    rc_a = rc_list_a; rc2_a = rc_a * rc_a; arr.cap_a = cap_a_;
+    int* cnt; int* lst;
+    if (alloc(&cnt, n, (const int*)nullptr) || alloc(&lst, (size_t)n * cap_a_, (const int*)nullptr))
+        return ctx->fail(FMD_ERR_CUDA, "list allocation failed");
+    cudaMemsetAsync(lst, 0, sizeof(int) * (size_t)n * cap_a_, ctx->stream);
+    arr.cnt_a = cnt; arr.list_a = lst;
+    if (cells_alloc(cells_a, n, h0, rc_a) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "cell allocation failed");
+    if (cap_b_ > 0) {
+        rc_b = rc_list_b; rc2_b = rc_b * rc_b; arr.cap_b = cap_b_;
+        if (alloc(&cnt, n, (const int*)nullptr) || alloc(&lst, (size_t)n * cap_b_, (const int*)nullptr))
+            return ctx->fail(FMD_ERR_CUDA, "list allocation failed");
+        cudaMemsetAsync(lst, 0, sizeof(int) * (size_t)n * cap_b_, ctx->stream);
+        arr.cnt_b = cnt; arr.list_b = lst;
+        if (cells_alloc(cells_b, n, h0, rc_b) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "cell allocation failed");
+    }
+    if (transpose) {
+        arr.in_cap = kInCap;
+        if (alloc(&cnt, n, (const int*)nullptr) || alloc(&lst, (size_t)n * kInCap, (const int*)nullptr))
+            return ctx->fail(FMD_ERR_CUDA, "list allocation failed");
+        arr.in_cnt = cnt; arr.in_list = lst;
+    }
+    return FMD_OK;
+}
+
+// Rebuild of every list this kind uses, as the driver does at gstep % nlup == 0.
+cudaError_t System::enqueue_rebuild(cudaStream_t st) {
+    cudaError_t e;
+    double* hh = arr.S->h;
+    if ((e = inv9_launch(hh, st)) != cudaSuccess) return e;
+    int* cnt_a = const_cast<int*>(arr.cnt_a);
+    int* list_a = const_cast<int*>(arr.list_a);
+    if (arr.kind == FMD_SYS_RIGID) {
+        if ((e = cells_build(cells_a, arr.pos, arr.n, hh, rc_a, ctx->d_err, st)) != cudaSuccess) return e;
+        return nlist_build(cells_a, LIST_SYM, arr.pos, nullptr, arr.n, hh, rc2_a, arr.cap_a, cnt_a, list_a,
+                           dropped, ctx->d_err, st);
+    }
+    if (arr.kind == FMD_SYS_AIREBO) {
+        if ((e = cells_build(cells_b, arr.pos, arr.n, hh, rc_b, ctx->d_err, st)) != cudaSuccess) return e;
+        if ((e = nlist_build(cells_b, LIST_INTRA, arr.pos, arr.mol_id, arr.n, hh, rc2_b, arr.cap_b,
+                             const_cast<int*>(arr.cnt_b), const_cast<int*>(arr.list_b), dropped + 1,
+                             ctx->d_err, st)) != cudaSuccess)
+            return e;
+    }
+    if ((e = cells_build(cells_a, arr.pos, arr.n, hh, rc_a, ctx->d_err, st)) != cudaSuccess) return e;
+    if ((e = nlist_build(cells_a, LIST_HALF, arr.pos, arr.mol_id, arr.n, hh, rc2_a, arr.cap_a, cnt_a, list_a,
+                         dropped, ctx->d_err, st)) != cudaSuccess)
+        return e;
+    return nlist_transpose(arr.cnt_a, arr.list_a, arr.cap_a, arr.n, const_cast<int*>(arr.in_cnt),
+                           const_cast<int*>(arr.in_list), arr.in_cap, ctx->d_err, st);
+}
+
+int System::init() {
+    cudaStream_t st = ctx->stream;
+    // Pre-loop order of the reference: lists from the unwrapped positions,
+    // then apply_pbc, then the first forces (LJ:813-828, AI:830-853).
+    if (enqueue_rebuild(st) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "list build launch failed");
+    if (apply_pbc_launch(arr.pos, arr.n, arr.S->h, st) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "apply_pbc failed");
+    if (enqueue_forces(arr, st) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "force launch failed");
+    if (enqueue_force_reduce(arr, st) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "reduce launch failed");
+    if (enqueue_ke(arr, st) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "kinetic launch failed");
+    int rc = ctx->sync_check("system init");
+    if (rc != FMD_OK) return rc;
+    initialized = true;
+    return FMD_OK;
+}
+
+cudaError_t System::enqueue_variant(bool rebuild, bool phase, cudaStream_t st) {
+    cudaError_t e;
+    if (rebuild && (e = enqueue_rebuild(st)) != cudaSuccess) return e;
+    return enqueue_step(arr, sp, phase, st);
+}
+
+cudaError_t System::enqueue_one(int g, cudaStream_t st) {
+    return enqueue_variant((g % p.nlup) == 0, g <= p.coldstart + p.warmup, st);
+}
+
+int System::run(int first, int last, fmd_obs* obs) {
+    int rc = enqueue(first, last);
+    if (rc != FMD_OK) return rc;
+    rc = ctx->sync_check("system run");
+    if (rc != FMD_OK) return rc;
+    if (obs) {
+        if (cudaMemcpy(obs, &arr.S->obs, sizeof(fmd_obs), cudaMemcpyDeviceToHost) != cudaSuccess)
+            return ctx->fail(FMD_ERR_CUDA, "observable copy failed");
+    }
+    return FMD_OK;
+}
+
+int System::enqueue(int first, int last) {
+    if (!initialized) return ctx->fail(FMD_ERR_STATE, "fmd_system_run before fmd_system_init");
+    if (last < first) return FMD_OK;
+    cudaStream_t st = ctx->stream;
+    const int g0 = first - 1;
+    cudaMemcpyAsync(&arr.S->gstep, &g0, sizeof(int), cudaMemcpyHostToDevice, st);
+    for (int g = first; g <= last; g++) {
+        if (p.use_graphs) {
+            const int r = (g % p.nlup) == 0, ph = g <= p.coldstart + p.warmup;
+            cudaGraphExec_t& ge = graphs[r][ph];
+            if (!ge) {
+                cudaGraph_t graph;
+                if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+                    return ctx->fail(FMD_ERR_CUDA, "graph capture failed to start");
+                cudaError_t e = enqueue_one(g, st);
+                cudaError_t e2 = cudaStreamEndCapture(st, &graph);
+                if (e != cudaSuccess || e2 != cudaSuccess)
+                    return ctx->fail(FMD_ERR_CUDA, std::string("graph capture failed: ") +
+                                                       cudaGetErrorString(e != cudaSuccess ? e : e2));
+                e = cudaGraphInstantiate(&ge, graph, 0);
+                cudaGraphDestroy(graph);
+                if (e != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, cudaGetErrorString(e));
+            }
+            if (cudaGraphLaunch(ge, st) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "graph launch failed");
+        } else {
+            if (enqueue_one(g, st) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "step launch failed");
+        }
+    }
+    return FMD_OK;
+}
+
+int System::nonfinite_check() {
+    // Cheap watchdog on the scalars only; kernels never trap.
+    SysScal s;
+    if (cudaMemcpy(&s, arr.S, sizeof(s), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return ctx->fail(FMD_ERR_CUDA, "scalar copy failed");
+    if (!std::isfinite(s.KE) || !std::isfinite(s.E[0]) || !std::isfinite(s.h[0]))
+        return ctx->fail(FMD_ERR_NONFINITE, "non-finite energy or cell");
+    return FMD_OK;
+}
+
+}  // namespace fmd
+
+// ------------------------------------------------------------------ C-ABI --
+struct fmd_system {
+    std::unique_ptr<fmd::System> sys;
+};
+
+static int make_params(const fmd_run_params* p, fmd::System& s) {
+    s.p = *p;
+    if (s.p.nlup <= 0) return FMD_ERR_ARG;
+    s.sp.dt = p->dt; s.sp.T = p->T; s.sp.T_cold = p->T_cold;
+    s.sp.coldstart = p->coldstart; s.sp.warmup = p->warmup;
+    s.sp.gavg_from = p->gavg_from; s.sp.gavg_to = p->gavg_to;
+    s.sp.nc = p->nc > 0 ? p->nc : 1; s.sp.nmol = p->nmol > 0 ? p->nmol : 1;
+    s.sp.schedule = 1;
+    return FMD_OK;
+}
+
+extern "C" int fmd_system_create_rigid(fmd_ctx* ctx, const fmd_run_params* p, int n, int natom,
+                                       const double* body, double I0, double Mmol, double rmcut,
+                                       int max_neigh, const double* pos, const double* vel,
+                                       const double* qv, const double* omg, const double* h,
+                                       const fmd_npt* npt, fmd_system** out) {
+    if (!ctx || !p || !out || !body || !pos || !vel || !qv || !omg || !h || !npt || n < 1 || natom < 1 ||
+        natom > 96 || max_neigh < 1)
+        return ctx ? ctx->fail(FMD_ERR_ARG, "fmd_system_create_rigid: bad argument") : FMD_ERR_ARG;
+    auto s = std::make_unique<fmd::System>();
+    s->ctx = ctx;
+    if (make_params(p, *s) != FMD_OK) return ctx->fail(FMD_ERR_ARG, "bad run parameters");
+    s->arr.kind = FMD_SYS_RIGID;
+    s->arr.n = n;
+    s->arr.natom = natom;
+    s->arr.Mmol = Mmol;
+    s->arr.I0 = I0;
+    s->arr.precision = p->precision;
+    const double rmc = rmcut + 3.0;
+    s->arr.rmcut2 = rmcut * rmcut;
+    int rc = s->alloc_common(pos, vel, h, npt);
+    if (rc != FMD_OK) return rc;
+    double* bd; double* q; double* w; double* T;
+    if (s->alloc(&bd, 3 * (size_t)natom, body) || s->alloc(&q, 4 * (size_t)n, qv) ||
+        s->alloc(&w, 3 * (size_t)n, omg) || s->alloc(&T, 3 * (size_t)n, (const double*)nullptr))
+        return ctx->fail(FMD_ERR_CUDA, "device allocation failed");
+    cudaMemsetAsync(T, 0, sizeof(double) * 3 * n, ctx->stream);
+    s->arr.body = bd; s->arr.qv = q; s->arr.omg = w; s->arr.T = T;
+    // The list radius is rmcut+3 (LJ:259); the force kernel skips pairs
+    // beyond rmcut (LJ:320).
+    if ((rc = s->alloc_lists(rmc, max_neigh, 0.0, 0, false)) != FMD_OK) return rc;
+    s->rc2_a = rmc * rmc;
+    out[0] = new fmd_system{std::move(s)};
+    return FMD_OK;
+}
+
+extern "C" int fmd_system_create_airebo(fmd_ctx* ctx, const fmd_run_params* p, int na, const double* pos,
+                                        const double* vel, const double* mass, const int* mol_id,
+                                        const double* h, const fmd_npt* npt, fmd_system** out) {
+    if (!ctx || !p || !out || !pos || !vel || !mass || !mol_id || !h || !npt || na < 2)
+        return ctx ? ctx->fail(FMD_ERR_ARG, "fmd_system_create_airebo: bad argument") : FMD_ERR_ARG;
+    auto s = std::make_unique<fmd::System>();
+    s->ctx = ctx;
+    if (make_params(p, *s) != FMD_OK) return ctx->fail(FMD_ERR_ARG, "bad run parameters");
+    s->arr.kind = FMD_SYS_AIREBO;
+    s->arr.n = na;
+    int rc = s->alloc_common(pos, vel, h, npt);
+    if (rc != FMD_OK) return rc;
+    double* m; int* mid;
+    if (s->alloc(&m, na, mass) || s->alloc(&mid, na, mol_id)) return ctx->fail(FMD_ERR_CUDA, "device allocation failed");
+    s->arr.mass = m; s->arr.mol_id = mid;
+    const double lj_rcut = 3.0 * 3.40;          // AI:120
+    const double rebo_rcut = 2.0 + 0.3;         // AI:116
+    if ((rc = s->alloc_lists(lj_rcut + 2.0, 400, rebo_rcut, 12, true)) != FMD_OK) return rc;
+    out[0] = new fmd_system{std::move(s)};
+    return FMD_OK;
+}
+
+extern "C" int fmd_system_create_mm(fmd_ctx* ctx, const fmd_run_params* p, int na, const double* pos,
+                                    const double* vel, const int* mol_id, const fmd_mm_topology* t,
+                                    const double* charge, const double* h, const fmd_npt* npt,
+                                    fmd_system** out) {
+    if (!ctx || !p || !out || !pos || !vel || !mol_id || !t || !h || !npt || na < 2)
+        return ctx ? ctx->fail(FMD_ERR_ARG, "fmd_system_create_mm: bad argument") : FMD_ERR_ARG;
+    auto s = std::make_unique<fmd::System>();
+    s->ctx = ctx;
+    if (make_params(p, *s) != FMD_OK) return ctx->fail(FMD_ERR_ARG, "bad run parameters");
+    s->arr.kind = FMD_SYS_MM;
+    s->arr.n = na;
+    int rc = s->alloc_common(pos, vel, h, npt);
+    if (rc != FMD_OK) return rc;
+    int* mid;
+    if (s->alloc(&mid, na, mol_id)) return ctx->fail(FMD_ERR_CUDA, "device allocation failed");
+    s->arr.mol_id = mid;
+    if ((rc = s->upload_topology(t)) != FMD_OK) return rc;
+    bool has_charge = false;
+    if (charge)
+        for (int i = 0; i < na && !has_charge; i++) has_charge = std::fabs(charge[i]) > 1e-10;   // MM:1110
+    s->arr.has_charge = has_charge ? 1 : 0;
+    if (has_charge) {
+        double* q;
+        if (s->alloc(&q, na, charge)) return ctx->fail(FMD_ERR_CUDA, "device allocation failed");
+        s->arr.charge = q;
+    }
+    const double rcut = 3.0 * 3.431;            // MM:114
+    if ((rc = s->alloc_lists(rcut + 2.0, 400, 0.0, 0, true)) != FMD_OK) return rc;
+    out[0] = new fmd_system{std::move(s)};
+    return FMD_OK;
+}
+
+int fmd::System::upload_topology(const fmd_mm_topology* t) {
+    MMTopoDev d{};
+    d.nb = t->nb; d.nang = t->nang; d.ndih = t->ndih; d.nimp = t->nimp;
+    int *i0, *i1, *i2, *i3, *mult;
+    double *x0, *x1, *x2;
+    if (alloc(&i0, t->nb, t->b_i0) || alloc(&i1, t->nb, t->b_i1) || alloc(&x0, t->nb, t->b_kb) ||
+        alloc(&x1, t->nb, t->b_r0))
+        return ctx->fail(FMD_ERR_CUDA, "topology upload failed");
+    d.b_i0 = i0; d.b_i1 = i1; d.b_kb = x0; d.b_r0 = x1;
+    if (alloc(&i0, t->nang, t->ang_i0) || alloc(&i1, t->nang, t->ang_i1) || alloc(&i2, t->nang, t->ang_i2) ||
+        alloc(&x0, t->nang, t->ang_kth) || alloc(&x1, t->nang, t->ang_th0))
+        return ctx->fail(FMD_ERR_CUDA, "topology upload failed");
+    d.a_i0 = i0; d.a_i1 = i1; d.a_i2 = i2; d.a_kth = x0; d.a_th0 = x1;
+    if (alloc(&i0, t->ndih, t->dih_i0) || alloc(&i1, t->ndih, t->dih_i1) || alloc(&i2, t->ndih, t->dih_i2) ||
+        alloc(&i3, t->ndih, t->dih_i3) || alloc(&x0, t->ndih, t->dih_vn) || alloc(&mult, t->ndih, t->dih_mult) ||
+        alloc(&x2, t->ndih, t->dih_gamma))
+        return ctx->fail(FMD_ERR_CUDA, "topology upload failed");
+    d.d_i0 = i0; d.d_i1 = i1; d.d_i2 = i2; d.d_i3 = i3; d.d_vn = x0; d.d_mult = mult; d.d_gamma = x2;
+    if (alloc(&i0, t->nimp, t->imp_i0) || alloc(&i1, t->nimp, t->imp_i1) || alloc(&i2, t->nimp, t->imp_i2) ||
+        alloc(&i3, t->nimp, t->imp_i3) || alloc(&x0, t->nimp, t->imp_ki) || alloc(&x1, t->nimp, t->imp_gamma))
+        return ctx->fail(FMD_ERR_CUDA, "topology upload failed");
+    d.m_i0 = i0; d.m_i1 = i1; d.m_i2 = i2; d.m_i3 = i3; d.m_ki = x0; d.m_gamma = x1;
+    arr.topo = d;
+    return FMD_OK;
+}
+
+extern "C" int fmd_system_init(fmd_system* s) {
+    if (!s) return FMD_ERR_ARG;
+    return s->sys->init();
+}
+
+extern "C" int fmd_system_run(fmd_system* s, int first, int last, fmd_obs* obs) {
+    if (!s) return FMD_ERR_ARG;
+    return s->sys->run(first, last, obs);
+}
+
+extern "C" int fmd_system_enqueue(fmd_system* s, int first, int last) {
+    if (!s) return FMD_ERR_ARG;
+    return s->sys->enqueue(first, last);
+}
+
+extern "C" int fmd_system_averages(fmd_system* s, fmd_avg* avg) {
+    if (!s || !avg) return FMD_ERR_ARG;
+    fmd::System& y = *s->sys;
+    if (cudaMemcpy(avg, &y.arr.S->avg, sizeof(fmd_avg), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return y.ctx->fail(FMD_ERR_CUDA, "average copy failed");
+    return FMD_OK;
+}
+
+extern "C" int fmd_system_download(fmd_system* s, double* pos, double* vel, double* qv, double* omg, double* h,
+                                   fmd_npt* npt) {
+    if (!s) return FMD_ERR_ARG;
+    fmd::System& y = *s->sys;
+    cudaStream_t st = y.ctx->stream;
+    const size_t n = y.arr.n;
+    if (pos) cudaMemcpyAsync(pos, y.arr.pos, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, st);
+    if (vel) cudaMemcpyAsync(vel, y.arr.vel, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, st);
+    if (qv && y.arr.qv) cudaMemcpyAsync(qv, y.arr.qv, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, st);
+    if (omg && y.arr.omg) cudaMemcpyAsync(omg, y.arr.omg, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, st);
+    if (h) cudaMemcpyAsync(h, y.arr.S->h, sizeof(double) * 9, cudaMemcpyDeviceToHost, st);
+    if (npt) cudaMemcpyAsync(npt, &y.arr.S->npt, sizeof(fmd_npt), cudaMemcpyDeviceToHost, st);
+    return y.ctx->sync_check("system download");
+}
+
+extern "C" int fmd_system_lists(fmd_system* s, int* cnt_a, int* list_a, int* cnt_b, int* list_b) {
+    if (!s) return FMD_ERR_ARG;
+    fmd::System& y = *s->sys;
+    cudaStream_t st = y.ctx->stream;
+    const size_t n = y.arr.n;
+    if (cnt_a) cudaMemcpyAsync(cnt_a, y.arr.cnt_a, sizeof(int) * n, cudaMemcpyDeviceToHost, st);
+    if (list_a) cudaMemcpyAsync(list_a, y.arr.list_a, sizeof(int) * n * y.arr.cap_a, cudaMemcpyDeviceToHost, st);
+    if (cnt_b && y.arr.cnt_b) cudaMemcpyAsync(cnt_b, y.arr.cnt_b, sizeof(int) * n, cudaMemcpyDeviceToHost, st);
+    if (list_b && y.arr.list_b)
+        cudaMemcpyAsync(list_b, y.arr.list_b, sizeof(int) * n * y.arr.cap_b, cudaMemcpyDeviceToHost, st);
+    return y.ctx->sync_check("system lists");
+}
+
+extern "C" int fmd_system_kernel_ms(fmd_system* s, int stage, int reps, double* ms) {
+    if (!s || !ms || reps < 1 || stage < 0 || stage > 3) return FMD_ERR_ARG;
+    fmd::System& y = *s->sys;
+    if (!y.initialized) return y.ctx->fail(FMD_ERR_STATE, "kernel timing before init");
+    cudaStream_t st = y.ctx->stream;
+    const StepArrays& a = y.arr;
+    const double* hh = a.S->h;
+    auto launch = [&]() -> cudaError_t {
+        switch (stage) {
+            case 0:
+                if (a.kind == FMD_SYS_RIGID)
+                    return rigid_launch(a.precision, a.pos, a.qv, a.body, hh, a.cnt_a, a.list_a, a.cap_a, a.n,
+                                        a.natom, a.rmcut2, a.F, a.T, a.part_f1, st);
+                // Timed into the scratch accumulator (F itself is left alone).
+                return lj_gather_launch(a.kind == FMD_SYS_AIREBO ? FMD_FF_AIREBO : FMD_FF_MM, a.pos, hh, a.cnt_a,
+                                        a.list_a, a.cap_a, a.in_cnt, a.in_list, a.in_cap, a.n, a.Facc, a.Facc,
+                                        a.part_f2, st);
+            case 1:
+                if (a.kind == FMD_SYS_AIREBO)
+                    return rebo_launch(a.pos, hh, a.cnt_b, a.list_b, a.cap_b, a.n, a.Facc, a.part_f1, st);
+                if (a.kind == FMD_SYS_MM) return mm_bonded_launch(a.topo, a.pos, hh, a.Facc, a.part_f1, st);
+                return rigid_launch(a.precision, a.pos, a.qv, a.body, hh, a.cnt_a, a.list_a, a.cap_a, a.n, a.natom,
+                                    a.rmcut2, a.F, a.T, a.part_f1, st);
+            case 2:
+                return y.enqueue_rebuild(st);
+            default:
+                return enqueue_forces(a, st);
+        }
+    };
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    launch();   // warm
+    cudaEventRecord(e0, st);
+    for (int r = 0; r < reps; r++) launch();
+    cudaEventRecord(e1, st);
+    cudaError_t err = cudaEventSynchronize(e1);
+    float tot = 0.f;
+    cudaEventElapsedTime(&tot, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    // Restore the invariant that the accumulator is zero between steps and
+    // that F holds the forces of the current positions.
+    cudaMemsetAsync(a.Facc, 0, sizeof(double) * 3 * a.n, st);
+    if (stage != 2) {
+        enqueue_forces(a, st);
+        enqueue_force_reduce(a, st);
+    }
+    int rc = y.ctx->sync_check("kernel timing");
+    if (err != cudaSuccess) return y.ctx->fail(FMD_ERR_CUDA, cudaGetErrorString(err));
+    *ms = (double)tot / reps;
+    return rc;
+}
+
+extern "C" int fmd_system_step_kernels(fmd_system* s, int rebuild, int phase, int* nk) {
+    if (!s || !nk) return FMD_ERR_ARG;
+    fmd::System& y = *s->sys;
+    cudaStream_t st = y.ctx->stream;
+    cudaGraph_t graph;
+    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return y.ctx->fail(FMD_ERR_CUDA, "capture failed");
+    cudaError_t e = y.enqueue_variant(rebuild != 0, phase != 0, st);
+    cudaError_t e2 = cudaStreamEndCapture(st, &graph);
+    if (e != cudaSuccess || e2 != cudaSuccess) return y.ctx->fail(FMD_ERR_CUDA, "capture failed");
+    size_t n = 0;
+    cudaGraphGetNodes(graph, nullptr, &n);
+    std::vector<cudaGraphNode_t> nodes(n);
+    cudaGraphGetNodes(graph, nodes.data(), &n);
+    int k = 0;
+    for (auto& nd : nodes) {
+        cudaGraphNodeType t;
+        cudaGraphNodeGetType(nd, &t);
+        if (t == cudaGraphNodeTypeKernel) k++;
+    }
+    cudaGraphDestroy(graph);
+    *nk = k;
+    return FMD_OK;
+}
+
+extern "C" int fmd_system_destroy(fmd_system* s) {
+    if (!s) return FMD_OK;
+    if (s->sys) {
+        cudaStreamSynchronize(s->sys->ctx->stream);
+        s->sys->release();
+    }
+    delete s;
+    return FMD_OK;
+}

@@ -1,0 +1,222 @@
+/*
+ * fullermd.h -- C-ABI of libfullermd_cuda.so, the B200 (sm_100a) implementation
+ * of fuller_md's per-step force-and-integrate path.
+ *
+ * Plain pointers and sizes only.  All arrays use the reference layouts: flat
+ * row-major double, positions pos[3*i+c], quaternions qv[4*i+c] (w,x,y,z),
+ * cell matrix h[3*r+c] whose COLUMNS are the lattice vectors, 9-component
+ * virials W[3*a+b], neighbour lists list[i*max_neigh+k] with counts cnt[i].
+ *
+ * Two families of entry points:
+ *  - host-pointer kernels (fmd_nlist_*, fmd_*_forces, fmd_*_step): each
+ *    replaces one reference routine, takes and returns host arrays, copies
+ *    them to and from the device, and is synchronous.  They are the parity
+ *    boundary the tests check against the reference.
+ *  - device-resident systems (fmd_system_*): own all state in HBM, run many
+ *    steps with no host round trip (lists rebuilt on the device, the step
+ *    replayed as a CUDA graph) and return observables.  The C++ drivers
+ *    fuller_*_gpu are built on these.
+ *
+ * Every function returns an fmd_status; fmd_ctx_last_error() explains a
+ * failure.  A context is bound to one device and one stream and is not
+ * thread-safe.  Reference citations are to focusnishikawa/fuller_md_en src/:
+ *   LJ = fuller_LJ_npt_md_serial_omp_acc.cpp, CORE = fuller_LJ_npt_md_core_serial.cpp,
+ *   AI = fuller_airebo_npt_md_serial_omp_acc.cpp, MM = fuller_LJ_npt_mmmd_serial_omp_acc.cpp
+ */
+#ifndef FULLERMD_H
+#define FULLERMD_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum fmd_status {
+    FMD_OK = 0,
+    FMD_ERR_ARG = 1,        /* bad argument (null pointer, size out of range) */
+    FMD_ERR_CUDA = 2,       /* CUDA runtime error or extension not usable */
+    FMD_ERR_CAPACITY = 3,   /* a fixed-size buffer would overflow */
+    FMD_ERR_NONFINITE = 4,  /* NaN/Inf detected in the state */
+    FMD_ERR_STATE = 5       /* call out of order (e.g. run before init) */
+};
+
+enum fmd_precision {
+    FMD_PREC_FP64 = 0,      /* all pair arithmetic in FP64 */
+    FMD_PREC_FP32_PAIR = 1  /* pair arithmetic in FP32, per-molecule sums in FP64 */
+};
+
+enum fmd_forcefield { FMD_FF_AIREBO = 0, FMD_FF_MM = 1 };
+enum fmd_kind { FMD_SYS_RIGID = 0, FMD_SYS_AIREBO = 1, FMD_SYS_MM = 2 };
+
+typedef struct fmd_ctx fmd_ctx;
+
+/* NPT thermostat/barostat state, field for field as NPTState
+ * (LJ:425, AI:511, MM:804). */
+typedef struct {
+    double xi, Q, Vg[9], W, Pe, Tt;
+    int Nf;
+} fmd_npt;
+
+/* Flat MM topology, as FlatTopology (MM:226-237) without mol_id. */
+typedef struct {
+    int nb;   const int *b_i0, *b_i1; const double *b_kb, *b_r0;
+    int nang; const int *ang_i0, *ang_i1, *ang_i2; const double *ang_kth, *ang_th0;
+    int ndih; const int *dih_i0, *dih_i1, *dih_i2, *dih_i3; const double *dih_vn;
+              const int *dih_mult; const double *dih_gamma;
+    int nimp; const int *imp_i0, *imp_i1, *imp_i2, *imp_i3; const double *imp_ki, *imp_gamma;
+} fmd_mm_topology;
+
+/* ------------------------------------------------------------------ context */
+int fmd_version(void);
+int fmd_ctx_create(fmd_ctx **out, int device);
+int fmd_ctx_destroy(fmd_ctx *ctx);
+/* Use the caller's CUDA stream (a cudaStream_t) instead of the context's own. */
+int fmd_ctx_set_stream(fmd_ctx *ctx, void *cuda_stream);
+void *fmd_ctx_get_stream(fmd_ctx *ctx);
+int fmd_ctx_synchronize(fmd_ctx *ctx);
+const char *fmd_ctx_last_error(const fmd_ctx *ctx);
+const char *fmd_status_string(int code);
+
+/* ------------------------------------------------------- host-pointer kernels */
+/* mat_inv9 (LJ:120-124), evaluated on the device. */
+int fmd_mat_inv9(fmd_ctx *ctx, const double *h, double *hi);
+/* apply_pbc (LJ:137-151, AI:149-161). */
+int fmd_apply_pbc(fmd_ctx *ctx, double *pos, const double *h, const double *hi, int n);
+
+/* nlist_build_sym (LJ:257-268, CORE:280-301): symmetric molecule list, pair
+ * test |mimg(r_j-r_i)|^2 < (rmcut+3)^2, rows ascending, first max_neigh kept.
+ * *dropped (may be NULL) receives the number of entries that did not fit. */
+int fmd_nlist_rigid(fmd_ctx *ctx, const double *pos, const double *h, const double *hi, int n,
+                    double rmcut, int max_neigh, int *nl_count, int *nl_list, int *dropped);
+/* build_nlist_lj (AI:263-272, MM:337-346): intermolecular half list, j>i
+ * ascending, |d|^2 < rc_list^2, first max_neigh kept. */
+int fmd_nlist_lj_half(fmd_ctx *ctx, const double *pos, const double *h, const double *hi, int na,
+                      const int *mol_id, double rc_list, int max_neigh, int *nlc, int *nll,
+                      int *dropped);
+/* build_nlist_rebo (AI:251-261): intramolecular symmetric list, |d|^2 < rc^2. */
+int fmd_nlist_rebo(fmd_ctx *ctx, const double *pos, const double *h, const double *hi, int na,
+                   const int *mol_id, double rc, int max_neigh, int *nlc, int *nll, int *dropped);
+
+/* forces (LJ:271-400, CORE:346-444): lab-frame sites from quaternions, then
+ * site-site shifted LJ over the symmetric list.  Overwrites Fv, Tv, Wm9;
+ * *Ep = potential energy. */
+int fmd_lj_rigid_forces(fmd_ctx *ctx, const double *pos, const double *qv, const double *body,
+                        const double *h, const double *hi, const int *nl_count, const int *nl_list,
+                        int max_neigh, int n, int natom, double rmcut2, int precision,
+                        double *Fv, double *Tv, double *Wm9, double *Ep);
+/* compute_rebo (AI:275-421): ADDS into F and vir9 like the reference; *E = energy. */
+int fmd_rebo_forces(fmd_ctx *ctx, const double *pos, const double *h, const double *hi,
+                    const int *nlc, const int *nll, int max_neigh, int na,
+                    double *F, double *vir9, double *E);
+/* compute_lj (AI:424-473) for ff=FMD_FF_AIREBO, MM LJ block (MM:711-764) for
+ * ff=FMD_FF_MM: ADDS into F and vir9; *E = energy. */
+int fmd_lj_half_forces(fmd_ctx *ctx, int ff, const double *pos, const double *h, const double *hi,
+                       const int *nlc, const int *nll, int max_neigh, int na,
+                       double *F, double *vir9, double *E);
+/* compute_forces (AI:477-495): zeroes F, vir9; E3 = {Ep, Ep_rebo, Ep_lj}.
+ * Lists use the reference widths 12 (REBO) and 400 (LJ). */
+int fmd_airebo_forces(fmd_ctx *ctx, const double *pos, const double *h, const double *hi,
+                      const int *nlc_r, const int *nll_r, const int *nlc_l, const int *nll_l,
+                      int na, double *F, double *vir9, double *E3);
+/* compute_forces (MM:351-788): zeroes F, vir9;
+ * E7 = {Eb, Ea, Ed, Ei, Elj, Ecoul, Etot}.  LJ list width 400. */
+int fmd_mm_forces(fmd_ctx *ctx, const fmd_mm_topology *t, const double *pos, const double *h,
+                  const double *hi, const int *nlc, const int *nll, const double *charge,
+                  const int *mol_id, int has_charge, int na, double *F, double *vir9, double *E7);
+
+/* step_npt (LJ:434-538): one rigid NPT step on host state; out2 = {Ep, KE}. */
+int fmd_rigid_step(fmd_ctx *ctx, double *pos, double *vel, double *qv, double *omg,
+                   double *Fv, double *Tv, double *Wm9, double *h, double *hi,
+                   const double *body, double I0, double Mmol, int n, int natom, double rmcut2,
+                   double dt, fmd_npt *npt, const int *nl_count, const int *nl_list,
+                   int max_neigh, int precision, double *out2);
+/* step_npt (AI:518-590); out4 = {Ep, Ep_rebo, Ep_lj, KE}. */
+int fmd_airebo_step(fmd_ctx *ctx, double *pos, double *vel, double *F, double *vir9,
+                    double *h, double *hi, const double *mass, int na, double dt, fmd_npt *npt,
+                    const int *nlc_r, const int *nll_r, const int *nlc_l, const int *nll_l,
+                    double *out4);
+/* step_npt (MM:811-890); out8 = {Eb, Ea, Ed, Ei, Elj, Ecoul, Etot, KE}. */
+int fmd_mm_step(fmd_ctx *ctx, double *pos, double *vel, double *F, double *vir9, double *h,
+                double *hi, int na, double dt, fmd_npt *npt, const fmd_mm_topology *t,
+                const int *nlc, const int *nll, const double *charge, const int *mol_id,
+                int has_charge, double *out8);
+
+/* ------------------------------------------------------ device-resident systems */
+typedef struct fmd_system fmd_system;
+
+/* Run schedule of a driver (LJ:830-897, AI:855-912, MM:1174-1236). */
+typedef struct {
+    double dt, T, Pe, T_cold;
+    int coldstart, warmup, nsteps;   /* total steps = coldstart + warmup + nsteps */
+    int nlup;                        /* list rebuild cadence (25 rigid, 20 atomistic) */
+    int gavg_from, gavg_to;          /* global-step averaging window */
+    int nc;                          /* lattice repeats, for a = h[0]/nc */
+    int nmol;                        /* energies are reported per molecule */
+    int precision;                   /* fmd_precision (rigid pair kernel) */
+    int use_graphs;                  /* 1: replay steps as CUDA graphs */
+} fmd_run_params;
+
+/* Observables of one step, as the reference monitor line computes them. */
+typedef struct {
+    int step;
+    double T, P, a, KE;
+    double E[8];   /* rigid: {Ep}; AIREBO: {Ep, Ep_rebo, Ep_lj};
+                      MM: {Eb, Ea, Ed, Ei, Elj, Ecoul, Etot} -- totals, not per molecule */
+} fmd_obs;
+
+/* Running averages over the window (the reference's sT, sP, sa, sE... sums). */
+typedef struct {
+    int n;
+    double sT, sP, sa;
+    double sE[8];  /* per-molecule energy sums in the program's own grouping */
+} fmd_avg;
+
+/* Rigid LJ system (LJ main, LJ:742-944).  pos/vel/qv/omg: n molecules. */
+int fmd_system_create_rigid(fmd_ctx *ctx, const fmd_run_params *p, int n, int natom,
+                            const double *body, double I0, double Mmol, double rmcut,
+                            int max_neigh, const double *pos, const double *vel, const double *qv,
+                            const double *omg, const double *h, const fmd_npt *npt,
+                            fmd_system **out);
+/* AIREBO system (AI main, AI:771-955). */
+int fmd_system_create_airebo(fmd_ctx *ctx, const fmd_run_params *p, int na, const double *pos,
+                             const double *vel, const double *mass, const int *mol_id,
+                             const double *h, const fmd_npt *npt, fmd_system **out);
+/* MM system (MM main, MM:1094-1279). */
+int fmd_system_create_mm(fmd_ctx *ctx, const fmd_run_params *p, int na, const double *pos,
+                         const double *vel, const int *mol_id, const fmd_mm_topology *t,
+                         const double *charge, const double *h, const fmd_npt *npt,
+                         fmd_system **out);
+/* The reference's pre-loop work: apply_pbc, neighbour lists, first forces
+ * (LJ:813-828, AI:830-853, MM:1152-1172). */
+int fmd_system_init(fmd_system *s);
+/* Advances global steps first..last inclusive (driver loop body of
+ * LJ:847-897 etc., including list rebuilds, the temperature schedule,
+ * cold/warm rescaling and window averages).  *last receives the observables
+ * of step `last` (may be NULL). */
+int fmd_system_run(fmd_system *s, int first, int last, fmd_obs *obs);
+/* As fmd_system_run but only enqueues the steps on the context stream and
+ * returns without synchronising (errors surface at the next synchronising
+ * call). */
+int fmd_system_enqueue(fmd_system *s, int first, int last);
+int fmd_system_averages(fmd_system *s, fmd_avg *avg);
+/* Copies the state to host arrays (any may be NULL). */
+int fmd_system_download(fmd_system *s, double *pos, double *vel, double *qv, double *omg,
+                        double *h, fmd_npt *npt);
+/* Current neighbour lists (reference layout) for inspection. */
+int fmd_system_lists(fmd_system *s, int *cnt_a, int *list_a, int *cnt_b, int *list_b);
+int fmd_system_destroy(fmd_system *s);
+
+/* Measurement helpers (no reference counterpart).  fmd_system_kernel_ms
+ * launches one stage `reps` times on the context stream between CUDA events
+ * and returns the mean duration per launch in milliseconds; stages:
+ *   0 the pair kernel (rigid site-site LJ, or the atomistic LJ gather),
+ *   1 the second force kernel (REBO, or MM bonded), 2 a full list rebuild,
+ *   3 one complete step (eager launches).
+ * The force stages leave F in place (they recompute the current forces).
+ * fmd_system_step_kernels returns the number of kernel launches of one step
+ * of each variant (list rebuild or not, cold/warm phase or not). */
+int fmd_system_kernel_ms(fmd_system *s, int stage, int reps, double *ms_per_launch);
+int fmd_system_step_kernels(fmd_system *s, int rebuild, int phase, int *nkernels);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,233 @@
+"""GPU parity through the C-ABI: every host-pointer entry point against the
+reference's recorded outputs (tests/golden) and the CPU oracle.
+
+Bars: neighbour lists bit-exact; FP64 forces/energies/virials to 1e-10
+relative (the kernels follow the reference's operation order where it feeds a
+decision, and differ only by FMA contraction, summation order and GPU libm
+ulps elsewhere); the FP32-pair rigid kernel to 1e-6 relative on energy,
+virial and pressure, 1e-4 on forces."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import csr_rows, rel, rows, same_rows
+from fuller_md_en_b200 import crystal
+from fuller_md_en_b200._lib import FMD_FF_MM, FMD_PREC_FP32_PAIR, FmdError
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-10
+RC_AI = 3.0 * 3.40 + 2.0
+RC_MM = 3.0 * 3.431 + 2.0
+
+
+def lists_from_golden(g, na):
+    cr = g["cnt_rebo"]
+    lr = np.zeros(na * 12, np.int32)
+    for k, r in enumerate(csr_rows(cr, g["csr_rebo"])):
+        lr[k * 12:k * 12 + len(r)] = r
+    return cr, lr
+
+
+# ----------------------------------------------------------------- lists --
+@pytest.mark.parametrize("nc", [1, 2])
+def test_airebo_lists_match_reference(ctx, golden, oracle, nc):
+    g = golden(f"airebo_nc{nc}")
+    na = g["pos"].size // 3
+    cr, lr, _ = ctx.build_nlist_rebo(g["pos"], g["h"], g["hi"], na, g["mol_id"])
+    assert np.array_equal(cr, g["cnt_rebo"]) and same_rows(rows(cr, lr, 12), csr_rows(cr, g["csr_rebo"]))
+    cl, ll, dropped = ctx.build_nlist_lj(g["pos"], g["h"], g["hi"], na, g["mol_id"])
+    oc, ol, odrop = oracle.nlist_half(g["pos"], g["h"], g["hi"], na, g["mol_id"], RC_AI)
+    assert np.array_equal(cl, g["cnt_lj"])
+    assert same_rows(rows(cl, ll, 400), rows(oc, ol, 400))
+    assert dropped == odrop
+
+
+@pytest.mark.parametrize("nc,seed,jitter", [(3, 1, 0.01), (3, 2, 0.1)])
+def test_airebo_lists_larger(ctx, oracle, nc, seed, jitter):
+    s = crystal.atomistic(nc, jitter=jitter, seed=seed)
+    na = s["pos"].size // 3
+    for fn, ofn, cap in ((ctx.build_nlist_rebo, lambda: oracle.nlist_intra(s["pos"], s["h"], s["hi"], na, s["mol_id"]), 12),
+                         (ctx.build_nlist_lj, lambda: oracle.nlist_half(s["pos"], s["h"], s["hi"], na, s["mol_id"], RC_AI), 400)):
+        c, l, dr = fn(s["pos"], s["h"], s["hi"], na, s["mol_id"])
+        oc, ol, odr = ofn()
+        assert np.array_equal(c, oc) and same_rows(rows(c, l, cap), rows(oc, ol, cap)) and dr == odr
+
+
+def test_lists_triclinic_cell(ctx, oracle):
+    """HCP cell (non-orthogonal h) with a shear: the image choice by round()
+    and the fractional-space cells must still give the reference's rows."""
+    s = crystal.atomistic(2, jitter=0.02, seed=4, st="HCP")
+    h = s["h"].copy()
+    h[2] += 1.7   # shear the third lattice vector
+    hi = crystal.inv9(h)
+    na = s["pos"].size // 3
+    c, l, dr = ctx.build_nlist_lj(s["pos"], h, hi, na, s["mol_id"])
+    oc, ol, odr = oracle.nlist_half(s["pos"], h, hi, na, s["mol_id"], RC_AI)
+    assert np.array_equal(c, oc) and same_rows(rows(c, l, 400), rows(oc, ol, 400)) and dr == odr
+
+
+def test_list_truncation_small_cap(ctx, oracle):
+    s = crystal.atomistic(1, jitter=0.05, seed=9)
+    na = s["pos"].size // 3
+    c, l, dr = ctx.build_nlist_lj(s["pos"], s["h"], s["hi"], na, s["mol_id"], max_neigh=7)
+    oc, ol, odr = oracle.nlist_half(s["pos"], s["h"], s["hi"], na, s["mol_id"], RC_AI, cap=7)
+    assert dr == odr > 0
+    assert np.array_equal(c, oc) and same_rows(rows(c, l, 7), rows(oc, ol, 7))
+
+
+def test_empty_and_bad_arguments(ctx):
+    c, l, dr = ctx.build_nlist_lj(np.zeros(0), np.eye(3).reshape(-1) * 10, np.eye(3).reshape(-1) / 10, 0,
+                                  np.zeros(0, np.int32))
+    assert c.size == 0 and dr == 0
+    with pytest.raises(FmdError):
+        ctx.build_nlist_lj(np.zeros(6), np.eye(3).reshape(-1), np.eye(3).reshape(-1), 2, np.zeros(2, np.int32),
+                           max_neigh=0)
+
+
+@pytest.mark.parametrize("nc", [2, 3])
+def test_rigid_list_matches_reference(ctx, golden, nc):
+    g = golden(f"rigid_nc{nc}")
+    n = g["pos"].size // 3
+    c, l, _ = ctx.nlist_build_sym(g["pos"], g["h"], g["hi"], n, float(g["rmcut"]))
+    assert np.array_equal(c, g["cnt"]) and same_rows(rows(c, l, 80), csr_rows(g["cnt"], g["csr"]))
+
+
+def test_rigid_list_nc10(ctx, oracle):
+    s = crystal.rigid(10, seed=1)
+    n = s["n"]
+    rmcut = 3.0 * 3.431 + 2 * s["Rmol"] + 1.0
+    c, l, dr = ctx.nlist_build_sym(s["pos"], s["h"], s["hi"], n, rmcut)
+    oc, ol, odr = oracle.nlist_sym(s["pos"], s["h"], s["hi"], n, rmcut)
+    assert np.array_equal(c, oc) and same_rows(rows(c, l, 80), rows(oc, ol, 80)) and dr == odr
+
+
+# ---------------------------------------------------------------- forces --
+@pytest.mark.parametrize("nc", [1, 2])
+def test_airebo_forces(ctx, golden, oracle, nc):
+    g = golden(f"airebo_nc{nc}")
+    na = g["pos"].size // 3
+    cr, lr = lists_from_golden(g, na)
+    cl, ll, _ = oracle.nlist_half(g["pos"], g["h"], g["hi"], na, g["mol_id"], RC_AI)
+    E, F, W = ctx.compute_forces_airebo(g["pos"], g["h"], g["hi"], cr, lr, cl, ll, na)
+    assert rel(E, g["E"]) < FP64_TOL and rel(F, g["F"]) < FP64_TOL and rel(W, g["W"]) < FP64_TOL
+    F1, W1 = np.zeros(3 * na), np.zeros(9)
+    e = ctx.compute_rebo(F1, W1, g["pos"], g["h"], g["hi"], cr, lr, na)
+    assert abs(e - g["E_rebo"]) < FP64_TOL * abs(g["E_rebo"]) and rel(F1, g["F_rebo"]) < FP64_TOL
+    assert rel(W1, g["W_rebo"]) < FP64_TOL
+    F2, W2 = np.zeros(3 * na), np.zeros(9)
+    e = ctx.compute_lj(F2, W2, g["pos"], g["h"], g["hi"], cl, ll, na)
+    assert abs(e - g["E_lj"]) < FP64_TOL * abs(g["E_lj"]) and rel(F2, g["F_lj"]) < FP64_TOL
+    assert rel(W2, g["W_lj"]) < FP64_TOL
+
+
+@pytest.mark.parametrize("nc", [2, 3])
+def test_rigid_forces_fp64(ctx, golden, nc):
+    g = golden(f"rigid_nc{nc}")
+    n = g["pos"].size // 3
+    rm = float(g["rmcut"])
+    cnt = g["cnt"]
+    lst = np.zeros(n * 80, np.int32)
+    for k, r in enumerate(csr_rows(cnt, g["csr"])):
+        lst[k * 80:k * 80 + len(r)] = r
+    e, F, T, W = ctx.forces(g["pos"], g["qv"], g["body"], g["h"], g["hi"], cnt, lst, n, 60, rm * rm)
+    assert abs(e - g["E"]) < FP64_TOL * abs(g["E"])
+    assert rel(F, g["F"]) < FP64_TOL and rel(T, g["T"]) < FP64_TOL and rel(W, g["W"]) < FP64_TOL
+
+
+@pytest.mark.parametrize("nc", [2, 3])
+def test_rigid_forces_fp32_pair(ctx, golden, nc):
+    g = golden(f"rigid_nc{nc}")
+    n = g["pos"].size // 3
+    rm = float(g["rmcut"])
+    cnt = g["cnt"]
+    lst = np.zeros(n * 80, np.int32)
+    for k, r in enumerate(csr_rows(cnt, g["csr"])):
+        lst[k * 80:k * 80 + len(r)] = r
+    e, F, T, W = ctx.forces(g["pos"], g["qv"], g["body"], g["h"], g["hi"], cnt, lst, n, 60, rm * rm,
+                            precision=FMD_PREC_FP32_PAIR)
+    assert abs(e - g["E"]) < 1e-6 * abs(g["E"])
+    # virial and pressure: normalised by the virial's Frobenius norm (the
+    # off-diagonal entries are near zero, so per-entry relative error is ill-posed)
+    assert np.max(np.abs(W - g["W"])) < 1e-6 * np.linalg.norm(g["W"])
+    assert rel(F, g["F"]) < 1e-4 and rel(T, g["T"]) < 1e-4
+
+
+def _mm_topo(g):
+    from fuller_md_en_b200 import Topology
+    t = {k[5:]: g[k] for k in g if k.startswith("topo_")}
+    return t, Topology(t["bonds"], t["kb"], t["r0"], t["angles"], t["kth"], t["th0"], t["dihedrals"], t["vn"],
+                       t["mult"], t["gamma"], t["impropers"], t["ki"], t["igamma"])
+
+
+def test_mm_forces(ctx, golden, oracle):
+    g = golden("mm_nc1")
+    t, topo = _mm_topo(g)
+    na = g["pos"].size // 3
+    cnt, lst, _ = ctx.build_nlist_lj(g["pos"], g["h"], g["hi"], na, t["mol_id"], rc_list=RC_MM)
+    oc, ol, _ = oracle.nlist_half(g["pos"], g["h"], g["hi"], na, t["mol_id"], RC_MM)
+    assert same_rows(rows(cnt, lst, 400), rows(oc, ol, 400))
+    E, F, W = ctx.compute_forces_mm(topo, g["pos"], g["h"], g["hi"], cnt, lst, na)
+    assert rel(E, g["E"]) < FP64_TOL and rel(F, g["F"]) < FP64_TOL and rel(W, g["W"]) < FP64_TOL
+    Eq, Fq, Wq = ctx.compute_forces_mm(topo, g["pos"], g["h"], g["hi"], cnt, lst, na, charge=g["charge"],
+                                       mol_id=t["mol_id"])
+    assert abs(Eq[5]) > 0 and rel(Eq, g["Eq"]) < FP64_TOL and rel(Fq, g["Fq"]) < FP64_TOL
+    F2, W2 = np.zeros(3 * na), np.zeros(9)
+    e = ctx.compute_lj(F2, W2, g["pos"], g["h"], g["hi"], cnt, lst, na, ff=FMD_FF_MM)
+    assert abs(e - g["E"][4]) < FP64_TOL * abs(g["E"][4])
+
+
+# ----------------------------------------------------------------- steps --
+@pytest.mark.parametrize("nc", [1, 2])
+def test_airebo_step(ctx, golden, oracle, nc):
+    g = golden(f"airebo_nc{nc}")
+    na = g["pos"].size // 3
+    cr, lr = lists_from_golden(g, na)
+    cl, ll, _ = oracle.nlist_half(g["pos"], g["h"], g["hi"], na, g["mol_id"], RC_AI)
+    st = dict(pos=g["pos"].copy(), vel=g["vel"].copy(), F=g["F"].copy(), vir9=g["W"].copy(), h=g["h"].copy(),
+              hi=g["hi"].copy(), mass=g["mass"], npt=g["npt0"].copy())
+    out = ctx.step_npt_airebo(st, 0.5, cr, lr, cl, ll)
+    assert rel(out, g["step_out"]) < FP64_TOL
+    for k in ("pos", "vel", "F", "vir9", "h", "hi", "npt"):
+        assert rel(st[k], g[f"step_{k}"]) < FP64_TOL, k
+
+
+@pytest.mark.parametrize("nc", [2, 3])
+def test_rigid_step(ctx, golden, nc):
+    g = golden(f"rigid_nc{nc}")
+    n = g["pos"].size // 3
+    rm = float(g["rmcut"])
+    cnt = g["cnt"]
+    lst = np.zeros(n * 80, np.int32)
+    for k, r in enumerate(csr_rows(cnt, g["csr"])):
+        lst[k * 80:k * 80 + len(r)] = r
+    st = dict(pos=g["pos"].copy(), vel=g["vel"].copy(), qv=g["qv"].copy(), omg=g["omg"].copy(), F=g["F"].copy(),
+              T=g["T"].copy(), W9=g["W"].copy(), h=g["h"].copy(), hi=g["hi"].copy(), npt=g["npt0"].copy())
+    Ep, KE = ctx.step_npt_rigid(st, g["body"], float(g["I0"]), float(g["Mmol"]), 60, rm * rm, 1.0, cnt, lst)
+    assert rel([Ep, KE], g["step_out"]) < FP64_TOL
+    for k in ("pos", "vel", "qv", "omg", "F", "T", "W9", "h", "hi", "npt"):
+        assert rel(st[k], g[f"step_{k}"]) < FP64_TOL, k
+
+
+def test_mm_step(ctx, golden):
+    g = golden("mm_nc1")
+    t, topo = _mm_topo(g)
+    na = g["pos"].size // 3
+    cnt, lst, _ = ctx.build_nlist_lj(g["pos"], g["h"], g["hi"], na, t["mol_id"], rc_list=RC_MM)
+    st = dict(pos=g["pos"].copy(), vel=g["vel"].copy(), F=g["F"].copy(), vir9=g["W"].copy(), h=g["h"].copy(),
+              hi=g["hi"].copy(), npt=g["npt0"].copy())
+    out = ctx.step_npt_mm(st, 0.1, topo, cnt, lst)
+    assert rel(out, g["step_out"]) < FP64_TOL
+    for k in ("pos", "vel", "F", "vir9", "h", "hi", "npt"):
+        assert rel(st[k], g[f"step_{k}"]) < FP64_TOL, k
+
+
+def test_geometry_helpers(ctx, oracle):
+    s = crystal.atomistic(1, jitter=0.3, seed=2)
+    h = s["h"].copy()
+    h[1] += 0.9
+    hi = ctx.mat_inv9(h)
+    assert np.array_equal(hi, oracle.mat_inv9(h))      # bitwise: IEEE division and no contraction
+    p = s["pos"] * 1.7 - 3.0
+    assert np.array_equal(ctx.apply_pbc(p, h, hi), oracle.apply_pbc(p, h, hi))
