@@ -233,8 +233,43 @@ extern "C" int fmd_nlist_rebo(fmd_ctx* ctx, const double* pos, const double* h, 
 
 namespace {
 
+// Every count in [0, cap] and every listed index in [0, n): caller-supplied
+// lists index device arrays, so they are checked before any launch.
+bool list_ok(fmd_ctx* ctx, const int* cnt, const int* list, int cap, int n, const char* what) {
+    for (int i = 0; i < n; i++) {
+        const int c = cnt[i];
+        if (c < 0 || c > cap) {
+            ctx->fail(FMD_ERR_ARG, std::string(what) + ": count out of range at row " + std::to_string(i));
+            return false;
+        }
+        const int* row = list + (size_t)i * cap;
+        for (int k = 0; k < c; k++)
+            if (row[k] < 0 || row[k] >= n) {
+                ctx->fail(FMD_ERR_ARG, std::string(what) + ": index out of range at row " + std::to_string(i));
+                return false;
+            }
+    }
+    return true;
+}
+
+bool index_ok(const int* a, int m, int n) {
+    for (int k = 0; k < m; k++)
+        if (a[k] < 0 || a[k] >= n) return false;
+    return true;
+}
+
+bool topo_index_ok(const fmd_mm_topology* t, int na) {
+    return index_ok(t->b_i0, t->nb, na) && index_ok(t->b_i1, t->nb, na) && index_ok(t->ang_i0, t->nang, na) &&
+           index_ok(t->ang_i1, t->nang, na) && index_ok(t->ang_i2, t->nang, na) &&
+           index_ok(t->dih_i0, t->ndih, na) && index_ok(t->dih_i1, t->ndih, na) &&
+           index_ok(t->dih_i2, t->ndih, na) && index_ok(t->dih_i3, t->ndih, na) &&
+           index_ok(t->imp_i0, t->nimp, na) && index_ok(t->imp_i1, t->nimp, na) &&
+           index_ok(t->imp_i2, t->nimp, na) && index_ok(t->imp_i3, t->nimp, na);
+}
+
 // Uploads a reference-layout list and its transpose for the LJ gather.
 int upload_half_list(fmd_ctx* ctx, const int* nlc, const int* nll, int cap, int na, StepArrays& a) {
+    if (!list_ok(ctx, nlc, nll, cap, na, "LJ list")) return FMD_ERR_ARG;
     int *dc, *dl, *ic, *il;
     int rc = up(ctx, S_CNT, nlc, na, &dc);
     if (!rc) rc = up(ctx, S_LIST, nll, (size_t)na * cap, &dl);
@@ -336,6 +371,7 @@ extern "C" int fmd_lj_rigid_forces(fmd_ctx* ctx, const double* pos, const double
     if (!pos || !qv || !body || !h || !hi || !nl_count || !nl_list || !Fv || !Tv || !Wm9 || !Ep || n < 1 ||
         natom < 1 || natom > 96 || max_neigh < 1)
         return ctx->fail(FMD_ERR_ARG, "fmd_lj_rigid_forces: bad argument");
+    if (!list_ok(ctx, nl_count, nl_list, max_neigh, n, "molecule list")) return FMD_ERR_ARG;
     StepArrays a;
     a.kind = FMD_SYS_RIGID; a.n = n; a.natom = natom; a.rmcut2 = rmcut2; a.precision = precision;
     double *dpos, *dq, *db, *dF, *dT;
@@ -383,6 +419,7 @@ static int atom_term(fmd_ctx* ctx, int term, int ff, const double* pos, const do
     double* part = a.part_f1;
     if (term == 0) {
         int *dc, *dl;
+        if (!list_ok(ctx, nlc, nll, max_neigh, na, "REBO list")) return FMD_ERR_ARG;
         rc = up(ctx, S_CNT2, nlc, na, &dc);
         if (!rc) rc = up(ctx, S_LIST2, nll, (size_t)na * max_neigh, &dl);
         if (rc) return rc;
@@ -446,6 +483,7 @@ int atom_setup(fmd_ctx* ctx, int kind, const double* pos, const double* h, const
 int airebo_lists(fmd_ctx* ctx, const int* nlc_r, const int* nll_r, const int* nlc_l, const int* nll_l, int na,
                  StepArrays& a) {
     int *dc, *dl;
+    if (!list_ok(ctx, nlc_r, nll_r, 12, na, "REBO list")) return FMD_ERR_ARG;
     int rc = up(ctx, S_CNT2, nlc_r, na, &dc);
     if (!rc) rc = up(ctx, S_LIST2, nll_r, (size_t)na * 12, &dl);
     if (rc) return rc;
@@ -481,7 +519,7 @@ extern "C" int fmd_mm_forces(fmd_ctx* ctx, const fmd_mm_topology* t, const doubl
                              const int* mol_id, int has_charge, int na, double* F, double* vir9, double* E7) {
     if (!ctx) return FMD_ERR_ARG;
     if (!topo_ok(t) || !pos || !h || !hi || !nlc || !nll || !F || !vir9 || !E7 || na < 1 ||
-        (has_charge && (!charge || !mol_id)))
+        (has_charge && (!charge || !mol_id)) || !topo_index_ok(t, na))
         return ctx->fail(FMD_ERR_ARG, "fmd_mm_forces: bad argument");
     StepArrays a;
     int rc = atom_setup(ctx, FMD_SYS_MM, pos, h, hi, nullptr, nullptr, na, a);
@@ -523,6 +561,7 @@ extern "C" int fmd_rigid_step(fmd_ctx* ctx, double* pos, double* vel, double* qv
     if (!pos || !vel || !qv || !omg || !Fv || !Tv || !Wm9 || !h || !hi || !body || !npt || !nl_count ||
         !nl_list || !out2 || n < 1 || natom < 1 || natom > 96 || max_neigh < 1)
         return ctx->fail(FMD_ERR_ARG, "fmd_rigid_step: bad argument");
+    if (!list_ok(ctx, nl_count, nl_list, max_neigh, n, "molecule list")) return FMD_ERR_ARG;
     StepArrays a;
     a.kind = FMD_SYS_RIGID; a.n = n; a.natom = natom; a.rmcut2 = rmcut2; a.Mmol = Mmol; a.I0 = I0;
     a.precision = precision;
@@ -596,7 +635,7 @@ extern "C" int fmd_mm_step(fmd_ctx* ctx, double* pos, double* vel, double* F, do
                            const double* charge, const int* mol_id, int has_charge, double* out8) {
     if (!ctx) return FMD_ERR_ARG;
     if (!pos || !vel || !F || !vir9 || !h || !hi || !npt || !topo_ok(t) || !nlc || !nll || !out8 || na < 1 ||
-        (has_charge && (!charge || !mol_id)))
+        (has_charge && (!charge || !mol_id)) || !topo_index_ok(t, na))
         return ctx->fail(FMD_ERR_ARG, "fmd_mm_step: bad argument");
     StepArrays a;
     int rc = atom_setup(ctx, FMD_SYS_MM, pos, h, hi, vir9, npt, na, a);

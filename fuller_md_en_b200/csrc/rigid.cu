@@ -152,16 +152,23 @@ k_rigid(const double* __restrict__ pos, const double* __restrict__ qv, const dou
                 for (int q = 0; q < 9; q++) acc[6 + q] += w[q];
                 acc[15] += e;
             } else {
-                const float mxf = (float)mx, myf = (float)my, mzf = (float)mz;
+                // The COM image (up to ~18 A) rounded to FP32 would carry a
+                // 1e-6 A error shared by all 3600 site pairs of the molecule
+                // pair; split it into hi + lo parts and add the small site
+                // difference first so each pair distance keeps ~1e-7 relative
+                // accuracy.
+                const float mxh = (float)mx, myh = (float)my, mzh = (float)mz;
+                const float mxl = (float)(mx - (double)mxh), myl = (float)(my - (double)myh),
+                            mzl = (float)(mz - (double)mzh);
                 const float rax = (float)ra.x, ray = (float)ra.y, raz = (float)ra.z;
                 const float sig2 = (float)rc.sig2, rcut2 = (float)rc.rcut2, c24 = (float)rc.c24,
                             c4 = (float)rc.c4, vsh = (float)rc.vshift;
-                float f0 = 0, f1 = 0, f2 = 0, w[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, e = 0;
+                float f0 = 0, f1 = 0, f2 = 0;
                 for (int b = 0; b < natom; b++) {
                     const Site<P> rb = sj[b];
-                    const float dx = (mxf + (float)rb.x) - rax;
-                    const float dy = (myf + (float)rb.y) - ray;
-                    const float dz = (mzf + (float)rb.z) - raz;
+                    const float dx = (mxh + ((float)rb.x - rax)) + mxl;
+                    const float dy = (myh + ((float)rb.y - ray)) + myl;
+                    const float dz = (mzh + ((float)rb.z - raz)) + mzl;
                     float r2 = dx * dx + dy * dy + dz * dz;
                     if (r2 < rcut2) {
                         r2 = fmaxf(r2, 0.25f);
@@ -169,10 +176,13 @@ k_rigid(const double* __restrict__ pos, const double* __restrict__ qv, const dou
                         const float fm = c24 * (2.0f * s12 - s6) * ri2;
                         const float fx = fm * dx, fy = fm * dy, fz = fm * dz;
                         f0 -= fx; f1 -= fy; f2 -= fz;
-                        e += c4 * (s12 - s6) - vsh;
-                        w[0] += dx * fx; w[1] += dx * fy; w[2] += dx * fz;
-                        w[3] += dy * fx; w[4] += dy * fy; w[5] += dy * fz;
-                        w[6] += dz * fx; w[7] += dz * fy; w[8] += dz * fz;
+                        // energy and virial: FP32 pair terms, FP64 sums, halved
+                        // for the symmetric list (LJ:339-341)
+                        const float hx = 0.5f * dx, hy = 0.5f * dy, hz = 0.5f * dz;
+                        acc[15] += (double)(0.5f * (c4 * (s12 - s6) - vsh));
+                        acc[6] += (double)(hx * fx); acc[7] += (double)(hx * fy); acc[8] += (double)(hx * fz);
+                        acc[9] += (double)(hy * fx); acc[10] += (double)(hy * fy); acc[11] += (double)(hy * fz);
+                        acc[12] += (double)(hz * fx); acc[13] += (double)(hz * fy); acc[14] += (double)(hz * fz);
                     }
                 }
                 const double rad[3] = {(double)ra.x, (double)ra.y, (double)ra.z};
@@ -180,9 +190,6 @@ k_rigid(const double* __restrict__ pos, const double* __restrict__ qv, const dou
                 acc[3] += rad[1] * (double)f2 - rad[2] * (double)f1;
                 acc[4] += rad[2] * (double)f0 - rad[0] * (double)f2;
                 acc[5] += rad[0] * (double)f1 - rad[1] * (double)f0;
-#pragma unroll
-                for (int q = 0; q < 9; q++) acc[6 + q] += 0.5 * (double)w[q];
-                acc[15] += 0.5 * (double)e;
             }
         }
         __syncthreads();

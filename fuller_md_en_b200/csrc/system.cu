@@ -307,6 +307,18 @@ extern "C" int fmd_system_create_mm(fmd_ctx* ctx, const fmd_run_params* p, int n
 }
 
 int fmd::System::upload_topology(const fmd_mm_topology* t) {
+    // Topology indices address device arrays: check them before any launch.
+    auto ok = [&](const int* a, int m) {
+        if (m > 0 && !a) return false;
+        for (int k = 0; k < m; k++)
+            if (a[k] < 0 || a[k] >= arr.n) return false;
+        return true;
+    };
+    if (t->nb < 0 || t->nang < 0 || t->ndih < 0 || t->nimp < 0 || !ok(t->b_i0, t->nb) || !ok(t->b_i1, t->nb) ||
+        !ok(t->ang_i0, t->nang) || !ok(t->ang_i1, t->nang) || !ok(t->ang_i2, t->nang) ||
+        !ok(t->dih_i0, t->ndih) || !ok(t->dih_i1, t->ndih) || !ok(t->dih_i2, t->ndih) || !ok(t->dih_i3, t->ndih) ||
+        !ok(t->imp_i0, t->nimp) || !ok(t->imp_i1, t->nimp) || !ok(t->imp_i2, t->nimp) || !ok(t->imp_i3, t->nimp))
+        return ctx->fail(FMD_ERR_ARG, "MM topology: index out of range");
     MMTopoDev d{};
     d.nb = t->nb; d.nang = t->nang; d.ndih = t->ndih; d.nimp = t->nimp;
     int *i0, *i1, *i2, *i3, *mult;
