@@ -73,6 +73,8 @@ _SIGS = {
                                     c_double, c_int, _dp, _dp, _dp, _dp]),
     "fmd_rebo_forces": (c_int, [c_void_p, _dp, _dp, _dp, _ip, _ip, c_int, c_int, _dp, _dp, _dp]),
     "fmd_lj_half_forces": (c_int, [c_void_p, c_int, _dp, _dp, _dp, _ip, _ip, c_int, c_int, _dp, _dp, _dp]),
+    "fmd_rebo_forces_noalloc": (c_int, [c_void_p, _dp, _dp, c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p,
+                                        c_void_p, c_void_p]),
     "fmd_airebo_forces": (c_int, [c_void_p, _dp, _dp, _dp, _ip, _ip, _ip, _ip, c_int, _dp, _dp, _dp]),
     "fmd_mm_forces": (c_int, [c_void_p, POINTER(MMTopology), _dp, _dp, _dp, _ip, _ip, _dp, _ip, c_int,
                               c_int, _dp, _dp, _dp]),

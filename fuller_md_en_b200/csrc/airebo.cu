@@ -282,6 +282,12 @@ cudaError_t rebo_launch(const double* pos, const double* hh, const int* cnt, con
     return cudaGetLastError();
 }
 
+cudaError_t rebo_launch_grid(const double* pos, const double* hh, const int* cnt, const int* list, int cap,
+                             int na, double* F, double* part, int nblocks, cudaStream_t st) {
+    k_rebo<<<nblocks, 128, 0, st>>>(pos, hh, cnt, list, cap, na, F, part);
+    return cudaGetLastError();
+}
+
 cudaError_t lj_gather_launch(int ff, const double* pos, const double* hh, const int* cnt, const int* list,
                              int cap, const int* in_cnt, const int* in_list, int in_cap, int na, double* F,
                              double* Facc, double* part, cudaStream_t st) {

@@ -57,6 +57,10 @@ constexpr int kNV = 10;                    // {E, W[9]} per block partial
 // REBO (a7): atomics into F, per-block {E, W9} partials in part[grid*kNV].
 cudaError_t rebo_launch(const double* pos, const double* hh, const int* cnt, const int* list,
                         int cap, int na, double* F, double* part, cudaStream_t st);
+// Same kernel on an explicit grid of `nblocks` blocks of 128 threads
+// (nblocks partial records).
+cudaError_t rebo_launch_grid(const double* pos, const double* hh, const int* cnt, const int* list,
+                             int cap, int na, double* F, double* part, int nblocks, cudaStream_t st);
 // Half-list LJ gather (a8, a14): F[i] = Facc[i] + LJ(i); Facc[i] zeroed
 // (Facc may alias F only if zero_acc == 0).  ff: FMD_FF_AIREBO / FMD_FF_MM.
 cudaError_t lj_gather_launch(int ff, const double* pos, const double* hh, const int* cnt,

@@ -106,6 +106,29 @@ int fmd_lj_rigid_forces(fmd_ctx *ctx, const double *pos, const double *qv, const
 int fmd_rebo_forces(fmd_ctx *ctx, const double *pos, const double *h, const double *hi,
                     const int *nlc, const int *nll, int max_neigh, int na,
                     double *F, double *vir9, double *E);
+/* No counterpart in the reference.  The REBO force of fmd_rebo_forces for
+ * callers that cannot allocate device memory: code inside a CUDA-graph
+ * capture owned by a framework, programs whose memory pool forbids side
+ * allocations, drivers that must not touch the allocator after start-up.
+ * It needs no fmd_ctx and calls no cudaMalloc/cudaFree or any allocating
+ * routine.  All arrays are DEVICE pointers except h and hi (9 doubles each,
+ * host): d_pos[3*na], the REBO list d_nlc[na], d_nll[na*max_neigh] (entries
+ * must be valid atom indices, as fmd_nlist_rebo produces them); d_F[3*na]
+ * and d_vir9[9] are ADDED into like compute_rebo (AI:275-421) does; *d_E
+ * receives the REBO energy.  Work is enqueued on `stream` (a cudaStream_t,
+ * NULL = default stream) and the call returns without synchronising.
+ * Scratch is a fixed file-scope device array (82 KB on every GPU that loads
+ * the library, held until exit) for the cell matrix and one partial record
+ * per 128 atoms: na is limited to 131,072; larger na returns
+ * FMD_ERR_CAPACITY and does nothing.  Every call shares that array and it
+ * keeps the last call's contents (each call rewrites all it reads), so calls
+ * that overlap on the GPU -- on different streams, or from several host
+ * threads -- race and must be serialised by the caller.  The first call on
+ * a device looks up the array's device address; make that first call before
+ * any stream capture. */
+int fmd_rebo_forces_noalloc(const double *d_pos, const double *h, const double *hi,
+                            const int *d_nlc, const int *d_nll, int max_neigh, int na,
+                            double *d_F, double *d_vir9, double *d_E, void *stream);
 /* compute_lj (AI:424-473) for ff=FMD_FF_AIREBO, MM LJ block (MM:711-764) for
  * ff=FMD_FF_MM: ADDS into F and vir9; *E = energy. */
 int fmd_lj_half_forces(fmd_ctx *ctx, int ff, const double *pos, const double *h, const double *hi,
