@@ -176,7 +176,7 @@ int list_call(fmd_ctx* ctx, int mode, const double* pos, const double* h, const 
     cudaMemsetAsync(dlist, 0, sizeof(int) * (size_t)n * cap, ctx->stream);
     cudaMemsetAsync(ddrop, 0, sizeof(int), ctx->stream);
     TmpCells tc;
-    if (cells_alloc(tc.cl, n, h, rc) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "cell allocation failed");
+    if (cells_alloc(tc.cl, n, h, rc, mode == LIST_INTRA ? 1 : 2) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "cell allocation failed");
     if (cells_build(tc.cl, dpos, n, hh, rc, ctx->d_err, ctx->stream) != cudaSuccess)
         return ctx->fail(FMD_ERR_CUDA, "cell build launch failed");
     const double rc2 = rc * rc;

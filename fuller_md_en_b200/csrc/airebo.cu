@@ -90,13 +90,14 @@ __device__ __forceinline__ void atomic_add3(double* F, int i, double x, double y
 }
 
 // Reference three-body forces on the neighbours of centre c (AI:361-419).
-__device__ void bo_three_body(double* __restrict__ F, const double* __restrict__ pos,
+// b = (1+gs)^-1/2 is passed in, so db/dgs = -1/2 (1+gs)^-3/2 = -b / (2 (1+gs)).
+__device__ __forceinline__ void bo_three_body(double* __restrict__ F, const double* __restrict__ pos,
                               const int* __restrict__ cnt, const int* __restrict__ list, int cap,
                               const double* h, const double* hi, int c, int skip, double bx, double by,
-                              double bz, double rb, double ux, double uy, double uz, double gs,
+                              double bz, double rb, double ux, double uy, double uz, double gs, double b,
                               double fcut, double va) {
     if (!(fabs(gs) > 1e-20 && va > 1e-20)) return;
-    const double dbp = -BO_DELTA * pow(1.0 + gs, -BO_DELTA - 1.0);
+    const double dbp = -BO_DELTA * b / (1.0 + gs);
     const double vh = 0.5 * fcut * va;
     const double coeff = -vh * dbp;
     const int m = cnt[c];
@@ -125,6 +126,11 @@ __device__ void bo_three_body(double* __restrict__ F, const double* __restrict__
     atomic_add3(F, c, fcx, fcy, fcz);
 }
 
+// Four threads per atom share its row (slots jn, jn+4, jn+8): a fullerene
+// atom has three bonds, so one bond per thread; this gives ~4x the
+// parallelism of one thread per atom for the latency-bound bond work.
+constexpr int kReboLanes = 4;
+
 __global__ void __launch_bounds__(128)
 k_rebo(const double* __restrict__ pos, const double* __restrict__ hh, const int* __restrict__ cnt,
        const int* __restrict__ list, int cap, int na, double* __restrict__ F, double* __restrict__ part) {
@@ -134,10 +140,13 @@ k_rebo(const double* __restrict__ pos, const double* __restrict__ hh, const int*
     double acc[kNV];
 #pragma unroll
     for (int k = 0; k < kNV; k++) acc[k] = 0.0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < na; i += gridDim.x * blockDim.x) {
+    const long long total = (long long)na * kReboLanes;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t / kReboLanes), lane = (int)(t % kReboLanes);
         const int m = cnt[i];
         double fix = 0.0, fiy = 0.0, fiz = 0.0;
-        for (int jn = 0; jn < m; jn++) {
+        for (int jn = lane; jn < m; jn += kReboLanes) {
             const int j = list[(size_t)i * cap + jn];
             if (j <= i) continue;
             double dx, dy, dz;
@@ -157,7 +166,8 @@ k_rebo(const double* __restrict__ pos, const double* __restrict__ hh, const int*
             const double ux = dx * rinv, uy = dy * rinv, uz = dz * rinv;
             const double gij = bo_sum(pos, cnt, list, cap, h, hi, i, j, dx, dy, dz, rij);
             const double gji = bo_sum(pos, cnt, list, cap, h, hi, j, i, -dx, -dy, -dz, rij);
-            const double bij = pow(1.0 + gij, -BO_DELTA), bji = pow(1.0 + gji, -BO_DELTA);
+            // (1+g)^-1/2 (AI:310, 323) as a reciprocal square root
+            const double bij = 1.0 / sqrt(1.0 + gij), bji = 1.0 / sqrt(1.0 + gji);
             const double bbar = 0.5 * (bij + bji);
             acc[0] += fcut * (vr - bbar * va);
             const double fpair = (dfcut * (vr - bbar * va) + fcut * (dvr - bbar * dva)) * rinv;
@@ -168,10 +178,11 @@ k_rebo(const double* __restrict__ pos, const double* __restrict__ hh, const int*
             for (int a = 0; a < 3; a++)
 #pragma unroll
                 for (int b = 0; b < 3; b++) acc[1 + a * 3 + b] -= d[a] * fpair * d[b];
-            bo_three_body(F, pos, cnt, list, cap, h, hi, i, j, dx, dy, dz, rij, ux, uy, uz, gij, fcut, va);
-            bo_three_body(F, pos, cnt, list, cap, h, hi, j, i, -dx, -dy, -dz, rij, -ux, -uy, -uz, gji, fcut, va);
+            bo_three_body(F, pos, cnt, list, cap, h, hi, i, j, dx, dy, dz, rij, ux, uy, uz, gij, bij, fcut, va);
+            bo_three_body(F, pos, cnt, list, cap, h, hi, j, i, -dx, -dy, -dz, rij, -ux, -uy, -uz, gji, bji, fcut,
+                          va);
         }
-        if (m > 0) atomic_add3(F, i, fix, fiy, fiz);
+        if (fix != 0.0 || fiy != 0.0 || fiz != 0.0) atomic_add3(F, i, fix, fiy, fiz);
     }
     block_sum_store<kNV>(acc, sm, part + (size_t)blockIdx.x * kNV);
 }
@@ -197,12 +208,28 @@ LJP lj_params(int ff) {
     return p;
 }
 
+// One component of the minimum image for a diagonal cell.  With zero
+// off-diagonals the reference's s = hi0*dx + hi1*dy + hi2*dz and
+// d = h0*s0 + h1*s1 + h2*s2 reduce exactly to these products (adding +-0
+// changes nothing), so this is bitwise the reference's mimg.
+__device__ __forceinline__ double mimg1(double d, double hii, double hii_inv) {
+    double s = __dmul_rn(hii_inv, d);
+    s = __dsub_rn(s, round(s));
+    return __dmul_rn(hii, s);
+}
+
 template <bool FULL_VIRIAL, bool COUNT>
 __device__ __forceinline__ void lj_pair(const double* __restrict__ pos, int j, double px, double py,
-                                        double pz, const double* h, const double* hi, const LJP& p,
+                                        double pz, const double* h, const double* hi, bool diag, const LJP& p,
                                         double& fx, double& fy, double& fz, double* acc) {
     double dx = __dsub_rn(pos[3 * j], px), dy = __dsub_rn(pos[3 * j + 1], py), dz = __dsub_rn(pos[3 * j + 2], pz);
-    mimg(dx, dy, dz, hi, h);
+    if (diag) {
+        dx = mimg1(dx, h[0], hi[0]);
+        dy = mimg1(dy, h[4], hi[4]);
+        dz = mimg1(dz, h[8], hi[8]);
+    } else {
+        mimg(dx, dy, dz, hi, h);
+    }
     double r2 = norm2_rn(dx, dy, dz);
     if (r2 > p.rc2) return;
     if (r2 < 0.25) r2 = 0.25;
@@ -226,7 +253,7 @@ __device__ __forceinline__ void lj_pair(const double* __restrict__ pos, int j, d
 }
 
 template <bool FULL_VIRIAL>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 3)
 k_lj_gather(const double* __restrict__ pos, const double* __restrict__ hh, const int* __restrict__ cnt,
             const int* __restrict__ list, int cap, const int* __restrict__ in_cnt,
             const int* __restrict__ in_list, int in_cap, int na, double* __restrict__ F,
@@ -235,6 +262,9 @@ k_lj_gather(const double* __restrict__ pos, const double* __restrict__ hh, const
     const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
     double h[9], hi[9];
     load_cell(hh, h, hi);
+    // Diagonal cell (FCC/BCC boxes under the diagonal barostat): uniform branch.
+    const bool diag = h[1] == 0.0 && h[2] == 0.0 && h[3] == 0.0 && h[5] == 0.0 && h[6] == 0.0 && h[7] == 0.0 &&
+                      hi[1] == 0.0 && hi[2] == 0.0 && hi[3] == 0.0 && hi[5] == 0.0 && hi[6] == 0.0 && hi[7] == 0.0;
     double acc[kNV];
 #pragma unroll
     for (int k = 0; k < kNV; k++) acc[k] = 0.0;
@@ -244,12 +274,12 @@ k_lj_gather(const double* __restrict__ pos, const double* __restrict__ hh, const
         const int m = cnt[i];
         const int* row = list + (size_t)i * cap;
         for (int k = lane; k < m; k += 32)
-            lj_pair<FULL_VIRIAL, true>(pos, row[k], px, py, pz, h, hi, p, fx, fy, fz, acc);
+            lj_pair<FULL_VIRIAL, true>(pos, row[k], px, py, pz, h, hi, diag, p, fx, fy, fz, acc);
         int mi = in_cnt[i];
         mi = mi < in_cap ? mi : in_cap;
         const int* irow = in_list + (size_t)i * in_cap;
         for (int k = lane; k < mi; k += 32)
-            lj_pair<FULL_VIRIAL, false>(pos, irow[k], px, py, pz, h, hi, p, fx, fy, fz, acc);
+            lj_pair<FULL_VIRIAL, false>(pos, irow[k], px, py, pz, h, hi, diag, p, fx, fy, fz, acc);
         fx = warp_sum(fx); fy = warp_sum(fy); fz = warp_sum(fz);
         if (lane == 0) {
             F[3 * i] = Facc[3 * i] + fx;

@@ -29,11 +29,13 @@ struct CellList {
     int cap_n[3] = {1, 1, 1};
     int cap_cells = 1;
     int n = 0;
+    int K = 1;                  // cells per cutoff length (cell width >= rc / K)
 };
 
 // Host helper: cells per axis for a cell matrix and list radius.
-void grid_dims_host(const double* h, double rc, int* n);
-cudaError_t cells_alloc(CellList& cl, int n, const double* h_host, double rc);
+void grid_dims_host(const double* h, double rc, int K, int* n);
+// K = 2 halves the candidate volume for large cutoffs; K = 1 suits small ones.
+cudaError_t cells_alloc(CellList& cl, int n, const double* h_host, double rc, int K = 1);
 void cells_free(CellList& cl);
 // hh = device pointer to {h[9], hi[9]}.  Bins pos[3*n] into cells.
 cudaError_t cells_build(CellList& cl, const double* pos, int n, const double* hh, double rc,

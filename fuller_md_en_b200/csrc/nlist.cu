@@ -25,7 +25,8 @@ namespace fmd {
 
 namespace {
 
-__host__ __device__ inline void grid_dims(const double* h, double rc, int* n, double* wmin) {
+// Cells per axis with cell width >= rc / K (K cells span the cutoff).
+__host__ __device__ inline void grid_dims(const double* h, double rc, int K, int* n, double* wmin) {
     // Columns of h are the lattice vectors; the perpendicular width along
     // vector a is V / |b x c|.
     const double c[3][3] = {{h[0], h[3], h[6]}, {h[1], h[4], h[7]}, {h[2], h[5], h[8]}};
@@ -40,25 +41,26 @@ __host__ __device__ inline void grid_dims(const double* h, double rc, int* n, do
         double x = u[1] * v[2] - u[2] * v[1], y = u[2] * v[0] - u[0] * v[2], z = u[0] * v[1] - u[1] * v[0];
         double w = V / sqrt(x * x + y * y + z * z);
         wm = w < wm ? w : wm;
-        int k = (int)floor(w / rcb);
+        int k = (int)floor(K * w / rcb);
         n[a] = k < 1 ? 1 : k;
     }
     *wmin = wm;
 }
 
-__global__ void k_grid(const double* __restrict__ hh, double rc, int c0, int c1, int c2, GridDev* g) {
+__global__ void k_grid(const double* __restrict__ hh, double rc, int K, int c0, int c1, int c2, GridDev* g) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     int n[3];
     double wmin;
-    grid_dims(hh, rc, n, &wmin);
+    grid_dims(hh, rc, K, n, &wmin);
     const int cap[3] = {c0, c1, c2};
     GridDev G;
     for (int a = 0; a < 3; a++) {
         // Fewer, wider cells are always correct, so clamp to the allocation.
         G.n[a] = n[a] < cap[a] ? n[a] : cap[a];
-        if (G.n[a] >= 3) { G.lo[a] = -1; G.span[a] = 3; }
-        else if (G.n[a] == 2) { G.lo[a] = 0; G.span[a] = 2; }
-        else { G.lo[a] = 0; G.span[a] = 1; }
+        // A pair within rc differs by at most K cells per axis; with fewer
+        // than 2K+1 cells the stencil is every cell of that axis, once.
+        if (G.n[a] >= 2 * K + 1) { G.lo[a] = -K; G.span[a] = 2 * K + 1; }
+        else { G.lo[a] = 0; G.span[a] = G.n[a]; }
     }
     G.ncell = G.n[0] * G.n[1] * G.n[2];
     G.prefilter = (wmin >= 2.0 * rc * (1.0 + 1e-5)) ? 1 : 0;
@@ -88,31 +90,31 @@ __global__ void k_bin(const double* __restrict__ pos, int n, const double* __res
     s4[i] = make_float4((float)s[0], (float)s[1], (float)s[2], 0.f);
 }
 
-// Exclusive scan of cell counts (one block; ncell is read on the device).
-__global__ void k_scan(const int* __restrict__ cell_count, const GridDev* __restrict__ g,
-                       int* __restrict__ cell_start) {
+// Exclusive scan of cell counts (one block of 1024 threads; ncell is read on
+// the device).  Each thread owns a contiguous run of cells, so there is a
+// single block-wide scan whatever ncell is.
+__global__ void __launch_bounds__(1024)
+k_scan(const int* __restrict__ cell_count, const GridDev* __restrict__ g, int* __restrict__ cell_start) {
     __shared__ int sm[1024];
-    __shared__ int carry;
     const int ncell = g->ncell;
-    if (threadIdx.x == 0) carry = 0;
+    const int per = (ncell + 1023) / 1024;
+    const int b0 = min(threadIdx.x * per, ncell), b1 = min(b0 + per, ncell);
+    int s = 0;
+    for (int c = b0; c < b1; c++) s += cell_count[c];
+    sm[threadIdx.x] = s;
     __syncthreads();
-    for (int base = 0; base < ncell; base += 1024) {
-        int idx = base + threadIdx.x;
-        int v = idx < ncell ? cell_count[idx] : 0;
-        sm[threadIdx.x] = v;
+    for (int o = 1; o < 1024; o <<= 1) {
+        const int t = threadIdx.x >= o ? sm[threadIdx.x - o] : 0;
         __syncthreads();
-        for (int o = 1; o < 1024; o <<= 1) {
-            int t = threadIdx.x >= o ? sm[threadIdx.x - o] : 0;
-            __syncthreads();
-            sm[threadIdx.x] += t;
-            __syncthreads();
-        }
-        if (idx < ncell) cell_start[idx] = carry + sm[threadIdx.x] - v;
-        __syncthreads();
-        if (threadIdx.x == 1023) carry += sm[1023];
+        sm[threadIdx.x] += t;
         __syncthreads();
     }
-    if (threadIdx.x == 0) cell_start[ncell] = carry;
+    int run = sm[threadIdx.x] - s;
+    for (int c = b0; c < b1; c++) {
+        cell_start[c] = run;
+        run += cell_count[c];
+    }
+    if (threadIdx.x == 1023) cell_start[ncell] = sm[1023];
 }
 
 __global__ void k_scatter(int n, const int* __restrict__ cell_of, const int* __restrict__ slot_of,
@@ -162,29 +164,43 @@ k_nlist(const GridDev* __restrict__ g, const int* __restrict__ cell_start,
         const int* __restrict__ mol_id, int n, const double* __restrict__ hh, double rc2, int cap,
         int words, int* __restrict__ cnt, int* __restrict__ list, int* __restrict__ dropped) {
     extern __shared__ unsigned bm_all[];
+    __shared__ double s_hh[18];
+    __shared__ GridDev G;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
     unsigned* bm = bm_all + (size_t)wib * words;
     for (int w = lane; w < words; w += 32) bm[w] = 0u;
-    __syncwarp();
-    double h[9], hi[9];
-#pragma unroll
-    for (int k = 0; k < 9; k++) { h[k] = hh[k]; hi[k] = hh[9 + k]; }
-    const GridDev G = *g;
+    if (threadIdx.x < 18) s_hh[threadIdx.x] = hh[threadIdx.x];
+    if (threadIdx.x == 0) G = *g;
+    __syncthreads();
+    const double* h = s_hh;
+    const double* hi = s_hh + 9;
+    // Diagonal cell: the reference's mimg reduces exactly to per-axis products.
+    const bool diag = h[1] == 0.0 && h[2] == 0.0 && h[3] == 0.0 && h[5] == 0.0 && h[6] == 0.0 && h[7] == 0.0 &&
+                      hi[1] == 0.0 && hi[2] == 0.0 && hi[3] == 0.0 && hi[5] == 0.0 && hi[6] == 0.0 && hi[7] == 0.0;
     for (int i = blockIdx.x * wpb + wib; i < n; i += gridDim.x * wpb) {
         const double px = pos[3 * i], py = pos[3 * i + 1], pz = pos[3 * i + 2];
         const float4 si = s4[i];
         const int mi = (MODE != LIST_SYM) ? mol_id[i] : 0;
         const int ci = cell_of[i];
-        const int cz = ci % G.n[2], cy = (ci / G.n[2]) % G.n[1], cx = ci / (G.n[1] * G.n[2]);
+        const int n1 = G.n[1], n2 = G.n[2];
+        const int cz = ci % n2, cy = (ci / n2) % n1, cx = ci / (n1 * n2);
         int jmin = INT_MAX, jmax = -1, tot = 0;
         for (int a = 0; a < G.span[0]; a++) {
             const int x = wrapc(cx + G.lo[0] + a, G.n[0]);
             for (int b = 0; b < G.span[1]; b++) {
-                const int y = wrapc(cy + G.lo[1] + b, G.n[1]);
-                for (int c = 0; c < G.span[2]; c++) {
-                    const int z = wrapc(cz + G.lo[2] + c, G.n[2]);
-                    const int cell = (x * G.n[1] + y) * G.n[2] + z;
-                    const int beg = cell_start[cell], end = cell_start[cell + 1];
+                const int y = wrapc(cy + G.lo[1] + b, n1);
+                // The z-run of stencil cells is contiguous in cell order: one
+                // candidate range, or two when it wraps around the box.
+                const int base = (x * n1 + y) * n2;
+                int z0 = cz + G.lo[2];
+                z0 += (z0 < 0) ? n2 : 0;
+                const int zlen = G.span[2];
+                const int first_len = (z0 + zlen <= n2) ? zlen : n2 - z0;
+                for (int part = 0; part < 2; part++) {
+                    const int zs = part == 0 ? z0 : 0;
+                    const int zl = part == 0 ? first_len : zlen - first_len;
+                    if (zl <= 0) continue;
+                    const int beg = cell_start[base + zs], end = cell_start[base + zs + zl];
                     for (int k = beg + lane; k < end; k += 32) {
                         const int j = cell_atoms[k];
                         bool ok = (MODE == LIST_HALF) ? (j > i) : (j != i);
@@ -204,7 +220,15 @@ k_nlist(const GridDev* __restrict__ g, const int* __restrict__ cell_start,
                         if (ok) {
                             double dx = __dsub_rn(pos[3 * j], px), dy = __dsub_rn(pos[3 * j + 1], py),
                                    dz = __dsub_rn(pos[3 * j + 2], pz);
-                            mimg(dx, dy, dz, hi, h);
+                            if (diag) {
+                                double s0 = __dmul_rn(hi[0], dx), s1 = __dmul_rn(hi[4], dy), s2 = __dmul_rn(hi[8], dz);
+                                s0 = __dsub_rn(s0, round(s0));
+                                s1 = __dsub_rn(s1, round(s1));
+                                s2 = __dsub_rn(s2, round(s2));
+                                dx = __dmul_rn(h[0], s0); dy = __dmul_rn(h[4], s1); dz = __dmul_rn(h[8], s2);
+                            } else {
+                                mimg(dx, dy, dz, hi, h);
+                            }
                             ok = norm2_rn(dx, dy, dz) < rc2;
                         }
                         if (ok) {
@@ -296,14 +320,15 @@ __global__ void k_inv9(double* hh) {
 
 }  // namespace
 
-void grid_dims_host(const double* h, double rc, int* n) {
+void grid_dims_host(const double* h, double rc, int K, int* n) {
     double wmin;
-    grid_dims(h, rc, n, &wmin);
+    grid_dims(h, rc, K, n, &wmin);
 }
 
-cudaError_t cells_alloc(CellList& cl, int n, const double* h_host, double rc) {
+cudaError_t cells_alloc(CellList& cl, int n, const double* h_host, double rc, int K) {
     int nd[3];
-    grid_dims_host(h_host, rc, nd);
+    cl.K = K;
+    grid_dims_host(h_host, rc, K, nd);
     cl.cap_cells = 1;
     for (int a = 0; a < 3; a++) {
         // Room for the box to grow to twice its width before cells get wider.
@@ -332,7 +357,7 @@ void cells_free(CellList& cl) {
 cudaError_t cells_build(CellList& cl, const double* pos, int n, const double* hh, double rc,
                         DevErr* err, cudaStream_t st) {
     (void)err;
-    k_grid<<<1, 32, 0, st>>>(hh, rc, cl.cap_n[0], cl.cap_n[1], cl.cap_n[2], cl.grid);
+    k_grid<<<1, 32, 0, st>>>(hh, rc, cl.K, cl.cap_n[0], cl.cap_n[1], cl.cap_n[2], cl.grid);
     cudaMemsetAsync(cl.cell_count, 0, sizeof(int) * cl.cap_cells, st);
     if (n > 0) {
         k_bin<<<(n + 255) / 256, 256, 0, st>>>(pos, n, hh, cl.grid, cl.cell_count, cl.cell_of, cl.slot_of, cl.s4);

@@ -209,65 +209,67 @@ __global__ void __launch_bounds__(kPB) k_rescale(StepArrays a) {
     block_sum_store<2>(acc, sm, a.part_ke + 2 * blockIdx.x);
 }
 
-// Fixed-order sum of nblk records of width nv, field k, by a 256-thread block.
-__device__ double block_reduce_field(const double* part, int nblk, int nv, int k, double* sm) {
-    double v[1] = {0.0};
-    for (int b = threadIdx.x; b < nblk; b += blockDim.x) v[0] += part[(size_t)b * nv + k];
-    double out[1];
-    block_sum_store<1>(v, sm, out);
-    __shared__ double bc;
-    if (threadIdx.x == 0) bc = out[0];
-    __syncthreads();
-    const double r = bc;
-    __syncthreads();
-    return r;
+// One pass over every partial array: each thread sums its strided records
+// (fixed order), then one CTA reduction for all fields.  Layout of t[]:
+// [0,10) part_f1 fields, [10,20) part_f2 fields, [20] part_f3, [21,23) kinetic.
+constexpr int kRedFields = 23;
+
+__device__ void reduce_all(const StepArrays& a, int nblk_f1, int nblk_ke, bool forces, bool kinetic,
+                           double* sm, double (&t)[kRedFields]) {
+    double acc[kRedFields];
+#pragma unroll
+    for (int k = 0; k < kRedFields; k++) acc[k] = 0.0;
+    if (forces) {
+        const int nv1 = a.kind == FMD_SYS_MM ? kMMNV : kNV;
+        for (int b = threadIdx.x; b < nblk_f1; b += blockDim.x)
+            for (int k = 0; k < nv1; k++) acc[k] += a.part_f1[(size_t)b * nv1 + k];
+        if (a.kind != FMD_SYS_RIGID)
+            for (int b = threadIdx.x; b < kForceBlocks; b += blockDim.x) {
+#pragma unroll
+                for (int k = 0; k < kNV; k++) acc[10 + k] += a.part_f2[(size_t)b * kNV + k];
+                if (a.kind == FMD_SYS_MM && a.has_charge) acc[20] += a.part_f3[b];
+            }
+    }
+    if (kinetic)
+        for (int b = threadIdx.x; b < nblk_ke; b += blockDim.x) {
+            acc[21] += a.part_ke[2 * b];
+            acc[22] += a.part_ke[2 * b + 1];
+        }
+    block_sum_store<kRedFields>(acc, sm, t);   // result valid in thread 0
 }
 
-// Writes the kinetic energies from the kinetic partials into S.
-__device__ void kinetic_from_partials(const StepArrays& a, int nblk, double* sm) {
-    const double s0 = block_reduce_field(a.part_ke, nblk, 2, 0, sm);
-    const double s1 = block_reduce_field(a.part_ke, nblk, 2, 1, sm);
-    if (threadIdx.x == 0) {
-        SysScal* S = a.S;
-        if (a.kind == FMD_SYS_RIGID) {
-            S->kt = 0.5 * a.Mmol * s0 / kConv;     // LJ:411
-            S->kr = 0.5 * a.I0 * s1 / kConv;       // LJ:420
-            S->KE = S->kt + S->kr;
-        } else {
-            S->KE = 0.5 * s0 / kConv;              // AI:506, MM:799
-        }
+// Thread 0: kinetic energies from the reduced sums.
+__device__ void kinetic_from_sums(const StepArrays& a, const double (&t)[kRedFields]) {
+    SysScal* S = a.S;
+    if (a.kind == FMD_SYS_RIGID) {
+        S->kt = 0.5 * a.Mmol * t[21] / kConv;     // LJ:411
+        S->kr = 0.5 * a.I0 * t[22] / kConv;       // LJ:420
+        S->KE = S->kt + S->kr;
+    } else {
+        S->KE = 0.5 * t[21] / kConv;              // AI:506, MM:799
     }
 }
 
-// Force partials -> S->W9, S->E.
-__device__ void forces_from_partials(const StepArrays& a, int nblk_f1, double* sm) {
+// Thread 0: virial and energies (program grouping) from the reduced sums.
+__device__ void forces_from_sums(const StepArrays& a, const double (&t)[kRedFields]) {
     SysScal* S = a.S;
     double e[8] = {0, 0, 0, 0, 0, 0, 0, 0}, w[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     if (a.kind == FMD_SYS_RIGID) {
-        e[0] = block_reduce_field(a.part_f1, nblk_f1, kNV, 0, sm);
-        for (int q = 0; q < 9; q++) w[q] = block_reduce_field(a.part_f1, nblk_f1, kNV, 1 + q, sm);
+        e[0] = t[0];
+        for (int q = 0; q < 9; q++) w[q] = t[1 + q];
     } else if (a.kind == FMD_SYS_AIREBO) {
-        const double er = block_reduce_field(a.part_f1, kForceBlocks, kNV, 0, sm);
-        const double el = block_reduce_field(a.part_f2, kForceBlocks, kNV, 0, sm);
-        for (int q = 0; q < 9; q++)
-            w[q] = block_reduce_field(a.part_f1, kForceBlocks, kNV, 1 + q, sm) +
-                   block_reduce_field(a.part_f2, kForceBlocks, kNV, 1 + q, sm);
-        e[0] = er + el; e[1] = er; e[2] = el;
+        e[1] = t[0]; e[2] = t[10]; e[0] = e[1] + e[2];
+        for (int q = 0; q < 9; q++) w[q] = t[1 + q] + t[11 + q];
     } else {
-        for (int q = 0; q < 4; q++) e[q] = block_reduce_field(a.part_f1, kForceBlocks, kMMNV, q, sm);
-        e[4] = block_reduce_field(a.part_f2, kForceBlocks, kNV, 0, sm);
-        e[5] = a.has_charge ? block_reduce_field(a.part_f3, kForceBlocks, 1, 0, sm) : 0.0;
+        for (int q = 0; q < 4; q++) e[q] = t[q];
+        e[4] = t[10];
+        e[5] = a.has_charge ? t[20] : 0.0;
         e[6] = e[0] + e[1] + e[2] + e[3] + e[4] + e[5];
         const int d[3] = {0, 4, 8};
-        for (int q = 0; q < 3; q++)
-            w[d[q]] = block_reduce_field(a.part_f1, kForceBlocks, kMMNV, 4 + q, sm) +
-                      block_reduce_field(a.part_f2, kForceBlocks, kNV, 1 + d[q], sm);
+        for (int q = 0; q < 3; q++) w[d[q]] = t[4 + q] + t[11 + d[q]];
     }
-    if (threadIdx.x == 0) {
-        for (int q = 0; q < 9; q++) S->W9[q] = w[q];
-        for (int q = 0; q < 8; q++) S->E[q] = e[q];
-    }
-    __syncthreads();
+    for (int q = 0; q < 9; q++) S->W9[q] = w[q];
+    for (int q = 0; q < 8; q++) S->E[q] = e[q];
 }
 
 // Observables, averages and the monitor record (LJ:874-897, AI:896-912, MM:1215-1236).
@@ -295,10 +297,12 @@ __device__ void record(SysScal* S, int kind, const StepParams& p) {
 }
 
 __global__ void __launch_bounds__(256) k_end(StepArrays a, StepParams p, int nblk_f1, int nblk_ke) {
-    __shared__ double sm[32];
-    forces_from_partials(a, nblk_f1, sm);
-    kinetic_from_partials(a, nblk_ke, sm);
+    __shared__ double sm[32 * kRedFields];
+    double t[kRedFields];
+    reduce_all(a, nblk_f1, nblk_ke, true, true, sm, t);
     if (threadIdx.x != 0) return;
+    forces_from_sums(a, t);
+    kinetic_from_sums(a, t);
     SysScal* S = a.S;
     const double hdt = 0.5 * p.dt;
     const bool rigid = a.kind == FMD_SYS_RIGID;
@@ -322,12 +326,14 @@ __global__ void __launch_bounds__(256) k_end(StepArrays a, StepParams p, int nbl
 }
 
 __global__ void __launch_bounds__(256) k_rescale_end(StepArrays a, StepParams p, int nblk_ke) {
-    __shared__ double sm[32];
+    __shared__ double sm[32 * kRedFields];
     SysScal* S = a.S;
     const bool doit = S->do_rescale != 0;
-    if (doit) kinetic_from_partials(a, nblk_ke, sm);
+    double t[kRedFields];
+    if (doit) reduce_all(a, 0, nblk_ke, false, true, sm, t);
     if (threadIdx.x != 0) return;
     if (doit) {
+        kinetic_from_sums(a, t);
         S->Tn = inst_T(S->KE, S->npt.Nf);
         S->npt.xi = 0;
         if (S->gstep <= p.coldstart)
@@ -337,13 +343,17 @@ __global__ void __launch_bounds__(256) k_rescale_end(StepArrays a, StepParams p,
 }
 
 __global__ void __launch_bounds__(256) k_ke_final(StepArrays a, int nblk_ke) {
-    __shared__ double sm[32];
-    kinetic_from_partials(a, nblk_ke, sm);
+    __shared__ double sm[32 * kRedFields];
+    double t[kRedFields];
+    reduce_all(a, 0, nblk_ke, false, true, sm, t);
+    if (threadIdx.x == 0) kinetic_from_sums(a, t);
 }
 
 __global__ void __launch_bounds__(256) k_force_final(StepArrays a, int nblk_f1) {
-    __shared__ double sm[32];
-    forces_from_partials(a, nblk_f1, sm);
+    __shared__ double sm[32 * kRedFields];
+    double t[kRedFields];
+    reduce_all(a, nblk_f1, 0, true, false, sm, t);
+    if (threadIdx.x == 0) forces_from_sums(a, t);
 }
 
 }  // namespace

@@ -76,7 +76,7 @@ int System::alloc_lists(double rc_list_a, int cap_a_, double rc_list_b, int cap_
         return ctx->fail(FMD_ERR_CUDA, "list allocation failed");
     cudaMemsetAsync(lst, 0, sizeof(int) * (size_t)n * cap_a_, ctx->stream);
     arr.cnt_a = cnt; arr.list_a = lst;
-    if (cells_alloc(cells_a, n, h0, rc_a) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "cell allocation failed");
+    if (cells_alloc(cells_a, n, h0, rc_a, 2) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "cell allocation failed");
     if (cap_b_ > 0) {
         rc_b = rc_list_b; rc2_b = rc_b * rc_b; arr.cap_b = cap_b_;
         if (alloc(&cnt, n, (const int*)nullptr) || alloc(&lst, (size_t)n * cap_b_, (const int*)nullptr))
@@ -133,6 +133,30 @@ int System::init() {
     int rc = ctx->sync_check("system init");
     if (rc != FMD_OK) return rc;
     initialized = true;
+    // Capture the four step variants now, so no host-side capture ever sits
+    // between two steps of a run.
+    if (p.use_graphs)
+        for (int r = 0; r < 2; r++)
+            for (int ph = 0; ph < 2; ph++)
+                if ((rc = capture(r != 0, ph != 0)) != FMD_OK) return rc;
+    return FMD_OK;
+}
+
+int System::capture(bool rebuild, bool phase) {
+    cudaGraphExec_t& ge = graphs[rebuild ? 1 : 0][phase ? 1 : 0];
+    if (ge) return FMD_OK;
+    cudaStream_t st = ctx->stream;
+    cudaGraph_t graph;
+    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return ctx->fail(FMD_ERR_CUDA, "graph capture failed to start");
+    cudaError_t e = enqueue_variant(rebuild, phase, st);
+    cudaError_t e2 = cudaStreamEndCapture(st, &graph);
+    if (e != cudaSuccess || e2 != cudaSuccess)
+        return ctx->fail(FMD_ERR_CUDA, std::string("graph capture failed: ") +
+                                           cudaGetErrorString(e != cudaSuccess ? e : e2));
+    e = cudaGraphInstantiate(&ge, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, cudaGetErrorString(e));
     return FMD_OK;
 }
 
@@ -167,21 +191,10 @@ int System::enqueue(int first, int last) {
     for (int g = first; g <= last; g++) {
         if (p.use_graphs) {
             const int r = (g % p.nlup) == 0, ph = g <= p.coldstart + p.warmup;
-            cudaGraphExec_t& ge = graphs[r][ph];
-            if (!ge) {
-                cudaGraph_t graph;
-                if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
-                    return ctx->fail(FMD_ERR_CUDA, "graph capture failed to start");
-                cudaError_t e = enqueue_one(g, st);
-                cudaError_t e2 = cudaStreamEndCapture(st, &graph);
-                if (e != cudaSuccess || e2 != cudaSuccess)
-                    return ctx->fail(FMD_ERR_CUDA, std::string("graph capture failed: ") +
-                                                       cudaGetErrorString(e != cudaSuccess ? e : e2));
-                e = cudaGraphInstantiate(&ge, graph, 0);
-                cudaGraphDestroy(graph);
-                if (e != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, cudaGetErrorString(e));
-            }
-            if (cudaGraphLaunch(ge, st) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "graph launch failed");
+            int rc = capture(r != 0, ph != 0);
+            if (rc != FMD_OK) return rc;
+            if (cudaGraphLaunch(graphs[r][ph], st) != cudaSuccess)
+                return ctx->fail(FMD_ERR_CUDA, "graph launch failed");
         } else {
             if (enqueue_one(g, st) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "step launch failed");
         }

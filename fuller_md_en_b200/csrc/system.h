@@ -28,6 +28,7 @@ struct System {
     cudaError_t enqueue_variant(bool rebuild, bool phase, cudaStream_t st);
     cudaError_t enqueue_one(int g, cudaStream_t st);
     int init();
+    int capture(bool rebuild, bool phase);
     int run(int first, int last, fmd_obs* obs);
     int enqueue(int first, int last);
     int nonfinite_check();
