@@ -64,6 +64,7 @@ _SIGS = {
     "fmd_ctx_synchronize": (c_int, [c_void_p]),
     "fmd_ctx_last_error": (c_char_p, [c_void_p]),
     "fmd_status_string": (c_char_p, [c_int]),
+    "fmd_device_info": (c_int, [c_int, c_char_p, c_int, POINTER(c_double)]),
     "fmd_mat_inv9": (c_int, [c_void_p, _dp, _dp]),
     "fmd_apply_pbc": (c_int, [c_void_p, _dp, _dp, _dp, c_int]),
     "fmd_nlist_rigid": (c_int, [c_void_p, _dp, _dp, _dp, c_int, c_double, c_int, _ip, _ip, _ip]),

@@ -58,6 +58,17 @@ extern "C" const char* fmd_status_string(int code) {
     }
 }
 
+extern "C" int fmd_device_info(int device, char* name, int name_cap, double* total_gib) {
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) {
+        cudaGetLastError();
+        return FMD_ERR_CUDA;
+    }
+    if (name && name_cap > 0) snprintf(name, name_cap, "%s", prop.name);
+    if (total_gib) *total_gib = prop.totalGlobalMem / 1024.0 / 1024.0 / 1024.0;
+    return FMD_OK;
+}
+
 extern "C" int fmd_ctx_create(fmd_ctx** out, int device) {
     if (!out) return FMD_ERR_ARG;
     *out = nullptr;

@@ -74,6 +74,9 @@ void *fmd_ctx_get_stream(fmd_ctx *ctx);
 int fmd_ctx_synchronize(fmd_ctx *ctx);
 const char *fmd_ctx_last_error(const fmd_ctx *ctx);
 const char *fmd_status_string(int code);
+/* Device name and total memory in GiB (the drivers' banner; replaces the
+ * OpenACC device queries acc_get_num_devices/acc_get_property, LJ:726-739). */
+int fmd_device_info(int device, char *name, int name_cap, double *total_gib);
 
 /* ------------------------------------------------------- host-pointer kernels */
 /* mat_inv9 (LJ:120-124), evaluated on the device. */

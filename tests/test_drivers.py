@@ -1,0 +1,343 @@
+"""The drop-in programs (fuller_*_gpu) against the reference programs.
+
+The reference programs are built from their own sources into
+oracle/_ref/bin (serial and OpenMP builds, exactly as the reference's build
+script compiles them) and run here on the CPU as the checker.  Both sides
+read the same fullerene library, written by ``write_library`` from this
+package's own C60 geometry in the .cc1 layout of
+FullereneLib/C60-76/C60-Ih.cc1 (count line, then "C idx x y z flag nbrs...").
+
+CPU tests: help text, banners, topology lines and the restart reader (our
+driver reads a restart file the reference wrote).  GPU tests: monitor and
+average lines of whole runs, OVITO frames, restart files read back by the
+reference, abort.md / stop.md control.
+"""
+from __future__ import annotations
+
+import os
+import re
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from fuller_md_en_b200 import crystal
+
+ROOT = Path(__file__).resolve().parents[1]
+BIN = ROOT / "fuller_md_en_b200" / "_bin"
+REFBIN = ROOT / "oracle" / "_ref" / "bin"
+
+OURS = {"lj": "fuller_LJ_npt_md_gpu", "ai": "fuller_airebo_npt_md_gpu", "mm": "fuller_LJ_npt_mmmd_gpu",
+        "core": "fuller_LJ_core_gpu"}
+REF = {"lj": "fuller_LJ_npt_md", "ai": "fuller_airebo_npt_md", "mm": "fuller_LJ_npt_mmmd", "core": "fuller_LJ_core"}
+
+
+def ours(prog: str) -> Path:
+    p = BIN / OURS[prog]
+    if not p.exists():
+        pytest.fail(f"{p} is not built (python -m fuller_md_en_b200.build)")
+    return p
+
+
+def ref(prog: str, omp: bool = False) -> Path:
+    p = REFBIN / f"{REF[prog]}_{'omp' if omp else 'serial'}"
+    if not p.exists():
+        pytest.skip(f"reference program {p.name} not built (make -C oracle ref)")
+    return p
+
+
+def write_library(root: Path) -> Path:
+    """FullereneLib-shaped directory holding C60-Ih.cc1 from crystal.c60_ih()."""
+    coords = crystal.c60_ih()
+    bonds = crystal.bonds_from_geometry(coords)
+    nbr = [[] for _ in range(len(coords))]
+    for i, j in bonds:
+        nbr[i].append(j + 1)
+        nbr[j].append(i + 1)
+    d = root / "FullereneLib" / "C60-76"
+    d.mkdir(parents=True, exist_ok=True)
+    lines = [f" {len(coords)}"]
+    for i, (x, y, z) in enumerate(coords):
+        lines.append(f"  C {i + 1:4d} {x:11.6f} {y:11.6f} {z:11.6f}    2" + "".join(f" {b:3d}" for b in nbr[i]))
+    (d / "C60-Ih.cc1").write_text("\n".join(lines) + "\n")
+    return root / "FullereneLib"
+
+
+def run(exe: Path, args: list[str], cwd: Path, timeout: int = 600, env: dict | None = None):
+    e = dict(os.environ)
+    e.setdefault("OMP_NUM_THREADS", str(min(16, os.cpu_count() or 1)))
+    if env:
+        e.update(env)
+    return subprocess.run([str(exe), *args], cwd=cwd, capture_output=True, text=True, timeout=timeout, env=e)
+
+
+@pytest.fixture()
+def work(tmp_path):
+    lib = write_library(tmp_path)
+    a = tmp_path / "ours"
+    b = tmp_path / "ref"
+    a.mkdir()
+    b.mkdir()
+    return {"lib": str(lib), "ours": a, "ref": b}
+
+
+_MODE = re.compile(r"GPU|OpenMP|OpenACC|Serial|CUDA|threads|Active device|GPU devices")
+
+
+def banner(text: str) -> list[str]:
+    """Lines up to the blank line after the banner's closing rule, without
+    the lines that name the build mode or device."""
+    out = []
+    for ln in text.splitlines():
+        if ln.strip() == "" and out and out[-1].startswith("===="):
+            break
+        if not _MODE.search(ln):
+            out.append(ln)
+    return out
+
+
+# ---------------------------------------------------------------- CPU tests
+@pytest.mark.parametrize("prog", ["lj", "ai", "mm"])
+def test_help_matches_reference(prog, work):
+    a = run(ours(prog), ["--help"], work["ours"])
+    b = run(ref(prog), ["--help"], work["ref"])
+    assert a.returncode == 0 and b.returncode == 0
+    assert a.stdout == b.stdout
+
+
+@pytest.mark.parametrize("prog,args", [
+    ("lj", ["--cell=2", "--crystal=hcp", "--temp=350"]),
+    ("ai", ["--cell=1", "--pres=0.5", "--dt=0.25"]),
+    ("mm", ["--cell=1", "--crystal=bcc", "--ff_kb=500"]),
+])
+def test_banner_matches_reference(prog, args, work):
+    args = args + ["--step=4", "--mon=2", f"--libdir={work['lib']}"]
+    a = run(ours(prog), args, work["ours"])
+    b = run(ref(prog), args, work["ref"])
+    assert b.returncode == 0, b.stderr
+    ba, bb = banner(a.stdout), banner(b.stdout)
+    assert len(bb) > 5
+    assert ba == bb
+
+
+def test_core_banner(work):
+    # The reference core program always runs its 1000 steps, so its banner is
+    # compared in the GPU run test; here the lines the program fixes.
+    a = run(ours("core"), ["--cell=2"], work["ours"])
+    lines = banner(a.stdout)
+    assert "  FCC cell        : 2x2x2  N=32 molecules" in lines
+    assert "  a0=14.17 A  T=300 K  P=0.0 GPa  dt=1.0 fs  steps=1000" in lines
+    assert "  MAX_NEIGH=80  VECTOR_LENGTH=128" in lines
+
+
+@pytest.mark.parametrize("prog", ["lj", "ai", "mm"])
+def test_unknown_fullerene_and_missing_library(prog, work):
+    a = run(ours(prog), ["--fullerene=C99", f"--libdir={work['lib']}"], work["ours"])
+    b = run(ref(prog), ["--fullerene=C99", f"--libdir={work['lib']}"], work["ref"])
+    assert a.returncode == b.returncode != 0
+    assert a.stderr.strip() == b.stderr.strip()
+    a = run(ours(prog), ["--fullerene=C70", f"--libdir={work['lib']}"], work["ours"])
+    b = run(ref(prog), ["--fullerene=C70", f"--libdir={work['lib']}"], work["ref"])
+    assert a.returncode == b.returncode != 0
+    assert a.stderr.strip() == b.stderr.strip()
+
+
+def test_core_rejects_bad_cell(work):
+    a = run(ours("core"), ["9"], work["ours"])
+    b = run(ref("core"), ["9"], work["ref"])
+    assert a.returncode == b.returncode == 1
+    assert a.stdout == b.stdout
+
+
+@pytest.mark.parametrize("prog,tag,unit", [("lj", "restart_LJ_serial", "mols"),
+                                           ("ai", "restart_airebo_serial", "atoms"),
+                                           ("mm", "restart_mmmd_serial", "atoms")])
+def test_restart_reader_reads_reference_file(prog, tag, unit, work):
+    base = ["--cell=1", "--step=4", "--mon=2", f"--libdir={work['lib']}"]
+    b = run(ref(prog), base + ["--restart=2"], work["ref"])
+    assert b.returncode == 0, b.stderr
+    files = sorted(work["ref"].glob("restart_*.rst"))
+    assert files, b.stdout
+    rst = files[0]
+    a = run(ours(prog), base + [f"--resfile={rst}"], work["ours"])
+    c = run(ref(prog), base + [f"--resfile={rst}"], work["ref"])
+    la = [ln for ln in a.stdout.splitlines() if "Restart" in ln]
+    lc = [ln for ln in c.stdout.splitlines() if "Restart" in ln]
+    assert len(lc) == 2 and lc[0].endswith(f"{unit})")
+    assert la == lc
+
+
+# ---------------------------------------------------------------- GPU tests
+_NUM = re.compile(r"^-?\d+(\.\d*)?([eE][-+]?\d+)?$")
+
+
+def monitor_rows(text: str) -> list[list[str]]:
+    rows = []
+    for ln in text.splitlines():
+        tok = ln.split()
+        if len(tok) >= 5 and tok[0].isdigit() and all(_NUM.match(t) or t in ("COLD", "WARM", "PROD") for t in tok):
+            rows.append(tok)
+    return rows
+
+
+def averages(text: str) -> dict[str, float]:
+    for ln in text.splitlines():
+        if "Averages (" in ln or ln.startswith("Avg("):
+            out = {"n": float(re.search(r"\((\d+)\)", ln).group(1))}
+            for k, v in re.findall(r"(\w+)=(-?[\d.]+)", ln):
+                out[k] = float(v)
+            return out
+    return {}
+
+
+def close_tok(x: str, y: str, rel: float) -> bool:
+    if not _NUM.match(x):
+        return x == y
+    dec = len(x.split(".")[1]) if "." in x else 0
+    a, b = float(x), float(y)
+    return abs(a - b) <= 1.01 * 10.0 ** (-dec) + rel * abs(b)
+
+
+def assert_rows_match(ra, rb, skip_last_col=True, rel=1e-6):
+    assert len(ra) == len(rb) and ra, (ra, rb)
+    for x, y in zip(ra, rb):
+        n = len(y) - (1 if skip_last_col else 0)    # last column: wall time
+        assert len(x) == len(y)
+        for i in range(n):
+            assert close_tok(x[i], y[i], rel), (x, y, i)
+
+
+def assert_avg_match(a, b, rel=1e-6):
+    assert a and a.keys() == b.keys(), (a, b)
+    for k in b:
+        assert abs(a[k] - b[k]) <= 1.01e-4 + rel * abs(b[k]) if k != "n" else a[k] == b[k], (k, a, b)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prog,args", [
+    ("ai", ["--cell=1", "--step=20", "--mon=5"]),
+    ("ai", ["--cell=1", "--coldstart=6", "--warmup=6", "--step=8", "--mon=3", "--warmup_mon=freq"]),
+    ("mm", ["--cell=1", "--step=40", "--mon=10"]),
+    ("mm", ["--cell=1", "--crystal=hcp", "--coldstart=10", "--warmup=10", "--step=20", "--mon=5"]),
+    ("lj", ["--cell=2", "--step=100", "--mon=20"]),
+    ("lj", ["--cell=2", "--crystal=bcc", "--coldstart=20", "--warmup=20", "--step=60", "--mon=10"]),
+])
+def test_driver_run_matches_reference(prog, args, work):
+    args = args + [f"--libdir={work['lib']}"]
+    a = run(ours(prog), args, work["ours"])
+    assert a.returncode == 0, a.stdout + a.stderr
+    b = run(ref(prog, omp=True), args, work["ref"])
+    assert b.returncode == 0, b.stderr
+    assert_rows_match(monitor_rows(a.stdout), monitor_rows(b.stdout))
+    assert_avg_match(averages(a.stdout), averages(b.stdout))
+    assert "Done (" in a.stdout
+
+
+@pytest.mark.gpu
+def test_core_driver_matches_reference(work):
+    a = run(ours("core"), ["2"], work["ours"])
+    assert a.returncode == 0, a.stdout + a.stderr
+    b = run(ref("core", omp=True), ["2"], work["ref"], timeout=1200)
+    assert b.returncode == 0, b.stderr
+    assert_rows_match(monitor_rows(a.stdout), monitor_rows(b.stdout))
+    assert_avg_match(averages(a.stdout), averages(b.stdout))
+    assert re.search(r"^Done \d+\.\ds$", a.stdout, re.M)
+
+
+def read_xyz(path: Path):
+    frames = []
+    lines = path.read_text().splitlines()
+    i = 0
+    while i < len(lines):
+        n = int(lines[i])
+        head = lines[i + 1]
+        body = np.array([[float(v) for v in ln.split()[1:]] for ln in lines[i + 2:i + 2 + n]])
+        frames.append((head, body))
+        i += 2 + n
+    return frames
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prog,ovito", [("ai", "ovito_traj_airebo"), ("mm", "ovito_traj_mmmd"),
+                                        ("lj", "ovito_traj_LJ")])
+def test_ovito_frames_match_reference(prog, ovito, work):
+    args = ["--cell=1", "--step=10", "--mon=5", "--ovito=5", f"--libdir={work['lib']}"]
+    a = run(ours(prog), args, work["ours"])
+    assert a.returncode == 0, a.stdout + a.stderr
+    b = run(ref(prog), args, work["ref"])
+    assert b.returncode == 0, b.stderr
+    fa = read_xyz(next(work["ours"].glob(f"{ovito}*.xyz")))
+    fb = read_xyz(next(work["ref"].glob(f"{ovito}*.xyz")))
+    assert len(fa) == len(fb) == 2
+    num = re.compile(r"-?\d+\.\d+")
+    for (ha, xa), (hb, xb) in zip(fa, fb):
+        assert num.sub("#", ha) == num.sub("#", hb)
+        np.testing.assert_allclose([float(v) for v in num.findall(ha)], [float(v) for v in num.findall(hb)],
+                                   rtol=1e-7, atol=2e-8)
+        assert xa.shape == xb.shape
+        np.testing.assert_array_equal(xa[:, 3], xb[:, 3])          # molecule index column
+        np.testing.assert_allclose(xa, xb, rtol=1e-6, atol=1e-7)
+
+
+def parse_restart(path: Path) -> dict[str, list[str]]:
+    out: dict[str, list[str]] = {}
+    for ln in path.read_text().splitlines():
+        tok = ln.split()
+        if not tok or tok[0].startswith("#"):
+            continue
+        out.setdefault(tok[0], []).append(" ".join(tok[1:]))
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prog,tag", [("ai", "restart_airebo"), ("mm", "restart_mmmd"), ("lj", "restart_LJ")])
+def test_restart_written_by_driver_resumes_in_both(prog, tag, work):
+    base = ["--cell=1", "--step=20", "--mon=5", f"--libdir={work['lib']}"]
+    full = run(ours(prog), base, work["ours"])
+    assert full.returncode == 0, full.stdout + full.stderr
+    a = run(ours(prog), base + ["--restart=10"], work["ours"])
+    assert a.returncode == 0, a.stdout + a.stderr
+    mid = work["ours"] / f"{tag}_gpu_00000010.rst"
+    assert mid.exists(), sorted(p.name for p in work["ours"].iterdir())
+    assert (work["ours"] / f"{tag}_gpu_20.rst").exists()
+    # same records and field counts as a restart file of the reference
+    b = run(ref(prog), base + ["--restart=10"], work["ref"])
+    assert b.returncode == 0, b.stderr
+    ra, rb = parse_restart(mid), parse_restart(work["ref"] / f"{tag}_serial_00000010.rst")
+    assert ra.keys() == rb.keys()
+    for k in rb:
+        assert len(ra[k]) == len(rb[k]), k
+        assert [len(x.split()) for x in ra[k]] == [len(x.split()) for x in rb[k]], k
+    # resume: ours and the reference from OUR file agree with the uninterrupted run
+    ra = run(ours(prog), base + [f"--resfile={mid}"], work["ours"])
+    rr = run(ref(prog), base + [f"--resfile={mid}"], work["ref"])
+    assert ra.returncode == 0 and rr.returncode == 0
+    tail = [r for r in monitor_rows(full.stdout) if int(r[0]) > 10]
+    assert_rows_match(monitor_rows(ra.stdout), tail)
+    assert_rows_match(monitor_rows(rr.stdout), tail)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prog", ["ai", "mm", "lj"])
+def test_abort_and_stop_control(prog, work):
+    base = ["--cell=1", "--step=30", "--mon=5", "--restart=10", f"--libdir={work['lib']}"]
+    for d in (work["ours"], work["ref"]):
+        (d / "abort.md").mkdir()
+    a = run(ours(prog), base, work["ours"])
+    b = run(ref(prog), base, work["ref"])
+    assert a.returncode == 0 and b.returncode == 0
+    msg = [ln for ln in b.stdout.splitlines() if "***" in ln]
+    assert msg == ["  *** abort.md detected at step 5 ***"]
+    assert [ln for ln in a.stdout.splitlines() if "***" in ln] == msg
+    assert len(list(work["ours"].glob("*_00000005.rst"))) == 1
+    for d in (work["ours"], work["ref"]):
+        (d / "abort.md").rmdir()
+        (d / "stop.md").mkdir()
+    a = run(ours(prog), base, work["ours"])
+    b = run(ref(prog), base, work["ref"])
+    assert a.returncode == 0 and b.returncode == 0
+    mb = [ln for ln in b.stdout.splitlines() if "***" in ln]
+    ma = [ln for ln in a.stdout.splitlines() if "***" in ln]
+    assert len(mb) == 2 and ma == mb
+    assert_rows_match(monitor_rows(a.stdout), monitor_rows(b.stdout))
