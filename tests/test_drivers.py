@@ -7,6 +7,12 @@ read the same fullerene library, written by ``write_library`` from this
 package's own C60 geometry in the .cc1 layout of
 FullereneLib/C60-76/C60-Ih.cc1 (count line, then "C idx x y z flag nbrs...").
 
+Whole runs are compared with the SERIAL reference build: the OpenMP AIREBO
+build accumulates REBO forces with `omp atomic` under dynamic scheduling
+(AI:284-417), so its trajectories differ from run to run (at cell=1 the
+printed E_REBO moves in the 4th decimal by step 10), while the serial build
+is deterministic.
+
 CPU tests: help text, banners, topology lines and the restart reader (our
 driver reads a restart file the reference wrote).  GPU tests: monitor and
 average lines of whole runs, OVITO frames, restart files read back by the
@@ -184,7 +190,7 @@ def monitor_rows(text: str) -> list[list[str]]:
 def averages(text: str) -> dict[str, float]:
     for ln in text.splitlines():
         if "Averages (" in ln or ln.startswith("Avg("):
-            out = {"n": float(re.search(r"\((\d+)\)", ln).group(1))}
+            out = {"n": float(re.search(r"\((\d+)", ln).group(1))}
             for k, v in re.findall(r"(\w+)=(-?[\d.]+)", ln):
                 out[k] = float(v)
             return out
@@ -227,7 +233,7 @@ def test_driver_run_matches_reference(prog, args, work):
     args = args + [f"--libdir={work['lib']}"]
     a = run(ours(prog), args, work["ours"])
     assert a.returncode == 0, a.stdout + a.stderr
-    b = run(ref(prog, omp=True), args, work["ref"])
+    b = run(ref(prog), args, work["ref"])
     assert b.returncode == 0, b.stderr
     assert_rows_match(monitor_rows(a.stdout), monitor_rows(b.stdout))
     assert_avg_match(averages(a.stdout), averages(b.stdout))
@@ -238,7 +244,7 @@ def test_driver_run_matches_reference(prog, args, work):
 def test_core_driver_matches_reference(work):
     a = run(ours("core"), ["2"], work["ours"])
     assert a.returncode == 0, a.stdout + a.stderr
-    b = run(ref("core", omp=True), ["2"], work["ref"], timeout=1200)
+    b = run(ref("core"), ["2"], work["ref"], timeout=1200)
     assert b.returncode == 0, b.stderr
     assert_rows_match(monitor_rows(a.stdout), monitor_rows(b.stdout))
     assert_avg_match(averages(a.stdout), averages(b.stdout))
@@ -298,13 +304,18 @@ def test_restart_written_by_driver_resumes_in_both(prog, tag, work):
     assert full.returncode == 0, full.stdout + full.stderr
     a = run(ours(prog), base + ["--restart=10"], work["ours"])
     assert a.returncode == 0, a.stdout + a.stderr
-    mid = work["ours"] / f"{tag}_gpu_00000010.rst"
-    assert mid.exists(), sorted(p.name for p in work["ours"].iterdir())
-    assert (work["ours"] / f"{tag}_gpu_20.rst").exists()
+    # restart_filename: "_<step>" zero-padded to the digits of the total
+    # step count, no suffix at the last step (LJ:583-588)
+    got = sorted(p.name for p in work["ours"].glob(f"{tag}_gpu*.rst"))
+    assert len(got) == 2 and got[1].endswith("_10.rst") and got[0] == got[1][:-7] + ".rst", got
+    mid = work["ours"] / got[1]
     # same records and field counts as a restart file of the reference
     b = run(ref(prog), base + ["--restart=10"], work["ref"])
     assert b.returncode == 0, b.stderr
-    ra, rb = parse_restart(mid), parse_restart(work["ref"] / f"{tag}_serial_00000010.rst")
+    refmid = sorted(work["ref"].glob(f"{tag}_serial*_10.rst"))
+    assert len(refmid) == 1
+    assert refmid[0].name.replace("_serial", "_gpu") == mid.name
+    ra, rb = parse_restart(mid), parse_restart(refmid[0])
     assert ra.keys() == rb.keys()
     for k in rb:
         assert len(ra[k]) == len(rb[k]), k
@@ -330,7 +341,7 @@ def test_abort_and_stop_control(prog, work):
     msg = [ln for ln in b.stdout.splitlines() if "***" in ln]
     assert msg == ["  *** abort.md detected at step 5 ***"]
     assert [ln for ln in a.stdout.splitlines() if "***" in ln] == msg
-    assert len(list(work["ours"].glob("*_00000005.rst"))) == 1
+    assert len(list(work["ours"].glob("*_05.rst"))) == 1
     for d in (work["ours"], work["ref"]):
         (d / "abort.md").rmdir()
         (d / "stop.md").mkdir()
