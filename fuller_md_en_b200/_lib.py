@@ -7,7 +7,7 @@ usable, every call raises.
 from __future__ import annotations
 
 import ctypes
-from ctypes import POINTER, c_char_p, c_double, c_int, c_void_p
+from ctypes import POINTER, c_char_p, c_double, c_float, c_int, c_void_p
 from pathlib import Path
 
 LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libfullermd_cuda.so"
@@ -102,6 +102,7 @@ _SIGS = {
     "fmd_system_destroy": (c_int, [c_void_p]),
     "fmd_system_kernel_ms": (c_int, [c_void_p, c_int, c_int, POINTER(c_double)]),
     "fmd_system_step_kernels": (c_int, [c_void_p, c_int, c_int, POINTER(c_int)]),
+    "fmd_umma_selftest": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, POINTER(c_float)]),
 }
 
 _lib = None

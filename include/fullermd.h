@@ -25,6 +25,8 @@
  */
 #ifndef FULLERMD_H
 #define FULLERMD_H
+#include <stdint.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -241,6 +243,13 @@ int fmd_system_destroy(fmd_system *s);
  * of each variant (list rebuild or not, cold/warm phase or not). */
 int fmd_system_kernel_ms(fmd_system *s, int stage, int reps, double *ms_per_launch);
 int fmd_system_step_kernels(fmd_system *s, int rebuild, int phase, int *nkernels);
+
+/* Tensor-core self test (no reference counterpart): D = A * Bt^T for one
+ * 128 x N x K BF16 tile through tcgen05.mma, FP32 result.  A is 128 x K and
+ * Bt is N x K, row-major bf16 bit patterns; mode bit 0 reads A MN-major and
+ * bit 1 reads B MN-major from shared memory (the operand orientations of the
+ * learned-potential kernels).  K, N multiples of 16 in [16, 256]. */
+int fmd_umma_selftest(fmd_ctx *ctx, const uint16_t *A, const uint16_t *Bt, int K, int N, int mode, float *D);
 
 #ifdef __cplusplus
 }
