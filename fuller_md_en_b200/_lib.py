@@ -50,6 +50,11 @@ class Obs(ctypes.Structure):
                 ("E", c_double * 8)]
 
 
+class SgTrainArgs(ctypes.Structure):
+    _fields_ = [("steps", c_int), ("batch", c_int), ("n_train", c_int), ("seed", c_int), ("lr", c_double),
+                ("lr_final", c_double), ("wE", c_double), ("wF", c_double), ("wW", c_double), ("clip", c_double)]
+
+
 class Avg(ctypes.Structure):
     _fields_ = [("n", c_int), ("sT", c_double), ("sP", c_double), ("sa", c_double), ("sE", c_double * 8)]
 
@@ -103,6 +108,25 @@ _SIGS = {
     "fmd_system_kernel_ms": (c_int, [c_void_p, c_int, c_int, POINTER(c_double)]),
     "fmd_system_step_kernels": (c_int, [c_void_p, c_int, c_int, POINTER(c_int)]),
     "fmd_umma_selftest": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, POINTER(c_float)]),
+    "fmd_sg_nparams": (c_int, []),
+    "fmd_sg_create": (c_int, [c_void_p, _dp, POINTER(c_void_p)]),
+    "fmd_sg_set_params": (c_int, [c_void_p, _dp]),
+    "fmd_sg_get_params": (c_int, [c_void_p, _dp]),
+    "fmd_sg_destroy": (c_int, [c_void_p]),
+    "fmd_sg_rebo_forces": (c_int, [c_void_p, _dp, _dp, _dp, _ip, _ip, c_int, c_int, _dp, _dp, _dp]),
+    "fmd_sg_last_rows": (c_int, [c_void_p, c_int, _ip, _ip, _ip, POINTER(c_float), POINTER(c_float),
+                                 POINTER(c_float)]),
+    "fmd_sg_data_create": (c_int, [c_void_p, POINTER(c_void_p)]),
+    "fmd_sg_data_destroy": (c_int, [c_void_p]),
+    "fmd_sg_data_count": (c_int, [c_void_p]),
+    "fmd_sg_data_add": (c_int, [c_void_p, _dp, _dp, _dp, _ip, _ip, c_int, c_int]),
+    "fmd_sg_data_add_system": (c_int, [c_void_p, c_void_p]),
+    "fmd_sg_data_get": (c_int, [c_void_p, c_int, _ip, _dp, _dp, _dp]),
+    "fmd_sg_loss_grad": (c_int, [c_void_p, _dp, _dp, _dp, _ip, _ip, c_int, c_int, _dp, c_double, _dp, c_double,
+                                 c_double, c_double, _dp, _dp]),
+    "fmd_sg_train": (c_int, [c_void_p, c_void_p, POINTER(SgTrainArgs), _dp]),
+    "fmd_sg_eval": (c_int, [c_void_p, c_void_p, c_int, c_int, _dp]),
+    "fmd_sg_feature_stats": (c_int, [c_void_p, c_void_p, c_int, c_int, _dp, _dp]),
 }
 
 _lib = None

@@ -7,6 +7,7 @@
 #include <memory>
 #include "step.h"
 #include "system.h"
+#include "sg_host.h"
 
 using namespace fmd;
 
@@ -495,4 +496,16 @@ extern "C" int fmd_system_destroy(fmd_system* s) {
     }
     delete s;
     return FMD_OK;
+}
+
+// Training snapshot of an AIREBO system: its positions, cell and current REBO
+// list, with reference values from the plain REBO kernel (sg_abi.cu).
+extern "C" int fmd_sg_data_add_system(fmd_sg_data* d, fmd_system* s) {
+    if (!d || !s || !s->sys) return FMD_ERR_ARG;
+    fmd::System& y = *s->sys;
+    if (y.arr.kind != FMD_SYS_AIREBO)
+        return y.ctx->fail(FMD_ERR_ARG, "fmd_sg_data_add_system: not an AIREBO system");
+    if (!y.initialized) return y.ctx->fail(FMD_ERR_STATE, "fmd_sg_data_add_system: system not initialised");
+    return fmd::sg_data_add_device(d, y.arr.pos, y.arr.S->h, y.arr.cnt_b, y.arr.list_b, y.arr.cap_b, y.arr.n,
+                                   y.ctx->stream);
 }

@@ -251,6 +251,75 @@ int fmd_system_step_kernels(fmd_system *s, int rebuild, int phase, int *nkernels
  * learned-potential kernels).  K, N multiples of 16 in [16, 256]. */
 int fmd_umma_selftest(fmd_ctx *ctx, const uint16_t *A, const uint16_t *Bt, int K, int N, int mode, float *D);
 
+/* ------------------------------------------- learned bond-order potential --
+ * No counterpart in the reference.  A network stands in for the bond order
+ * b_ij of compute_rebo (AI:275-421); the pair functions, b_bar and the
+ * reference's force construction are kept.  Row = directed bond i->j of the
+ * REBO list with r_ij <= 2.0; its 32 descriptors are sums over i's other
+ * bonded neighbours k of fc(r_ik) T_a((r_ik-1.55)/0.45) T_b(cos theta_jik)
+ * (Chebyshev T, a<4, b<8; descriptor 31 is a constant bias input).  Network:
+ * three 128-wide SiLU layers (unit 127 of each is a constant bias unit),
+ * linear output y, b = b0 + bs*y, evaluated with BF16 operands and FP32
+ * accumulation on the tensor cores.
+ * Parameter vector (doubles, fmd_sg_nparams() of them):
+ *   W1[32][128] W2[128][128] W3[128][128] w4[128] m[32] s[32] b0 bs
+ * (W[in][out]; descriptors are normalised as (x-m)/s before the network). */
+typedef struct fmd_sg fmd_sg;
+int fmd_sg_nparams(void);
+int fmd_sg_create(fmd_ctx *ctx, const double *params, fmd_sg **out);
+int fmd_sg_set_params(fmd_sg *s, const double *params);
+int fmd_sg_get_params(fmd_sg *s, double *params);
+int fmd_sg_destroy(fmd_sg *s);
+/* As fmd_rebo_forces with the learned bond order: ADDS into F and vir9,
+ * *E = energy.  The REBO list must be symmetric (as fmd_nlist_rebo makes it). */
+int fmd_sg_rebo_forces(fmd_sg *s, const double *pos, const double *h, const double *hi, const int *nlc,
+                       const int *nll, int max_neigh, int na, double *F, double *vir9, double *E);
+/* Rows of the last fmd_sg_rebo_forces call: *nrows, and (each may be NULL)
+ * row_i, row_j, normalised BF16 descriptors xn[rows*32] as floats, b[rows],
+ * gx[rows*32] = db/dxn.  cap_rows = capacity of the arrays. */
+int fmd_sg_last_rows(fmd_sg *s, int cap_rows, int *nrows, int *row_i, int *row_j, float *xn, float *b, float *gx);
+
+/* Training data: snapshots whose reference REBO energy, forces and virial are
+ * computed on the device by the plain REBO kernel (fmd_rebo_forces). */
+typedef struct fmd_sg_data fmd_sg_data;
+int fmd_sg_data_create(fmd_ctx *ctx, fmd_sg_data **out);
+int fmd_sg_data_destroy(fmd_sg_data *d);
+int fmd_sg_data_count(const fmd_sg_data *d);
+int fmd_sg_data_add(fmd_sg_data *d, const double *pos, const double *h, const double *hi, const int *nlc,
+                    const int *nll, int max_neigh, int na);
+/* Current state of a running AIREBO system (device to device). */
+int fmd_sg_data_add_system(fmd_sg_data *d, fmd_system *sys);
+/* Reference values of snapshot k: *na, *E, W9[9], F[3*na] (any may be NULL but na). */
+int fmd_sg_data_get(fmd_sg_data *d, int k, int *na, double *E, double *W9, double *F);
+
+/* Mean and standard deviation of the raw descriptors over the rows of
+ * snapshots [first, first+n): the normalisation m, s of a new model. */
+int fmd_sg_feature_stats(fmd_sg *s, fmd_sg_data *d, int first, int n, double *mean, double *stdev);
+
+/* Loss L = wF mean(dF^2) + wE (dE/na)^2 + wW mean((dW/na)^2) of the REBO
+ * term against given reference values, and dL/dparams (the layout of the
+ * parameter vector; zeros for m, s, b0, bs, which do not train). */
+int fmd_sg_loss_grad(fmd_sg *s, const double *pos, const double *h, const double *hi, const int *nlc,
+                     const int *nll, int max_neigh, int na, const double *F_ref, double E_ref,
+                     const double *W_ref, double wE, double wF, double wW, double *loss, double *grad);
+
+typedef struct {
+    int steps;          /* Adam updates */
+    int batch;          /* snapshots per update (drawn uniformly with `seed`) */
+    int n_train;        /* draw from snapshots [0, n_train); <= 0: all */
+    int seed;
+    double lr, lr_final;  /* cosine schedule from lr to lr_final */
+    double wE, wF, wW;  /* loss weights */
+    double clip;        /* per-component gradient clip (<= 0: none) */
+} fmd_sg_train_args;
+/* Adam training with the tensor-core forward/backward kernels.
+ * history[2*k] = mean loss of step k, history[2*k+1] = force RMSE of step k
+ * (eV/A, over the step's batch, before the update); may be NULL. */
+int fmd_sg_train(fmd_sg *s, fmd_sg_data *d, const fmd_sg_train_args *a, double *history);
+/* Force RMSE (eV/A) against the reference REBO forces of snapshots
+ * [first, first+n): rmse[n]. */
+int fmd_sg_eval(fmd_sg *s, fmd_sg_data *d, int first, int n, double *rmse);
+
 #ifdef __cplusplus
 }
 #endif
