@@ -55,6 +55,12 @@ class SgTrainArgs(ctypes.Structure):
                 ("lr_final", c_double), ("wE", c_double), ("wF", c_double), ("wW", c_double), ("clip", c_double)]
 
 
+class SgStatus(ctypes.Structure):
+    """fmd_sg_status: judge record of the learned REBO term of a system."""
+    _fields_ = [("attached", c_int), ("active", c_int), ("judged", c_int), ("takeover_step", c_int),
+                ("rmse_last", c_double), ("rmse_max", c_double)]
+
+
 class Avg(ctypes.Structure):
     _fields_ = [("n", c_int), ("sT", c_double), ("sP", c_double), ("sa", c_double), ("sE", c_double * 8)]
 
@@ -127,6 +133,8 @@ _SIGS = {
     "fmd_sg_train": (c_int, [c_void_p, c_void_p, POINTER(SgTrainArgs), _dp]),
     "fmd_sg_eval": (c_int, [c_void_p, c_void_p, c_int, c_int, _dp]),
     "fmd_sg_feature_stats": (c_int, [c_void_p, c_void_p, c_int, c_int, _dp, _dp]),
+    "fmd_system_use_surrogate": (c_int, [c_void_p, c_void_p, c_int, c_double]),
+    "fmd_system_surrogate_status": (c_int, [c_void_p, POINTER(SgStatus)]),
 }
 
 _lib = None

@@ -399,11 +399,27 @@ class System:
         self.ctx.check(self.ctx.lib.fmd_system_kernel_ms(self.h, stage, reps, ctypes.byref(ms)), "kernel_ms")
         return ms.value
 
-    def step_kernels(self, rebuild: bool, phase: bool = False) -> int:
+    def step_kernels(self, rebuild: bool, phase: bool = False, judge: bool = False) -> int:
         k = ctypes.c_int(0)
-        self.ctx.check(self.ctx.lib.fmd_system_step_kernels(self.h, int(rebuild), int(phase), ctypes.byref(k)),
-                       "step_kernels")
+        self.ctx.check(self.ctx.lib.fmd_system_step_kernels(self.h, int(rebuild), int(phase) | (2 * int(judge)),
+                                                            ctypes.byref(k)), "step_kernels")
         return k.value
+
+    def use_surrogate(self, model, judge_every: int = 100, rmse_max: float = 0.025) -> None:
+        """Learned REBO term from `model` (a surrogate.Surrogate, or None for
+        the plain kernel), judged by the plain REBO kernel every `judge_every`
+        global steps; above `rmse_max` eV/A force RMSE the plain kernel takes
+        over for the rest of the run."""
+        self._sg_model = model              # the model must outlive its use here
+        hm = model.h if model is not None else None
+        self.ctx.check(self.ctx.lib.fmd_system_use_surrogate(self.h, hm, int(judge_every), float(rmse_max)),
+                       "fmd_system_use_surrogate")
+
+    def surrogate_status(self) -> dict:
+        st = _lib.SgStatus()
+        self.ctx.check(self.ctx.lib.fmd_system_surrogate_status(self.h, ctypes.byref(st)),
+                       "fmd_system_surrogate_status")
+        return {k: getattr(st, k) for k, _ in st._fields_}
 
     def close(self) -> None:
         if self.h:

@@ -206,9 +206,12 @@ int list_call(fmd_ctx* ctx, int mode, const double* pos, const double* h, const 
 
 extern "C" int fmd_mat_inv9(fmd_ctx* ctx, const double* h, double* hi) {
     if (!ctx || !h || !hi) return ctx ? ctx->fail(FMD_ERR_ARG, "fmd_mat_inv9: null") : FMD_ERR_ARG;
+    // {h, hi}: the slot holds 18 doubles, the kernel writes hi into [9, 18)
     double* hh;
-    int rc = up(ctx, S_HH, h, 9, &hh);
+    int rc = up<double>(ctx, S_HH, nullptr, 18, &hh);
     if (rc) return rc;
+    if (cudaMemcpyAsync(hh, h, sizeof(double) * 9, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess)
+        return ctx->fail(FMD_ERR_CUDA, "host to device copy failed");
     if (inv9_launch(hh, ctx->stream) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "launch failed");
     down(ctx, hi, hh + 9, 9);
     return ctx->sync_check("mat_inv9");

@@ -90,7 +90,11 @@ constexpr int kReboLanes = 4;
 
 __global__ void __launch_bounds__(128)
 k_rebo(const double* __restrict__ pos, const double* __restrict__ hh, const int* __restrict__ cnt,
-       const int* __restrict__ list, int cap, int na, double* __restrict__ F, double* __restrict__ part) {
+       const int* __restrict__ list, int cap, int na, double* __restrict__ F, double* __restrict__ part,
+       const int* __restrict__ gate, int want) {
+    // Gated launch (learned REBO term): runs only when *gate == want; the
+    // decision is uniform over the grid, so no partial is written otherwise.
+    if (gate != nullptr && *gate != want) return;
     __shared__ double sm[32 * kNV];
     double h[9], hi[9];
     load_cell(hh, h, hi);
@@ -265,13 +269,20 @@ __global__ void k_reduce(const double* __restrict__ part, int nblk, int nv, doub
 
 cudaError_t rebo_launch(const double* pos, const double* hh, const int* cnt, const int* list, int cap,
                         int na, double* F, double* part, cudaStream_t st) {
-    k_rebo<<<kForceBlocks, 128, 0, st>>>(pos, hh, cnt, list, cap, na, F, part);
+    k_rebo<<<kForceBlocks, 128, 0, st>>>(pos, hh, cnt, list, cap, na, F, part, nullptr, 0);
     return cudaGetLastError();
 }
 
 cudaError_t rebo_launch_grid(const double* pos, const double* hh, const int* cnt, const int* list, int cap,
                              int na, double* F, double* part, int nblocks, cudaStream_t st) {
-    k_rebo<<<nblocks, 128, 0, st>>>(pos, hh, cnt, list, cap, na, F, part);
+    k_rebo<<<nblocks, 128, 0, st>>>(pos, hh, cnt, list, cap, na, F, part, nullptr, 0);
+    return cudaGetLastError();
+}
+
+cudaError_t rebo_launch_gated(const double* pos, const double* hh, const int* cnt, const int* list, int cap,
+                              int na, double* F, double* part, int nblocks, const int* gate, int want,
+                              cudaStream_t st) {
+    k_rebo<<<nblocks, 128, 0, st>>>(pos, hh, cnt, list, cap, na, F, part, gate, want);
     return cudaGetLastError();
 }
 

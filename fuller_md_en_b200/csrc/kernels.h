@@ -63,6 +63,10 @@ cudaError_t rebo_launch(const double* pos, const double* hh, const int* cnt, con
 // (nblocks partial records).
 cudaError_t rebo_launch_grid(const double* pos, const double* hh, const int* cnt, const int* list,
                              int cap, int na, double* F, double* part, int nblocks, cudaStream_t st);
+// Same, but the whole grid returns at once unless *gate == want (device int).
+cudaError_t rebo_launch_gated(const double* pos, const double* hh, const int* cnt, const int* list, int cap,
+                              int na, double* F, double* part, int nblocks, const int* gate, int want,
+                              cudaStream_t st);
 // Half-list LJ gather (a8, a14): F[i] = Facc[i] + LJ(i); Facc[i] zeroed
 // (Facc may alias F only if zero_acc == 0).  ff: FMD_FF_AIREBO / FMD_FF_MM.
 cudaError_t lj_gather_launch(int ff, const double* pos, const double* hh, const int* cnt,

@@ -84,6 +84,11 @@ bool params_ok(const double* p) {
 
 }  // namespace
 
+void fmd::sg_model_images(const fmd_sg* m, const uint16_t** img, const float** vec) {
+    *img = m->img;
+    *vec = m->vec;
+}
+
 extern "C" int fmd_sg_nparams(void) { return fmd::sg::NPARAM; }
 
 extern "C" int fmd_sg_set_params(fmd_sg* s, const double* params) {

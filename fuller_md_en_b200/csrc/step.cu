@@ -23,6 +23,7 @@
 #include <cmath>
 #include "step.h"
 #include "geom.cuh"
+#include "sg_host.h"
 
 namespace fmd {
 namespace {
@@ -359,17 +360,19 @@ __global__ void __launch_bounds__(256) k_force_final(StepArrays a, int nblk_f1) 
 }  // namespace
 
 int force_partial_blocks(const StepArrays& a) {
-    return a.kind == FMD_SYS_RIGID ? rigid_grid(a.n) : kForceBlocks;
+    return a.kind == FMD_SYS_RIGID ? rigid_grid(a.n) : (a.kind == FMD_SYS_AIREBO ? a.rebo_blocks : kForceBlocks);
 }
 
-cudaError_t enqueue_forces(const StepArrays& a, cudaStream_t st) {
+cudaError_t enqueue_forces(const StepArrays& a, cudaStream_t st, bool judge) {
     cudaError_t e = cudaSuccess;
     const double* hh = a.S->h;
     if (a.kind == FMD_SYS_RIGID) {
         e = rigid_launch(a.precision, a.pos, a.qv, a.body, hh, a.cnt_a, a.list_a, a.cap_a, a.n, a.natom,
                          a.rmcut2, a.F, a.T, a.part_f1, st);
     } else if (a.kind == FMD_SYS_AIREBO) {
-        if ((e = rebo_launch(a.pos, hh, a.cnt_b, a.list_b, a.cap_b, a.n, a.Facc, a.part_f1, st)) != cudaSuccess) return e;
+        if (a.sg) e = sg_enqueue_rebo(*a.sg, a, judge, st);
+        else e = rebo_launch(a.pos, hh, a.cnt_b, a.list_b, a.cap_b, a.n, a.Facc, a.part_f1, st);
+        if (e != cudaSuccess) return e;
         e = lj_gather_launch(FMD_FF_AIREBO, a.pos, hh, a.cnt_a, a.list_a, a.cap_a, a.in_cnt, a.in_list, a.in_cap,
                              a.n, a.F, a.Facc, a.part_f2, st);
     } else {
@@ -393,11 +396,12 @@ cudaError_t enqueue_ke(const StepArrays& a, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-cudaError_t enqueue_step(const StepArrays& a, const StepParams& p, bool rescale_phase, cudaStream_t st) {
+cudaError_t enqueue_step(const StepArrays& a, const StepParams& p, bool rescale_phase, cudaStream_t st,
+                         bool judge) {
     cudaError_t e;
     k_begin<<<1, 32, 0, st>>>(a.S, a.kind, p);
     k_kick<<<kForceBlocks, kPB, 0, st>>>(a, p.dt);
-    if ((e = enqueue_forces(a, st)) != cudaSuccess) return e;
+    if ((e = enqueue_forces(a, st, judge)) != cudaSuccess) return e;
     k_kick2<<<kForceBlocks, kPB, 0, st>>>(a, p.dt);
     k_end<<<1, 256, 0, st>>>(a, p, force_partial_blocks(a), kForceBlocks);
     if (rescale_phase && p.schedule) {

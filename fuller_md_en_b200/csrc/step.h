@@ -20,7 +20,15 @@ struct SysScal {
     int gstep;
     fmd_obs obs;
     fmd_avg avg;
+    // Learned REBO term (AIREBO systems with a model attached): the plain
+    // kernel judges it every few steps and takes over above a force RMSE.
+    int sg_off;              // 1: the plain REBO kernel has taken over
+    int sg_judged;           // judge evaluations so far
+    int sg_takeover;         // global step of the takeover (0: none)
+    double sg_rmse_last, sg_rmse_max;
 };
+
+struct SgStep;   // learned REBO term of a system (sg_host.h)
 
 // Device pointers and sizes of one step.
 struct StepArrays {
@@ -45,6 +53,8 @@ struct StepArrays {
     MMTopoDev topo{};
     double rmcut2 = 0, Mmol = 0, I0 = 0;
     int precision = FMD_PREC_FP64;
+    SgStep* sg = nullptr;          // AIREBO: learned REBO term instead of the plain kernel
+    int rebo_blocks = kForceBlocks;  // partial records the REBO term writes into part_f1
 };
 
 struct StepParams {
@@ -54,14 +64,17 @@ struct StepParams {
 };
 
 // Force evaluation of the step's kind; fills partials and F (and T).
-cudaError_t enqueue_forces(const StepArrays& a, cudaStream_t st);
+// judge: AIREBO with a learned REBO term also runs the plain REBO kernel and
+// compares the two (sg_step.cu).
+cudaError_t enqueue_forces(const StepArrays& a, cudaStream_t st, bool judge = false);
 // Reduces the force partials into S->W9 / S->E (one small kernel).
 cudaError_t enqueue_force_reduce(const StepArrays& a, cudaStream_t st);
 // Recomputes S->KE (and kt, kr) from the velocities.
 cudaError_t enqueue_ke(const StepArrays& a, cudaStream_t st);
 // One step_npt (+ driver schedule if p.schedule); rescale_phase selects the
 // cold/warm velocity rescale kernels.
-cudaError_t enqueue_step(const StepArrays& a, const StepParams& p, bool rescale_phase, cudaStream_t st);
+cudaError_t enqueue_step(const StepArrays& a, const StepParams& p, bool rescale_phase, cudaStream_t st,
+                         bool judge = false);
 // Observables / averages for the pre-loop state (not a step).
 int force_partial_blocks(const StepArrays& a);
 

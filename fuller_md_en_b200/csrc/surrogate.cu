@@ -32,12 +32,14 @@ using namespace dev;
 
 __global__ void k_sg_count(const double* __restrict__ pos, const double* __restrict__ hh,
                            const int* __restrict__ cnt, const int* __restrict__ list, int cap, int na,
-                           int* __restrict__ acnt) {
+                           int* __restrict__ acnt, const int* __restrict__ gate) {
     double h[9], hi[9];
     load_cell(hh, h, hi);
+    // A set gate (the plain kernel has taken over) leaves every atom without rows.
+    const bool off = gate != nullptr && *gate != 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < na; i += gridDim.x * blockDim.x) {
         int c = 0;
-        for (int jn = 0; jn < cnt[i]; jn++) {
+        for (int jn = 0; jn < (off ? 0 : cnt[i]); jn++) {
             double x, y, z;
             bond_vec(pos, i, list[(size_t)i * cap + jn], h, hi, x, y, z);
             c += bond_kept(sqrt(norm2_rn(x, y, z)));
@@ -72,7 +74,8 @@ __global__ void __launch_bounds__(1024) k_sg_scan(const int* __restrict__ acnt, 
 __global__ void k_sg_rows(const double* __restrict__ pos, const double* __restrict__ hh,
                           const int* __restrict__ cnt, const int* __restrict__ list, int cap, int na,
                           const int* __restrict__ aoff, int* __restrict__ row_i, int* __restrict__ row_s,
-                          int* __restrict__ rowid) {
+                          int* __restrict__ rowid, const int* __restrict__ gate) {
+    if (gate != nullptr && *gate != 0) return;
     double h[9], hi[9];
     load_cell(hh, h, hi);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < na; i += gridDim.x * blockDim.x) {
@@ -503,13 +506,13 @@ cudaError_t pack_params(const double* P, uint16_t* img, float* vec, cudaStream_t
 }
 
 cudaError_t build_rows(Work& w, const float* vec, const double* pos, const double* hh, const int* cnt,
-                       const int* list, int cap, int na, cudaStream_t st) {
+                       const int* list, int cap, int na, cudaStream_t st, const int* gate) {
     if (na > w.na_cap || cap != w.cap) return cudaErrorInvalidValue;
     w.na_used = na;
     const int nb = (na + 255) / 256;
-    k_sg_count<<<nb, 256, 0, st>>>(pos, hh, cnt, list, cap, na, w.acnt);
+    k_sg_count<<<nb, 256, 0, st>>>(pos, hh, cnt, list, cap, na, w.acnt, gate);
     k_sg_scan<<<1, 1024, 0, st>>>(w.acnt, na, w.aoff);
-    k_sg_rows<<<nb, 256, 0, st>>>(pos, hh, cnt, list, cap, na, w.aoff, w.row_i, w.row_s, w.rowid);
+    k_sg_rows<<<nb, 256, 0, st>>>(pos, hh, cnt, list, cap, na, w.aoff, w.row_i, w.row_s, w.rowid, gate);
     k_sg_desc<<<kRowBlocks, 128, 0, st>>>(pos, hh, cnt, list, cap, na, w.aoff, w.row_i, w.row_s, w.rowid, vec,
                                           w.r_cap, w.X, w.partner, w.err);
     return cudaGetLastError();
@@ -536,8 +539,8 @@ cudaError_t assemble(Work& w, const float* vec, const double* pos, const double*
 
 cudaError_t rebo_forces(Work& w, const uint16_t* img, const float* vec, const double* pos, const double* hh,
                         const int* cnt, const int* list, int cap, int na, double* F, double* part,
-                        cudaStream_t st) {
-    cudaError_t e = build_rows(w, vec, pos, hh, cnt, list, cap, na, st);
+                        cudaStream_t st, const int* gate) {
+    cudaError_t e = build_rows(w, vec, pos, hh, cnt, list, cap, na, st, gate);
     if (e == cudaSuccess) e = run_mlp(w, img, vec, st);
     if (e == cudaSuccess) e = assemble(w, vec, pos, hh, cnt, list, cap, na, F, part, st);
     return e;

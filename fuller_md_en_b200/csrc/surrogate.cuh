@@ -58,13 +58,15 @@ void work_free(Work& w);
 cudaError_t pack_params(const double* P, uint16_t* img, float* vec, cudaStream_t st);
 
 // Rows, descriptors, network, forces: F += REBO(learned b), part = per-block
-// {E, W9} (kRowBlocks records).  hh = {h, hi} on the device.
+// {E, W9} (kRowBlocks records).  hh = {h, hi} on the device.  A non-null
+// gate (device int) that is set makes the pass produce no rows: F is left
+// alone and the partials are zero.
 cudaError_t rebo_forces(Work& w, const uint16_t* img, const float* vec, const double* pos, const double* hh,
                         const int* cnt, const int* list, int cap, int na, double* F, double* part,
-                        cudaStream_t st);
+                        cudaStream_t st, const int* gate = nullptr);
 // The stages of rebo_forces, for tests and training.
 cudaError_t build_rows(Work& w, const float* vec, const double* pos, const double* hh, const int* cnt,
-                       const int* list, int cap, int na, cudaStream_t st);
+                       const int* list, int cap, int na, cudaStream_t st, const int* gate = nullptr);
 cudaError_t run_mlp(Work& w, const uint16_t* img, const float* vec, cudaStream_t st);
 cudaError_t assemble(Work& w, const float* vec, const double* pos, const double* hh, const int* cnt,
                      const int* list, int cap, int na, double* F, double* part, cudaStream_t st);

@@ -2,7 +2,9 @@
 // rebuilds on the device every nlup steps, each step replayed as a CUDA graph
 // (one graph per {rebuild, cold/warm} variant, captured on first use).
 // The host only sees observables at the steps it asks for.
+#include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstring>
 #include <memory>
 #include "step.h"
@@ -26,10 +28,18 @@ cudaError_t dupload(T** p, const T* src, size_t count, cudaStream_t st) {
 }
 }  // namespace
 
+void System::drop_graphs() {
+    for (auto& a : graphs)
+        for (auto& b : a)
+            for (auto& g : b)
+                if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+}
+
 void System::release() {
-    for (auto& row : graphs)
-        for (auto& g : row)
-            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    drop_graphs();
+    if (sg) sg::work_free(sg->work);
+    sg.reset();
+    arr.sg = nullptr;
     for (void* p : owned) cudaFree(p);
     owned.clear();
     cells_free(cells_a);
@@ -143,14 +153,14 @@ int System::init() {
     return FMD_OK;
 }
 
-int System::capture(bool rebuild, bool phase) {
-    cudaGraphExec_t& ge = graphs[rebuild ? 1 : 0][phase ? 1 : 0];
+int System::capture(bool rebuild, bool phase, bool judge) {
+    cudaGraphExec_t& ge = graphs[rebuild ? 1 : 0][phase ? 1 : 0][judge ? 1 : 0];
     if (ge) return FMD_OK;
     cudaStream_t st = ctx->stream;
     cudaGraph_t graph;
     if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
         return ctx->fail(FMD_ERR_CUDA, "graph capture failed to start");
-    cudaError_t e = enqueue_variant(rebuild, phase, st);
+    cudaError_t e = enqueue_variant(rebuild, phase, st, judge);
     cudaError_t e2 = cudaStreamEndCapture(st, &graph);
     if (e != cudaSuccess || e2 != cudaSuccess)
         return ctx->fail(FMD_ERR_CUDA, std::string("graph capture failed: ") +
@@ -161,14 +171,14 @@ int System::capture(bool rebuild, bool phase) {
     return FMD_OK;
 }
 
-cudaError_t System::enqueue_variant(bool rebuild, bool phase, cudaStream_t st) {
+cudaError_t System::enqueue_variant(bool rebuild, bool phase, cudaStream_t st, bool judge) {
     cudaError_t e;
     if (rebuild && (e = enqueue_rebuild(st)) != cudaSuccess) return e;
-    return enqueue_step(arr, sp, phase, st);
+    return enqueue_step(arr, sp, phase, st, judge);
 }
 
 cudaError_t System::enqueue_one(int g, cudaStream_t st) {
-    return enqueue_variant((g % p.nlup) == 0, g <= p.coldstart + p.warmup, st);
+    return enqueue_variant((g % p.nlup) == 0, g <= p.coldstart + p.warmup, st, judge_step(g));
 }
 
 int System::run(int first, int last, fmd_obs* obs) {
@@ -191,10 +201,10 @@ int System::enqueue(int first, int last) {
     cudaMemcpyAsync(&arr.S->gstep, &g0, sizeof(int), cudaMemcpyHostToDevice, st);
     for (int g = first; g <= last; g++) {
         if (p.use_graphs) {
-            const int r = (g % p.nlup) == 0, ph = g <= p.coldstart + p.warmup;
-            int rc = capture(r != 0, ph != 0);
+            const int r = (g % p.nlup) == 0, ph = g <= p.coldstart + p.warmup, j = judge_step(g);
+            int rc = capture(r != 0, ph != 0, j != 0);
             if (rc != FMD_OK) return rc;
-            if (cudaGraphLaunch(graphs[r][ph], st) != cudaSuccess)
+            if (cudaGraphLaunch(graphs[r][ph][j], st) != cudaSuccess)
                 return ctx->fail(FMD_ERR_CUDA, "graph launch failed");
         } else {
             if (enqueue_one(g, st) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "step launch failed");
@@ -427,6 +437,8 @@ extern "C" int fmd_system_kernel_ms(fmd_system* s, int stage, int reps, double* 
                                         a.list_a, a.cap_a, a.in_cnt, a.in_list, a.in_cap, a.n, a.Facc, a.Facc,
                                         a.part_f2, st);
             case 1:
+                if (a.kind == FMD_SYS_AIREBO && a.sg)   // the REBO term the step uses
+                    return sg_enqueue_rebo(*a.sg, a, false, st);
                 if (a.kind == FMD_SYS_AIREBO)
                     return rebo_launch(a.pos, hh, a.cnt_b, a.list_b, a.cap_b, a.n, a.Facc, a.part_f1, st);
                 if (a.kind == FMD_SYS_MM) return mm_bonded_launch(a.topo, a.pos, hh, a.Facc, a.part_f1, st);
@@ -470,7 +482,7 @@ extern "C" int fmd_system_step_kernels(fmd_system* s, int rebuild, int phase, in
     cudaGraph_t graph;
     if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
         return y.ctx->fail(FMD_ERR_CUDA, "capture failed");
-    cudaError_t e = y.enqueue_variant(rebuild != 0, phase != 0, st);
+    cudaError_t e = y.enqueue_variant(rebuild != 0, phase != 0, st, (phase & 2) != 0);
     cudaError_t e2 = cudaStreamEndCapture(st, &graph);
     if (e != cudaSuccess || e2 != cudaSuccess) return y.ctx->fail(FMD_ERR_CUDA, "capture failed");
     size_t n = 0;
@@ -495,6 +507,87 @@ extern "C" int fmd_system_destroy(fmd_system* s) {
         s->sys->release();
     }
     delete s;
+    return FMD_OK;
+}
+
+// ------------------------------------------------- learned REBO term ------
+int fmd::System::use_surrogate(fmd_sg* model, int judge_every, double rmse_max) {
+    cudaStream_t st = ctx->stream;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "fmd_system_use_surrogate: sync");
+    drop_graphs();                       // captured graphs hold the old REBO term
+    if (!model) {
+        arr.sg = nullptr;
+        arr.rebo_blocks = kForceBlocks;
+    } else {
+        if (!sg) {
+            auto g = std::make_unique<SgStep>();
+            if (sg::work_alloc(g->work, arr.n, arr.cap_b) != cudaSuccess)
+                return ctx->fail(FMD_ERR_CUDA, "fmd_system_use_surrogate: workspace allocation failed");
+            if (alloc(&g->Fj, 3 * (size_t)arr.n, (const double*)nullptr) ||
+                alloc(&g->part_j, (size_t)sg::kRowBlocks * kNV, (const double*)nullptr)) {
+                sg::work_free(g->work);
+                return ctx->fail(FMD_ERR_CUDA, "fmd_system_use_surrogate: allocation failed");
+            }
+            sg = std::move(g);
+        }
+        sg_model_images(model, &sg->img, &sg->vec);
+        sg->judge_every = judge_every;
+        sg->rmse_max = rmse_max;
+        arr.sg = sg.get();
+        arr.rebo_blocks = sg::kRowBlocks;
+        // part_f1 holds max(kForceBlocks, n) records; the learned term writes kRowBlocks.
+        if (std::max(kForceBlocks, arr.n) < sg::kRowBlocks) {
+            double* p1;
+            if (alloc(&p1, (size_t)sg::kRowBlocks * kNV, (const double*)nullptr))
+                return ctx->fail(FMD_ERR_CUDA, "fmd_system_use_surrogate: allocation failed");
+            arr.part_f1 = p1;
+        }
+    }
+    // fresh judge record: the learned term is active again
+    SysScal z;
+    std::memset(&z, 0, sizeof(z));
+    const size_t off = offsetof(SysScal, sg_off);
+    if (cudaMemcpyAsync(reinterpret_cast<char*>(arr.S) + off, reinterpret_cast<const char*>(&z) + off,
+                        sizeof(SysScal) - off, cudaMemcpyHostToDevice, st) != cudaSuccess)
+        return ctx->fail(FMD_ERR_CUDA, "fmd_system_use_surrogate: copy failed");
+    int rc = ctx->sync_check("fmd_system_use_surrogate");
+    if (rc != FMD_OK || !initialized) return rc;
+    // The forces of the current state come from the new REBO term.
+    if (enqueue_forces(arr, st) != cudaSuccess || enqueue_force_reduce(arr, st) != cudaSuccess)
+        return ctx->fail(FMD_ERR_CUDA, "fmd_system_use_surrogate: force launch failed");
+    if ((rc = ctx->sync_check("fmd_system_use_surrogate")) != FMD_OK) return rc;
+    if (p.use_graphs)
+        for (int r = 0; r < 2; r++)
+            for (int ph = 0; ph < 2; ph++)
+                for (int j = 0; j < 2; j++)
+                    if ((j == 0 || arr.sg) && (rc = capture(r != 0, ph != 0, j != 0)) != FMD_OK) return rc;
+    return FMD_OK;
+}
+
+extern "C" int fmd_system_use_surrogate(fmd_system* s, fmd_sg* model, int judge_every, double rmse_max) {
+    if (!s || !s->sys) return FMD_ERR_ARG;
+    fmd::System& y = *s->sys;
+    if (y.arr.kind != FMD_SYS_AIREBO)
+        return y.ctx->fail(FMD_ERR_ARG, "fmd_system_use_surrogate: not an AIREBO system");
+    if (model && (judge_every < 0 || !(rmse_max > 0.0)))
+        return y.ctx->fail(FMD_ERR_ARG, "fmd_system_use_surrogate: judge_every < 0 or rmse_max <= 0");
+    return y.use_surrogate(model, judge_every, rmse_max);
+}
+
+extern "C" int fmd_system_surrogate_status(fmd_system* s, fmd_sg_status* out) {
+    if (!s || !s->sys || !out) return FMD_ERR_ARG;
+    fmd::System& y = *s->sys;
+    SysScal h;
+    if (cudaMemcpyAsync(&h, y.arr.S, sizeof(h), cudaMemcpyDeviceToHost, y.ctx->stream) != cudaSuccess)
+        return y.ctx->fail(FMD_ERR_CUDA, "fmd_system_surrogate_status: copy failed");
+    int rc = y.ctx->sync_check("fmd_system_surrogate_status");
+    if (rc != FMD_OK) return rc;
+    out->attached = y.arr.sg != nullptr;
+    out->active = y.arr.sg != nullptr && h.sg_off == 0;
+    out->judged = h.sg_judged;
+    out->takeover_step = h.sg_takeover;
+    out->rmse_last = h.sg_rmse_last;
+    out->rmse_max = h.sg_rmse_max;
     return FMD_OK;
 }
 

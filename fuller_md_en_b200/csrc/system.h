@@ -1,6 +1,8 @@
 // system.h -- host-side owner of one device-resident system.
 #pragma once
+#include <memory>
 #include <vector>
+#include "sg_host.h"
 #include "step.h"
 
 namespace fmd {
@@ -17,18 +19,23 @@ struct System {
     double h0[9] = {0};
     int* dropped = nullptr;            // device: {list a, list b} overflow counts
     bool initialized = false;
-    cudaGraphExec_t graphs[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    // one graph per {rebuild, cold/warm phase, judge of the learned REBO term}
+    cudaGraphExec_t graphs[2][2][2] = {};
     std::vector<void*> owned;
+    std::unique_ptr<SgStep> sg;        // learned REBO term (AIREBO only), nullptr: plain
 
     template <class T> cudaError_t alloc(T** p, size_t count, const T* src);
     int alloc_common(const double* pos, const double* vel, const double* h, const fmd_npt* npt);
     int alloc_lists(double rc_list_a, int cap_a, double rc_list_b, int cap_b, bool transpose);
     int upload_topology(const fmd_mm_topology* t);
     cudaError_t enqueue_rebuild(cudaStream_t st);
-    cudaError_t enqueue_variant(bool rebuild, bool phase, cudaStream_t st);
+    cudaError_t enqueue_variant(bool rebuild, bool phase, cudaStream_t st, bool judge = false);
     cudaError_t enqueue_one(int g, cudaStream_t st);
+    bool judge_step(int g) const { return arr.sg && arr.sg->judge_every > 0 && g % arr.sg->judge_every == 0; }
     int init();
-    int capture(bool rebuild, bool phase);
+    int capture(bool rebuild, bool phase, bool judge = false);
+    void drop_graphs();
+    int use_surrogate(fmd_sg* model, int judge_every, double rmse_max);
     int run(int first, int last, fmd_obs* obs);
     int enqueue(int first, int last);
     int nonfinite_check();

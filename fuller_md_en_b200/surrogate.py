@@ -213,3 +213,57 @@ class Dataset:
             self.close()
         except Exception:
             pass
+
+
+def generate_dataset(ctx, nc: int = 5, runs: int = 40, steps: int = 50, every: int = 1,
+                     T_range=(300.0, 1500.0), P_range=(0.0, 5.0), jitter: float = 0.01, dt: float = 0.5,
+                     nlup: int = 20, seed: int = 0) -> "Dataset":
+    """Training snapshots from the plain AIREBO kernel's own trajectories.
+
+    `runs` short NPT runs of C60 FCC nc x nc x nc, each at a temperature and
+    pressure drawn uniformly from T_range (K) and P_range (GPa) with its own
+    seed, advance `steps` steps on the device; every `every` steps the state
+    is added (device to device) with its REBO energy, forces and virial from
+    the plain kernel.  The reference force field heats its crystal within
+    about a hundred steps (by then REBO rows fill their 12 slots, truncation
+    makes the list asymmetric and the states are no longer a C60 crystal), so
+    runs are kept to the first 50 steps."""
+    from . import crystal
+    from .api import RunConfig, System
+    rng = np.random.default_rng(seed)
+    data = Dataset(ctx)
+    for r in range(runs):
+        T = float(rng.uniform(*T_range))
+        P = float(rng.uniform(*P_range))
+        s = crystal.atomistic(nc, jitter=jitter, seed=int(rng.integers(1 << 30)), T=T)
+        na = s["pos"].size // 3
+        cfg = RunConfig(dt=dt, T=T, Pe=P, nsteps=steps, nlup=nlup, gavg_from=1, gavg_to=steps, nc=nc,
+                        nmol=s["nmol"])
+        sysd = System.airebo(ctx, cfg, s["pos"], s["vel"], s["mass"], s["mol_id"], s["h"],
+                             crystal.npt_atom(T, P, na))
+        sysd.init()
+        for g in range(1, steps + 1):
+            sysd.enqueue(g, g)
+            if g % every == 0:
+                data.add_system(sysd)
+        ctx.synchronize()
+        sysd.close()
+    return data
+
+
+def fit(ctx, data: "Dataset", steps: int = 2000, batch: int = 4, lr: float = 3e-3, lr_final: float = 3e-5,
+        wE: float = 0.1, wF: float = 1.0, wW: float = 0.1, n_train: int = 0, seed: int = 0,
+        b0: float = 0.9, bs: float = 0.05) -> tuple["Surrogate", np.ndarray]:
+    """A new model trained on the GPU: descriptor normalisation from the
+    training snapshots, then Adam with the tensor-core forward/backward
+    kernels.  Returns (model, history[steps, 2] = loss, batch force RMSE)."""
+    P = init_params(seed)
+    P["b0"], P["bs"] = b0, bs
+    S = Surrogate(ctx, P)
+    n = n_train if n_train > 0 else len(data)
+    m, sd = S.feature_stats(data, 0, n)
+    P["m"], P["s"] = m, sd + 1e-3
+    S.set_params(P)
+    hist = S.train(data, steps=steps, batch=batch, lr=lr, lr_final=lr_final, wE=wE, wF=wF, wW=wW, seed=seed,
+                   n_train=n)
+    return S, hist

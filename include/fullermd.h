@@ -240,7 +240,8 @@ int fmd_system_destroy(fmd_system *s);
  *   3 one complete step (eager launches).
  * The force stages leave F in place (they recompute the current forces).
  * fmd_system_step_kernels returns the number of kernel launches of one step
- * of each variant (list rebuild or not, cold/warm phase or not). */
+ * of each variant (list rebuild or not; phase bit 0: cold/warm phase, bit 1:
+ * a judge step of the learned REBO term). */
 int fmd_system_kernel_ms(fmd_system *s, int stage, int reps, double *ms_per_launch);
 int fmd_system_step_kernels(fmd_system *s, int rebuild, int phase, int *nkernels);
 
@@ -319,6 +320,29 @@ int fmd_sg_train(fmd_sg *s, fmd_sg_data *d, const fmd_sg_train_args *a, double *
 /* Force RMSE (eV/A) against the reference REBO forces of snapshots
  * [first, first+n): rmse[n]. */
 int fmd_sg_eval(fmd_sg *s, fmd_sg_data *d, int first, int n, double *rmse);
+
+/* Learned REBO term inside a device-resident AIREBO system (no counterpart
+ * in the reference).  From the next step on, the system's REBO term comes
+ * from `model`; the plain REBO kernel stays beside it as judge and fallback:
+ * on every global step divisible by judge_every (0: never) it evaluates the
+ * same positions, the force RMSE sqrt(mean_k (F_learned,k - F_plain,k)^2)
+ * over the 3n components is recorded, and if it exceeds rmse_max (eV/A) the
+ * plain result replaces the learned one for that step and the plain kernel
+ * takes over for the rest of the run.  Everything stays on the device and
+ * inside the step's CUDA graph.  model == NULL returns to the plain kernel.
+ * Each call resets the judge record; if the system is initialised, the
+ * current forces are recomputed with the new term.  The model must outlive
+ * its use by the system; fmd_sg_set_params takes effect at the next step. */
+typedef struct {
+    int attached;        /* a model is attached */
+    int active;          /* the learned term is in use (no takeover yet) */
+    int judged;          /* judge evaluations so far */
+    int takeover_step;   /* global step of the takeover, 0: none */
+    double rmse_last;    /* force RMSE of the last judge step, eV/A */
+    double rmse_max;     /* largest judged force RMSE, eV/A */
+} fmd_sg_status;
+int fmd_system_use_surrogate(fmd_system *s, fmd_sg *model, int judge_every, double rmse_max);
+int fmd_system_surrogate_status(fmd_system *s, fmd_sg_status *st);
 
 #ifdef __cplusplus
 }

@@ -243,6 +243,17 @@ def test_mm_step(ctx, golden):
         assert rel(st[k], g[f"step_{k}"]) < FP64_TOL, k
 
 
+def test_mat_inv9_on_a_fresh_context(oracle):
+    """The first call on a new context sizes its cell scratch for {h, hi}."""
+    from fuller_md_en_b200 import Context
+    c = Context(0)
+    h = crystal.atomistic(1, seed=3)["h"].copy()
+    h[3] += 0.4
+    assert np.array_equal(c.mat_inv9(h), oracle.mat_inv9(h))
+    assert np.array_equal(c.mat_inv9(h), oracle.mat_inv9(h))
+    c.close()
+
+
 def test_geometry_helpers(ctx, oracle):
     s = crystal.atomistic(1, jitter=0.3, seed=2)
     h = s["h"].copy()
