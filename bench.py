@@ -120,12 +120,16 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def make_system(ctx, rank: int):
+def make_system(ctx, rank: int, precision=None):
+    """The workload; the reference's FP64 pair arithmetic unless `precision`
+    says otherwise."""
     from fuller_md_en_b200 import RunConfig, System, crystal
+    from fuller_md_en_b200._lib import FMD_PREC_FP64
     s = crystal.atomistic(NC, jitter=JITTER, seed=SEED + rank, T=T_K)
     na = s["pos"].size // 3
     cfg = RunConfig(dt=DT, T=T_K, Pe=P_GPA, nsteps=10 ** 6, nlup=NLUP, gavg_from=1, gavg_to=10 ** 6, nc=NC,
-                    nmol=s["nmol"], use_graphs=1)
+                    nmol=s["nmol"], use_graphs=1,
+                    precision=FMD_PREC_FP64 if precision is None else precision)
     npt = crystal.npt_atom(T_K, P_GPA, na)
     return s, na, cfg, npt
 
@@ -138,6 +142,24 @@ def list_bytes(sysd, na):
     ca, la, cb, lb = sysd.lists(400, 12)
     n_out = int(ca.sum())
     return 2 * (n_out * 4) + 2 * na * 4 + na * 24 + 3 * na * 24, n_out
+
+
+def timed_steps(ctx, stream, sysd, K, flush):
+    """CUDA-event time (ms) of global steps 1..K of an initialised system,
+    L2 flushed before each step outside its window."""
+    import torch
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    torch.cuda.synchronize()
+    ctx.synchronize()
+    for k in range(K):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        ev[k][0].record(stream)
+        sysd.enqueue(1 + k, 1 + k)
+        ev[k][1].record(stream)
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    return [a.elapsed_time(b) for a, b in ev]
 
 
 def run_ours(args, ws, rank, local):
@@ -207,6 +229,16 @@ def run_ours(args, ws, rank, local):
     launches = sum(n_reb if (1 + k) % NLUP == 0 else n_prod for k in range(K))
     sysd.close()
 
+    # ---------------- the same steps with FP32 pair arithmetic ----------------
+    from fuller_md_en_b200._lib import FMD_PREC_FP32_PAIR
+    _, _, cfg32, _ = make_system(ctx, rank, precision=FMD_PREC_FP32_PAIR)
+    sys32 = System.airebo(ctx, cfg32, s["pos"], s["vel"], s["mass"], s["mol_id"], s["h"], npt)
+    sys32.init()
+    ms32 = float(sum(timed_steps(ctx, stream, sys32, K, flush)))
+    lj32_ms = sys32.kernel_ms(0, 20)
+    sys32.close()
+    value32 = ws * na * K / (ms32 / 1e3)
+
     # ---------------- learned surrogate on the same workload ----------------
     sg_res = None
     if not args.no_surrogate:
@@ -243,6 +275,9 @@ def run_ours(args, ws, rank, local):
         "metric": METRIC, "value": value, "unit": "atom-steps/s", "n_gpus": ws, "steps": K, "warmup": W,
         "ms_per_step": ms_total / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
+        "fp32_pair": {"value": value32, "ms_per_step": ms32 / K, "lj_gather_ms": lj32_ms,
+                      "note": "same steps with FP32 LJ pair algebra (FP64 minimum image, cutoff test and sums; "
+                              "energy/virial within 1e-6 of the FP64 oracle)"},
         "config": {"workload": WORKLOAD, "atoms_per_gpu": na, "global_atoms": na * ws,
                    "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
                    "l2": "flushed between timed steps (512 MB write outside the timed windows); "

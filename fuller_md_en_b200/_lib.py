@@ -73,6 +73,7 @@ _SIGS = {
     "fmd_ctx_set_stream": (c_int, [c_void_p, c_void_p]),
     "fmd_ctx_get_stream": (c_void_p, [c_void_p]),
     "fmd_ctx_synchronize": (c_int, [c_void_p]),
+    "fmd_ctx_set_precision": (c_int, [c_void_p, c_int]),
     "fmd_ctx_last_error": (c_char_p, [c_void_p]),
     "fmd_status_string": (c_char_p, [c_int]),
     "fmd_device_info": (c_int, [c_int, c_char_p, c_int, POINTER(c_double)]),

@@ -79,6 +79,11 @@ class Context:
     def stream(self) -> int:
         return int(self.lib.fmd_ctx_get_stream(self.h) or 0)
 
+    def set_precision(self, precision: int) -> None:
+        """Pair arithmetic of the atomistic LJ term in host-pointer calls
+        (_lib.FMD_PREC_FP64 or _lib.FMD_PREC_FP32_PAIR)."""
+        self.check(self.lib.fmd_ctx_set_precision(self.h, int(precision)), "fmd_ctx_set_precision")
+
     def synchronize(self) -> None:
         self.check(self.lib.fmd_ctx_synchronize(self.h), "synchronize")
 

@@ -128,7 +128,7 @@ namespace {
 enum Slot {
     S_POS = 0, S_HH, S_MOL, S_CNT, S_LIST, S_CNT2, S_LIST2, S_INCNT, S_INLIST, S_DROP,
     S_F, S_FACC, S_T, S_QV, S_BODY, S_VEL, S_OMG, S_MASS, S_PART1, S_PART2, S_PART3, S_PARTKE,
-    S_SCAL, S_CHARGE, S_TOPO0
+    S_SCAL, S_CHARGE, S_RSLOT, S_TOPO0
 };
 
 template <class T>
@@ -203,6 +203,14 @@ int list_call(fmd_ctx* ctx, int mode, const double* pos, const double* h, const 
 }
 
 }  // namespace
+
+extern "C" int fmd_ctx_set_precision(fmd_ctx* ctx, int precision) {
+    if (!ctx) return FMD_ERR_ARG;
+    if (precision != FMD_PREC_FP64 && precision != FMD_PREC_FP32_PAIR)
+        return ctx->fail(FMD_ERR_ARG, "fmd_ctx_set_precision: unknown precision");
+    ctx->precision = precision;
+    return FMD_OK;
+}
 
 extern "C" int fmd_mat_inv9(fmd_ctx* ctx, const double* h, double* hi) {
     if (!ctx || !h || !hi) return ctx ? ctx->fail(FMD_ERR_ARG, "fmd_mat_inv9: null") : FMD_ERR_ARG;
@@ -387,6 +395,7 @@ extern "C" int fmd_lj_rigid_forces(fmd_ctx* ctx, const double* pos, const double
         return ctx->fail(FMD_ERR_ARG, "fmd_lj_rigid_forces: bad argument");
     if (!list_ok(ctx, nl_count, nl_list, max_neigh, n, "molecule list")) return FMD_ERR_ARG;
     StepArrays a;
+    a.precision = ctx->precision;
     a.kind = FMD_SYS_RIGID; a.n = n; a.natom = natom; a.rmcut2 = rmcut2; a.precision = precision;
     double *dpos, *dq, *db, *dF, *dT;
     int *dc, *dl;
@@ -422,6 +431,7 @@ static int atom_term(fmd_ctx* ctx, int term, int ff, const double* pos, const do
     if (!pos || !h || !hi || !nlc || !nll || !F || !vir9 || !E || na < 1 || max_neigh < 1)
         return ctx->fail(FMD_ERR_ARG, "force term: bad argument");
     StepArrays a;
+    a.precision = ctx->precision;
     a.n = na;
     double *dpos, *dF, *dFacc, *hh;
     int rc = up(ctx, S_POS, pos, 3 * (size_t)na, &dpos);
@@ -437,7 +447,10 @@ static int atom_term(fmd_ctx* ctx, int term, int ff, const double* pos, const do
         rc = up(ctx, S_CNT2, nlc, na, &dc);
         if (!rc) rc = up(ctx, S_LIST2, nll, (size_t)na * max_neigh, &dl);
         if (rc) return rc;
-        if (rebo_launch(dpos, hh, dc, dl, max_neigh, na, dF, part, ctx->stream) != cudaSuccess)
+        double* slots;
+        if ((rc = up<double>(ctx, S_RSLOT, nullptr, (size_t)na * max_neigh * kReboSlotDoubles, &slots))) return rc;
+        if (rebo_slots_launch(dpos, hh, dc, dl, max_neigh, na, slots, dF, part, kForceBlocks, nullptr, 0,
+                              ctx->stream) != cudaSuccess)
             return ctx->fail(FMD_ERR_CUDA, "rebo launch failed");
     } else {
         if ((rc = upload_half_list(ctx, nlc, nll, max_neigh, na, a))) return rc;
@@ -445,7 +458,7 @@ static int atom_term(fmd_ctx* ctx, int term, int ff, const double* pos, const do
         if (cudaMemcpyAsync(dFacc, dF, sizeof(double) * 3 * na, cudaMemcpyDeviceToDevice, ctx->stream) != cudaSuccess)
             return ctx->fail(FMD_ERR_CUDA, "copy failed");
         if (lj_gather_launch(ff, dpos, hh, a.cnt_a, a.list_a, a.cap_a, a.in_cnt, a.in_list, a.in_cap, na, dF, dFacc,
-                             part, ctx->stream) != cudaSuccess)
+                             part, ctx->stream, ctx->precision) != cudaSuccess)
             return ctx->fail(FMD_ERR_CUDA, "lj launch failed");
     }
     double* red;
@@ -502,6 +515,7 @@ int airebo_lists(fmd_ctx* ctx, const int* nlc_r, const int* nll_r, const int* nl
     if (!rc) rc = up(ctx, S_LIST2, nll_r, (size_t)na * 12, &dl);
     if (rc) return rc;
     a.cnt_b = dc; a.list_b = dl; a.cap_b = 12;
+    if ((rc = up<double>(ctx, S_RSLOT, nullptr, (size_t)na * 12 * kReboSlotDoubles, &a.rebo_slots))) return rc;
     return upload_half_list(ctx, nlc_l, nll_l, 400, na, a);
 }
 
@@ -514,6 +528,7 @@ extern "C" int fmd_airebo_forces(fmd_ctx* ctx, const double* pos, const double* 
     if (!pos || !h || !hi || !nlc_r || !nll_r || !nlc_l || !nll_l || !F || !vir9 || !E3 || na < 1)
         return ctx->fail(FMD_ERR_ARG, "fmd_airebo_forces: bad argument");
     StepArrays a;
+    a.precision = ctx->precision;
     int rc = atom_setup(ctx, FMD_SYS_AIREBO, pos, h, hi, nullptr, nullptr, na, a);
     if (!rc) rc = airebo_lists(ctx, nlc_r, nll_r, nlc_l, nll_l, na, a);
     if (rc) return rc;
@@ -536,6 +551,7 @@ extern "C" int fmd_mm_forces(fmd_ctx* ctx, const fmd_mm_topology* t, const doubl
         (has_charge && (!charge || !mol_id)) || !topo_index_ok(t, na))
         return ctx->fail(FMD_ERR_ARG, "fmd_mm_forces: bad argument");
     StepArrays a;
+    a.precision = ctx->precision;
     int rc = atom_setup(ctx, FMD_SYS_MM, pos, h, hi, nullptr, nullptr, na, a);
     if (!rc) rc = upload_half_list(ctx, nlc, nll, 400, na, a);
     if (!rc) rc = upload_topo(ctx, t, a.topo);
@@ -577,6 +593,7 @@ extern "C" int fmd_rigid_step(fmd_ctx* ctx, double* pos, double* vel, double* qv
         return ctx->fail(FMD_ERR_ARG, "fmd_rigid_step: bad argument");
     if (!list_ok(ctx, nl_count, nl_list, max_neigh, n, "molecule list")) return FMD_ERR_ARG;
     StepArrays a;
+    a.precision = ctx->precision;
     a.kind = FMD_SYS_RIGID; a.n = n; a.natom = natom; a.rmcut2 = rmcut2; a.Mmol = Mmol; a.I0 = I0;
     a.precision = precision;
     double *dpos, *dvel, *dq, *dw, *dF, *dT, *db;
@@ -621,6 +638,7 @@ extern "C" int fmd_airebo_step(fmd_ctx* ctx, double* pos, double* vel, double* F
         !out4 || na < 1)
         return ctx->fail(FMD_ERR_ARG, "fmd_airebo_step: bad argument");
     StepArrays a;
+    a.precision = ctx->precision;
     int rc = atom_setup(ctx, FMD_SYS_AIREBO, pos, h, hi, vir9, npt, na, a);
     double *dvel, *dm;
     if (!rc) rc = up(ctx, S_VEL, vel, 3 * (size_t)na, &dvel);
@@ -652,6 +670,7 @@ extern "C" int fmd_mm_step(fmd_ctx* ctx, double* pos, double* vel, double* F, do
         (has_charge && (!charge || !mol_id)) || !topo_index_ok(t, na))
         return ctx->fail(FMD_ERR_ARG, "fmd_mm_step: bad argument");
     StepArrays a;
+    a.precision = ctx->precision;
     int rc = atom_setup(ctx, FMD_SYS_MM, pos, h, hi, vir9, npt, na, a);
     double* dvel;
     if (!rc) rc = up(ctx, S_VEL, vel, 3 * (size_t)na, &dvel);

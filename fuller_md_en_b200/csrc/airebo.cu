@@ -148,6 +148,151 @@ k_rebo(const double* __restrict__ pos, const double* __restrict__ hh, const int*
     block_sum_store<kNV>(acc, sm, part + (size_t)blockIdx.x * kNV);
 }
 
+// ------------------------------------------------- REBO on slot records --
+// The fast REBO path precomputes, once per step, the geometry of every
+// occupied REBO list slot (i, jn): the minimum-image bond vector d, r, 1/r,
+// f_c(r) and f_c'(r).  The bond kernel then reads these records instead of
+// recomputing each neighbour's image, square root and divisions for every
+// bond it takes part in (each slot is used by up to 4 (cap-1) bond terms).
+// The arithmetic is the reference's (AI:275-421) with cos = (d_a.d_b)/(r_a r_b)
+// evaluated as (d_a.d_b) (1/r_a)(1/r_b) and one reciprocal shared by G and G'.
+struct Slot {
+    double dx, dy, dz, r, rinv, fc, dfc, pad;
+};
+
+__global__ void __launch_bounds__(256)
+k_rebo_slots(const double* __restrict__ pos, const double* __restrict__ hh, const int* __restrict__ cnt,
+             const int* __restrict__ list, int cap, int na, Slot* __restrict__ sl,
+             const int* __restrict__ gate, int want) {
+    if (gate != nullptr && *gate != want) return;
+    __shared__ double s_hh[18];
+    if (threadIdx.x < 18) s_hh[threadIdx.x] = hh[threadIdx.x];
+    __syncthreads();
+    const long long tot = (long long)na * cap;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t / cap), jn = (int)(t % cap);
+        if (jn >= cnt[i]) continue;
+        double x, y, z;
+        bond_vec(pos, i, list[t], s_hh, s_hh + 9, x, y, z);
+        const double r = sqrt(norm2_rn(x, y, z));
+        Slot q;
+        q.dx = x; q.dy = y; q.dz = z; q.r = r; q.rinv = 1.0 / r;
+        // r > DMAX_CC is skipped by every use (AI:304, 370); f_c = 0 there.
+        q.fc = r > DMAX_CC ? 0.0 : sw_fc(r);
+        q.dfc = r > DMAX_CC ? 0.0 : sw_dfc(r);
+        q.pad = 0.0;
+        sl[t] = q;
+    }
+}
+
+__device__ __forceinline__ void ang_g_dg(double x, double& g, double& dg) {
+    const double c2 = G_C0 * G_C0, d2 = G_D0 * G_D0, hh = 1.0 + x, inv = 1.0 / (d2 + hh * hh);
+    g = G_A0 * (1.0 + c2 / d2 - c2 * inv);
+    dg = G_A0 * 2.0 * c2 * hh * inv * inv;
+}
+
+// Sum over centre c's other slots of f_c G(cos) for the bond c -> skip whose
+// vector is s*(bx,by,bz) with s = +-1 (AI:301-309).
+__device__ __forceinline__ double bo_sum_sl(const Slot* __restrict__ sl, const int* __restrict__ list, int cap,
+                                            int c, int m, int skip, double bx, double by, double bz, double rbinv) {
+    double gs = 0.0;
+    for (int kn = 0; kn < m; kn++) {
+        const size_t o = (size_t)c * cap + kn;
+        if (list[o] == skip) continue;
+        const Slot q = sl[o];
+        if (q.fc < 1e-15) continue;
+        const double ct = clamp1((bx * q.dx + by * q.dy + bz * q.dz) * (rbinv * q.rinv));
+        double g, dg;
+        ang_g_dg(ct, g, dg);
+        gs += q.fc * g;
+    }
+    return gs;
+}
+
+// Reference three-body forces on the neighbours of centre c (AI:361-419).
+__device__ __forceinline__ void bo_three_body_sl(double* __restrict__ F, const Slot* __restrict__ sl,
+                                                 const int* __restrict__ list, int cap, int c, int m, int skip,
+                                                 double bx, double by, double bz, double rbinv, double ux,
+                                                 double uy, double uz, double gs, double b, double fcut, double va) {
+    if (!(fabs(gs) > 1e-20 && va > 1e-20)) return;
+    const double dbp = -BO_DELTA * b / (1.0 + gs);
+    const double coeff = -(0.5 * fcut * va) * dbp;
+    double fcx = 0.0, fcy = 0.0, fcz = 0.0;
+    for (int kn = 0; kn < m; kn++) {
+        const size_t o = (size_t)c * cap + kn;
+        const int k = list[o];
+        if (k == skip) continue;
+        const Slot q = sl[o];
+        if (q.fc < 1e-15) continue;
+        const double rx = q.dx * q.rinv, ry = q.dy * q.rinv, rz = q.dz * q.rinv;
+        const double ct = clamp1((bx * q.dx + by * q.dy + bz * q.dz) * (rbinv * q.rinv));
+        double gv, dgv;
+        ang_g_dg(ct, gv, dgv);
+        const double a1 = coeff * q.dfc * gv, a2 = coeff * q.fc * dgv;
+        const double fx = a1 * rx + a2 * ((ux - ct * rx) * q.rinv);
+        const double fy = a1 * ry + a2 * ((uy - ct * ry) * q.rinv);
+        const double fz = a1 * rz + a2 * ((uz - ct * rz) * q.rinv);
+        atomic_add3(F, k, fx, fy, fz);
+        fcx -= fx; fcy -= fy; fcz -= fz;
+    }
+    atomic_add3(F, c, fcx, fcy, fcz);
+}
+
+__global__ void __launch_bounds__(128)
+k_rebo_sl(const Slot* __restrict__ sl, const int* __restrict__ cnt, const int* __restrict__ list, int cap, int na,
+          double* __restrict__ F, double* __restrict__ part, const int* __restrict__ gate, int want) {
+    if (gate != nullptr && *gate != want) return;
+    __shared__ double sm[32 * kNV];
+    double acc[kNV];
+#pragma unroll
+    for (int k = 0; k < kNV; k++) acc[k] = 0.0;
+    const long long total = (long long)na * kReboLanes;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t / kReboLanes), lane = (int)(t % kReboLanes);
+        const int m = cnt[i];
+        double fix = 0.0, fiy = 0.0, fiz = 0.0;
+        for (int jn = lane; jn < m; jn += kReboLanes) {
+            const size_t o = (size_t)i * cap + jn;
+            const int j = list[o];
+            if (j <= i) continue;
+            const Slot q = sl[o];
+            const double rij = q.r;
+            if (rij > DMAX_CC) continue;
+            const double fcut = q.fc, dfcut = q.dfc;
+            if (fcut < 1e-15 && dfcut == 0) continue;
+            const double dx = q.dx, dy = q.dy, dz = q.dz, rinv = q.rinv;
+            // V_R, V_A and derivatives (AI:173-183)
+            const double ea = A_CC * exp(-ALPHA_CC * rij);
+            const double qr = Q_CC * rinv;
+            const double vr = (1.0 + qr) * ea;
+            const double dvr = (-qr * rinv) * ea + (1.0 + qr) * (-ALPHA_CC) * ea;
+            const double e1 = exp(-BETA1_CC * rij), e2 = exp(-BETA2_CC * rij), e3 = exp(-BETA3_CC * rij);
+            const double va = B1_CC * e1 + B2_CC * e2 + B3_CC * e3;
+            const double dva = -BETA1_CC * B1_CC * e1 - BETA2_CC * B2_CC * e2 - BETA3_CC * B3_CC * e3;
+            const double ux = dx * rinv, uy = dy * rinv, uz = dz * rinv;
+            const int mj = cnt[j];
+            const double gij = bo_sum_sl(sl, list, cap, i, m, j, dx, dy, dz, rinv);
+            const double gji = bo_sum_sl(sl, list, cap, j, mj, i, -dx, -dy, -dz, rinv);
+            const double bij = 1.0 / sqrt(1.0 + gij), bji = 1.0 / sqrt(1.0 + gji);
+            const double bbar = 0.5 * (bij + bji);
+            acc[0] += fcut * (vr - bbar * va);
+            const double fpair = (dfcut * (vr - bbar * va) + fcut * (dvr - bbar * dva)) * rinv;
+            fix += fpair * dx; fiy += fpair * dy; fiz += fpair * dz;
+            atomic_add3(F, j, -fpair * dx, -fpair * dy, -fpair * dz);
+            const double d[3] = {dx, dy, dz};
+#pragma unroll
+            for (int a = 0; a < 3; a++)
+#pragma unroll
+                for (int b = 0; b < 3; b++) acc[1 + a * 3 + b] -= d[a] * fpair * d[b];
+            bo_three_body_sl(F, sl, list, cap, i, m, j, dx, dy, dz, rinv, ux, uy, uz, gij, bij, fcut, va);
+            bo_three_body_sl(F, sl, list, cap, j, mj, i, -dx, -dy, -dz, rinv, -ux, -uy, -uz, gji, bji, fcut, va);
+        }
+        if (fix != 0.0 || fiy != 0.0 || fiz != 0.0) atomic_add3(F, i, fix, fiy, fiz);
+    }
+    block_sum_store<kNV>(acc, sm, part + (size_t)blockIdx.x * kNV);
+}
+
 struct LJP {
     double sig2, c4, c24, rc2, vshift;
 };
@@ -179,26 +324,40 @@ __device__ __forceinline__ double mimg1(double d, double hii, double hii_inv) {
     return __dmul_rn(hii, s);
 }
 
-template <bool FULL_VIRIAL, bool COUNT>
-__device__ __forceinline__ void lj_pair(const double* __restrict__ pos, int j, double px, double py,
-                                        double pz, const double* h, const double* hi, bool diag, const LJP& p,
+// FP32 copies of the pair constants (FP32-pair precision).  sigma^2 is kept
+// as a head + tail pair: its FP32 rounding would scale every s^6 by the same
+// factor, a bias that the near-cancelling repulsive and attractive virial
+// sums amplify about tenfold; c4 and c24 scale both parts alike and stay single.
+struct LJF {
+    float sig2, sig2_lo, c4, c24;
+};
+
+// One listed pair seen from atom i: d = r_j - r_i after the minimum image.
+// The cutoff test is the reference's FP64 one in both precisions, so both
+// modes interact through exactly the reference's pair set.  FP64: the
+// reference's arithmetic (AI:447-466).  FP32: the pair algebra (1/r^2, s^6,
+// s^12, fm) in FP32; the minimum image, r^2, the force, energy and virial
+// accumulation stay FP64.  COUNT: this side counts energy and virial.
+template <bool FULL_VIRIAL, bool F32, bool COUNT>
+__device__ __forceinline__ void lj_pair(double dx, double dy, double dz, const LJP& p, const LJF& pf,
                                         double& fx, double& fy, double& fz, double* acc) {
-    double dx = __dsub_rn(pos[3 * j], px), dy = __dsub_rn(pos[3 * j + 1], py), dz = __dsub_rn(pos[3 * j + 2], pz);
-    if (diag) {
-        dx = mimg1(dx, h[0], hi[0]);
-        dy = mimg1(dy, h[4], hi[4]);
-        dz = mimg1(dz, h[8], hi[8]);
-    } else {
-        mimg(dx, dy, dz, hi, h);
-    }
     double r2 = norm2_rn(dx, dy, dz);
     if (r2 > p.rc2) return;
     if (r2 < 0.25) r2 = 0.25;
-    const double ri2 = 1.0 / r2, s2 = p.sig2 * ri2, s6 = s2 * s2 * s2, s12 = s6 * s6;
-    const double fm = p.c24 * (2 * s12 - s6) * ri2;
+    double fm, e = 0.0;
+    if (F32) {
+        const float ri2 = __frcp_rn((float)r2);
+        const float s2 = fmaf(pf.sig2, ri2, pf.sig2_lo * ri2), s6 = s2 * s2 * s2, s12 = s6 * s6;
+        fm = (double)(pf.c24 * (2.f * s12 - s6) * ri2);
+        if (COUNT) e = (double)(pf.c4 * (s12 - s6)) - p.vshift;
+    } else {
+        const double ri2 = 1.0 / r2, s2 = p.sig2 * ri2, s6 = s2 * s2 * s2, s12 = s6 * s6;
+        fm = p.c24 * (2 * s12 - s6) * ri2;
+        if (COUNT) e = p.c4 * (s12 - s6) - p.vshift;
+    }
     fx -= fm * dx; fy -= fm * dy; fz -= fm * dz;
     if (COUNT) {
-        acc[0] += p.c4 * (s12 - s6) - p.vshift;
+        acc[0] += e;
         if (FULL_VIRIAL) {
             const double d[3] = {dx, dy, dz};
 #pragma unroll
@@ -213,34 +372,69 @@ __device__ __forceinline__ void lj_pair(const double* __restrict__ pos, int j, d
     }
 }
 
-template <bool FULL_VIRIAL>
-__global__ void __launch_bounds__(256, 3)
+// Entries per lane in flight: the index loads of U entries are issued
+// together, then their positions, then the pair arithmetic, so one warp has
+// U dependent load chains outstanding instead of one.
+constexpr int kLJUnroll = 4;
+
+template <bool FULL_VIRIAL, bool F32>
+__global__ void __launch_bounds__(256, 2)
 k_lj_gather(const double* __restrict__ pos, const double* __restrict__ hh, const int* __restrict__ cnt,
             const int* __restrict__ list, int cap, const int* __restrict__ in_cnt,
             const int* __restrict__ in_list, int in_cap, int na, double* __restrict__ F,
             double* __restrict__ Facc, LJP p, double* __restrict__ part) {
     __shared__ double sm[32 * kNV];
+    __shared__ double s_hh[18];
+    if (threadIdx.x < 18) s_hh[threadIdx.x] = hh[threadIdx.x];
+    __syncthreads();
     const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
-    double h[9], hi[9];
-    load_cell(hh, h, hi);
+    const double* h = s_hh;
+    const double* hi = s_hh + 9;
     // Diagonal cell (FCC/BCC boxes under the diagonal barostat): uniform branch.
     const bool diag = h[1] == 0.0 && h[2] == 0.0 && h[3] == 0.0 && h[5] == 0.0 && h[6] == 0.0 && h[7] == 0.0 &&
                       hi[1] == 0.0 && hi[2] == 0.0 && hi[3] == 0.0 && hi[5] == 0.0 && hi[6] == 0.0 && hi[7] == 0.0;
+    const LJF pf{(float)p.sig2, (float)(p.sig2 - (double)(float)p.sig2), (float)p.c4, (float)p.c24};
     double acc[kNV];
 #pragma unroll
     for (int k = 0; k < kNV; k++) acc[k] = 0.0;
     for (int i = blockIdx.x * wpb + (threadIdx.x >> 5); i < na; i += gridDim.x * wpb) {
         const double px = pos[3 * i], py = pos[3 * i + 1], pz = pos[3 * i + 2];
         double fx = 0.0, fy = 0.0, fz = 0.0;
-        const int m = cnt[i];
+        // Outgoing entries (the reference row, j > i) then incoming ones
+        // (transposed rows, j < i) as one index range [0, mo + mi).
+        const int mo = cnt[i];
+        const int mi = min(in_cnt[i], in_cap);
+        const int tot = mo + mi;
         const int* row = list + (size_t)i * cap;
-        for (int k = lane; k < m; k += 32)
-            lj_pair<FULL_VIRIAL, true>(pos, row[k], px, py, pz, h, hi, diag, p, fx, fy, fz, acc);
-        int mi = in_cnt[i];
-        mi = mi < in_cap ? mi : in_cap;
-        const int* irow = in_list + (size_t)i * in_cap;
-        for (int k = lane; k < mi; k += 32)
-            lj_pair<FULL_VIRIAL, false>(pos, irow[k], px, py, pz, h, hi, diag, p, fx, fy, fz, acc);
+        const int* irow = in_list + (size_t)i * in_cap - mo;
+        for (int b = lane; b < tot; b += 32 * kLJUnroll) {
+            int jj[kLJUnroll];
+#pragma unroll
+            for (int u = 0; u < kLJUnroll; u++) {
+                const int k = b + 32 * u;
+                jj[u] = k < mo ? row[k] : (k < tot ? irow[k] : -1);
+            }
+            double qx[kLJUnroll], qy[kLJUnroll], qz[kLJUnroll];
+#pragma unroll
+            for (int u = 0; u < kLJUnroll; u++) {
+                const int j = jj[u] < 0 ? i : jj[u];
+                qx[u] = pos[3 * j]; qy[u] = pos[3 * j + 1]; qz[u] = pos[3 * j + 2];
+            }
+#pragma unroll
+            for (int u = 0; u < kLJUnroll; u++) {
+                if (jj[u] < 0) continue;
+                double dx = __dsub_rn(qx[u], px), dy = __dsub_rn(qy[u], py), dz = __dsub_rn(qz[u], pz);
+                if (diag) {
+                    dx = mimg1(dx, h[0], hi[0]);
+                    dy = mimg1(dy, h[4], hi[4]);
+                    dz = mimg1(dz, h[8], hi[8]);
+                } else {
+                    mimg(dx, dy, dz, hi, h);
+                }
+                if (b + 32 * u < mo) lj_pair<FULL_VIRIAL, F32, true>(dx, dy, dz, p, pf, fx, fy, fz, acc);
+                else lj_pair<FULL_VIRIAL, F32, false>(dx, dy, dz, p, pf, fx, fy, fz, acc);
+            }
+        }
         fx = warp_sum(fx); fy = warp_sum(fy); fz = warp_sum(fz);
         if (lane == 0) {
             F[3 * i] = Facc[3 * i] + fx;
@@ -286,14 +480,29 @@ cudaError_t rebo_launch_gated(const double* pos, const double* hh, const int* cn
     return cudaGetLastError();
 }
 
+cudaError_t rebo_slots_launch(const double* pos, const double* hh, const int* cnt, const int* list, int cap,
+                              int na, double* slots, double* F, double* part, int nblocks, const int* gate,
+                              int want, cudaStream_t st) {
+    Slot* sl = reinterpret_cast<Slot*>(slots);
+    k_rebo_slots<<<kForceBlocks, 256, 0, st>>>(pos, hh, cnt, list, cap, na, sl, gate, want);
+    k_rebo_sl<<<nblocks, 128, 0, st>>>(sl, cnt, list, cap, na, F, part, gate, want);
+    return cudaGetLastError();
+}
+
 cudaError_t lj_gather_launch(int ff, const double* pos, const double* hh, const int* cnt, const int* list,
                              int cap, const int* in_cnt, const int* in_list, int in_cap, int na, double* F,
-                             double* Facc, double* part, cudaStream_t st) {
+                             double* Facc, double* part, cudaStream_t st, int precision) {
     const LJP p = lj_params(ff);
-    if (ff == FMD_FF_AIREBO)
-        k_lj_gather<true><<<kForceBlocks, 256, 0, st>>>(pos, hh, cnt, list, cap, in_cnt, in_list, in_cap, na, F, Facc, p, part);
-    else
-        k_lj_gather<false><<<kForceBlocks, 256, 0, st>>>(pos, hh, cnt, list, cap, in_cnt, in_list, in_cap, na, F, Facc, p, part);
+    const bool f32 = precision == FMD_PREC_FP32_PAIR;
+#define FMD_LJ_ARGS pos, hh, cnt, list, cap, in_cnt, in_list, in_cap, na, F, Facc, p, part
+    if (ff == FMD_FF_AIREBO) {
+        if (f32) k_lj_gather<true, true><<<kForceBlocks, 256, 0, st>>>(FMD_LJ_ARGS);
+        else k_lj_gather<true, false><<<kForceBlocks, 256, 0, st>>>(FMD_LJ_ARGS);
+    } else {
+        if (f32) k_lj_gather<false, true><<<kForceBlocks, 256, 0, st>>>(FMD_LJ_ARGS);
+        else k_lj_gather<false, false><<<kForceBlocks, 256, 0, st>>>(FMD_LJ_ARGS);
+    }
+#undef FMD_LJ_ARGS
     return cudaGetLastError();
 }
 

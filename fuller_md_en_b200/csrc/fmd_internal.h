@@ -64,6 +64,8 @@ struct fmd_ctx {
     std::vector<fmd::DevBuf> scratch;
     // pinned staging for scalars
     double* h_scalars = nullptr;
+    // pair arithmetic of the atomistic LJ terms in host-pointer calls (fmd_precision)
+    int precision = FMD_PREC_FP64;
 
     int fail(int code, const std::string& m) {
         last_code = code;

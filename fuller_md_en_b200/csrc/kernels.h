@@ -67,12 +67,21 @@ cudaError_t rebo_launch_grid(const double* pos, const double* hh, const int* cnt
 cudaError_t rebo_launch_gated(const double* pos, const double* hh, const int* cnt, const int* list, int cap,
                               int na, double* F, double* part, int nblocks, const int* gate, int want,
                               cudaStream_t st);
+// REBO through per-slot geometry records (the fast path): `slots` holds
+// kReboSlotDoubles doubles per list slot (na * cap records, device scratch
+// owned by the caller); otherwise as rebo_launch_gated (gate may be null).
+constexpr int kReboSlotDoubles = 8;
+cudaError_t rebo_slots_launch(const double* pos, const double* hh, const int* cnt, const int* list, int cap,
+                              int na, double* slots, double* F, double* part, int nblocks, const int* gate,
+                              int want, cudaStream_t st);
 // Half-list LJ gather (a8, a14): F[i] = Facc[i] + LJ(i); Facc[i] zeroed
-// (Facc may alias F only if zero_acc == 0).  ff: FMD_FF_AIREBO / FMD_FF_MM.
+// (unless Facc == F).  ff: FMD_FF_AIREBO / FMD_FF_MM.  precision:
+// FMD_PREC_FP64 (the reference's arithmetic) or FMD_PREC_FP32_PAIR (pair
+// algebra in FP32, FP64 minimum image, cutoff test and accumulation).
 cudaError_t lj_gather_launch(int ff, const double* pos, const double* hh, const int* cnt,
                              const int* list, int cap, const int* in_cnt, const int* in_list,
                              int in_cap, int na, double* F, double* Facc, double* part,
-                             cudaStream_t st);
+                             cudaStream_t st, int precision = FMD_PREC_FP64);
 // Rigid site-site LJ (a5-a6): writes F, T; per-block {E, W9} partials (grid n).
 cudaError_t rigid_launch(int precision, const double* pos, const double* qv, const double* body,
                          const double* hh, const int* cnt, const int* list, int cap, int n,

@@ -62,10 +62,12 @@ cudaError_t sg_enqueue_rebo(SgStep& g, const StepArrays& a, bool judge, cudaStre
     cudaError_t e = sg::rebo_forces(g.work, g.img, g.vec, a.pos, hh, a.cnt_b, a.list_b, a.cap_b, a.n, a.Facc,
                                     a.part_f1, st, off);
     if (e != cudaSuccess) return e;
-    e = rebo_launch_gated(a.pos, hh, a.cnt_b, a.list_b, a.cap_b, a.n, a.Facc, a.part_f1, sg::kRowBlocks, off, 1, st);
+    e = rebo_slots_launch(a.pos, hh, a.cnt_b, a.list_b, a.cap_b, a.n, a.rebo_slots, a.Facc, a.part_f1,
+                          sg::kRowBlocks, off, 1, st);
     if (e != cudaSuccess || !judge) return e;
     if ((e = cudaMemsetAsync(g.Fj, 0, sizeof(double) * 3 * (size_t)a.n, st)) != cudaSuccess) return e;
-    e = rebo_launch_gated(a.pos, hh, a.cnt_b, a.list_b, a.cap_b, a.n, g.Fj, g.part_j, sg::kRowBlocks, off, 0, st);
+    e = rebo_slots_launch(a.pos, hh, a.cnt_b, a.list_b, a.cap_b, a.n, a.rebo_slots, g.Fj, g.part_j, sg::kRowBlocks,
+                          off, 0, st);
     if (e != cudaSuccess) return e;
     k_sg_judge<<<1, kJudgeThreads, 0, st>>>(a.S, a.Facc, g.Fj, g.part_j, a.part_f1, 3 * a.n, sg::kRowBlocks,
                                             g.rmse_max);

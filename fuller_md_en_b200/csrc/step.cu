@@ -371,16 +371,19 @@ cudaError_t enqueue_forces(const StepArrays& a, cudaStream_t st, bool judge) {
                          a.rmcut2, a.F, a.T, a.part_f1, st);
     } else if (a.kind == FMD_SYS_AIREBO) {
         if (a.sg) e = sg_enqueue_rebo(*a.sg, a, judge, st);
+        else if (a.rebo_slots)
+            e = rebo_slots_launch(a.pos, hh, a.cnt_b, a.list_b, a.cap_b, a.n, a.rebo_slots, a.Facc, a.part_f1,
+                                  kForceBlocks, nullptr, 0, st);
         else e = rebo_launch(a.pos, hh, a.cnt_b, a.list_b, a.cap_b, a.n, a.Facc, a.part_f1, st);
         if (e != cudaSuccess) return e;
         e = lj_gather_launch(FMD_FF_AIREBO, a.pos, hh, a.cnt_a, a.list_a, a.cap_a, a.in_cnt, a.in_list, a.in_cap,
-                             a.n, a.F, a.Facc, a.part_f2, st);
+                             a.n, a.F, a.Facc, a.part_f2, st, a.precision);
     } else {
         if ((e = mm_bonded_launch(a.topo, a.pos, hh, a.Facc, a.part_f1, st)) != cudaSuccess) return e;
         if (a.has_charge)
             if ((e = mm_coulomb_launch(a.pos, hh, a.charge, a.mol_id, a.n, a.Facc, a.part_f3, st)) != cudaSuccess) return e;
         e = lj_gather_launch(FMD_FF_MM, a.pos, hh, a.cnt_a, a.list_a, a.cap_a, a.in_cnt, a.in_list, a.in_cap,
-                             a.n, a.F, a.Facc, a.part_f2, st);
+                             a.n, a.F, a.Facc, a.part_f2, st, a.precision);
     }
     return e;
 }

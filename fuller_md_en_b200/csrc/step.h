@@ -46,6 +46,7 @@ struct StepArrays {
     const int* cnt_a = nullptr; const int* list_a = nullptr; int cap_a = 0;     // LJ half / rigid
     const int* in_cnt = nullptr; const int* in_list = nullptr; int in_cap = 0;  // LJ incoming
     const int* cnt_b = nullptr; const int* list_b = nullptr; int cap_b = 0;     // REBO
+    double* rebo_slots = nullptr;   // [n * cap_b * kReboSlotDoubles] REBO slot records (fast path)
     double* part_f1 = nullptr;  // REBO / rigid / bonded partials
     double* part_f2 = nullptr;  // LJ partials
     double* part_f3 = nullptr;  // Coulomb partials

@@ -95,6 +95,8 @@ int System::alloc_lists(double rc_list_a, int cap_a_, double rc_list_b, int cap_
         cudaMemsetAsync(lst, 0, sizeof(int) * (size_t)n * cap_b_, ctx->stream);
         arr.cnt_b = cnt; arr.list_b = lst;
         if (cells_alloc(cells_b, n, h0, rc_b) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "cell allocation failed");
+        if (alloc(&arr.rebo_slots, (size_t)n * cap_b_ * kReboSlotDoubles, (const double*)nullptr))
+            return ctx->fail(FMD_ERR_CUDA, "list allocation failed");
     }
     if (transpose) {
         arr.in_cap = kInCap;
@@ -286,6 +288,7 @@ extern "C" int fmd_system_create_airebo(fmd_ctx* ctx, const fmd_run_params* p, i
     if (make_params(p, *s) != FMD_OK) return ctx->fail(FMD_ERR_ARG, "bad run parameters");
     s->arr.kind = FMD_SYS_AIREBO;
     s->arr.n = na;
+    s->arr.precision = p->precision;
     int rc = s->alloc_common(pos, vel, h, npt);
     if (rc != FMD_OK) return rc;
     double* m; int* mid;
@@ -309,6 +312,7 @@ extern "C" int fmd_system_create_mm(fmd_ctx* ctx, const fmd_run_params* p, int n
     if (make_params(p, *s) != FMD_OK) return ctx->fail(FMD_ERR_ARG, "bad run parameters");
     s->arr.kind = FMD_SYS_MM;
     s->arr.n = na;
+    s->arr.precision = p->precision;
     int rc = s->alloc_common(pos, vel, h, npt);
     if (rc != FMD_OK) return rc;
     int* mid;
@@ -435,12 +439,13 @@ extern "C" int fmd_system_kernel_ms(fmd_system* s, int stage, int reps, double* 
                 // Timed into the scratch accumulator (F itself is left alone).
                 return lj_gather_launch(a.kind == FMD_SYS_AIREBO ? FMD_FF_AIREBO : FMD_FF_MM, a.pos, hh, a.cnt_a,
                                         a.list_a, a.cap_a, a.in_cnt, a.in_list, a.in_cap, a.n, a.Facc, a.Facc,
-                                        a.part_f2, st);
+                                        a.part_f2, st, a.precision);
             case 1:
                 if (a.kind == FMD_SYS_AIREBO && a.sg)   // the REBO term the step uses
                     return sg_enqueue_rebo(*a.sg, a, false, st);
                 if (a.kind == FMD_SYS_AIREBO)
-                    return rebo_launch(a.pos, hh, a.cnt_b, a.list_b, a.cap_b, a.n, a.Facc, a.part_f1, st);
+                    return rebo_slots_launch(a.pos, hh, a.cnt_b, a.list_b, a.cap_b, a.n, a.rebo_slots, a.Facc,
+                                             a.part_f1, kForceBlocks, nullptr, 0, st);
                 if (a.kind == FMD_SYS_MM) return mm_bonded_launch(a.topo, a.pos, hh, a.Facc, a.part_f1, st);
                 return rigid_launch(a.precision, a.pos, a.qv, a.body, hh, a.cnt_a, a.list_a, a.cap_a, a.n, a.natom,
                                     a.rmcut2, a.F, a.T, a.part_f1, st);

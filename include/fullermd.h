@@ -42,7 +42,8 @@ enum fmd_status {
 
 enum fmd_precision {
     FMD_PREC_FP64 = 0,      /* all pair arithmetic in FP64 */
-    FMD_PREC_FP32_PAIR = 1  /* pair arithmetic in FP32, per-molecule sums in FP64 */
+    FMD_PREC_FP32_PAIR = 1  /* pair arithmetic in FP32; minimum image, cutoff tests
+                               and force/energy/virial sums in FP64 */
 };
 
 enum fmd_forcefield { FMD_FF_AIREBO = 0, FMD_FF_MM = 1 };
@@ -74,6 +75,10 @@ int fmd_ctx_destroy(fmd_ctx *ctx);
 int fmd_ctx_set_stream(fmd_ctx *ctx, void *cuda_stream);
 void *fmd_ctx_get_stream(fmd_ctx *ctx);
 int fmd_ctx_synchronize(fmd_ctx *ctx);
+/* Pair arithmetic of the atomistic LJ term (AIREBO and MM) in this context's
+ * host-pointer calls (fmd_precision; default FMD_PREC_FP64, the reference's
+ * arithmetic).  No counterpart in the reference. */
+int fmd_ctx_set_precision(fmd_ctx *ctx, int precision);
 const char *fmd_ctx_last_error(const fmd_ctx *ctx);
 const char *fmd_status_string(int code);
 /* Device name and total memory in GiB (the drivers' banner; replaces the
@@ -178,7 +183,8 @@ typedef struct {
     int gavg_from, gavg_to;          /* global-step averaging window */
     int nc;                          /* lattice repeats, for a = h[0]/nc */
     int nmol;                        /* energies are reported per molecule */
-    int precision;                   /* fmd_precision (rigid pair kernel) */
+    int precision;                   /* fmd_precision of the pair kernel (rigid site-site
+                                        LJ, atomistic LJ of AIREBO and MM) */
     int use_graphs;                  /* 1: replay steps as CUDA graphs */
 } fmd_run_params;
 

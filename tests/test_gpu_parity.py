@@ -174,6 +174,32 @@ def test_rigid_forces_fp32_pair(ctx, golden, nc):
     assert rel(F, g["F"]) < 1e-4 and rel(T, g["T"]) < 1e-4
 
 
+@pytest.mark.parametrize("nc,mm", [(5, False), (3, True)])
+def test_atomistic_lj_fp32_pair(ctx, oracle, nc, mm):
+    """FP32 pair algebra in the atomistic LJ gather (AIREBO at the benchmark
+    size, 30,000 atoms; MM at nc=3): energy and virial within 1e-6 of the
+    FP64 oracle, the same pair set (the cutoff test stays FP64)."""
+    from fuller_md_en_b200._lib import FMD_FF_AIREBO, FMD_PREC_FP64
+    s = crystal.atomistic(nc, jitter=0.01, seed=9)
+    na = s["pos"].size // 3
+    pos = s["pos"].copy()
+    oracle.apply_pbc(pos, s["h"], s["hi"])
+    cl, ll, _ = ctx.build_nlist_lj(pos, s["h"], s["hi"], na, s["mol_id"], rc_list=RC_MM if mm else RC_AI)
+    oe, oF, oW = oracle.lj(pos, s["h"], s["hi"], cl, ll, na, mm=mm)
+    F, W = np.zeros(3 * na), np.zeros(9)
+    ctx.set_precision(FMD_PREC_FP32_PAIR)
+    try:
+        e = ctx.compute_lj(F, W, pos, s["h"], s["hi"], cl, ll, na, ff=FMD_FF_MM if mm else FMD_FF_AIREBO)
+    finally:
+        ctx.set_precision(FMD_PREC_FP64)
+    assert abs(e - oe) < 1e-6 * abs(oe), (e, oe)
+    assert np.max(np.abs(W - oW)) < 1e-6 * np.linalg.norm(oW)
+    assert rel(F, oF) < 1e-4
+    F64, W64 = np.zeros(3 * na), np.zeros(9)
+    e64 = ctx.compute_lj(F64, W64, pos, s["h"], s["hi"], cl, ll, na, ff=FMD_FF_MM if mm else FMD_FF_AIREBO)
+    assert abs(e64 - oe) < FP64_TOL * abs(oe) and rel(F64, oF) < FP64_TOL and rel(W64, oW) < FP64_TOL
+
+
 def _mm_topo(g):
     from fuller_md_en_b200 import Topology
     t = {k[5:]: g[k] for k in g if k.startswith("topo_")}
