@@ -244,6 +244,11 @@ def run_ours(args, ws, rank, local):
     if not args.no_surrogate:
         sg_res = run_surrogate(args, ctx, stream, s, na, cfg, npt, flush, ws, local, value)
 
+    # ---------------- batched MM replicas (uneven sizes, one launch per phase) ----------------
+    batch_res = None
+    if not args.no_batch:
+        batch_res = run_batch(args, ctx, stream, flush, ws, rank)
+
     # ---------------- end to end through the public API ----------------
     e2e = None
     if rank == 0 or ws > 1:
@@ -293,8 +298,44 @@ def run_ours(args, ws, rank, local):
         "clocks": clk,
         "e2e": e2e,
         "surrogate": sg_res,
+        "batch": batch_res,
     }
     return res
+
+
+def run_batch(args, ctx, stream, flush, ws, rank):
+    """64 MM replicas of C60 FCC, nc in {2,3,4,5} round-robin (16 each of
+    1,920 / 6,480 / 15,360 / 30,000 atoms), T ~ U(100,1000) K, P ~ U(0,5) GPa,
+    dt 0.1 fs: each step phase one launch over all replicas, launch shapes
+    from the autotuner; steps 1..K timed with CUDA events."""
+    from fuller_md_en_b200 import Batch, mm_replica
+    rng = np.random.default_rng(SEED + 7 * rank)
+    R = 64
+    t0 = time.perf_counter()
+    reps = [mm_replica(ctx, 2 + r % 4, float(rng.uniform(100.0, 1000.0)), float(rng.uniform(0.0, 5.0)),
+                       seed=SEED + 1000 * rank + r, jitter=0.01) for r in range(R)]
+    t1 = time.perf_counter()
+    b = Batch(ctx, reps, autotune=True)
+    t2 = time.perf_counter()
+    atoms = sum(s.n for s in reps)
+    K = args.steps
+    step_ms = timed_steps(ctx, stream, b, K, flush)
+    obs = b.observables()
+    if not all(math.isfinite(o.E[6]) for o in obs):
+        raise RuntimeError("non-finite energy in the batched replicas")
+    ms = float(sum(step_ms))
+    tune = b.tuning()
+    nk = [b.step_kernels(False), b.step_kernels(True)]
+    b.close()
+    for s_ in reps:
+        s_.close()
+    return {"value": ws * atoms * K / (ms / 1e3), "unit": "atom-steps/s", "ms_per_step": ms / K,
+            "replicas": R, "atoms": atoms, "sizes": "16 x {1920, 6480, 15360, 30000}",
+            "workload": "MM (bond+angle+dihedral+improper+LJ; reference charges are zero, so no Coulomb), "
+                        "C60 FCC nc in {2,3,4,5} round-robin, T ~ U(100,1000) K, P ~ U(0,5) GPa, dt 0.1 fs, "
+                        "lists every 20 steps",
+            "kernels_per_step": {"plain": nk[0], "rebuild": nk[1]},
+            "tuning": tune, "setup_s": {"systems": t1 - t0, "batch_and_autotune": t2 - t1}}
 
 
 def run_surrogate(args, ctx, stream, s, na, cfg, npt, flush, ws, local, plain_value):
@@ -452,6 +493,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-surrogate", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--sg-train-steps", type=int, default=6000)
     args = ap.parse_args()
     if args.warmup < 3:

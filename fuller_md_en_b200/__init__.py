@@ -4,6 +4,6 @@ C-ABI (include/fullermd.h, libfullermd_cuda.so), with C++ drop-in drivers
 (fuller_*_gpu) and this Python mirror of the reference routines.
 """
 from ._lib import FmdError, load, LIB_PATH  # noqa: F401
-from .api import Context, System, Topology, RunConfig  # noqa: F401
+from .api import Batch, Context, System, Topology, RunConfig, mm_replica  # noqa: F401
 
-__all__ = ["Context", "System", "Topology", "RunConfig", "FmdError", "load", "LIB_PATH"]
+__all__ = ["Batch", "Context", "System", "Topology", "RunConfig", "mm_replica", "FmdError", "load", "LIB_PATH"]

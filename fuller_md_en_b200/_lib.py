@@ -61,6 +61,13 @@ class SgStatus(ctypes.Structure):
                 ("rmse_last", c_double), ("rmse_max", c_double)]
 
 
+class BatchTuning(ctypes.Structure):
+    """fmd_batch_tuning: launch shapes the batch autotuner chose."""
+    _fields_ = [("lj_threads", c_int), ("lj_unroll", c_int), ("lj_atoms_per_block", c_int),
+                ("bonded_threads", c_int), ("bonded_terms_per_block", c_int), ("lj_ms", c_double),
+                ("bonded_ms", c_double), ("blocks_lj", c_int), ("blocks_bonded", c_int), ("blocks_atom", c_int)]
+
+
 class Avg(ctypes.Structure):
     _fields_ = [("n", c_int), ("sT", c_double), ("sP", c_double), ("sa", c_double), ("sE", c_double * 8)]
 
@@ -135,6 +142,13 @@ _SIGS = {
     "fmd_sg_eval": (c_int, [c_void_p, c_void_p, c_int, c_int, _dp]),
     "fmd_sg_feature_stats": (c_int, [c_void_p, c_void_p, c_int, c_int, _dp, _dp]),
     "fmd_system_use_surrogate": (c_int, [c_void_p, c_void_p, c_int, c_double]),
+    "fmd_batch_create": (c_int, [c_void_p, c_int, POINTER(c_void_p), c_int, POINTER(c_void_p)]),
+    "fmd_batch_run": (c_int, [c_void_p, c_int, c_int]),
+    "fmd_batch_enqueue": (c_int, [c_void_p, c_int, c_int]),
+    "fmd_batch_observables": (c_int, [c_void_p, POINTER(Obs)]),
+    "fmd_batch_get_tuning": (c_int, [c_void_p, POINTER(BatchTuning)]),
+    "fmd_batch_step_kernels": (c_int, [c_void_p, c_int, c_int, POINTER(c_int)]),
+    "fmd_batch_destroy": (c_int, [c_void_p]),
     "fmd_system_surrogate_status": (c_int, [c_void_p, POINTER(SgStatus)]),
 }
 

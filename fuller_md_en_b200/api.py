@@ -436,3 +436,70 @@ class System:
             self.close()
         except Exception:
             pass
+
+
+class Batch:
+    """Replicas advanced together (fmd_batch): MM systems of one context,
+    each phase of a step one launch over all of them.  The systems stay
+    usable for download/averages/lists and must outlive the batch."""
+
+    def __init__(self, ctx: Context, systems: list, autotune: bool = True):
+        self.ctx = ctx
+        self.systems = list(systems)
+        arr = (ctypes.c_void_p * len(self.systems))(*[s.h.value if isinstance(s.h, ctypes.c_void_p) else s.h
+                                                       for s in self.systems])
+        out = ctypes.c_void_p()
+        ctx.check(ctx.lib.fmd_batch_create(ctx.h, len(self.systems), arr, int(autotune), ctypes.byref(out)),
+                  "fmd_batch_create")
+        self.h = out
+
+    def enqueue(self, first: int, last: int) -> None:
+        self.ctx.check(self.ctx.lib.fmd_batch_enqueue(self.h, first, last), "fmd_batch_enqueue")
+
+    def run(self, first: int, last: int) -> list:
+        self.ctx.check(self.ctx.lib.fmd_batch_run(self.h, first, last), "fmd_batch_run")
+        return self.observables()
+
+    def observables(self) -> list:
+        obs = (Obs * len(self.systems))()
+        self.ctx.check(self.ctx.lib.fmd_batch_observables(self.h, obs), "fmd_batch_observables")
+        return list(obs)
+
+    def tuning(self) -> dict:
+        t = _lib.BatchTuning()
+        self.ctx.check(self.ctx.lib.fmd_batch_get_tuning(self.h, ctypes.byref(t)), "fmd_batch_get_tuning")
+        return {k: getattr(t, k) for k, _ in t._fields_}
+
+    def step_kernels(self, rebuild: bool, phase: bool = False) -> int:
+        k = ctypes.c_int(0)
+        self.ctx.check(self.ctx.lib.fmd_batch_step_kernels(self.h, int(rebuild), int(phase), ctypes.byref(k)),
+                       "fmd_batch_step_kernels")
+        return k.value
+
+    def close(self) -> None:
+        if self.h:
+            self.ctx.lib.fmd_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def mm_replica(ctx: Context, nc: int, T: float, P: float, dt: float = 0.1, seed: int = 42, nlup: int = 20,
+               nsteps: int = 10 ** 6, jitter: float = 0.0, precision: int = _lib.FMD_PREC_FP64) -> System:
+    """An MM system of C60 FCC nc x nc x nc (Ih C60 geometry, reference force
+    constants) at temperature T (K) and pressure P (GPa), not yet initialised."""
+    from . import crystal
+    coords = crystal.c60_ih()
+    bonds = crystal.bonds_from_geometry(coords)
+    s = crystal.atomistic(nc, coords=coords, jitter=jitter, seed=seed, T=T, mol_base=0)
+    na, nmol = s["pos"].size // 3, s["nmol"]
+    t = crystal.mm_topology(coords, bonds, nmol)
+    topo = Topology(t["bonds"], t["kb"], t["r0"], t["angles"], t["kth"], t["th0"], t["dihedrals"], t["vn"],
+                    t["mult"], t["gamma"], t["impropers"], t["ki"], t["igamma"])
+    cfg = RunConfig(dt=dt, T=T, Pe=P, nsteps=nsteps, nlup=nlup, gavg_from=1, gavg_to=nsteps, nc=nc, nmol=nmol,
+                    precision=precision)
+    return System.mm(ctx, cfg, s["pos"], s["vel"], s["mol_id"], topo, s["h"], crystal.npt_atom(T, P, na))

@@ -178,3 +178,78 @@ def rigid(nc: int, coords: np.ndarray | None = None, T: float = 300.0, seed: int
     return {"pos": centres.reshape(-1).copy(), "vel": vel.reshape(-1).copy(), "omg": omg.reshape(-1).copy(),
             "qv": qv.reshape(-1).copy(), "body": coords.reshape(-1).copy(), "h": h, "hi": inv9(h), "n": n,
             "natom": natom, "I0": i0, "Mmol": mmol, "Rmol": rmol, "a0": a0}
+
+
+KCAL2EV = 1.0 / 23.06054783          # MM:111
+
+
+def _dihedral0(c, i, j, k, l) -> float:
+    """Reference dihedral angle of four atoms (MM:240-252)."""
+    b1 = [c[j][a] - c[i][a] for a in range(3)]
+    b2 = [c[k][a] - c[j][a] for a in range(3)]
+    b3 = [c[l][a] - c[k][a] for a in range(3)]
+    mx, my, mz = b1[1] * b2[2] - b1[2] * b2[1], b1[2] * b2[0] - b1[0] * b2[2], b1[0] * b2[1] - b1[1] * b2[0]
+    nx, ny, nz = b2[1] * b3[2] - b2[2] * b3[1], b2[2] * b3[0] - b2[0] * b3[2], b2[0] * b3[1] - b2[1] * b3[0]
+    mm, nn = mx * mx + my * my + mz * mz, nx * nx + ny * ny + nz * nz
+    if mm < 1e-20 or nn < 1e-20:
+        return 0.0
+    b2len = math.sqrt(b2[0] * b2[0] + b2[1] * b2[1] + b2[2] * b2[2])
+    cp = (mx * nx + my * ny + mz * nz) / math.sqrt(mm * nn)
+    cp = min(max(cp, -1.0), 1.0)
+    sp = (mx * b3[0] + my * b3[1] + mz * b3[2]) * b2len / math.sqrt(mm * nn)
+    return math.atan2(sp, cp)
+
+
+def mm_topology(coords: np.ndarray, bonds: np.ndarray, nmol: int, kb: float = 469.0, kth: float = 63.0,
+                v2: float = 14.5, kimp: float = 15.0) -> dict:
+    """Flat MM topology of nmol copies of one molecule (build_flat_topology,
+    MM:254-334): bonds from the sorted bond pairs with r0 from the geometry,
+    angles i-j-k over each atom's neighbour pairs, dihedrals i-j-k-l over each
+    bond, impropers on three-coordinated atoms, gamma = 2 phi0 + pi; force
+    constants in kcal/mol converted to eV; copy m offsets indices by m natom."""
+    c = [tuple(float(x) for x in row) for row in np.asarray(coords, np.float64).reshape(-1, 3)]
+    na = len(c)
+    bl = [(int(a), int(b)) for a, b in np.asarray(bonds, np.int64).reshape(-1, 2)]
+    adj = [[] for _ in range(na)]
+    for a, b in bl:
+        adj[a].append(b)
+        adj[b].append(a)
+    # sqrt of the same left-to-right sum of squares as the reference
+    br0 = [math.sqrt((c[a][0] - c[b][0]) * (c[a][0] - c[b][0]) + (c[a][1] - c[b][1]) * (c[a][1] - c[b][1]) +
+                     (c[a][2] - c[b][2]) * (c[a][2] - c[b][2])) for a, b in bl]
+    an, ath = [], []
+    for j in range(na):
+        for ii in range(len(adj[j])):
+            for kk in range(ii + 1, len(adj[j])):
+                i, k = adj[j][ii], adj[j][kk]
+                u = [c[i][q] - c[j][q] for q in range(3)]
+                v = [c[k][q] - c[j][q] for q in range(3)]
+                du = math.sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2])
+                dv = math.sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2])
+                ct = min(max((u[0] * v[0] + u[1] * v[1] + u[2] * v[2]) / (du * dv), -1.0), 1.0)
+                an.append((i, j, k))
+                ath.append(math.acos(ct))
+    dh, dg = [], []
+    for bj, bk in bl:
+        for i in adj[bj]:
+            if i == bk:
+                continue
+            for l in adj[bk]:
+                if l == bj or l == i:
+                    continue
+                dh.append((i, bj, bk, l))
+                dg.append(2 * _dihedral0(c, i, bj, bk, l) + math.pi)
+    im, ig = [], []
+    for i in range(na):
+        if len(adj[i]) == 3:
+            j, k, l = adj[i]
+            im.append((i, j, k, l))
+            ig.append(2 * _dihedral0(c, j, i, k, l) + math.pi)
+    rep = lambda a: np.concatenate([np.asarray(a, np.int32) + m * na for m in range(nmol)])
+    tile = lambda a: np.tile(np.asarray(a, np.float64), nmol)
+    return {"bonds": rep(bl), "kb": np.full(len(bl) * nmol, kb * KCAL2EV), "r0": tile(br0),
+            "angles": rep(an), "kth": np.full(len(an) * nmol, kth * KCAL2EV), "th0": tile(ath),
+            "dihedrals": rep(dh), "vn": np.full(len(dh) * nmol, v2 * KCAL2EV),
+            "mult": np.full(len(dh) * nmol, 2, np.int32), "gamma": tile(dg),
+            "impropers": rep(im), "ki": np.full(len(im) * nmol, kimp * KCAL2EV), "igamma": tile(ig),
+            "mol_id": np.repeat(np.arange(nmol, dtype=np.int32), na)}

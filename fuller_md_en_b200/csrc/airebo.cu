@@ -19,6 +19,7 @@
 #include "kernels.h"
 #include "geom.cuh"
 #include "rebo_fn.cuh"
+#include "step.h"
 
 namespace fmd {
 namespace {
@@ -298,7 +299,7 @@ struct LJP {
 };
 
 // Reference constants, computed with the reference's expressions.
-LJP lj_params(int ff) {
+__host__ __device__ LJP lj_params_dev(int ff) {
     LJP p;
     if (ff == FMD_FF_AIREBO) {  // AI:119-124
         const double sig = 3.40, eps = 2.84e-3, rc = 3.0 * sig;
@@ -313,6 +314,7 @@ LJP lj_params(int ff) {
     }
     return p;
 }
+LJP lj_params(int ff) { return lj_params_dev(ff); }
 
 // One component of the minimum image for a diagonal cell.  With zero
 // off-diagonals the reference's s = hi0*dx + hi1*dy + hi2*dz and
@@ -377,14 +379,15 @@ __device__ __forceinline__ void lj_pair(double dx, double dy, double dz, const L
 // U dependent load chains outstanding instead of one.
 constexpr int kLJUnroll = 4;
 
-template <bool FULL_VIRIAL, bool F32>
-__global__ void __launch_bounds__(256, 2)
-k_lj_gather(const double* __restrict__ pos, const double* __restrict__ hh, const int* __restrict__ cnt,
-            const int* __restrict__ list, int cap, const int* __restrict__ in_cnt,
-            const int* __restrict__ in_list, int in_cap, int na, double* __restrict__ F,
-            double* __restrict__ Facc, LJP p, double* __restrict__ part) {
-    __shared__ double sm[32 * kNV];
-    __shared__ double s_hh[18];
+// One gather pass over atoms blk, blk + nblk, ... (in warps) of one system;
+// per-block {E, W9} into part[blk].  sm: 32 * kNV doubles, s_hh: 18.
+template <bool FULL_VIRIAL, bool F32, int U>
+__device__ __forceinline__ void lj_gather_body(const double* __restrict__ pos, const double* __restrict__ hh,
+                                               const int* __restrict__ cnt, const int* __restrict__ list, int cap,
+                                               const int* __restrict__ in_cnt, const int* __restrict__ in_list,
+                                               int in_cap, int na, double* __restrict__ F,
+                                               double* __restrict__ Facc, const LJP& p, double* __restrict__ part,
+                                               int blk, int nblk, double* sm, double* s_hh) {
     if (threadIdx.x < 18) s_hh[threadIdx.x] = hh[threadIdx.x];
     __syncthreads();
     const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
@@ -397,7 +400,7 @@ k_lj_gather(const double* __restrict__ pos, const double* __restrict__ hh, const
     double acc[kNV];
 #pragma unroll
     for (int k = 0; k < kNV; k++) acc[k] = 0.0;
-    for (int i = blockIdx.x * wpb + (threadIdx.x >> 5); i < na; i += gridDim.x * wpb) {
+    for (int i = blk * wpb + (threadIdx.x >> 5); i < na; i += nblk * wpb) {
         const double px = pos[3 * i], py = pos[3 * i + 1], pz = pos[3 * i + 2];
         double fx = 0.0, fy = 0.0, fz = 0.0;
         // Outgoing entries (the reference row, j > i) then incoming ones
@@ -407,21 +410,21 @@ k_lj_gather(const double* __restrict__ pos, const double* __restrict__ hh, const
         const int tot = mo + mi;
         const int* row = list + (size_t)i * cap;
         const int* irow = in_list + (size_t)i * in_cap - mo;
-        for (int b = lane; b < tot; b += 32 * kLJUnroll) {
-            int jj[kLJUnroll];
+        for (int b = lane; b < tot; b += 32 * U) {
+            int jj[U];
 #pragma unroll
-            for (int u = 0; u < kLJUnroll; u++) {
+            for (int u = 0; u < U; u++) {
                 const int k = b + 32 * u;
                 jj[u] = k < mo ? row[k] : (k < tot ? irow[k] : -1);
             }
-            double qx[kLJUnroll], qy[kLJUnroll], qz[kLJUnroll];
+            double qx[U], qy[U], qz[U];
 #pragma unroll
-            for (int u = 0; u < kLJUnroll; u++) {
+            for (int u = 0; u < U; u++) {
                 const int j = jj[u] < 0 ? i : jj[u];
                 qx[u] = pos[3 * j]; qy[u] = pos[3 * j + 1]; qz[u] = pos[3 * j + 2];
             }
 #pragma unroll
-            for (int u = 0; u < kLJUnroll; u++) {
+            for (int u = 0; u < U; u++) {
                 if (jj[u] < 0) continue;
                 double dx = __dsub_rn(qx[u], px), dy = __dsub_rn(qy[u], py), dz = __dsub_rn(qz[u], pz);
                 if (diag) {
@@ -443,7 +446,34 @@ k_lj_gather(const double* __restrict__ pos, const double* __restrict__ hh, const
             if (Facc != F) { Facc[3 * i] = 0.0; Facc[3 * i + 1] = 0.0; Facc[3 * i + 2] = 0.0; }
         }
     }
-    block_sum_store<kNV>(acc, sm, part + (size_t)blockIdx.x * kNV);
+    block_sum_store<kNV>(acc, sm, part + (size_t)blk * kNV);
+}
+
+template <bool FULL_VIRIAL, bool F32>
+__global__ void __launch_bounds__(256, 2)
+k_lj_gather(const double* __restrict__ pos, const double* __restrict__ hh, const int* __restrict__ cnt,
+            const int* __restrict__ list, int cap, const int* __restrict__ in_cnt,
+            const int* __restrict__ in_list, int in_cap, int na, double* __restrict__ F,
+            double* __restrict__ Facc, LJP p, double* __restrict__ part) {
+    __shared__ double sm[32 * kNV];
+    __shared__ double s_hh[18];
+    lj_gather_body<FULL_VIRIAL, F32, kLJUnroll>(pos, hh, cnt, list, cap, in_cnt, in_list, in_cap, na, F, Facc, p,
+                                                part, blockIdx.x, gridDim.x, sm, s_hh);
+}
+
+// Replica batch: the same gather over every replica in one launch; block b
+// serves replica r = batch_rep(off, R, b) as its local block b - off[r].
+template <bool FULL_VIRIAL, bool F32, int U, int NT>
+__global__ void __launch_bounds__(NT)
+k_b_lj_gather(const StepArrays* __restrict__ As, const int* __restrict__ off, int R, int ff) {
+    __shared__ double sm[32 * kNV];
+    __shared__ double s_hh[18];
+    const int r = batch_rep(off, R, blockIdx.x);
+    const StepArrays& a = As[r];
+    const LJP p = lj_params_dev(ff);
+    lj_gather_body<FULL_VIRIAL, F32, U>(a.pos, a.S->h, a.cnt_a, a.list_a, a.cap_a, a.in_cnt, a.in_list, a.in_cap,
+                                        a.n, a.F, a.Facc, p, a.part_f2, blockIdx.x - off[r], off[r + 1] - off[r], sm,
+                                        s_hh);
 }
 
 __global__ void k_reduce(const double* __restrict__ part, int nblk, int nv, double* __restrict__ out) {
@@ -503,6 +533,20 @@ cudaError_t lj_gather_launch(int ff, const double* pos, const double* hh, const 
         else k_lj_gather<false, false><<<kForceBlocks, 256, 0, st>>>(FMD_LJ_ARGS);
     }
 #undef FMD_LJ_ARGS
+    return cudaGetLastError();
+}
+
+cudaError_t batch_lj_launch(const StepArrays* As, const int* off, int R, int nblocks, int ff, int precision,
+                            int threads, int unroll, cudaStream_t st) {
+    const bool fv = ff == FMD_FF_AIREBO, f32 = precision == FMD_PREC_FP32_PAIR;
+#define FMD_BLJ(FV, F32, U, NT) k_b_lj_gather<FV, F32, U, NT><<<nblocks, NT, 0, st>>>(As, off, R, ff)
+#define FMD_BLJ_NT(FV, F32, U) if (threads == 128) FMD_BLJ(FV, F32, U, 128); else FMD_BLJ(FV, F32, U, 256)
+#define FMD_BLJ_U(FV, F32) if (unroll == 2) { FMD_BLJ_NT(FV, F32, 2); } else { FMD_BLJ_NT(FV, F32, 4); }
+    if (fv) { if (f32) { FMD_BLJ_U(true, true) } else { FMD_BLJ_U(true, false) } }
+    else { if (f32) { FMD_BLJ_U(false, true) } else { FMD_BLJ_U(false, false) } }
+#undef FMD_BLJ_U
+#undef FMD_BLJ_NT
+#undef FMD_BLJ
     return cudaGetLastError();
 }
 

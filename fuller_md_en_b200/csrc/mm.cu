@@ -14,6 +14,7 @@
 #include <cmath>
 #include "kernels.h"
 #include "geom.cuh"
+#include "step.h"
 
 namespace fmd {
 namespace {
@@ -70,17 +71,17 @@ __device__ double torsion(double* F, const double* __restrict__ pos, const doubl
     return e;
 }
 
-__global__ void __launch_bounds__(128)
-k_mm_bonded(MMTopoDev t, const double* __restrict__ pos, const double* __restrict__ hh,
-            double* __restrict__ F, double* __restrict__ part) {
-    __shared__ double sm[32 * kMMNV];
+// Terms blk*blockDim + tid, strided by nblk*blockDim; partials into part[blk].
+__device__ __forceinline__ void mm_bonded_body(const MMTopoDev& t, const double* __restrict__ pos,
+                                               const double* __restrict__ hh, double* __restrict__ F,
+                                               double* __restrict__ part, int blk, int nblk, double* sm) {
     double h[9], hi[9];
     load_cell(hh, h, hi);
     double acc[kMMNV];   // Eb Ea Ed Ei W00 W11 W22
 #pragma unroll
     for (int k = 0; k < kMMNV; k++) acc[k] = 0.0;
     const int total = t.nb + t.nang + t.ndih + t.nimp;
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < total; q += gridDim.x * blockDim.x) {
+    for (int q = blk * blockDim.x + threadIdx.x; q < total; q += nblk * blockDim.x) {
         if (q < t.nb) {                                           // MM:384-447
             const int b = q, i = t.b_i0[b], j = t.b_i1[b];
             double dx, dy, dz;
@@ -125,7 +126,23 @@ k_mm_bonded(MMTopoDev t, const double* __restrict__ pos, const double* __restric
                               t.m_gamma[p]);
         }
     }
-    block_sum_store<kMMNV>(acc, sm, part + (size_t)blockIdx.x * kMMNV);
+    block_sum_store<kMMNV>(acc, sm, part + (size_t)blk * kMMNV);
+}
+
+__global__ void __launch_bounds__(128)
+k_mm_bonded(MMTopoDev t, const double* __restrict__ pos, const double* __restrict__ hh,
+            double* __restrict__ F, double* __restrict__ part) {
+    __shared__ double sm[32 * kMMNV];
+    mm_bonded_body(t, pos, hh, F, part, blockIdx.x, gridDim.x, sm);
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT) k_b_mm_bonded(const StepArrays* __restrict__ As, const int* __restrict__ off,
+                                                    int R) {
+    __shared__ double sm[32 * kMMNV];
+    const int r = batch_rep(off, R, blockIdx.x);
+    const StepArrays& a = As[r];
+    mm_bonded_body(a.topo, a.pos, a.S->h, a.Facc, a.part_f1, blockIdx.x - off[r], off[r + 1] - off[r], sm);
 }
 
 constexpr int kTile = 128;
@@ -183,6 +200,13 @@ k_coulomb(const double* __restrict__ pos, const double* __restrict__ hh, const d
 cudaError_t mm_bonded_launch(const MMTopoDev& t, const double* pos, const double* hh, double* Facc,
                              double* part, cudaStream_t st) {
     k_mm_bonded<<<kForceBlocks, 128, 0, st>>>(t, pos, hh, Facc, part);
+    return cudaGetLastError();
+}
+
+cudaError_t batch_mm_bonded_launch(const StepArrays* As, const int* off, int R, int nblocks, int threads,
+                                   cudaStream_t st) {
+    if (threads == 256) k_b_mm_bonded<256><<<nblocks, 256, 0, st>>>(As, off, R);
+    else k_b_mm_bonded<128><<<nblocks, 128, 0, st>>>(As, off, R);
     return cudaGetLastError();
 }
 

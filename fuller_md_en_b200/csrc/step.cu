@@ -49,8 +49,9 @@ __device__ void npt_half(fmd_npt& s, double hdt, double ke, double ke_p, const d
     for (int a = 0; a < 3; a++) s.Vg[a * 4] = clampd(s.Vg[a * 4], -vg_lim, vg_lim);
 }
 
-__global__ void k_begin(SysScal* S, int kind, StepParams p) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+}  // namespace
+
+__device__ void begin_body(SysScal* S, int kind, const StepParams& p) {
     fmd_npt& npt = S->npt;
     if (p.schedule) {
         const int g = ++S->gstep;
@@ -83,6 +84,13 @@ __global__ void k_begin(SysScal* S, int kind, StepParams p) {
     S->sc_v2 = sc_nh * exp(-hdt * eps2 / 3.0);
 }
 
+namespace {
+
+__global__ void k_begin(SysScal* S, int kind, StepParams p) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    begin_body(S, kind, p);
+}
+
 // LJ:166-174.
 __device__ __forceinline__ void quat_step(double* q, double wx, double wy, double wz, double dt) {
     double dq[4];
@@ -98,14 +106,16 @@ __device__ __forceinline__ void quat_step(double* q, double wx, double wy, doubl
     for (int k = 0; k < 4; k++) q[k] = o[k] * inv;
 }
 
-__global__ void __launch_bounds__(kPB) k_kick(StepArrays a, double dt) {
+}  // namespace
+
+__device__ void kick_body(const StepArrays& a, double dt, int blk, int nblk) {
     const SysScal* S = a.S;
     const double hdt = 0.5 * dt, sc_v = S->sc_v, sc_nh = S->sc_nh;
     const double* hi = S->hi_old;
     const double* h = S->h;
     const bool rigid = a.kind == FMD_SYS_RIGID;
     const double cF = rigid ? kConv / a.Mmol : kConv / kMC, cT = rigid ? kConv / a.I0 : 0.0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+    for (int i = blk * blockDim.x + threadIdx.x; i < a.n; i += nblk * blockDim.x) {
         const double mi = (a.mass != nullptr) ? kConv / a.mass[i] : cF;
         double v[3], p[3];
         for (int c = 0; c < 3; c++) {
@@ -135,15 +145,15 @@ __global__ void __launch_bounds__(kPB) k_kick(StepArrays a, double dt) {
     }
 }
 
-// Second half-kick with per-block sums of m v^2 (atomistic) or v^2 and w^2 (rigid).
-__global__ void __launch_bounds__(kPB) k_kick2(StepArrays a, double dt) {
-    __shared__ double sm[32 * 2];
+// Second half-kick with per-block sums of m v^2 (atomistic) or v^2 and w^2
+// (rigid) into part_ke[2 * blk]; sm holds 64 doubles.
+__device__ void kick2_body(const StepArrays& a, double dt, int blk, int nblk, double* sm) {
     const SysScal* S = a.S;
     const double hdt = 0.5 * dt, sc_v2 = S->sc_v2, sc_nh = S->sc_nh;
     const bool rigid = a.kind == FMD_SYS_RIGID;
     const double cF = rigid ? kConv / a.Mmol : kConv / kMC, cT = rigid ? kConv / a.I0 : 0.0;
     double acc[2] = {0.0, 0.0};
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+    for (int i = blk * blockDim.x + threadIdx.x; i < a.n; i += nblk * blockDim.x) {
         const double mi = (a.mass != nullptr) ? kConv / a.mass[i] : cF;
         double vv = 0;
         for (int c = 0; c < 3; c++) {
@@ -164,7 +174,16 @@ __global__ void __launch_bounds__(kPB) k_kick2(StepArrays a, double dt) {
             acc[0] += (a.mass != nullptr ? a.mass[i] : kMC) * vv;
         }
     }
-    block_sum_store<2>(acc, sm, a.part_ke + 2 * blockIdx.x);
+    block_sum_store<2>(acc, sm, a.part_ke + 2 * blk);
+}
+
+namespace {
+
+__global__ void __launch_bounds__(kPB) k_kick(StepArrays a, double dt) { kick_body(a, dt, blockIdx.x, gridDim.x); }
+
+__global__ void __launch_bounds__(kPB) k_kick2(StepArrays a, double dt) {
+    __shared__ double sm[32 * 2];
+    kick2_body(a, dt, blockIdx.x, gridDim.x, sm);
 }
 
 __global__ void __launch_bounds__(kPB) k_ke_partial(StepArrays a) {
@@ -185,14 +204,15 @@ __global__ void __launch_bounds__(kPB) k_ke_partial(StepArrays a) {
     block_sum_store<2>(acc, sm, a.part_ke + 2 * blockIdx.x);
 }
 
-__global__ void __launch_bounds__(kPB) k_rescale(StepArrays a) {
-    __shared__ double sm[32 * 2];
+}  // namespace
+
+__device__ void rescale_body(const StepArrays& a, int blk, int nblk, double* sm) {
     const SysScal* S = a.S;
     const bool rigid = a.kind == FMD_SYS_RIGID;
     const bool doit = S->do_rescale != 0;
     const double sc = S->scale;
     double acc[2] = {0.0, 0.0};
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+    for (int i = blk * blockDim.x + threadIdx.x; i < a.n; i += nblk * blockDim.x) {
         double vv = 0, ww = 0;
         for (int c = 0; c < 3; c++) {
             double v = a.vel[3 * i + c];
@@ -207,7 +227,14 @@ __global__ void __launch_bounds__(kPB) k_rescale(StepArrays a) {
         if (rigid) { acc[0] += vv; acc[1] += ww; }
         else acc[0] += (a.mass != nullptr ? a.mass[i] : kMC) * vv;
     }
-    block_sum_store<2>(acc, sm, a.part_ke + 2 * blockIdx.x);
+    block_sum_store<2>(acc, sm, a.part_ke + 2 * blk);
+}
+
+namespace {
+
+__global__ void __launch_bounds__(kPB) k_rescale(StepArrays a) {
+    __shared__ double sm[32 * 2];
+    rescale_body(a, blockIdx.x, gridDim.x, sm);
 }
 
 // One pass over every partial array: each thread sums its strided records
@@ -216,7 +243,7 @@ __global__ void __launch_bounds__(kPB) k_rescale(StepArrays a) {
 constexpr int kRedFields = 23;
 
 __device__ void reduce_all(const StepArrays& a, int nblk_f1, int nblk_ke, bool forces, bool kinetic,
-                           double* sm, double (&t)[kRedFields]) {
+                           double* sm, double (&t)[kRedFields], int nblk_f2 = kForceBlocks) {
     double acc[kRedFields];
 #pragma unroll
     for (int k = 0; k < kRedFields; k++) acc[k] = 0.0;
@@ -225,11 +252,12 @@ __device__ void reduce_all(const StepArrays& a, int nblk_f1, int nblk_ke, bool f
         for (int b = threadIdx.x; b < nblk_f1; b += blockDim.x)
             for (int k = 0; k < nv1; k++) acc[k] += a.part_f1[(size_t)b * nv1 + k];
         if (a.kind != FMD_SYS_RIGID)
-            for (int b = threadIdx.x; b < kForceBlocks; b += blockDim.x) {
+            for (int b = threadIdx.x; b < nblk_f2; b += blockDim.x) {
 #pragma unroll
                 for (int k = 0; k < kNV; k++) acc[10 + k] += a.part_f2[(size_t)b * kNV + k];
-                if (a.kind == FMD_SYS_MM && a.has_charge) acc[20] += a.part_f3[b];
             }
+        if (a.kind == FMD_SYS_MM && a.has_charge)
+            for (int b = threadIdx.x; b < kForceBlocks; b += blockDim.x) acc[20] += a.part_f3[b];
     }
     if (kinetic)
         for (int b = threadIdx.x; b < nblk_ke; b += blockDim.x) {
@@ -297,10 +325,12 @@ __device__ void record(SysScal* S, int kind, const StepParams& p) {
     for (int q = 0; q < 8; q++) o.E[q] = S->E[q];
 }
 
-__global__ void __launch_bounds__(256) k_end(StepArrays a, StepParams p, int nblk_f1, int nblk_ke) {
-    __shared__ double sm[32 * kRedFields];
+}  // namespace
+
+__device__ void end_body(const StepArrays& a, const StepParams& p, int nblk_f1, int nblk_ke, int nblk_f2,
+                         double* sm) {
     double t[kRedFields];
-    reduce_all(a, nblk_f1, nblk_ke, true, true, sm, t);
+    reduce_all(a, nblk_f1, nblk_ke, true, true, sm, t, nblk_f2);
     if (threadIdx.x != 0) return;
     forces_from_sums(a, t);
     kinetic_from_sums(a, t);
@@ -326,8 +356,7 @@ __global__ void __launch_bounds__(256) k_end(StepArrays a, StepParams p, int nbl
     if (!phase) record(S, a.kind, p);
 }
 
-__global__ void __launch_bounds__(256) k_rescale_end(StepArrays a, StepParams p, int nblk_ke) {
-    __shared__ double sm[32 * kRedFields];
+__device__ void rescale_end_body(const StepArrays& a, const StepParams& p, int nblk_ke, double* sm) {
     SysScal* S = a.S;
     const bool doit = S->do_rescale != 0;
     double t[kRedFields];
@@ -343,11 +372,60 @@ __global__ void __launch_bounds__(256) k_rescale_end(StepArrays a, StepParams p,
     record(S, a.kind, p);
 }
 
+namespace {
+
+__global__ void __launch_bounds__(256) k_end(StepArrays a, StepParams p, int nblk_f1, int nblk_ke) {
+    __shared__ double sm[32 * kRedFields];
+    end_body(a, p, nblk_f1, nblk_ke, kForceBlocks, sm);
+}
+
+__global__ void __launch_bounds__(256) k_rescale_end(StepArrays a, StepParams p, int nblk_ke) {
+    __shared__ double sm[32 * kRedFields];
+    rescale_end_body(a, p, nblk_ke, sm);
+}
+
 __global__ void __launch_bounds__(256) k_ke_final(StepArrays a, int nblk_ke) {
     __shared__ double sm[32 * kRedFields];
     double t[kRedFields];
     reduce_all(a, 0, nblk_ke, false, true, sm, t);
     if (threadIdx.x == 0) kinetic_from_sums(a, t);
+}
+
+// ---- replica batch: each single-system kernel once over all replicas ----
+__global__ void k_b_begin(BatchDev b) {
+    if (threadIdx.x != 0) return;
+    const StepArrays& a = b.A[blockIdx.x];
+    begin_body(a.S, a.kind, b.P[blockIdx.x]);
+}
+
+__global__ void __launch_bounds__(kPB) k_b_kick(BatchDev b) {
+    const int r = batch_rep(b.off_atom, b.R, blockIdx.x);
+    kick_body(b.A[r], b.P[r].dt, blockIdx.x - b.off_atom[r], b.off_atom[r + 1] - b.off_atom[r]);
+}
+
+__global__ void __launch_bounds__(kPB) k_b_kick2(BatchDev b) {
+    __shared__ double sm[32 * 2];
+    const int r = batch_rep(b.off_atom, b.R, blockIdx.x);
+    kick2_body(b.A[r], b.P[r].dt, blockIdx.x - b.off_atom[r], b.off_atom[r + 1] - b.off_atom[r], sm);
+}
+
+__global__ void __launch_bounds__(kPB) k_b_rescale(BatchDev b) {
+    __shared__ double sm[32 * 2];
+    const int r = batch_rep(b.off_atom, b.R, blockIdx.x);
+    rescale_body(b.A[r], blockIdx.x - b.off_atom[r], b.off_atom[r + 1] - b.off_atom[r], sm);
+}
+
+__global__ void __launch_bounds__(256) k_b_end(BatchDev b) {
+    __shared__ double sm[32 * kRedFields];
+    const int r = blockIdx.x;
+    end_body(b.A[r], b.P[r], b.off_f1[r + 1] - b.off_f1[r], b.off_atom[r + 1] - b.off_atom[r],
+             b.off_lj[r + 1] - b.off_lj[r], sm);
+}
+
+__global__ void __launch_bounds__(256) k_b_rescale_end(BatchDev b) {
+    __shared__ double sm[32 * kRedFields];
+    const int r = blockIdx.x;
+    rescale_end_body(b.A[r], b.P[r], b.off_atom[r + 1] - b.off_atom[r], sm);
 }
 
 __global__ void __launch_bounds__(256) k_force_final(StepArrays a, int nblk_f1) {
@@ -410,6 +488,24 @@ cudaError_t enqueue_step(const StepArrays& a, const StepParams& p, bool rescale_
     if (rescale_phase && p.schedule) {
         k_rescale<<<kForceBlocks, kPB, 0, st>>>(a);
         k_rescale_end<<<1, 256, 0, st>>>(a, p, kForceBlocks);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t enqueue_batch_step(const BatchDev& b, bool rescale_phase, cudaStream_t st) {
+    cudaError_t e;
+    k_b_begin<<<b.R, 32, 0, st>>>(b);
+    k_b_kick<<<b.nblk_atom, kPB, 0, st>>>(b);
+    if (b.kind == FMD_SYS_MM)
+        if ((e = batch_mm_bonded_launch(b.A, b.off_f1, b.R, b.nblk_f1, b.f1_threads, st)) != cudaSuccess) return e;
+    if ((e = batch_lj_launch(b.A, b.off_lj, b.R, b.nblk_lj, b.ff, b.precision, b.lj_threads, b.lj_unroll, st)) !=
+        cudaSuccess)
+        return e;
+    k_b_kick2<<<b.nblk_atom, kPB, 0, st>>>(b);
+    k_b_end<<<b.R, 256, 0, st>>>(b);
+    if (rescale_phase) {
+        k_b_rescale<<<b.nblk_atom, kPB, 0, st>>>(b);
+        k_b_rescale_end<<<b.R, 256, 0, st>>>(b);
     }
     return cudaGetLastError();
 }

@@ -79,4 +79,40 @@ cudaError_t enqueue_step(const StepArrays& a, const StepParams& p, bool rescale_
 // Observables / averages for the pre-loop state (not a step).
 int force_partial_blocks(const StepArrays& a);
 
+// ------------------------------------------------------- replica batches --
+// A batched launch covers R replicas: block b belongs to replica r with
+// off[r] <= b < off[r + 1] and acts as block b - off[r] of a grid of
+// off[r + 1] - off[r] blocks for that replica alone, so each replica keeps
+// its own grid size (and partial-record count) inside one launch.
+__device__ __forceinline__ int batch_rep(const int* __restrict__ off, int R, int b) {
+    int lo = 0, hi = R - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= b) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Device tables of a batch: per-replica arrays and parameters, and the block
+// offsets of each launch class (R + 1 entries each).
+struct BatchDev {
+    int R = 0;
+    const StepArrays* A = nullptr;
+    const StepParams* P = nullptr;
+    const int* off_atom = nullptr;   // per-particle kernels (kicks, rescale)
+    const int* off_lj = nullptr;     // LJ gather (part_f2 records)
+    const int* off_f1 = nullptr;     // bonded terms (part_f1 records)
+    int nblk_atom = 0, nblk_lj = 0, nblk_f1 = 0;   // totals (off[R])
+    int lj_threads = 256, lj_unroll = 4, f1_threads = 128;
+    int kind = FMD_SYS_MM, ff = FMD_FF_MM, precision = FMD_PREC_FP64;
+};
+// LJ gather / MM bonded terms over all replicas in one launch each.
+cudaError_t batch_lj_launch(const StepArrays* As, const int* off, int R, int nblocks, int ff, int precision,
+                            int threads, int unroll, cudaStream_t st);
+cudaError_t batch_mm_bonded_launch(const StepArrays* As, const int* off, int R, int nblocks, int threads,
+                                   cudaStream_t st);
+// One step of every replica (the single-system step's launches, each once
+// for the whole batch); rescale_phase as in enqueue_step.
+cudaError_t enqueue_batch_step(const BatchDev& b, bool rescale_phase, cudaStream_t st);
+
 }  // namespace fmd

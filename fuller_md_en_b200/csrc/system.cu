@@ -228,9 +228,6 @@ int System::nonfinite_check() {
 }  // namespace fmd
 
 // ------------------------------------------------------------------ C-ABI --
-struct fmd_system {
-    std::unique_ptr<fmd::System> sys;
-};
 
 static int make_params(const fmd_run_params* p, fmd::System& s) {
     s.p = *p;

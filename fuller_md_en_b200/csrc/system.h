@@ -44,3 +44,8 @@ struct System {
 };
 
 }  // namespace fmd
+
+// The C-ABI handle of a system (include/fullermd.h).
+struct fmd_system {
+    std::unique_ptr<fmd::System> sys;
+};

@@ -251,6 +251,41 @@ int fmd_system_destroy(fmd_system *s);
 int fmd_system_kernel_ms(fmd_system *s, int stage, int reps, double *ms_per_launch);
 int fmd_system_step_kernels(fmd_system *s, int rebuild, int phase, int *nkernels);
 
+/* ------------------------------------------------------- replica batches --
+ * No counterpart in the reference (its programs run one system each).  A
+ * batch advances R MM systems of one context together -- different sizes,
+ * cells, temperatures and pressures -- with every phase of the step one
+ * launch over all replicas and each step one CUDA graph; every replica gets
+ * the results of its own kernels run alone.  The systems stay owned by the
+ * caller (they must outlive the batch) and keep serving fmd_system_download,
+ * fmd_system_averages and fmd_system_lists; they must share nlup, coldstart,
+ * warmup and precision, carry no charges and no learned REBO term, and are
+ * initialised here if they are not yet.  autotune != 0 times the LJ gather
+ * and bonded kernels over candidate launch shapes on the batch itself and
+ * keeps the fastest (cached per device, replica count and atom count; the
+ * forces of the current state are recomputed afterwards). */
+typedef struct fmd_batch fmd_batch;
+typedef struct {
+    int lj_threads;               /* threads per block of the LJ gather */
+    int lj_unroll;                /* list entries in flight per lane (neighbours per warp / 32) */
+    int lj_atoms_per_block;       /* sites per block of the LJ gather */
+    int bonded_threads;           /* threads per block of the bonded terms */
+    int bonded_terms_per_block;
+    double lj_ms, bonded_ms;      /* timed duration of the chosen shapes, ms per launch */
+    int blocks_lj, blocks_bonded, blocks_atom;   /* launch sizes over the whole batch */
+} fmd_batch_tuning;
+int fmd_batch_create(fmd_ctx *ctx, int nrep, fmd_system *const *systems, int autotune, fmd_batch **out);
+/* Global steps first..last of every replica (as fmd_system_run); _run
+ * synchronises, _enqueue does not. */
+int fmd_batch_run(fmd_batch *b, int first, int last);
+int fmd_batch_enqueue(fmd_batch *b, int first, int last);
+/* Observables of the last step of each replica: obs[nrep]. */
+int fmd_batch_observables(fmd_batch *b, fmd_obs *obs);
+int fmd_batch_get_tuning(fmd_batch *b, fmd_batch_tuning *t);
+/* Kernel launches of one batch step (rebuild or not, cold/warm phase or not). */
+int fmd_batch_step_kernels(fmd_batch *b, int rebuild, int phase, int *nkernels);
+int fmd_batch_destroy(fmd_batch *b);
+
 /* Tensor-core self test (no reference counterpart): D = A * Bt^T for one
  * 128 x N x K BF16 tile through tcgen05.mma, FP32 result.  A is 128 x K and
  * Bt is N x K, row-major bf16 bit patterns; mode bit 0 reads A MN-major and
