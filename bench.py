@@ -218,6 +218,7 @@ def run_ours(args, ws, rank, local):
     per_step = {"lj_gather": stages["lj_gather"], "rebo": stages["rebo"],
                 "list_rebuild": stages["list_rebuild"] / NLUP}
     lj_bytes, n_pairs_listed = list_bytes(sysd, na)
+    lj_shape = sysd.lj_shape()
     peak, peak_src = peaks()
     achieved = lj_bytes / (stages["lj_gather"] / 1e3) / 1e9
     traffic = None
@@ -292,6 +293,7 @@ def run_ours(args, ws, rank, local):
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_src, "traffic": traffic,
                      "algorithmic_bytes_per_launch": lj_bytes, "listed_pairs": n_pairs_listed,
+                     "launch_shape": lj_shape,
                      "launch_ms": stages["lj_gather"]},
         "stage_ms_per_step": per_step,
         "gpu_launches": launches,

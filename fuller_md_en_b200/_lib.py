@@ -121,6 +121,7 @@ _SIGS = {
     "fmd_system_destroy": (c_int, [c_void_p]),
     "fmd_system_kernel_ms": (c_int, [c_void_p, c_int, c_int, POINTER(c_double)]),
     "fmd_system_step_kernels": (c_int, [c_void_p, c_int, c_int, POINTER(c_int)]),
+    "fmd_system_lj_shape": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int), POINTER(c_int), POINTER(c_int)]),
     "fmd_umma_selftest": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, POINTER(c_float)]),
     "fmd_sg_nparams": (c_int, []),
     "fmd_sg_create": (c_int, [c_void_p, _dp, POINTER(c_void_p)]),

@@ -410,6 +410,12 @@ class System:
                                                             ctypes.byref(k)), "step_kernels")
         return k.value
 
+    def lj_shape(self) -> dict:
+        """Launch shape of the LJ gather chosen by the autotuner at init."""
+        v = [ctypes.c_int(0) for _ in range(4)]
+        self.ctx.check(self.ctx.lib.fmd_system_lj_shape(self.h, *[ctypes.byref(x) for x in v]), "fmd_system_lj_shape")
+        return dict(zip(("threads", "unroll", "pipelined", "blocks"), (x.value for x in v)))
+
     def use_surrogate(self, model, judge_every: int = 100, rmse_max: float = 0.025) -> None:
         """Learned REBO term from `model` (a surrogate.Surrogate, or None for
         the plain kernel), judged by the plain REBO kernel every `judge_every`

@@ -188,7 +188,7 @@ int list_call(fmd_ctx* ctx, int mode, const double* pos, const double* h, const 
     cudaMemsetAsync(ddrop, 0, sizeof(int), ctx->stream);
     TmpCells tc;
     if (cells_alloc(tc.cl, n, h, rc, mode == LIST_INTRA ? 1 : 2) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "cell allocation failed");
-    if (cells_build(tc.cl, dpos, n, hh, rc, ctx->d_err, ctx->stream) != cudaSuccess)
+    if (cells_build(tc.cl, dpos, n, hh, rc, ctx->d_err, ctx->stream, dmol) != cudaSuccess)
         return ctx->fail(FMD_ERR_CUDA, "cell build launch failed");
     const double rc2 = rc * rc;
     if (nlist_build(tc.cl, mode, dpos, dmol, n, hh, rc2, cap, dcnt, dlist, ddrop, ctx->d_err, ctx->stream) != cudaSuccess)
@@ -324,7 +324,8 @@ int upload_scal(fmd_ctx* ctx, const double* h, const double* hi, const double* W
 
 int alloc_partials(fmd_ctx* ctx, StepArrays& a) {
     int rc = up<double>(ctx, S_PART1, nullptr, (size_t)std::max(kForceBlocks, a.n) * kNV, &a.part_f1);
-    if (!rc) rc = up<double>(ctx, S_PART2, nullptr, (size_t)kForceBlocks * kNV, &a.part_f2);
+    if (!rc) rc = up<double>(ctx, S_PART2, nullptr, (size_t)kLJMaxBlocks * kNV, &a.part_f2);
+    a.lj_blocks = lj_gather_blocks(a.kind == FMD_SYS_MM ? FMD_FF_MM : FMD_FF_AIREBO, a.precision, a.lj_shape);
     if (!rc) rc = up<double>(ctx, S_PART3, nullptr, (size_t)kForceBlocks, &a.part_f3);
     if (!rc) rc = up<double>(ctx, S_PARTKE, nullptr, (size_t)kForceBlocks * 2, &a.part_ke);
     return rc;
@@ -463,7 +464,8 @@ static int atom_term(fmd_ctx* ctx, int term, int ff, const double* pos, const do
     }
     double* red;
     if ((rc = up<double>(ctx, S_PART3, nullptr, 16, &red))) return rc;
-    if (reduce_partials(part, kForceBlocks, kNV, red, ctx->stream) != cudaSuccess)
+    if (reduce_partials(part, term == 0 ? kForceBlocks : lj_gather_blocks(ff, ctx->precision, LJShape{}), kNV, red,
+                        ctx->stream) != cudaSuccess)
         return ctx->fail(FMD_ERR_CUDA, "reduce launch failed");
     double r[kNV];
     down(ctx, F, dF, 3 * (size_t)na);

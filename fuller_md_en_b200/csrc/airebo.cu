@@ -15,6 +15,7 @@
 // once, as in the reference.  The cutoff decision uses the reference's
 // operation order, and mimg(-d) == -mimg(d) bitwise, so both sides of a pair
 // always agree on whether it interacts.
+#include <algorithm>
 #include <cmath>
 #include "kernels.h"
 #include "geom.cuh"
@@ -239,57 +240,138 @@ __device__ __forceinline__ void bo_three_body_sl(double* __restrict__ F, const S
     atomic_add3(F, c, fcx, fcy, fcz);
 }
 
-__global__ void __launch_bounds__(128)
-k_rebo_sl(const Slot* __restrict__ sl, const int* __restrict__ cnt, const int* __restrict__ list, int cap, int na,
-          double* __restrict__ F, double* __restrict__ part, const int* __restrict__ gate, int want) {
+// Bond order of every directed slot c -> j (AI:301-323 for centre c):
+// g = sum over c's other slots of f_c G(cos), b = (1 + g)^-1/2, the pair
+// functions of r_cj (AI:173-183) and the three-body coefficient
+// coeff = -(f_c V_A / 2) db/dg (AI:361-365; zero where the reference skips
+// the three-body block).  bo[t] = {b, g, coeff, vr, dvr, va, dva, ok}.
+struct SlotBO {
+    double b, g, coeff, vr, dvr, va, dva, ok;
+};
+
+__device__ __forceinline__ void rebo_pair_fn(double r, double rinv, double& vr, double& dvr, double& va,
+                                             double& dva) {
+    const double ea = A_CC * exp(-ALPHA_CC * r);
+    const double qr = Q_CC * rinv;
+    vr = (1.0 + qr) * ea;
+    dvr = (-qr * rinv) * ea + (1.0 + qr) * (-ALPHA_CC) * ea;
+    const double e1 = exp(-BETA1_CC * r), e2 = exp(-BETA2_CC * r), e3 = exp(-BETA3_CC * r);
+    va = B1_CC * e1 + B2_CC * e2 + B3_CC * e3;
+    dva = -BETA1_CC * B1_CC * e1 - BETA2_CC * B2_CC * e2 - BETA3_CC * B3_CC * e3;
+}
+
+// Three-body coefficient of centre c for a bond with f_c and V_A.
+__device__ __forceinline__ double three_body_coeff(double gs, double b, double fcut, double va) {
+    if (!(fabs(gs) > 1e-20 && va > 1e-20)) return 0.0;
+    const double dbp = -BO_DELTA * b / (1.0 + gs);
+    return -(0.5 * fcut * va) * dbp;
+}
+
+__global__ void __launch_bounds__(256)
+k_rebo_bo(const Slot* __restrict__ sl, const int* __restrict__ cnt, const int* __restrict__ list, int cap, int na,
+          SlotBO* __restrict__ bo, const int* __restrict__ gate, int want) {
+    if (gate != nullptr && *gate != want) return;
+    const long long tot = (long long)na * cap;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(t / cap), jn = (int)(t % cap);
+        const int m = cnt[c];
+        if (jn >= m) continue;
+        const Slot q = sl[t];
+        SlotBO o;
+        o.ok = 0.0;
+        // the reference's bond gate (AI:292-296)
+        if (q.r <= DMAX_CC && !(q.fc < 1e-15 && q.dfc == 0)) {
+            const double g = bo_sum_sl(sl, list, cap, c, m, list[t], q.dx, q.dy, q.dz, q.rinv);
+            o.g = g;
+            o.b = 1.0 / sqrt(1.0 + g);
+            rebo_pair_fn(q.r, q.rinv, o.vr, o.dvr, o.va, o.dva);
+            o.coeff = three_body_coeff(g, o.b, q.fc, o.va);
+            o.ok = 1.0;
+        }
+        bo[t] = o;
+    }
+}
+
+// Three-body forces of centre c for the bond c -> skip with coefficient coeff
+// (AI:368-419) on c's other neighbours k, and the reaction on c.
+__device__ __forceinline__ void three_body_sl(double* __restrict__ F, const Slot* __restrict__ sl,
+                                              const int* __restrict__ list, int cap, int c, int m, int skip,
+                                              double bx, double by, double bz, double rbinv, double coeff) {
+    if (coeff == 0.0) return;
+    const double ux = bx * rbinv, uy = by * rbinv, uz = bz * rbinv;
+    double fcx = 0.0, fcy = 0.0, fcz = 0.0;
+    for (int kn = 0; kn < m; kn++) {
+        const size_t o = (size_t)c * cap + kn;
+        const int k = list[o];
+        if (k == skip) continue;
+        const Slot q = sl[o];
+        if (q.fc < 1e-15) continue;
+        const double rx = q.dx * q.rinv, ry = q.dy * q.rinv, rz = q.dz * q.rinv;
+        const double ct = clamp1((bx * q.dx + by * q.dy + bz * q.dz) * (rbinv * q.rinv));
+        double gv, dgv;
+        ang_g_dg(ct, gv, dgv);
+        const double a1 = coeff * q.dfc * gv, a2 = coeff * q.fc * dgv;
+        const double fx = a1 * rx + a2 * ((ux - ct * rx) * q.rinv);
+        const double fy = a1 * ry + a2 * ((uy - ct * ry) * q.rinv);
+        const double fz = a1 * rz + a2 * ((uz - ct * rz) * q.rinv);
+        atomic_add3(F, k, fx, fy, fz);
+        fcx -= fx; fcy -= fy; fcz -= fz;
+    }
+    atomic_add3(F, c, fcx, fcy, fcz);
+}
+
+// Forces, one thread per directed slot i -> j.  The reference enumerates
+// bonds from the row of the lower index (AI:288) and evaluates the three-body
+// blocks of both ends from their own rows.  Here the slot i -> j does the
+// three-body block of centre i, and for j > i also the pair term; when the
+// list is asymmetric (rows truncated at cap) and j's row lacks i, the owning
+// slot (j > i) also computes b_ji and centre j's block from j's row, and a
+// slot with j < i whose partner is missing does nothing (the reference never
+// visits that bond).
+__global__ void __launch_bounds__(256)
+k_rebo_force(const Slot* __restrict__ sl, const SlotBO* __restrict__ bo, const int* __restrict__ cnt,
+             const int* __restrict__ list, int cap, int na, double* __restrict__ F, double* __restrict__ part,
+             const int* __restrict__ gate, int want) {
     if (gate != nullptr && *gate != want) return;
     __shared__ double sm[32 * kNV];
     double acc[kNV];
 #pragma unroll
     for (int k = 0; k < kNV; k++) acc[k] = 0.0;
-    const long long total = (long long)na * kReboLanes;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-         t += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(t / kReboLanes), lane = (int)(t % kReboLanes);
+    const long long tot = (long long)na * cap;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t / cap), jn = (int)(t % cap);
         const int m = cnt[i];
-        double fix = 0.0, fiy = 0.0, fiz = 0.0;
-        for (int jn = lane; jn < m; jn += kReboLanes) {
-            const size_t o = (size_t)i * cap + jn;
-            const int j = list[o];
-            if (j <= i) continue;
-            const Slot q = sl[o];
-            const double rij = q.r;
-            if (rij > DMAX_CC) continue;
-            const double fcut = q.fc, dfcut = q.dfc;
-            if (fcut < 1e-15 && dfcut == 0) continue;
-            const double dx = q.dx, dy = q.dy, dz = q.dz, rinv = q.rinv;
-            // V_R, V_A and derivatives (AI:173-183)
-            const double ea = A_CC * exp(-ALPHA_CC * rij);
-            const double qr = Q_CC * rinv;
-            const double vr = (1.0 + qr) * ea;
-            const double dvr = (-qr * rinv) * ea + (1.0 + qr) * (-ALPHA_CC) * ea;
-            const double e1 = exp(-BETA1_CC * rij), e2 = exp(-BETA2_CC * rij), e3 = exp(-BETA3_CC * rij);
-            const double va = B1_CC * e1 + B2_CC * e2 + B3_CC * e3;
-            const double dva = -BETA1_CC * B1_CC * e1 - BETA2_CC * B2_CC * e2 - BETA3_CC * B3_CC * e3;
-            const double ux = dx * rinv, uy = dy * rinv, uz = dz * rinv;
-            const int mj = cnt[j];
-            const double gij = bo_sum_sl(sl, list, cap, i, m, j, dx, dy, dz, rinv);
-            const double gji = bo_sum_sl(sl, list, cap, j, mj, i, -dx, -dy, -dz, rinv);
-            const double bij = 1.0 / sqrt(1.0 + gij), bji = 1.0 / sqrt(1.0 + gji);
-            const double bbar = 0.5 * (bij + bji);
-            acc[0] += fcut * (vr - bbar * va);
-            const double fpair = (dfcut * (vr - bbar * va) + fcut * (dvr - bbar * dva)) * rinv;
-            fix += fpair * dx; fiy += fpair * dy; fiz += fpair * dz;
-            atomic_add3(F, j, -fpair * dx, -fpair * dy, -fpair * dz);
-            const double d[3] = {dx, dy, dz};
-#pragma unroll
-            for (int a = 0; a < 3; a++)
-#pragma unroll
-                for (int b = 0; b < 3; b++) acc[1 + a * 3 + b] -= d[a] * fpair * d[b];
-            bo_three_body_sl(F, sl, list, cap, i, m, j, dx, dy, dz, rinv, ux, uy, uz, gij, bij, fcut, va);
-            bo_three_body_sl(F, sl, list, cap, j, mj, i, -dx, -dy, -dz, rinv, -ux, -uy, -uz, gji, bji, fcut, va);
+        if (jn >= m) continue;
+        const SlotBO o = bo[t];
+        if (o.ok == 0.0) continue;
+        const int j = list[t];
+        const int mj = cnt[j];
+        int pn = -1;                          // partner slot j -> i
+        for (int kn = 0; kn < mj; kn++)
+            if (list[(size_t)j * cap + kn] == i) { pn = kn; break; }
+        if (j < i && pn < 0) continue;
+        const Slot q = sl[t];
+        three_body_sl(F, sl, list, cap, i, m, j, q.dx, q.dy, q.dz, q.rinv, o.coeff);
+        if (j < i) continue;
+        double bji;
+        if (pn >= 0) {
+            bji = bo[(size_t)j * cap + pn].b;
+        } else {
+            const double gji = bo_sum_sl(sl, list, cap, j, mj, i, -q.dx, -q.dy, -q.dz, q.rinv);
+            bji = 1.0 / sqrt(1.0 + gji);
+            three_body_sl(F, sl, list, cap, j, mj, i, -q.dx, -q.dy, -q.dz, q.rinv,
+                          three_body_coeff(gji, bji, q.fc, o.va));
         }
-        if (fix != 0.0 || fiy != 0.0 || fiz != 0.0) atomic_add3(F, i, fix, fiy, fiz);
+        const double bbar = 0.5 * (o.b + bji);
+        acc[0] += q.fc * (o.vr - bbar * o.va);
+        const double fpair = (q.dfc * (o.vr - bbar * o.va) + q.fc * (o.dvr - bbar * o.dva)) * q.rinv;
+        atomic_add3(F, i, fpair * q.dx, fpair * q.dy, fpair * q.dz);
+        atomic_add3(F, j, -fpair * q.dx, -fpair * q.dy, -fpair * q.dz);
+        const double d[3] = {q.dx, q.dy, q.dz};
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+#pragma unroll
+            for (int b = 0; b < 3; b++) acc[1 + a * 3 + b] -= d[a] * fpair * d[b];
     }
     block_sum_store<kNV>(acc, sm, part + (size_t)blockIdx.x * kNV);
 }
@@ -326,6 +408,16 @@ __device__ __forceinline__ double mimg1(double d, double hii, double hii_inv) {
     return __dmul_rn(hii, s);
 }
 
+// 1/x for x in the FP32 normal range: the FP32 hardware reciprocal (relative
+// error ~2^-23) refined by one Newton-Raphson step y + y (1 - x y), which
+// squares the error (~1e-14), in place of a full IEEE division.
+__device__ __forceinline__ double rcp_nr(double x) {
+    float yf;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"((float)x));
+    const double y = (double)yf;
+    return fma(y, fma(-x, y, 1.0), y);
+}
+
 // FP32 copies of the pair constants (FP32-pair precision).  sigma^2 is kept
 // as a head + tail pair: its FP32 rounding would scale every s^6 by the same
 // factor, a bias that the near-cancelling repulsive and attractive virial
@@ -353,7 +445,7 @@ __device__ __forceinline__ void lj_pair(double dx, double dy, double dz, const L
         fm = (double)(pf.c24 * (2.f * s12 - s6) * ri2);
         if (COUNT) e = (double)(pf.c4 * (s12 - s6)) - p.vshift;
     } else {
-        const double ri2 = 1.0 / r2, s2 = p.sig2 * ri2, s6 = s2 * s2 * s2, s12 = s6 * s6;
+        const double ri2 = rcp_nr(r2), s2 = p.sig2 * ri2, s6 = s2 * s2 * s2, s12 = s6 * s6;
         fm = p.c24 * (2 * s12 - s6) * ri2;
         if (COUNT) e = p.c4 * (s12 - s6) - p.vshift;
     }
@@ -374,14 +466,31 @@ __device__ __forceinline__ void lj_pair(double dx, double dy, double dz, const L
     }
 }
 
-// Entries per lane in flight: the index loads of U entries are issued
+// Entries per lane in flight (U): the index loads of U entries are issued
 // together, then their positions, then the pair arithmetic, so one warp has
-// U dependent load chains outstanding instead of one.
-constexpr int kLJUnroll = 4;
+// U dependent load chains outstanding instead of one.  PIPE additionally
+// software-pipelines the lane's loop: the indices and positions of the next
+// U entries are loaded before the current U are computed, so their latency
+// overlaps the arithmetic.
+template <int U>
+__device__ __forceinline__ void lj_fetch(const double* __restrict__ pos, const int* __restrict__ row,
+                                         const int* __restrict__ irow, int mo, int tot, int b, int i, int (&jj)[U],
+                                         double (&qx)[U], double (&qy)[U], double (&qz)[U]) {
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+        const int k = b + 32 * u;
+        jj[u] = k < mo ? row[k] : (k < tot ? irow[k] : -1);
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+        const int j = jj[u] < 0 ? i : jj[u];
+        qx[u] = pos[3 * j]; qy[u] = pos[3 * j + 1]; qz[u] = pos[3 * j + 2];
+    }
+}
 
 // One gather pass over atoms blk, blk + nblk, ... (in warps) of one system;
 // per-block {E, W9} into part[blk].  sm: 32 * kNV doubles, s_hh: 18.
-template <bool FULL_VIRIAL, bool F32, int U>
+template <bool FULL_VIRIAL, bool F32, int U, bool PIPE>
 __device__ __forceinline__ void lj_gather_body(const double* __restrict__ pos, const double* __restrict__ hh,
                                                const int* __restrict__ cnt, const int* __restrict__ list, int cap,
                                                const int* __restrict__ in_cnt, const int* __restrict__ in_list,
@@ -410,23 +519,23 @@ __device__ __forceinline__ void lj_gather_body(const double* __restrict__ pos, c
         const int tot = mo + mi;
         const int* row = list + (size_t)i * cap;
         const int* irow = in_list + (size_t)i * in_cap - mo;
+        int jj[U];
+        double qx[U], qy[U], qz[U];
+        if (PIPE && lane < tot) lj_fetch<U>(pos, row, irow, mo, tot, lane, i, jj, qx, qy, qz);
         for (int b = lane; b < tot; b += 32 * U) {
-            int jj[U];
+            int jc[U];
+            double cx[U], cy[U], cz[U];
+            if (PIPE) {
 #pragma unroll
-            for (int u = 0; u < U; u++) {
-                const int k = b + 32 * u;
-                jj[u] = k < mo ? row[k] : (k < tot ? irow[k] : -1);
-            }
-            double qx[U], qy[U], qz[U];
-#pragma unroll
-            for (int u = 0; u < U; u++) {
-                const int j = jj[u] < 0 ? i : jj[u];
-                qx[u] = pos[3 * j]; qy[u] = pos[3 * j + 1]; qz[u] = pos[3 * j + 2];
+                for (int u = 0; u < U; u++) { jc[u] = jj[u]; cx[u] = qx[u]; cy[u] = qy[u]; cz[u] = qz[u]; }
+                if (b + 32 * U < tot) lj_fetch<U>(pos, row, irow, mo, tot, b + 32 * U, i, jj, qx, qy, qz);
+            } else {
+                lj_fetch<U>(pos, row, irow, mo, tot, b, i, jc, cx, cy, cz);
             }
 #pragma unroll
             for (int u = 0; u < U; u++) {
-                if (jj[u] < 0) continue;
-                double dx = __dsub_rn(qx[u], px), dy = __dsub_rn(qy[u], py), dz = __dsub_rn(qz[u], pz);
+                if (jc[u] < 0) continue;
+                double dx = __dsub_rn(cx[u], px), dy = __dsub_rn(cy[u], py), dz = __dsub_rn(cz[u], pz);
                 if (diag) {
                     dx = mimg1(dx, h[0], hi[0]);
                     dy = mimg1(dy, h[4], hi[4]);
@@ -449,16 +558,16 @@ __device__ __forceinline__ void lj_gather_body(const double* __restrict__ pos, c
     block_sum_store<kNV>(acc, sm, part + (size_t)blk * kNV);
 }
 
-template <bool FULL_VIRIAL, bool F32>
-__global__ void __launch_bounds__(256, 2)
+template <bool FULL_VIRIAL, bool F32, int U, bool PIPE, int NT>
+__global__ void __launch_bounds__(NT)
 k_lj_gather(const double* __restrict__ pos, const double* __restrict__ hh, const int* __restrict__ cnt,
             const int* __restrict__ list, int cap, const int* __restrict__ in_cnt,
             const int* __restrict__ in_list, int in_cap, int na, double* __restrict__ F,
             double* __restrict__ Facc, LJP p, double* __restrict__ part) {
     __shared__ double sm[32 * kNV];
     __shared__ double s_hh[18];
-    lj_gather_body<FULL_VIRIAL, F32, kLJUnroll>(pos, hh, cnt, list, cap, in_cnt, in_list, in_cap, na, F, Facc, p,
-                                                part, blockIdx.x, gridDim.x, sm, s_hh);
+    lj_gather_body<FULL_VIRIAL, F32, U, PIPE>(pos, hh, cnt, list, cap, in_cnt, in_list, in_cap, na, F, Facc, p,
+                                              part, blockIdx.x, gridDim.x, sm, s_hh);
 }
 
 // Replica batch: the same gather over every replica in one launch; block b
@@ -471,7 +580,7 @@ k_b_lj_gather(const StepArrays* __restrict__ As, const int* __restrict__ off, in
     const int r = batch_rep(off, R, blockIdx.x);
     const StepArrays& a = As[r];
     const LJP p = lj_params_dev(ff);
-    lj_gather_body<FULL_VIRIAL, F32, U>(a.pos, a.S->h, a.cnt_a, a.list_a, a.cap_a, a.in_cnt, a.in_list, a.in_cap,
+    lj_gather_body<FULL_VIRIAL, F32, U, false>(a.pos, a.S->h, a.cnt_a, a.list_a, a.cap_a, a.in_cnt, a.in_list, a.in_cap,
                                         a.n, a.F, a.Facc, p, a.part_f2, blockIdx.x - off[r], off[r + 1] - off[r], sm,
                                         s_hh);
 }
@@ -514,25 +623,70 @@ cudaError_t rebo_slots_launch(const double* pos, const double* hh, const int* cn
                               int na, double* slots, double* F, double* part, int nblocks, const int* gate,
                               int want, cudaStream_t st) {
     Slot* sl = reinterpret_cast<Slot*>(slots);
+    SlotBO* bo = reinterpret_cast<SlotBO*>(slots + (size_t)na * cap * 8);
     k_rebo_slots<<<kForceBlocks, 256, 0, st>>>(pos, hh, cnt, list, cap, na, sl, gate, want);
-    k_rebo_sl<<<nblocks, 128, 0, st>>>(sl, cnt, list, cap, na, F, part, gate, want);
+    k_rebo_bo<<<kForceBlocks, 256, 0, st>>>(sl, cnt, list, cap, na, bo, gate, want);
+    k_rebo_force<<<nblocks, 256, 0, st>>>(sl, bo, cnt, list, cap, na, F, part, gate, want);
     return cudaGetLastError();
+}
+
+namespace {
+
+// Resident blocks per SM of one LJ gather instantiation (queried once).
+template <bool FV, bool F32, int U, bool PIPE, int NT>
+int lj_occupancy() {
+    static int occ = -1;
+    if (occ < 0) {
+        int b = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_lj_gather<FV, F32, U, PIPE, NT>, NT, 0) != cudaSuccess)
+            b = 1;
+        occ = b < 1 ? 1 : b;
+    }
+    return occ;
+}
+
+template <bool FV, bool F32, int U, bool PIPE, int NT>
+int lj_dispatch(bool launch, const double* pos, const double* hh, const int* cnt, const int* list, int cap,
+                const int* in_cnt, const int* in_list, int in_cap, int na, double* F, double* Facc, const LJP& p,
+                double* part, cudaStream_t st) {
+    const int nb = std::min(kLJMaxBlocks, lj_occupancy<FV, F32, U, PIPE, NT>() * kSMs);
+    if (launch)
+        k_lj_gather<FV, F32, U, PIPE, NT><<<nb, NT, 0, st>>>(pos, hh, cnt, list, cap, in_cnt, in_list, in_cap, na,
+                                                             F, Facc, p, part);
+    return nb;
+}
+
+// Launches (launch == true) or sizes the gather of one shape; returns its grid.
+int lj_select(bool launch, int ff, int precision, const LJShape& sh, const double* pos, const double* hh,
+              const int* cnt, const int* list, int cap, const int* in_cnt, const int* in_list, int in_cap, int na,
+              double* F, double* Facc, double* part, cudaStream_t st) {
+    const LJP p = lj_params(ff);
+    const bool fv = ff == FMD_FF_AIREBO, f32 = precision == FMD_PREC_FP32_PAIR;
+#define FMD_LJ_CALL(FV, F32, U, PIPE, NT) \
+    return lj_dispatch<FV, F32, U, PIPE, NT>(launch, pos, hh, cnt, list, cap, in_cnt, in_list, in_cap, na, F, Facc, p, part, st)
+#define FMD_LJ_NT(FV, F32, U, PIPE) \
+    if (sh.threads == 128) { FMD_LJ_CALL(FV, F32, U, PIPE, 128); } else { FMD_LJ_CALL(FV, F32, U, PIPE, 256); }
+#define FMD_LJ_PIPE(FV, F32, U) if (sh.pipe) { FMD_LJ_NT(FV, F32, U, true) } else { FMD_LJ_NT(FV, F32, U, false) }
+#define FMD_LJ_U(FV, F32) if (sh.unroll == 2) { FMD_LJ_PIPE(FV, F32, 2) } else { FMD_LJ_PIPE(FV, F32, 4) }
+    if (fv) { if (f32) { FMD_LJ_U(true, true) } else { FMD_LJ_U(true, false) } }
+    else { if (f32) { FMD_LJ_U(false, true) } else { FMD_LJ_U(false, false) } }
+#undef FMD_LJ_U
+#undef FMD_LJ_PIPE
+#undef FMD_LJ_NT
+#undef FMD_LJ_CALL
+}
+
+}  // namespace
+
+int lj_gather_blocks(int ff, int precision, const LJShape& sh) {
+    return lj_select(false, ff, precision, sh, nullptr, nullptr, nullptr, nullptr, 0, nullptr, nullptr, 0, 0, nullptr,
+                     nullptr, nullptr, nullptr);
 }
 
 cudaError_t lj_gather_launch(int ff, const double* pos, const double* hh, const int* cnt, const int* list,
                              int cap, const int* in_cnt, const int* in_list, int in_cap, int na, double* F,
-                             double* Facc, double* part, cudaStream_t st, int precision) {
-    const LJP p = lj_params(ff);
-    const bool f32 = precision == FMD_PREC_FP32_PAIR;
-#define FMD_LJ_ARGS pos, hh, cnt, list, cap, in_cnt, in_list, in_cap, na, F, Facc, p, part
-    if (ff == FMD_FF_AIREBO) {
-        if (f32) k_lj_gather<true, true><<<kForceBlocks, 256, 0, st>>>(FMD_LJ_ARGS);
-        else k_lj_gather<true, false><<<kForceBlocks, 256, 0, st>>>(FMD_LJ_ARGS);
-    } else {
-        if (f32) k_lj_gather<false, true><<<kForceBlocks, 256, 0, st>>>(FMD_LJ_ARGS);
-        else k_lj_gather<false, false><<<kForceBlocks, 256, 0, st>>>(FMD_LJ_ARGS);
-    }
-#undef FMD_LJ_ARGS
+                             double* Facc, double* part, cudaStream_t st, int precision, const LJShape& sh) {
+    lj_select(true, ff, precision, sh, pos, hh, cnt, list, cap, in_cnt, in_list, in_cap, na, F, Facc, part, st);
     return cudaGetLastError();
 }
 

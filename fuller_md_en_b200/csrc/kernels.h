@@ -26,6 +26,8 @@ struct CellList {
     int* slot_of = nullptr;     // [n]
     int* cell_of = nullptr;     // [n]
     float4* s4 = nullptr;       // [n] fractional coordinates (FP32)
+    float4* s4s = nullptr;      // [n] the same in cell order (cell_atoms order)
+    int* mols = nullptr;        // [n] molecule ids in cell order
     int cap_n[3] = {1, 1, 1};
     int cap_cells = 1;
     int n = 0;
@@ -37,9 +39,10 @@ void grid_dims_host(const double* h, double rc, int K, int* n);
 // K = 2 halves the candidate volume for large cutoffs; K = 1 suits small ones.
 cudaError_t cells_alloc(CellList& cl, int n, const double* h_host, double rc, int K = 1);
 void cells_free(CellList& cl);
-// hh = device pointer to {h[9], hi[9]}.  Bins pos[3*n] into cells.
+// hh = device pointer to {h[9], hi[9]}.  Bins pos[3*n] into cells; mol_id
+// (may be null) is copied into cell order beside the fractional coordinates.
 cudaError_t cells_build(CellList& cl, const double* pos, int n, const double* hh, double rc,
-                        DevErr* err, cudaStream_t st);
+                        DevErr* err, cudaStream_t st, const int* mol_id = nullptr);
 
 // -------------------------------------------------------- neighbour lists ----
 enum ListMode { LIST_SYM = 0, LIST_INTRA = 1, LIST_HALF = 2 };
@@ -54,6 +57,7 @@ size_t nlist_bitmap_smem(int n, int* warps_per_block);
 
 // ---------------------------------------------------------------- forces ----
 constexpr int kForceBlocks = kSMs * 4;     // grid of the reduction-producing kernels
+constexpr int kLJMaxBlocks = kSMs * 8;     // LJ gather grid cap (partial records of part_f2)
 constexpr int kNV = 10;                    // {E, W[9]} per block partial
 
 // REBO (a7): atomics into F, per-block {E, W9} partials in part[grid*kNV].
@@ -67,10 +71,11 @@ cudaError_t rebo_launch_grid(const double* pos, const double* hh, const int* cnt
 cudaError_t rebo_launch_gated(const double* pos, const double* hh, const int* cnt, const int* list, int cap,
                               int na, double* F, double* part, int nblocks, const int* gate, int want,
                               cudaStream_t st);
-// REBO through per-slot geometry records (the fast path): `slots` holds
-// kReboSlotDoubles doubles per list slot (na * cap records, device scratch
-// owned by the caller); otherwise as rebo_launch_gated (gate may be null).
-constexpr int kReboSlotDoubles = 8;
+// REBO through per-slot records (the fast path): `slots` holds
+// kReboSlotDoubles doubles per list slot (na * cap geometry records, then
+// na * cap bond-order records; device scratch owned by the caller); otherwise
+// as rebo_launch_gated (gate may be null).
+constexpr int kReboSlotDoubles = 16;
 cudaError_t rebo_slots_launch(const double* pos, const double* hh, const int* cnt, const int* list, int cap,
                               int na, double* slots, double* F, double* part, int nblocks, const int* gate,
                               int want, cudaStream_t st);
@@ -78,10 +83,18 @@ cudaError_t rebo_slots_launch(const double* pos, const double* hh, const int* cn
 // (unless Facc == F).  ff: FMD_FF_AIREBO / FMD_FF_MM.  precision:
 // FMD_PREC_FP64 (the reference's arithmetic) or FMD_PREC_FP32_PAIR (pair
 // algebra in FP32, FP64 minimum image, cutoff test and accumulation).
+// shape: threads per block (128/256), list entries in flight per lane (2/4)
+// and software pipelining; the grid is one full wave of the instantiation
+// (resident blocks per SM x SMs, at most kLJMaxBlocks) and writes that many
+// partial records -- lj_gather_blocks returns it.
+struct LJShape {
+    int threads = 256, unroll = 4, pipe = 0;
+};
+int lj_gather_blocks(int ff, int precision, const LJShape& shape);
 cudaError_t lj_gather_launch(int ff, const double* pos, const double* hh, const int* cnt,
                              const int* list, int cap, const int* in_cnt, const int* in_list,
                              int in_cap, int na, double* F, double* Facc, double* part,
-                             cudaStream_t st, int precision = FMD_PREC_FP64);
+                             cudaStream_t st, int precision = FMD_PREC_FP64, const LJShape& shape = LJShape{});
 // Rigid site-site LJ (a5-a6): writes F, T; per-block {E, W9} partials (grid n).
 cudaError_t rigid_launch(int precision, const double* pos, const double* qv, const double* body,
                          const double* hh, const int* cnt, const int* list, int cap, int n,

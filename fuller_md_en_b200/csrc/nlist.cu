@@ -117,11 +117,19 @@ k_scan(const int* __restrict__ cell_count, const GridDev* __restrict__ g, int* _
     if (threadIdx.x == 1023) cell_start[ncell] = sm[1023];
 }
 
+// Cell order: the candidate loop of the list kernel then reads ids,
+// fractional coordinates and molecule ids contiguously (coalesced) instead
+// of gathering them through the ids.
 __global__ void k_scatter(int n, const int* __restrict__ cell_of, const int* __restrict__ slot_of,
-                          const int* __restrict__ cell_start, int* __restrict__ cell_atoms) {
+                          const int* __restrict__ cell_start, int* __restrict__ cell_atoms,
+                          const float4* __restrict__ s4, const int* __restrict__ mol_id, float4* __restrict__ s4s,
+                          int* __restrict__ mols) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    cell_atoms[cell_start[cell_of[i]] + slot_of[i]] = i;
+    const int k = cell_start[cell_of[i]] + slot_of[i];
+    cell_atoms[k] = i;
+    s4s[k] = s4[i];
+    mols[k] = mol_id ? mol_id[i] : 0;
 }
 
 __device__ __forceinline__ int wrapc(int x, int n) {
@@ -160,9 +168,9 @@ template <int MODE>
 __global__ void __launch_bounds__(256)
 k_nlist(const GridDev* __restrict__ g, const int* __restrict__ cell_start,
         const int* __restrict__ cell_atoms, const int* __restrict__ cell_of,
-        const float4* __restrict__ s4, const double* __restrict__ pos,
-        const int* __restrict__ mol_id, int n, const double* __restrict__ hh, double rc2, int cap,
-        int words, int* __restrict__ cnt, int* __restrict__ list, int* __restrict__ dropped) {
+        const float4* __restrict__ s4, const float4* __restrict__ s4s, const int* __restrict__ mols,
+        const double* __restrict__ pos, const int* __restrict__ mol_id, int n, const double* __restrict__ hh,
+        double rc2, int cap, int words, int* __restrict__ cnt, int* __restrict__ list, int* __restrict__ dropped) {
     extern __shared__ unsigned bm_all[];
     __shared__ double s_hh[18];
     __shared__ GridDev G;
@@ -205,11 +213,11 @@ k_nlist(const GridDev* __restrict__ g, const int* __restrict__ cell_start,
                         const int j = cell_atoms[k];
                         bool ok = (MODE == LIST_HALF) ? (j > i) : (j != i);
                         if (ok && MODE != LIST_SYM) {
-                            const int mj = mol_id[j];
+                            const int mj = mols[k];
                             ok = (MODE == LIST_INTRA) ? (mj == mi) : (mj != mi);
                         }
                         if (ok && G.prefilter) {
-                            const float4 sj = s4[j];
+                            const float4 sj = s4s[k];
                             float dx = sj.x - si.x, dy = sj.y - si.y, dz = sj.z - si.z;
                             dx -= rintf(dx); dy -= rintf(dy); dz -= rintf(dz);
                             float ex = G.hf[0] * dx + G.hf[1] * dy + G.hf[2] * dz;
@@ -345,17 +353,19 @@ cudaError_t cells_alloc(CellList& cl, int n, const double* h_host, double rc, in
     if ((e = cudaMalloc(&cl.slot_of, sizeof(int) * nn)) != cudaSuccess) return e;
     if ((e = cudaMalloc(&cl.cell_of, sizeof(int) * nn)) != cudaSuccess) return e;
     if ((e = cudaMalloc(&cl.s4, sizeof(float4) * nn)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&cl.s4s, sizeof(float4) * nn)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&cl.mols, sizeof(int) * nn)) != cudaSuccess) return e;
     return cudaSuccess;
 }
 
 void cells_free(CellList& cl) {
     cudaFree(cl.grid); cudaFree(cl.cell_count); cudaFree(cl.cell_start); cudaFree(cl.cell_atoms);
-    cudaFree(cl.slot_of); cudaFree(cl.cell_of); cudaFree(cl.s4);
+    cudaFree(cl.slot_of); cudaFree(cl.cell_of); cudaFree(cl.s4); cudaFree(cl.s4s); cudaFree(cl.mols);
     cl = CellList();
 }
 
 cudaError_t cells_build(CellList& cl, const double* pos, int n, const double* hh, double rc,
-                        DevErr* err, cudaStream_t st) {
+                        DevErr* err, cudaStream_t st, const int* mol_id) {
     (void)err;
     k_grid<<<1, 32, 0, st>>>(hh, rc, cl.K, cl.cap_n[0], cl.cap_n[1], cl.cap_n[2], cl.grid);
     cudaMemsetAsync(cl.cell_count, 0, sizeof(int) * cl.cap_cells, st);
@@ -364,7 +374,8 @@ cudaError_t cells_build(CellList& cl, const double* pos, int n, const double* hh
     }
     k_scan<<<1, 1024, 0, st>>>(cl.cell_count, cl.grid, cl.cell_start);
     if (n > 0) {
-        k_scatter<<<(n + 255) / 256, 256, 0, st>>>(n, cl.cell_of, cl.slot_of, cl.cell_start, cl.cell_atoms);
+        k_scatter<<<(n + 255) / 256, 256, 0, st>>>(n, cl.cell_of, cl.slot_of, cl.cell_start, cl.cell_atoms, cl.s4,
+                                                   mol_id, cl.s4s, cl.mols);
     }
     return cudaGetLastError();
 }
@@ -397,7 +408,8 @@ cudaError_t launch_nlist(const CellList& cl, const double* pos, const int* mol_i
     if (blocks > kSMs * 16) blocks = kSMs * 16;
     if (blocks < 1) blocks = 1;
     k_nlist<MODE><<<blocks, 32 * wpb, smem, st>>>(cl.grid, cl.cell_start, cl.cell_atoms, cl.cell_of, cl.s4,
-                                                  pos, mol_id, n, hh, rc2, cap, words, cnt, list, dropped);
+                                                  cl.s4s, cl.mols, pos, mol_id, n, hh, rc2, cap, words, cnt, list,
+                                                  dropped);
     return cudaGetLastError();
 }
 }  // namespace

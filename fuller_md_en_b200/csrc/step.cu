@@ -29,6 +29,7 @@ namespace fmd {
 namespace {
 
 constexpr int kPB = 256;   // threads of per-particle kernels
+constexpr int kRedThreads = 512;   // the one-block reductions of the partial records
 constexpr double kMC = 12.011;
 
 __device__ __forceinline__ double clampd(double x, double lo, double hi) {
@@ -243,14 +244,21 @@ __global__ void __launch_bounds__(kPB) k_rescale(StepArrays a) {
 constexpr int kRedFields = 23;
 
 __device__ void reduce_all(const StepArrays& a, int nblk_f1, int nblk_ke, bool forces, bool kinetic,
-                           double* sm, double (&t)[kRedFields], int nblk_f2 = kForceBlocks) {
+                           double* sm, double (&t)[kRedFields], int nblk_f2) {
     double acc[kRedFields];
 #pragma unroll
     for (int k = 0; k < kRedFields; k++) acc[k] = 0.0;
     if (forces) {
-        const int nv1 = a.kind == FMD_SYS_MM ? kMMNV : kNV;
-        for (int b = threadIdx.x; b < nblk_f1; b += blockDim.x)
-            for (int k = 0; k < nv1; k++) acc[k] += a.part_f1[(size_t)b * nv1 + k];
+        // record widths as compile-time constants so each thread's loads issue together
+        if (a.kind == FMD_SYS_MM) {
+            for (int b = threadIdx.x; b < nblk_f1; b += blockDim.x)
+#pragma unroll
+                for (int k = 0; k < kMMNV; k++) acc[k] += a.part_f1[(size_t)b * kMMNV + k];
+        } else {
+            for (int b = threadIdx.x; b < nblk_f1; b += blockDim.x)
+#pragma unroll
+                for (int k = 0; k < kNV; k++) acc[k] += a.part_f1[(size_t)b * kNV + k];
+        }
         if (a.kind != FMD_SYS_RIGID)
             for (int b = threadIdx.x; b < nblk_f2; b += blockDim.x) {
 #pragma unroll
@@ -360,7 +368,7 @@ __device__ void rescale_end_body(const StepArrays& a, const StepParams& p, int n
     SysScal* S = a.S;
     const bool doit = S->do_rescale != 0;
     double t[kRedFields];
-    if (doit) reduce_all(a, 0, nblk_ke, false, true, sm, t);
+    if (doit) reduce_all(a, 0, nblk_ke, false, true, sm, t, 0);
     if (threadIdx.x != 0) return;
     if (doit) {
         kinetic_from_sums(a, t);
@@ -374,20 +382,20 @@ __device__ void rescale_end_body(const StepArrays& a, const StepParams& p, int n
 
 namespace {
 
-__global__ void __launch_bounds__(256) k_end(StepArrays a, StepParams p, int nblk_f1, int nblk_ke) {
+__global__ void __launch_bounds__(kRedThreads) k_end(StepArrays a, StepParams p, int nblk_f1, int nblk_ke) {
     __shared__ double sm[32 * kRedFields];
-    end_body(a, p, nblk_f1, nblk_ke, kForceBlocks, sm);
+    end_body(a, p, nblk_f1, nblk_ke, a.lj_blocks, sm);
 }
 
-__global__ void __launch_bounds__(256) k_rescale_end(StepArrays a, StepParams p, int nblk_ke) {
+__global__ void __launch_bounds__(kRedThreads) k_rescale_end(StepArrays a, StepParams p, int nblk_ke) {
     __shared__ double sm[32 * kRedFields];
     rescale_end_body(a, p, nblk_ke, sm);
 }
 
-__global__ void __launch_bounds__(256) k_ke_final(StepArrays a, int nblk_ke) {
+__global__ void __launch_bounds__(kRedThreads) k_ke_final(StepArrays a, int nblk_ke) {
     __shared__ double sm[32 * kRedFields];
     double t[kRedFields];
-    reduce_all(a, 0, nblk_ke, false, true, sm, t);
+    reduce_all(a, 0, nblk_ke, false, true, sm, t, 0);
     if (threadIdx.x == 0) kinetic_from_sums(a, t);
 }
 
@@ -428,10 +436,10 @@ __global__ void __launch_bounds__(256) k_b_rescale_end(BatchDev b) {
     rescale_end_body(b.A[r], b.P[r], b.off_atom[r + 1] - b.off_atom[r], sm);
 }
 
-__global__ void __launch_bounds__(256) k_force_final(StepArrays a, int nblk_f1) {
+__global__ void __launch_bounds__(kRedThreads) k_force_final(StepArrays a, int nblk_f1) {
     __shared__ double sm[32 * kRedFields];
     double t[kRedFields];
-    reduce_all(a, nblk_f1, 0, true, false, sm, t);
+    reduce_all(a, nblk_f1, 0, true, false, sm, t, a.lj_blocks);
     if (threadIdx.x == 0) forces_from_sums(a, t);
 }
 
@@ -455,25 +463,25 @@ cudaError_t enqueue_forces(const StepArrays& a, cudaStream_t st, bool judge) {
         else e = rebo_launch(a.pos, hh, a.cnt_b, a.list_b, a.cap_b, a.n, a.Facc, a.part_f1, st);
         if (e != cudaSuccess) return e;
         e = lj_gather_launch(FMD_FF_AIREBO, a.pos, hh, a.cnt_a, a.list_a, a.cap_a, a.in_cnt, a.in_list, a.in_cap,
-                             a.n, a.F, a.Facc, a.part_f2, st, a.precision);
+                             a.n, a.F, a.Facc, a.part_f2, st, a.precision, a.lj_shape);
     } else {
         if ((e = mm_bonded_launch(a.topo, a.pos, hh, a.Facc, a.part_f1, st)) != cudaSuccess) return e;
         if (a.has_charge)
             if ((e = mm_coulomb_launch(a.pos, hh, a.charge, a.mol_id, a.n, a.Facc, a.part_f3, st)) != cudaSuccess) return e;
         e = lj_gather_launch(FMD_FF_MM, a.pos, hh, a.cnt_a, a.list_a, a.cap_a, a.in_cnt, a.in_list, a.in_cap,
-                             a.n, a.F, a.Facc, a.part_f2, st, a.precision);
+                             a.n, a.F, a.Facc, a.part_f2, st, a.precision, a.lj_shape);
     }
     return e;
 }
 
 cudaError_t enqueue_force_reduce(const StepArrays& a, cudaStream_t st) {
-    k_force_final<<<1, 256, 0, st>>>(a, force_partial_blocks(a));
+    k_force_final<<<1, kRedThreads, 0, st>>>(a, force_partial_blocks(a));
     return cudaGetLastError();
 }
 
 cudaError_t enqueue_ke(const StepArrays& a, cudaStream_t st) {
     k_ke_partial<<<kForceBlocks, kPB, 0, st>>>(a);
-    k_ke_final<<<1, 256, 0, st>>>(a, kForceBlocks);
+    k_ke_final<<<1, kRedThreads, 0, st>>>(a, kForceBlocks);
     return cudaGetLastError();
 }
 
@@ -484,10 +492,10 @@ cudaError_t enqueue_step(const StepArrays& a, const StepParams& p, bool rescale_
     k_kick<<<kForceBlocks, kPB, 0, st>>>(a, p.dt);
     if ((e = enqueue_forces(a, st, judge)) != cudaSuccess) return e;
     k_kick2<<<kForceBlocks, kPB, 0, st>>>(a, p.dt);
-    k_end<<<1, 256, 0, st>>>(a, p, force_partial_blocks(a), kForceBlocks);
+    k_end<<<1, kRedThreads, 0, st>>>(a, p, force_partial_blocks(a), kForceBlocks);
     if (rescale_phase && p.schedule) {
         k_rescale<<<kForceBlocks, kPB, 0, st>>>(a);
-        k_rescale_end<<<1, 256, 0, st>>>(a, p, kForceBlocks);
+        k_rescale_end<<<1, kRedThreads, 0, st>>>(a, p, kForceBlocks);
     }
     return cudaGetLastError();
 }

@@ -54,6 +54,8 @@ struct StepArrays {
     MMTopoDev topo{};
     double rmcut2 = 0, Mmol = 0, I0 = 0;
     int precision = FMD_PREC_FP64;
+    LJShape lj_shape{};            // launch shape of the atomistic LJ gather
+    int lj_blocks = 0;             // its grid = partial records in part_f2
     SgStep* sg = nullptr;          // AIREBO: learned REBO term instead of the plain kernel
     int rebo_blocks = kForceBlocks;  // partial records the REBO term writes into part_f1
 };

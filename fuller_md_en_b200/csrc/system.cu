@@ -6,7 +6,9 @@
 #include <cmath>
 #include <cstddef>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <tuple>
 #include "step.h"
 #include "system.h"
 #include "sg_host.h"
@@ -59,7 +61,7 @@ int System::alloc_common(const double* pos_h, const double* vel_h, const double*
     if (alloc(&arr.pos, 3 * (size_t)n, pos_h) || alloc(&arr.vel, 3 * (size_t)n, vel_h) ||
         alloc(&arr.F, 3 * (size_t)n, (const double*)nullptr) || alloc(&arr.Facc, 3 * (size_t)n, (const double*)nullptr) ||
         alloc(&arr.part_f1, (size_t)std::max(kForceBlocks, n) * kNV, (const double*)nullptr) ||
-        alloc(&arr.part_f2, (size_t)kForceBlocks * kNV, (const double*)nullptr) ||
+        alloc(&arr.part_f2, (size_t)kLJMaxBlocks * kNV, (const double*)nullptr) ||
         alloc(&arr.part_f3, (size_t)kForceBlocks, (const double*)nullptr) ||
         alloc(&arr.part_ke, (size_t)kForceBlocks * 2, (const double*)nullptr) ||
         alloc(&dropped, 2, (const int*)nullptr) || alloc(&arr.S, 1, (const SysScal*)nullptr))
@@ -120,18 +122,67 @@ cudaError_t System::enqueue_rebuild(cudaStream_t st) {
                            dropped, ctx->d_err, st);
     }
     if (arr.kind == FMD_SYS_AIREBO) {
-        if ((e = cells_build(cells_b, arr.pos, arr.n, hh, rc_b, ctx->d_err, st)) != cudaSuccess) return e;
+        if ((e = cells_build(cells_b, arr.pos, arr.n, hh, rc_b, ctx->d_err, st, arr.mol_id)) != cudaSuccess) return e;
         if ((e = nlist_build(cells_b, LIST_INTRA, arr.pos, arr.mol_id, arr.n, hh, rc2_b, arr.cap_b,
                              const_cast<int*>(arr.cnt_b), const_cast<int*>(arr.list_b), dropped + 1,
                              ctx->d_err, st)) != cudaSuccess)
             return e;
     }
-    if ((e = cells_build(cells_a, arr.pos, arr.n, hh, rc_a, ctx->d_err, st)) != cudaSuccess) return e;
+    if ((e = cells_build(cells_a, arr.pos, arr.n, hh, rc_a, ctx->d_err, st, arr.mol_id)) != cudaSuccess) return e;
     if ((e = nlist_build(cells_a, LIST_HALF, arr.pos, arr.mol_id, arr.n, hh, rc2_a, arr.cap_a, cnt_a, list_a,
                          dropped, ctx->d_err, st)) != cudaSuccess)
         return e;
     return nlist_transpose(arr.cnt_a, arr.list_a, arr.cap_a, arr.n, const_cast<int*>(arr.in_cnt),
                            const_cast<int*>(arr.in_list), arr.in_cap, ctx->d_err, st);
+}
+
+// Launch shape of the atomistic LJ gather: every candidate (threads per
+// block, list entries in flight per lane, software pipelining) is timed on
+// this system's own lists at set-up and the fastest kept; the choice is
+// cached per (device, kind, atoms, list width, precision) for the process.
+int System::tune_lj() {
+    static std::map<std::tuple<int, int, int, int, int>, LJShape> cache;
+    const int ff = arr.kind == FMD_SYS_AIREBO ? FMD_FF_AIREBO : FMD_FF_MM;
+    const auto key = std::make_tuple(ctx->device, arr.kind, arr.n, arr.cap_a, arr.precision);
+    cudaStream_t st = ctx->stream;
+    auto it = cache.find(key);
+    if (it != cache.end()) {
+        arr.lj_shape = it->second;
+    } else {
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        float best = 1e30f;
+        LJShape pick;
+        for (int nt : {128, 256})
+            for (int u : {2, 4})
+                for (int pipe : {0, 1}) {
+                    const LJShape sh{nt, u, pipe};
+                    auto go = [&]() {
+                        return lj_gather_launch(ff, arr.pos, arr.S->h, arr.cnt_a, arr.list_a, arr.cap_a, arr.in_cnt,
+                                                arr.in_list, arr.in_cap, arr.n, arr.Facc, arr.Facc, arr.part_f2, st,
+                                                arr.precision, sh);
+                    };
+                    go();
+                    cudaEventRecord(e0, st);
+                    for (int r = 0; r < 3; r++) go();
+                    cudaEventRecord(e1, st);
+                    cudaEventSynchronize(e1);
+                    float ms = 0.f;
+                    cudaEventElapsedTime(&ms, e0, e1);
+                    if (ms < best) { best = ms; pick = sh; }
+                }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        // the timing runs accumulated into Facc
+        cudaMemsetAsync(arr.Facc, 0, sizeof(double) * 3 * (size_t)arr.n, st);
+        const int rc = ctx->sync_check("LJ launch-shape tuning");
+        if (rc != FMD_OK) return rc;
+        cache[key] = pick;
+        arr.lj_shape = pick;
+    }
+    arr.lj_blocks = lj_gather_blocks(ff, arr.precision, arr.lj_shape);
+    return FMD_OK;
 }
 
 int System::init() {
@@ -140,6 +191,10 @@ int System::init() {
     // then apply_pbc, then the first forces (LJ:813-828, AI:830-853).
     if (enqueue_rebuild(st) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "list build launch failed");
     if (apply_pbc_launch(arr.pos, arr.n, arr.S->h, st) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "apply_pbc failed");
+    if (arr.kind != FMD_SYS_RIGID) {
+        const int rc = tune_lj();
+        if (rc != FMD_OK) return rc;
+    }
     if (enqueue_forces(arr, st) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "force launch failed");
     if (enqueue_force_reduce(arr, st) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "reduce launch failed");
     if (enqueue_ke(arr, st) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "kinetic launch failed");
@@ -286,6 +341,7 @@ extern "C" int fmd_system_create_airebo(fmd_ctx* ctx, const fmd_run_params* p, i
     s->arr.kind = FMD_SYS_AIREBO;
     s->arr.n = na;
     s->arr.precision = p->precision;
+    s->arr.lj_blocks = lj_gather_blocks(FMD_FF_AIREBO, p->precision, s->arr.lj_shape);
     int rc = s->alloc_common(pos, vel, h, npt);
     if (rc != FMD_OK) return rc;
     double* m; int* mid;
@@ -310,6 +366,7 @@ extern "C" int fmd_system_create_mm(fmd_ctx* ctx, const fmd_run_params* p, int n
     s->arr.kind = FMD_SYS_MM;
     s->arr.n = na;
     s->arr.precision = p->precision;
+    s->arr.lj_blocks = lj_gather_blocks(FMD_FF_MM, p->precision, s->arr.lj_shape);
     int rc = s->alloc_common(pos, vel, h, npt);
     if (rc != FMD_OK) return rc;
     int* mid;
@@ -436,7 +493,7 @@ extern "C" int fmd_system_kernel_ms(fmd_system* s, int stage, int reps, double* 
                 // Timed into the scratch accumulator (F itself is left alone).
                 return lj_gather_launch(a.kind == FMD_SYS_AIREBO ? FMD_FF_AIREBO : FMD_FF_MM, a.pos, hh, a.cnt_a,
                                         a.list_a, a.cap_a, a.in_cnt, a.in_list, a.in_cap, a.n, a.Facc, a.Facc,
-                                        a.part_f2, st, a.precision);
+                                        a.part_f2, st, a.precision, a.lj_shape);
             case 1:
                 if (a.kind == FMD_SYS_AIREBO && a.sg)   // the REBO term the step uses
                     return sg_enqueue_rebo(*a.sg, a, false, st);
@@ -475,6 +532,16 @@ extern "C" int fmd_system_kernel_ms(fmd_system* s, int stage, int reps, double* 
     if (err != cudaSuccess) return y.ctx->fail(FMD_ERR_CUDA, cudaGetErrorString(err));
     *ms = (double)tot / reps;
     return rc;
+}
+
+extern "C" int fmd_system_lj_shape(fmd_system* s, int* threads, int* unroll, int* pipelined, int* blocks) {
+    if (!s || !s->sys) return FMD_ERR_ARG;
+    const StepArrays& a = s->sys->arr;
+    if (threads) *threads = a.lj_shape.threads;
+    if (unroll) *unroll = a.lj_shape.unroll;
+    if (pipelined) *pipelined = a.lj_shape.pipe;
+    if (blocks) *blocks = a.lj_blocks;
+    return FMD_OK;
 }
 
 extern "C" int fmd_system_step_kernels(fmd_system* s, int rebuild, int phase, int* nk) {

@@ -33,6 +33,7 @@ struct System {
     cudaError_t enqueue_one(int g, cudaStream_t st);
     bool judge_step(int g) const { return arr.sg && arr.sg->judge_every > 0 && g % arr.sg->judge_every == 0; }
     int init();
+    int tune_lj();
     int capture(bool rebuild, bool phase, bool judge = false);
     void drop_graphs();
     int use_surrogate(fmd_sg* model, int judge_every, double rmse_max);

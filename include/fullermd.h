@@ -249,6 +249,10 @@ int fmd_system_destroy(fmd_system *s);
  * of each variant (list rebuild or not; phase bit 0: cold/warm phase, bit 1:
  * a judge step of the learned REBO term). */
 int fmd_system_kernel_ms(fmd_system *s, int stage, int reps, double *ms_per_launch);
+/* Launch shape of the atomistic LJ gather that fmd_system_init's autotuner
+ * chose (threads per block, list entries in flight per lane, software
+ * pipelining 0/1, grid blocks); any pointer may be NULL. */
+int fmd_system_lj_shape(fmd_system *s, int *threads, int *unroll, int *pipelined, int *blocks);
 int fmd_system_step_kernels(fmd_system *s, int rebuild, int phase, int *nkernels);
 
 /* ------------------------------------------------------- replica batches --

@@ -122,6 +122,25 @@ def test_airebo_forces(ctx, golden, oracle, nc):
     assert rel(W2, g["W_lj"]) < FP64_TOL
 
 
+@pytest.mark.parametrize("cap,jitter", [(2, 0.05), (3, 0.3), (12, 0.4)])
+def test_rebo_truncated_and_crowded_rows(ctx, oracle, cap, jitter):
+    """REBO with rows truncated at `cap` (the reference keeps the first cap
+    partners, so i may list j while j's row lacks i) and with crowded rows
+    from a strongly jittered crystal: the slot passes against the oracle."""
+    s = crystal.atomistic(1, jitter=jitter, seed=77)
+    na = s["pos"].size // 3
+    pos = oracle.apply_pbc(s["pos"].copy(), s["h"], s["hi"])
+    cnt, lst, _ = oracle.nlist_intra(pos, s["h"], s["hi"], na, s["mol_id"], cap=cap)
+    if cap < 12:
+        rowsets = [set(lst[k * cap:k * cap + cnt[k]]) for k in range(na)]
+        assert any(i not in rowsets[j] for i in range(na) for j in rowsets[i])   # asymmetric
+    oe, oF, oW = oracle.rebo(pos, s["h"], s["hi"], cnt, lst, na, cap=cap)
+    F, W = np.zeros(3 * na), np.zeros(9)
+    e = ctx.compute_rebo(F, W, pos, s["h"], s["hi"], cnt, lst, na, max_neigh=cap)
+    assert abs(e - oe) < FP64_TOL * abs(oe)
+    assert rel(F, oF) < FP64_TOL and rel(W, oW) < FP64_TOL
+
+
 @pytest.mark.parametrize("nc", [2, 3])
 def test_rigid_forces_fp64(ctx, golden, nc):
     g = golden(f"rigid_nc{nc}")
