@@ -402,9 +402,13 @@ LJP lj_params(int ff) { return lj_params_dev(ff); }
 // off-diagonals the reference's s = hi0*dx + hi1*dy + hi2*dz and
 // d = h0*s0 + h1*s1 + h2*s2 reduce exactly to these products (adding +-0
 // changes nothing), so this is bitwise the reference's mimg.
+// For |s| < 1.5 (always so for wrapped positions) round(s), half away from
+// zero, is one of -1, 0, 1 and two comparisons give it exactly.
 __device__ __forceinline__ double mimg1(double d, double hii, double hii_inv) {
     double s = __dmul_rn(hii_inv, d);
-    s = __dsub_rn(s, round(s));
+    double r = s >= 0.5 ? 1.0 : (s <= -0.5 ? -1.0 : 0.0);
+    if (!(fabs(s) < 1.5)) r = round(s);
+    s = __dsub_rn(s, r);
     return __dmul_rn(hii, s);
 }
 

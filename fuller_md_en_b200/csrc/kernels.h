@@ -41,18 +41,19 @@ cudaError_t cells_alloc(CellList& cl, int n, const double* h_host, double rc, in
 void cells_free(CellList& cl);
 // hh = device pointer to {h[9], hi[9]}.  Bins pos[3*n] into cells; mol_id
 // (may be null) is copied into cell order beside the fractional coordinates.
+// gate (device int, may be null): the cell-grid kernels do nothing while it is set.
 cudaError_t cells_build(CellList& cl, const double* pos, int n, const double* hh, double rc,
-                        DevErr* err, cudaStream_t st, const int* mol_id = nullptr);
+                        DevErr* err, cudaStream_t st, const int* mol_id = nullptr, const int* gate = nullptr);
 
 // -------------------------------------------------------- neighbour lists ----
 enum ListMode { LIST_SYM = 0, LIST_INTRA = 1, LIST_HALF = 2 };
 // Reference-exact list into cnt[n], list[n*cap]; *dropped (device int) += overflow.
 cudaError_t nlist_build(const CellList& cl, int mode, const double* pos, const int* mol_id, int n,
                         const double* hh, double rc2, int cap, int* cnt, int* list, int* dropped,
-                        DevErr* err, cudaStream_t st);
+                        DevErr* err, cudaStream_t st, const int* gate = nullptr);
 // Incoming (transposed) entries of a half list, sorted ascending per row.
 cudaError_t nlist_transpose(const int* cnt, const int* list, int cap, int n, int* in_cnt,
-                            int* in_list, int in_cap, DevErr* err, cudaStream_t st);
+                            int* in_list, int in_cap, DevErr* err, cudaStream_t st, const int* gate = nullptr);
 size_t nlist_bitmap_smem(int n, int* warps_per_block);
 
 // ---------------------------------------------------------------- forces ----

@@ -1,0 +1,316 @@
+// molnlist.cu -- neighbour lists of atomistic systems whose molecules are
+// contiguous index ranges (every crystal the reference builds: AI:781-786,
+// MM:1094-1111), bit-exact with the reference's O(N^2) builders
+// (build_nlist_rebo AI:251-261, build_nlist_lj AI:263-272, MM:337-346).
+//
+// With contiguous molecules, j > i between different molecules means
+// molecule(j) > molecule(i), so the half-list row of atom i is the accepted
+// atoms of the higher-numbered neighbour molecules in ascending order: the row
+// comes out sorted without a bitmap, its first `cap` entries are the
+// reference's truncation, and the candidates of one molecule are contiguous
+// in memory (coalesced loads).  The incoming (transposed) rows of the LJ
+// gather come out of the same walk over lower-numbered molecules, keeping
+// (i, j) when it passes the same FP64 test and sits inside row i's first
+// `cap` entries.  Intramolecular (REBO) rows walk the atom's own molecule.
+//
+// Candidate molecules: a centre c and radius R per molecule, and molecule
+// pairs with |c_A - c_B| <= rc + R_A + R_B (minimum image).  For a diagonal
+// cell the reference's minimum image is the true nearest image per axis, the
+// distance is a metric on the torus, and the triangle inequality makes the
+// molecule test conservative.  For other cells, when a molecule has more
+// partners than the table holds (a disintegrating crystal), the system falls
+// back to the cell-grid builder (nlist.cu) for that rebuild: a device flag
+// gates the two paths inside one CUDA graph.
+#include <cmath>
+
+#include "geom.cuh"
+#include "kernels.h"
+#include "molnlist.h"
+
+namespace fmd {
+namespace {
+
+__device__ __forceinline__ bool diag_cell(const double* h, const double* hi) {
+    return h[1] == 0.0 && h[2] == 0.0 && h[3] == 0.0 && h[5] == 0.0 && h[6] == 0.0 && h[7] == 0.0 &&
+           hi[1] == 0.0 && hi[2] == 0.0 && hi[3] == 0.0 && hi[5] == 0.0 && hi[6] == 0.0 && hi[7] == 0.0;
+}
+
+// One component of the reference's minimum image in a diagonal cell (the
+// general formula with zero off-diagonals; round(s) by comparisons for |s| < 1.5).
+__device__ __forceinline__ double mimg_axis(double d, double hii, double hii_inv) {
+    double s = __dmul_rn(hii_inv, d);
+    double r = s >= 0.5 ? 1.0 : (s <= -0.5 ? -1.0 : 0.0);
+    if (!(fabs(s) < 1.5)) r = round(s);
+    s = __dsub_rn(s, r);
+    return __dmul_rn(hii, s);
+}
+
+// The reference's pair test r^2 < rc2 for d = pos[j] - pos[i] (AI:258, 268).
+__device__ __forceinline__ bool pair_in(const double* __restrict__ pos, int i, int j, const double* h,
+                                        const double* hi, bool diag, double rc2) {
+    double dx = __dsub_rn(pos[3 * j], pos[3 * i]), dy = __dsub_rn(pos[3 * j + 1], pos[3 * i + 1]),
+           dz = __dsub_rn(pos[3 * j + 2], pos[3 * i + 2]);
+    if (diag) {
+        dx = mimg_axis(dx, h[0], hi[0]);
+        dy = mimg_axis(dy, h[4], hi[4]);
+        dz = mimg_axis(dz, h[8], hi[8]);
+    } else {
+        mimg(dx, dy, dz, hi, h);
+    }
+    return norm2_rn(dx, dy, dz) < rc2;
+}
+
+// Centre (mean of the minimum images relative to the first atom) and radius
+// (largest minimum-image distance of an atom from the centre) per molecule;
+// one warp per molecule.  Resets the partner-overflow flag.
+__global__ void k_mol_centre(const double* __restrict__ pos, const double* __restrict__ hh,
+                             const int* __restrict__ off, int M, double* __restrict__ cen, double* __restrict__ rad,
+                             int* __restrict__ flag) {
+    const double* h = hh;
+    const double* hi = hh + 9;
+    const int lane = threadIdx.x & 31;
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (blockIdx.x == 0 && threadIdx.x == 0) flag[1] = 0;
+    if (w >= M) return;
+    const int a0 = off[w], a1 = off[w + 1];
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    for (int a = a0 + lane; a < a1; a += 32) {
+        double dx = pos[3 * a] - pos[3 * a0], dy = pos[3 * a + 1] - pos[3 * a0 + 1], dz = pos[3 * a + 2] - pos[3 * a0 + 2];
+        mimg(dx, dy, dz, hi, h);
+        sx += dx; sy += dy; sz += dz;
+    }
+    sx = warp_sum(sx); sy = warp_sum(sy); sz = warp_sum(sz);
+    const double inv = 1.0 / (a1 - a0);
+    const double cx = pos[3 * a0] + sx * inv, cy = pos[3 * a0 + 1] + sy * inv, cz = pos[3 * a0 + 2] + sz * inv;
+    double r2 = 0.0;
+    for (int a = a0 + lane; a < a1; a += 32) {
+        double dx = pos[3 * a] - cx, dy = pos[3 * a + 1] - cy, dz = pos[3 * a + 2] - cz;
+        mimg(dx, dy, dz, hi, h);
+        r2 = fmax(r2, dx * dx + dy * dy + dz * dz);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) r2 = fmax(r2, __shfl_xor_sync(kFull, r2, o));
+    if (lane == 0) {
+        cen[3 * w] = cx; cen[3 * w + 1] = cy; cen[3 * w + 2] = cz;
+        rad[w] = sqrt(r2);
+    }
+}
+
+// Partner molecules of each molecule (both directions, ascending); one warp
+// per molecule.  flag[0] = 1 when the molecule path is valid for this
+// rebuild (diagonal cell, no table overflow), else 0.
+__global__ void k_mol_pairs(const double* __restrict__ hh, int M, const double* __restrict__ cen,
+                            const double* __restrict__ rad, double rc, int pmax, int* __restrict__ npart,
+                            int* __restrict__ part, int* __restrict__ flag) {
+    const double* h = hh;
+    const double* hi = hh + 9;
+    const int lane = threadIdx.x & 31;
+    const int A = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (A >= M) return;
+    const double cx = cen[3 * A], cy = cen[3 * A + 1], cz = cen[3 * A + 2], ra = rad[A];
+    int n = 0;
+    for (int b0 = 0; b0 < M; b0 += 32) {
+        const int B = b0 + lane;
+        bool ok = false;
+        if (B < M && B != A) {
+            double dx = cen[3 * B] - cx, dy = cen[3 * B + 1] - cy, dz = cen[3 * B + 2] - cz;
+            mimg(dx, dy, dz, hi, h);
+            const double lim = (rc + ra + rad[B]) * (1.0 + 1e-9) + 1e-6;   // rounding margin
+            ok = dx * dx + dy * dy + dz * dz <= lim * lim;
+        }
+        const unsigned m = __ballot_sync(kFull, ok);
+        const int k = n + __popc(m & ((1u << lane) - 1u));
+        if (ok && k < pmax) part[(size_t)A * pmax + k] = B;
+        n += __popc(m);
+    }
+    if (lane == 0) {
+        npart[A] = n < pmax ? n : pmax;
+        if (n > pmax) atomicOr(&flag[1], 1);
+    }
+}
+
+__global__ void k_mol_decide(const double* __restrict__ hh, int* __restrict__ flag) {
+    if (threadIdx.x == 0) flag[0] = (diag_cell(hh, hh + 9) && flag[1] == 0) ? 1 : 0;
+}
+
+// Emits the accepted candidates j = c0 .. c1-1 (ascending) of the row being
+// built; `emitted` counts every accepted candidate, entries past `cap` are
+// not stored.
+__device__ __forceinline__ void emit_range(const double* __restrict__ pos, int i, int c0, int c1, const double* h,
+                                           const double* hi, bool diag, double rc2, bool intra, int cap,
+                                           int* __restrict__ row, int& emitted, int lane) {
+    for (int b = c0; b < c1; b += 32) {
+        const int j = b + lane;
+        const bool ok = j < c1 && (!intra || j != i) && pair_in(pos, i, j, h, hi, diag, rc2);
+        const unsigned m = __ballot_sync(kFull, ok);
+        const int k = emitted + __popc(m & ((1u << lane) - 1u));
+        if (ok && k < cap) row[k] = j;
+        emitted += __popc(m);
+    }
+}
+
+// Rows of the intermolecular half list (MODE 0) or the intramolecular list
+// (MODE 1); one warp per atom.
+template <int MODE>
+__global__ void __launch_bounds__(256)
+k_mol_rows(const double* __restrict__ pos, const double* __restrict__ hh, int n, const int* __restrict__ off,
+           const int* __restrict__ amol, const int* __restrict__ npart, const int* __restrict__ part, int pmax,
+           double rc2, int cap, int* __restrict__ cnt, int* __restrict__ list, int* __restrict__ tot,
+           int* __restrict__ dropped, const int* __restrict__ flag) {
+    if (MODE == 0 && flag[0] == 0) return;
+    __shared__ double s_hh[18];
+    if (threadIdx.x < 18) s_hh[threadIdx.x] = hh[threadIdx.x];
+    __syncthreads();
+    const double* h = s_hh;
+    const double* hi = s_hh + 9;
+    const bool diag = diag_cell(h, hi);
+    const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    for (int i = blockIdx.x * wpb + (threadIdx.x >> 5); i < n; i += gridDim.x * wpb) {
+        const int A = amol[i];
+        int* row = list + (size_t)i * cap;
+        int emitted = 0;
+        if (MODE == 1) {
+            emit_range(pos, i, off[A], off[A + 1], h, hi, diag, rc2, true, cap, row, emitted, lane);
+        } else {
+            const int np = npart[A];
+            for (int p = 0; p < np; p++) {
+                const int B = part[(size_t)A * pmax + p];
+                if (B < A) continue;
+                emit_range(pos, i, off[B], off[B + 1], h, hi, diag, rc2, false, cap, row, emitted, lane);
+            }
+        }
+        if (lane == 0) {
+            cnt[i] = emitted < cap ? emitted : cap;
+            if (tot) tot[i] = emitted;
+            if (emitted > cap && dropped) atomicAdd(dropped, emitted - cap);
+        }
+    }
+}
+
+// Incoming rows of the half list: for atom j, the atoms i < j of lower
+// neighbour molecules whose row holds j (the FP64 test from i's side, and j
+// within row i's first `cap` accepted entries); one warp per atom.
+__global__ void __launch_bounds__(256)
+k_mol_incoming(const double* __restrict__ pos, const double* __restrict__ hh, int n, const int* __restrict__ off,
+               const int* __restrict__ amol, const int* __restrict__ npart, const int* __restrict__ part, int pmax,
+               double rc2, int cap, const int* __restrict__ list, const int* __restrict__ tot,
+               int* __restrict__ in_cnt, int* __restrict__ in_list, int in_cap, DevErr* err,
+               const int* __restrict__ flag) {
+    if (flag[0] == 0) return;
+    __shared__ double s_hh[18];
+    if (threadIdx.x < 18) s_hh[threadIdx.x] = hh[threadIdx.x];
+    __syncthreads();
+    const double* h = s_hh;
+    const double* hi = s_hh + 9;
+    const bool diag = diag_cell(h, hi);
+    const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    for (int j = blockIdx.x * wpb + (threadIdx.x >> 5); j < n; j += gridDim.x * wpb) {
+        const int B = amol[j];
+        int* row = in_list + (size_t)j * in_cap;
+        int emitted = 0;
+        const int np = npart[B];
+        for (int p = 0; p < np; p++) {
+            const int A = part[(size_t)B * pmax + p];
+            if (A > B) break;                      // partners are ascending
+            for (int b = off[A]; b < off[A + 1]; b += 32) {
+                const int i = b + lane;
+                bool ok = i < off[A + 1] && pair_in(pos, i, j, h, hi, diag, rc2);
+                if (ok && tot[i] > cap) ok = j <= list[(size_t)i * cap + cap - 1];
+                const unsigned m = __ballot_sync(kFull, ok);
+                const int k = emitted + __popc(m & ((1u << lane) - 1u));
+                if (ok && k < in_cap) row[k] = i;
+                emitted += __popc(m);
+            }
+        }
+        if (lane == 0) {
+            in_cnt[j] = emitted < in_cap ? emitted : in_cap;
+            if (emitted > in_cap && atomicCAS(&err->code, FMD_OK, FMD_ERR_CAPACITY) == FMD_OK) {
+                err->where = K_TRANSPOSE; err->index = j; err->value = emitted;
+            }
+        }
+    }
+}
+
+constexpr int kRowBlocksMol = kSMs * 8;
+
+}  // namespace
+
+cudaError_t mol_lists_alloc(MolLists& m, int n, const int* mol_id_host) {
+    m = MolLists();
+    if (n <= 0 || !mol_id_host) return cudaSuccess;
+    // contiguous molecules: each id forms one run
+    std::vector<int> off;
+    off.push_back(0);
+    for (int k = 1; k < n; k++)
+        if (mol_id_host[k] != mol_id_host[k - 1]) off.push_back(k);
+    off.push_back(n);
+    const int M = (int)off.size() - 1;
+    {
+        std::vector<int> ids;
+        for (int a = 0; a < M; a++) ids.push_back(mol_id_host[off[a]]);
+        std::sort(ids.begin(), ids.end());
+        for (int a = 1; a < M; a++)
+            if (ids[a] == ids[a - 1]) return cudaSuccess;     // an id in two runs: not contiguous
+    }
+    std::vector<int> amol(n);
+    for (int a = 0; a < M; a++)
+        for (int k = off[a]; k < off[a + 1]; k++) amol[k] = a;
+    m.M = M;
+    m.pmax = std::min(M, kMolPartners);
+    cudaError_t e;
+    auto A = [&](void** p, size_t bytes) {
+        if (e == cudaSuccess) e = cudaMalloc(p, bytes);
+    };
+    e = cudaSuccess;
+    A((void**)&m.off, sizeof(int) * (M + 1));
+    A((void**)&m.amol, sizeof(int) * n);
+    A((void**)&m.cen, sizeof(double) * 3 * M);
+    A((void**)&m.rad, sizeof(double) * M);
+    A((void**)&m.npart, sizeof(int) * M);
+    A((void**)&m.part, sizeof(int) * (size_t)M * m.pmax);
+    A((void**)&m.tot, sizeof(int) * n);
+    A((void**)&m.flag, sizeof(int) * 2);
+    if (e == cudaSuccess) e = cudaMemcpy(m.off, off.data(), sizeof(int) * (M + 1), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(m.amol, amol.data(), sizeof(int) * n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(m.flag, 0, sizeof(int) * 2);
+    if (e != cudaSuccess) {
+        mol_lists_free(m);
+        return e;
+    }
+    m.n = n;
+    m.ok = true;
+    return cudaSuccess;
+}
+
+void mol_lists_free(MolLists& m) {
+    cudaFree(m.off); cudaFree(m.amol); cudaFree(m.cen); cudaFree(m.rad); cudaFree(m.npart); cudaFree(m.part);
+    cudaFree(m.tot); cudaFree(m.flag);
+    m = MolLists();
+}
+
+cudaError_t mol_partners(MolLists& m, const double* pos, const double* hh, double rc, cudaStream_t st) {
+    const int wblocks = (m.M * 32 + 255) / 256;
+    k_mol_centre<<<wblocks, 256, 0, st>>>(pos, hh, m.off, m.M, m.cen, m.rad, m.flag);
+    k_mol_pairs<<<wblocks, 256, 0, st>>>(hh, m.M, m.cen, m.rad, rc, m.pmax, m.npart, m.part, m.flag);
+    k_mol_decide<<<1, 32, 0, st>>>(hh, m.flag);
+    return cudaGetLastError();
+}
+
+cudaError_t mol_rows_intra(const MolLists& m, const double* pos, const double* hh, double rc2, int cap, int* cnt,
+                           int* list, int* dropped, cudaStream_t st) {
+    k_mol_rows<1><<<kRowBlocksMol, 256, 0, st>>>(pos, hh, m.n, m.off, m.amol, m.npart, m.part, m.pmax, rc2, cap, cnt,
+                                                 list, nullptr, dropped, m.flag);
+    return cudaGetLastError();
+}
+
+cudaError_t mol_rows_half(const MolLists& m, const double* pos, const double* hh, double rc2, int cap, int* cnt,
+                          int* list, int* in_cnt, int* in_list, int in_cap, int* dropped, DevErr* err,
+                          cudaStream_t st) {
+    k_mol_rows<0><<<kRowBlocksMol, 256, 0, st>>>(pos, hh, m.n, m.off, m.amol, m.npart, m.part, m.pmax, rc2, cap, cnt,
+                                                 list, m.tot, dropped, m.flag);
+    k_mol_incoming<<<kRowBlocksMol, 256, 0, st>>>(pos, hh, m.n, m.off, m.amol, m.npart, m.part, m.pmax, rc2, cap,
+                                                  list, m.tot, in_cnt, in_list, in_cap, err, m.flag);
+    return cudaGetLastError();
+}
+
+}  // namespace fmd

@@ -1,0 +1,42 @@
+// molnlist.h -- neighbour lists of atomistic systems built molecule by
+// molecule (molnlist.cu).  Not part of the public C-ABI.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "fmd_internal.h"
+
+namespace fmd {
+
+constexpr int kMolPartners = 256;   // partner molecules per molecule (table width)
+
+struct MolLists {
+    bool ok = false;          // molecules are contiguous index ranges
+    int n = 0, M = 0, pmax = 0;
+    int* off = nullptr;       // [M + 1] first atom of each molecule
+    int* amol = nullptr;      // [n] molecule of each atom
+    double* cen = nullptr;    // [3 M] centres
+    double* rad = nullptr;    // [M] radii
+    int* npart = nullptr;     // [M] partner count
+    int* part = nullptr;      // [M * pmax] partners, ascending
+    int* tot = nullptr;       // [n] accepted half-list partners before truncation
+    int* flag = nullptr;      // [2] {molecule path valid, partner overflow}
+};
+
+// Host set-up from the atoms' molecule ids; m.ok stays false (the cell-grid
+// builder is used) unless every molecule is one contiguous index range.
+cudaError_t mol_lists_alloc(MolLists& m, int n, const int* mol_id_host);
+void mol_lists_free(MolLists& m);
+// Centres, radii and partner molecules for list radius rc; sets flag[0].
+cudaError_t mol_partners(MolLists& m, const double* pos, const double* hh, double rc, cudaStream_t st);
+// Intramolecular rows (always valid for contiguous molecules).
+cudaError_t mol_rows_intra(const MolLists& m, const double* pos, const double* hh, double rc2, int cap, int* cnt,
+                           int* list, int* dropped, cudaStream_t st);
+// Half-list rows and their incoming rows; no-ops unless flag[0] is set.
+cudaError_t mol_rows_half(const MolLists& m, const double* pos, const double* hh, double rc2, int cap, int* cnt,
+                          int* list, int* in_cnt, int* in_list, int in_cap, int* dropped, DevErr* err,
+                          cudaStream_t st);
+
+}  // namespace fmd

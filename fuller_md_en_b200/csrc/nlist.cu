@@ -69,11 +69,13 @@ __global__ void k_grid(const double* __restrict__ hh, double rc, int K, int c0, 
     *g = G;
 }
 
+// gate (may be null): a set value means the molecule path builds this list.
 __global__ void k_bin(const double* __restrict__ pos, int n, const double* __restrict__ hh,
                       const GridDev* __restrict__ g, int* __restrict__ cell_count,
-                      int* __restrict__ cell_of, int* __restrict__ slot_of, float4* __restrict__ s4) {
+                      int* __restrict__ cell_of, int* __restrict__ slot_of, float4* __restrict__ s4,
+                      const int* __restrict__ gate) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    if (i >= n || (gate && *gate)) return;
     const double* hi = hh + 9;
     double x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
     double s[3] = {hi[0] * x + hi[1] * y + hi[2] * z, hi[3] * x + hi[4] * y + hi[5] * z,
@@ -94,7 +96,9 @@ __global__ void k_bin(const double* __restrict__ pos, int n, const double* __res
 // the device).  Each thread owns a contiguous run of cells, so there is a
 // single block-wide scan whatever ncell is.
 __global__ void __launch_bounds__(1024)
-k_scan(const int* __restrict__ cell_count, const GridDev* __restrict__ g, int* __restrict__ cell_start) {
+k_scan(const int* __restrict__ cell_count, const GridDev* __restrict__ g, int* __restrict__ cell_start,
+       const int* __restrict__ gate) {
+    if (gate && *gate) return;
     __shared__ int sm[1024];
     const int ncell = g->ncell;
     const int per = (ncell + 1023) / 1024;
@@ -123,9 +127,9 @@ k_scan(const int* __restrict__ cell_count, const GridDev* __restrict__ g, int* _
 __global__ void k_scatter(int n, const int* __restrict__ cell_of, const int* __restrict__ slot_of,
                           const int* __restrict__ cell_start, int* __restrict__ cell_atoms,
                           const float4* __restrict__ s4, const int* __restrict__ mol_id, float4* __restrict__ s4s,
-                          int* __restrict__ mols) {
+                          int* __restrict__ mols, const int* __restrict__ gate) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    if (i >= n || (gate && *gate)) return;
     const int k = cell_start[cell_of[i]] + slot_of[i];
     cell_atoms[k] = i;
     s4s[k] = s4[i];
@@ -170,7 +174,9 @@ k_nlist(const GridDev* __restrict__ g, const int* __restrict__ cell_start,
         const int* __restrict__ cell_atoms, const int* __restrict__ cell_of,
         const float4* __restrict__ s4, const float4* __restrict__ s4s, const int* __restrict__ mols,
         const double* __restrict__ pos, const int* __restrict__ mol_id, int n, const double* __restrict__ hh,
-        double rc2, int cap, int words, int* __restrict__ cnt, int* __restrict__ list, int* __restrict__ dropped) {
+        double rc2, int cap, int words, int* __restrict__ cnt, int* __restrict__ list, int* __restrict__ dropped,
+        const int* __restrict__ gate) {
+    if (gate && *gate) return;
     extern __shared__ unsigned bm_all[];
     __shared__ double s_hh[18];
     __shared__ GridDev G;
@@ -268,7 +274,8 @@ k_nlist(const GridDev* __restrict__ g, const int* __restrict__ cell_start,
 // Scatter half-list entries (i -> j) into row j of the incoming list.
 __global__ void k_transpose_scatter(const int* __restrict__ cnt, const int* __restrict__ list, int cap,
                                     int n, int* __restrict__ in_cnt, int* __restrict__ in_list,
-                                    int in_cap, DevErr* err) {
+                                    int in_cap, DevErr* err, const int* __restrict__ gate) {
+    if (gate && *gate) return;
     const int lane = threadIdx.x & 31;
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (i >= n) return;
@@ -285,7 +292,9 @@ __global__ void k_transpose_scatter(const int* __restrict__ cnt, const int* __re
 
 // Sorts each incoming row ascending through the bitmap.
 __global__ void __launch_bounds__(256)
-k_transpose_sort(int n, int* __restrict__ in_cnt, int* __restrict__ in_list, int in_cap, int words) {
+k_transpose_sort(int n, int* __restrict__ in_cnt, int* __restrict__ in_list, int in_cap, int words,
+                 const int* __restrict__ gate) {
+    if (gate && *gate) return;
     extern __shared__ unsigned bm_all[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
     unsigned* bm = bm_all + (size_t)wib * words;
@@ -365,17 +374,18 @@ void cells_free(CellList& cl) {
 }
 
 cudaError_t cells_build(CellList& cl, const double* pos, int n, const double* hh, double rc,
-                        DevErr* err, cudaStream_t st, const int* mol_id) {
+                        DevErr* err, cudaStream_t st, const int* mol_id, const int* gate) {
     (void)err;
     k_grid<<<1, 32, 0, st>>>(hh, rc, cl.K, cl.cap_n[0], cl.cap_n[1], cl.cap_n[2], cl.grid);
     cudaMemsetAsync(cl.cell_count, 0, sizeof(int) * cl.cap_cells, st);
     if (n > 0) {
-        k_bin<<<(n + 255) / 256, 256, 0, st>>>(pos, n, hh, cl.grid, cl.cell_count, cl.cell_of, cl.slot_of, cl.s4);
+        k_bin<<<(n + 255) / 256, 256, 0, st>>>(pos, n, hh, cl.grid, cl.cell_count, cl.cell_of, cl.slot_of, cl.s4,
+                                               gate);
     }
-    k_scan<<<1, 1024, 0, st>>>(cl.cell_count, cl.grid, cl.cell_start);
+    k_scan<<<1, 1024, 0, st>>>(cl.cell_count, cl.grid, cl.cell_start, gate);
     if (n > 0) {
         k_scatter<<<(n + 255) / 256, 256, 0, st>>>(n, cl.cell_of, cl.slot_of, cl.cell_start, cl.cell_atoms, cl.s4,
-                                                   mol_id, cl.s4s, cl.mols);
+                                                   mol_id, cl.s4s, cl.mols, gate);
     }
     return cudaGetLastError();
 }
@@ -394,7 +404,7 @@ namespace {
 template <int MODE>
 cudaError_t launch_nlist(const CellList& cl, const double* pos, const int* mol_id, int n,
                          const double* hh, double rc2, int cap, int* cnt, int* list, int* dropped,
-                         cudaStream_t st) {
+                         cudaStream_t st, const int* gate) {
     int wpb;
     size_t smem = nlist_bitmap_smem(n, &wpb);
     if (smem > 200 * 1024) return cudaErrorInvalidValue;
@@ -409,28 +419,29 @@ cudaError_t launch_nlist(const CellList& cl, const double* pos, const int* mol_i
     if (blocks < 1) blocks = 1;
     k_nlist<MODE><<<blocks, 32 * wpb, smem, st>>>(cl.grid, cl.cell_start, cl.cell_atoms, cl.cell_of, cl.s4,
                                                   cl.s4s, cl.mols, pos, mol_id, n, hh, rc2, cap, words, cnt, list,
-                                                  dropped);
+                                                  dropped, gate);
     return cudaGetLastError();
 }
 }  // namespace
 
 cudaError_t nlist_build(const CellList& cl, int mode, const double* pos, const int* mol_id, int n,
                         const double* hh, double rc2, int cap, int* cnt, int* list, int* dropped,
-                        DevErr* err, cudaStream_t st) {
+                        DevErr* err, cudaStream_t st, const int* gate) {
     (void)err;
     if (n <= 0) return cudaSuccess;
     switch (mode) {
-        case LIST_SYM: return launch_nlist<LIST_SYM>(cl, pos, mol_id, n, hh, rc2, cap, cnt, list, dropped, st);
-        case LIST_INTRA: return launch_nlist<LIST_INTRA>(cl, pos, mol_id, n, hh, rc2, cap, cnt, list, dropped, st);
-        default: return launch_nlist<LIST_HALF>(cl, pos, mol_id, n, hh, rc2, cap, cnt, list, dropped, st);
+        case LIST_SYM: return launch_nlist<LIST_SYM>(cl, pos, mol_id, n, hh, rc2, cap, cnt, list, dropped, st, gate);
+        case LIST_INTRA:
+            return launch_nlist<LIST_INTRA>(cl, pos, mol_id, n, hh, rc2, cap, cnt, list, dropped, st, gate);
+        default: return launch_nlist<LIST_HALF>(cl, pos, mol_id, n, hh, rc2, cap, cnt, list, dropped, st, gate);
     }
 }
 
 cudaError_t nlist_transpose(const int* cnt, const int* list, int cap, int n, int* in_cnt, int* in_list,
-                            int in_cap, DevErr* err, cudaStream_t st) {
+                            int in_cap, DevErr* err, cudaStream_t st, const int* gate) {
     if (n <= 0) return cudaSuccess;
     cudaMemsetAsync(in_cnt, 0, sizeof(int) * n, st);
-    k_transpose_scatter<<<(n * 32 + 255) / 256, 256, 0, st>>>(cnt, list, cap, n, in_cnt, in_list, in_cap, err);
+    k_transpose_scatter<<<(n * 32 + 255) / 256, 256, 0, st>>>(cnt, list, cap, n, in_cnt, in_list, in_cap, err, gate);
     int wpb;
     size_t smem = nlist_bitmap_smem(n, &wpb);
     if (smem > 200 * 1024) return cudaErrorInvalidValue;
@@ -441,7 +452,7 @@ cudaError_t nlist_transpose(const int* cnt, const int* list, int cap, int n, int
     }
     int blocks = (n + wpb - 1) / wpb;
     if (blocks > kSMs * 16) blocks = kSMs * 16;
-    k_transpose_sort<<<blocks, 32 * wpb, smem, st>>>(n, in_cnt, in_list, in_cap, (n + 31) / 32);
+    k_transpose_sort<<<blocks, 32 * wpb, smem, st>>>(n, in_cnt, in_list, in_cap, (n + 31) / 32, gate);
     return cudaGetLastError();
 }
 

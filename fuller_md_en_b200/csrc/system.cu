@@ -46,6 +46,7 @@ void System::release() {
     owned.clear();
     cells_free(cells_a);
     cells_free(cells_b);
+    mol_lists_free(mol);
 }
 
 template <class T>
@@ -122,18 +123,36 @@ cudaError_t System::enqueue_rebuild(cudaStream_t st) {
                            dropped, ctx->d_err, st);
     }
     if (arr.kind == FMD_SYS_AIREBO) {
-        if ((e = cells_build(cells_b, arr.pos, arr.n, hh, rc_b, ctx->d_err, st, arr.mol_id)) != cudaSuccess) return e;
-        if ((e = nlist_build(cells_b, LIST_INTRA, arr.pos, arr.mol_id, arr.n, hh, rc2_b, arr.cap_b,
-                             const_cast<int*>(arr.cnt_b), const_cast<int*>(arr.list_b), dropped + 1,
-                             ctx->d_err, st)) != cudaSuccess)
-            return e;
+        if (mol.ok) {
+            if ((e = mol_rows_intra(mol, arr.pos, hh, rc2_b, arr.cap_b, const_cast<int*>(arr.cnt_b),
+                                    const_cast<int*>(arr.list_b), dropped + 1, st)) != cudaSuccess)
+                return e;
+        } else {
+            if ((e = cells_build(cells_b, arr.pos, arr.n, hh, rc_b, ctx->d_err, st, arr.mol_id)) != cudaSuccess) return e;
+            if ((e = nlist_build(cells_b, LIST_INTRA, arr.pos, arr.mol_id, arr.n, hh, rc2_b, arr.cap_b,
+                                 const_cast<int*>(arr.cnt_b), const_cast<int*>(arr.list_b), dropped + 1,
+                                 ctx->d_err, st)) != cudaSuccess)
+                return e;
+        }
     }
-    if ((e = cells_build(cells_a, arr.pos, arr.n, hh, rc_a, ctx->d_err, st, arr.mol_id)) != cudaSuccess) return e;
+    // Half list: the molecule path when valid for this rebuild (decided on
+    // the device), else the cell-grid path; both are in the graph, gated.
+    const int* gate = nullptr;
+    if (mol.ok) {
+        if ((e = mol_partners(mol, arr.pos, hh, rc_a, st)) != cudaSuccess) return e;
+        gate = mol.flag;
+    }
+    if ((e = cells_build(cells_a, arr.pos, arr.n, hh, rc_a, ctx->d_err, st, arr.mol_id, gate)) != cudaSuccess) return e;
     if ((e = nlist_build(cells_a, LIST_HALF, arr.pos, arr.mol_id, arr.n, hh, rc2_a, arr.cap_a, cnt_a, list_a,
-                         dropped, ctx->d_err, st)) != cudaSuccess)
+                         dropped, ctx->d_err, st, gate)) != cudaSuccess)
         return e;
-    return nlist_transpose(arr.cnt_a, arr.list_a, arr.cap_a, arr.n, const_cast<int*>(arr.in_cnt),
-                           const_cast<int*>(arr.in_list), arr.in_cap, ctx->d_err, st);
+    if ((e = nlist_transpose(arr.cnt_a, arr.list_a, arr.cap_a, arr.n, const_cast<int*>(arr.in_cnt),
+                             const_cast<int*>(arr.in_list), arr.in_cap, ctx->d_err, st, gate)) != cudaSuccess)
+        return e;
+    if (mol.ok)
+        return mol_rows_half(mol, arr.pos, hh, rc2_a, arr.cap_a, cnt_a, list_a, const_cast<int*>(arr.in_cnt),
+                             const_cast<int*>(arr.in_list), arr.in_cap, dropped, ctx->d_err, st);
+    return cudaSuccess;
 }
 
 // Launch shape of the atomistic LJ gather: every candidate (threads per
@@ -350,6 +369,7 @@ extern "C" int fmd_system_create_airebo(fmd_ctx* ctx, const fmd_run_params* p, i
     const double lj_rcut = 3.0 * 3.40;          // AI:120
     const double rebo_rcut = 2.0 + 0.3;         // AI:116
     if ((rc = s->alloc_lists(lj_rcut + 2.0, 400, rebo_rcut, 12, true)) != FMD_OK) return rc;
+    if (fmd::mol_lists_alloc(s->mol, na, mol_id) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "list allocation failed");
     out[0] = new fmd_system{std::move(s)};
     return FMD_OK;
 }
@@ -384,6 +404,7 @@ extern "C" int fmd_system_create_mm(fmd_ctx* ctx, const fmd_run_params* p, int n
     }
     const double rcut = 3.0 * 3.431;            // MM:114
     if ((rc = s->alloc_lists(rcut + 2.0, 400, 0.0, 0, true)) != FMD_OK) return rc;
+    if (fmd::mol_lists_alloc(s->mol, na, mol_id) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "list allocation failed");
     out[0] = new fmd_system{std::move(s)};
     return FMD_OK;
 }

@@ -2,6 +2,7 @@
 #pragma once
 #include <memory>
 #include <vector>
+#include "molnlist.h"
 #include "sg_host.h"
 #include "step.h"
 
@@ -15,6 +16,7 @@ struct System {
     StepParams sp{};
     StepArrays arr{};
     CellList cells_a, cells_b;
+    MolLists mol;                      // molecule-wise list builder (contiguous molecules)
     double rc_a = 0, rc2_a = 0, rc_b = 0, rc2_b = 0;
     double h0[9] = {0};
     int* dropped = nullptr;            // device: {list a, list b} overflow counts
