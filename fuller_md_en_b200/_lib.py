@@ -63,7 +63,7 @@ class SgStatus(ctypes.Structure):
 
 class BatchTuning(ctypes.Structure):
     """fmd_batch_tuning: launch shapes the batch autotuner chose."""
-    _fields_ = [("lj_threads", c_int), ("lj_unroll", c_int), ("lj_atoms_per_block", c_int),
+    _fields_ = [("lj_threads", c_int), ("lj_unroll", c_int), ("lj_atoms_per_block", c_int), ("lj_staged", c_int),
                 ("bonded_threads", c_int), ("bonded_terms_per_block", c_int), ("lj_ms", c_double),
                 ("bonded_ms", c_double), ("blocks_lj", c_int), ("blocks_bonded", c_int), ("blocks_atom", c_int)]
 
@@ -122,6 +122,7 @@ _SIGS = {
     "fmd_system_kernel_ms": (c_int, [c_void_p, c_int, c_int, POINTER(c_double)]),
     "fmd_system_step_kernels": (c_int, [c_void_p, c_int, c_int, POINTER(c_int)]),
     "fmd_system_lj_shape": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int), POINTER(c_int), POINTER(c_int)]),
+    "fmd_system_set_lj_shape": (c_int, [c_void_p, c_int, c_int, c_int]),
     "fmd_umma_selftest": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, POINTER(c_float)]),
     "fmd_sg_nparams": (c_int, []),
     "fmd_sg_create": (c_int, [c_void_p, _dp, POINTER(c_void_p)]),

@@ -416,6 +416,10 @@ class System:
         self.ctx.check(self.ctx.lib.fmd_system_lj_shape(self.h, *[ctypes.byref(x) for x in v]), "fmd_system_lj_shape")
         return dict(zip(("threads", "unroll", "pipelined", "blocks"), (x.value for x in v)))
 
+    def set_lj_shape(self, threads: int, unroll: int, feed: int) -> None:
+        """Pins the LJ gather's launch shape (feed 0 plain, 1 pipelined, 2 staged rows)."""
+        self.ctx.check(self.ctx.lib.fmd_system_set_lj_shape(self.h, threads, unroll, feed), "fmd_system_set_lj_shape")
+
     def use_surrogate(self, model, judge_every: int = 100, rmse_max: float = 0.025) -> None:
         """Learned REBO term from `model` (a surrogate.Surrogate, or None for
         the plain kernel), judged by the plain REBO kernel every `judge_every`

@@ -296,11 +296,11 @@ int upload_half_list(fmd_ctx* ctx, const int* nlc, const int* nll, int cap, int 
     int rc = up(ctx, S_CNT, nlc, na, &dc);
     if (!rc) rc = up(ctx, S_LIST, nll, (size_t)na * cap, &dl);
     if (!rc) rc = up<int>(ctx, S_INCNT, nullptr, na, &ic);
-    if (!rc) rc = up<int>(ctx, S_INLIST, nullptr, (size_t)na * kInCap, &il);
+    if (!rc) rc = up<int>(ctx, S_INLIST, nullptr, (size_t)na * (kInCap + cap), &il);
     if (rc) return rc;
-    if (nlist_transpose(dc, dl, cap, na, ic, il, kInCap, ctx->d_err, ctx->stream) != cudaSuccess)
+    if (nlist_transpose(dc, dl, cap, na, ic, il, kInCap + cap, ctx->d_err, ctx->stream) != cudaSuccess)
         return ctx->fail(FMD_ERR_CUDA, "transpose launch failed");
-    a.cnt_a = dc; a.list_a = dl; a.cap_a = cap; a.in_cnt = ic; a.in_list = il; a.in_cap = kInCap;
+    a.cnt_a = dc; a.list_a = dl; a.cap_a = cap; a.in_cnt = ic; a.in_list = il; a.in_cap = kInCap + cap;
     return FMD_OK;
 }
 
@@ -325,7 +325,7 @@ int upload_scal(fmd_ctx* ctx, const double* h, const double* hi, const double* W
 int alloc_partials(fmd_ctx* ctx, StepArrays& a) {
     int rc = up<double>(ctx, S_PART1, nullptr, (size_t)std::max(kForceBlocks, a.n) * kNV, &a.part_f1);
     if (!rc) rc = up<double>(ctx, S_PART2, nullptr, (size_t)kLJMaxBlocks * kNV, &a.part_f2);
-    a.lj_blocks = lj_gather_blocks(a.kind == FMD_SYS_MM ? FMD_FF_MM : FMD_FF_AIREBO, a.precision, a.lj_shape);
+    a.lj_blocks = lj_gather_blocks(a.kind == FMD_SYS_MM ? FMD_FF_MM : FMD_FF_AIREBO, a.precision, a.lj_shape, 0);
     if (!rc) rc = up<double>(ctx, S_PART3, nullptr, (size_t)kForceBlocks, &a.part_f3);
     if (!rc) rc = up<double>(ctx, S_PARTKE, nullptr, (size_t)kForceBlocks * 2, &a.part_ke);
     return rc;
@@ -464,7 +464,7 @@ static int atom_term(fmd_ctx* ctx, int term, int ff, const double* pos, const do
     }
     double* red;
     if ((rc = up<double>(ctx, S_PART3, nullptr, 16, &red))) return rc;
-    if (reduce_partials(part, term == 0 ? kForceBlocks : lj_gather_blocks(ff, ctx->precision, LJShape{}), kNV, red,
+    if (reduce_partials(part, term == 0 ? kForceBlocks : lj_gather_blocks(ff, ctx->precision, LJShape{}, 0), kNV, red,
                         ctx->stream) != cudaSuccess)
         return ctx->fail(FMD_ERR_CUDA, "reduce launch failed");
     double r[kNV];

@@ -17,10 +17,12 @@
 // always agree on whether it interacts.
 #include <algorithm>
 #include <cmath>
+#include <map>
 #include "kernels.h"
 #include "geom.cuh"
 #include "rebo_fn.cuh"
 #include "step.h"
+#include "umma.cuh"
 
 namespace fmd {
 namespace {
@@ -477,13 +479,13 @@ __device__ __forceinline__ void lj_pair(double dx, double dy, double dz, const L
 // U entries are loaded before the current U are computed, so their latency
 // overlaps the arithmetic.
 template <int U>
-__device__ __forceinline__ void lj_fetch(const double* __restrict__ pos, const int* __restrict__ row,
-                                         const int* __restrict__ irow, int mo, int tot, int b, int i, int (&jj)[U],
-                                         double (&qx)[U], double (&qy)[U], double (&qz)[U]) {
+__device__ __forceinline__ void lj_fetch(const double* __restrict__ pos, const int* __restrict__ row, int tot,
+                                         int b, int i, int (&jj)[U], double (&qx)[U], double (&qy)[U],
+                                         double (&qz)[U]) {
 #pragma unroll
     for (int u = 0; u < U; u++) {
         const int k = b + 32 * u;
-        jj[u] = k < mo ? row[k] : (k < tot ? irow[k] : -1);
+        jj[u] = k < tot ? row[k] : -1;
     }
 #pragma unroll
     for (int u = 0; u < U; u++) {
@@ -494,9 +496,12 @@ __device__ __forceinline__ void lj_fetch(const double* __restrict__ pos, const i
 
 // One gather pass over atoms blk, blk + nblk, ... (in warps) of one system;
 // per-block {E, W9} into part[blk].  sm: 32 * kNV doubles, s_hh: 18.
+// Row i of the full list (in_list, stride in_cap, in_cnt[i] entries) is the
+// incoming entries (j < i, from the transposed half list) followed by the
+// reference row (j > i), so a pair is counted for energy and virial on the
+// side where j > i.
 template <bool FULL_VIRIAL, bool F32, int U, bool PIPE>
 __device__ __forceinline__ void lj_gather_body(const double* __restrict__ pos, const double* __restrict__ hh,
-                                               const int* __restrict__ cnt, const int* __restrict__ list, int cap,
                                                const int* __restrict__ in_cnt, const int* __restrict__ in_list,
                                                int in_cap, int na, double* __restrict__ F,
                                                double* __restrict__ Facc, const LJP& p, double* __restrict__ part,
@@ -516,25 +521,20 @@ __device__ __forceinline__ void lj_gather_body(const double* __restrict__ pos, c
     for (int i = blk * wpb + (threadIdx.x >> 5); i < na; i += nblk * wpb) {
         const double px = pos[3 * i], py = pos[3 * i + 1], pz = pos[3 * i + 2];
         double fx = 0.0, fy = 0.0, fz = 0.0;
-        // Outgoing entries (the reference row, j > i) then incoming ones
-        // (transposed rows, j < i) as one index range [0, mo + mi).
-        const int mo = cnt[i];
-        const int mi = min(in_cnt[i], in_cap);
-        const int tot = mo + mi;
-        const int* row = list + (size_t)i * cap;
-        const int* irow = in_list + (size_t)i * in_cap - mo;
+        const int tot = min(in_cnt[i], in_cap);
+        const int* row = in_list + (size_t)i * in_cap;
         int jj[U];
         double qx[U], qy[U], qz[U];
-        if (PIPE && lane < tot) lj_fetch<U>(pos, row, irow, mo, tot, lane, i, jj, qx, qy, qz);
+        if (PIPE && lane < tot) lj_fetch<U>(pos, row, tot, lane, i, jj, qx, qy, qz);
         for (int b = lane; b < tot; b += 32 * U) {
             int jc[U];
             double cx[U], cy[U], cz[U];
             if (PIPE) {
 #pragma unroll
                 for (int u = 0; u < U; u++) { jc[u] = jj[u]; cx[u] = qx[u]; cy[u] = qy[u]; cz[u] = qz[u]; }
-                if (b + 32 * U < tot) lj_fetch<U>(pos, row, irow, mo, tot, b + 32 * U, i, jj, qx, qy, qz);
+                if (b + 32 * U < tot) lj_fetch<U>(pos, row, tot, b + 32 * U, i, jj, qx, qy, qz);
             } else {
-                lj_fetch<U>(pos, row, irow, mo, tot, b, i, jc, cx, cy, cz);
+                lj_fetch<U>(pos, row, tot, b, i, jc, cx, cy, cz);
             }
 #pragma unroll
             for (int u = 0; u < U; u++) {
@@ -547,7 +547,7 @@ __device__ __forceinline__ void lj_gather_body(const double* __restrict__ pos, c
                 } else {
                     mimg(dx, dy, dz, hi, h);
                 }
-                if (b + 32 * u < mo) lj_pair<FULL_VIRIAL, F32, true>(dx, dy, dz, p, pf, fx, fy, fz, acc);
+                if (jc[u] > i) lj_pair<FULL_VIRIAL, F32, true>(dx, dy, dz, p, pf, fx, fy, fz, acc);
                 else lj_pair<FULL_VIRIAL, F32, false>(dx, dy, dz, p, pf, fx, fy, fz, acc);
             }
         }
@@ -564,14 +564,150 @@ __device__ __forceinline__ void lj_gather_body(const double* __restrict__ pos, c
 
 template <bool FULL_VIRIAL, bool F32, int U, bool PIPE, int NT>
 __global__ void __launch_bounds__(NT)
-k_lj_gather(const double* __restrict__ pos, const double* __restrict__ hh, const int* __restrict__ cnt,
-            const int* __restrict__ list, int cap, const int* __restrict__ in_cnt,
+k_lj_gather(const double* __restrict__ pos, const double* __restrict__ hh, const int* __restrict__ in_cnt,
             const int* __restrict__ in_list, int in_cap, int na, double* __restrict__ F,
             double* __restrict__ Facc, LJP p, double* __restrict__ part) {
     __shared__ double sm[32 * kNV];
     __shared__ double s_hh[18];
-    lj_gather_body<FULL_VIRIAL, F32, U, PIPE>(pos, hh, cnt, list, cap, in_cnt, in_list, in_cap, na, F, Facc, p,
-                                              part, blockIdx.x, gridDim.x, sm, s_hh);
+    lj_gather_body<FULL_VIRIAL, F32, U, PIPE>(pos, hh, in_cnt, in_list, in_cap, na, F, Facc, p, part, blockIdx.x,
+                                              gridDim.x, sm, s_hh);
+}
+
+// Row-staged gather: each warp copies its next atom's full row into a
+// shared-memory buffer with one bulk asynchronous copy (cp.async.bulk,
+// completion on an mbarrier) while it computes the current atom from the
+// other buffer, so the row stream from HBM overlaps the pair arithmetic
+// instead of sitting on each iteration's dependency chain.  Requires row
+// stride in_cap % 4 == 0 (16-byte aligned rows).  Every wait is bounded: on a
+// timeout the kernel records K_LJ in err, waits (bounded) for its own copy in
+// flight and returns.
+__device__ __forceinline__ void bulk_row(int* dst, const int* src, uint32_t bytes, uint64_t* mbar) {
+    const uint32_t m = umma::smem_u32(mbar), d = umma::smem_u32(dst);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(m), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(d), "l"(src), "r"(bytes), "r"(m)
+                 : "memory");
+}
+
+template <bool FULL_VIRIAL, bool F32, int U, int NT>
+__device__ __forceinline__ void lj_gather_staged_body(const double* __restrict__ pos, const double* __restrict__ hh,
+                                                      const int* __restrict__ in_cnt, const int* __restrict__ in_list,
+                                                      int in_cap, int na, double* __restrict__ F,
+                                                      double* __restrict__ Facc, const LJP& p,
+                                                      double* __restrict__ part, DevErr* err, int blk, int nblk,
+                                                      unsigned char* dsm, double* sm, double* s_hh) {
+    constexpr int W = NT / 32;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int* bufs = reinterpret_cast<int*>(dsm) + (size_t)w * 2 * in_cap;
+    uint64_t* mb = reinterpret_cast<uint64_t*>(dsm + (size_t)W * 2 * in_cap * sizeof(int)) + 2 * w;
+    if (lane == 0) {
+        umma::mbar_init(&mb[0], 1);
+        umma::mbar_init(&mb[1], 1);
+    }
+    if (threadIdx.x < 18) s_hh[threadIdx.x] = hh[threadIdx.x];
+    __syncthreads();
+    const double* h = s_hh;
+    const double* hi = s_hh + 9;
+    const bool diag = h[1] == 0.0 && h[2] == 0.0 && h[3] == 0.0 && h[5] == 0.0 && h[6] == 0.0 && h[7] == 0.0 &&
+                      hi[1] == 0.0 && hi[2] == 0.0 && hi[3] == 0.0 && hi[5] == 0.0 && hi[6] == 0.0 && hi[7] == 0.0;
+    const LJF pf{(float)p.sig2, (float)(p.sig2 - (double)(float)p.sig2), (float)p.c4, (float)p.c24};
+    double acc[kNV];
+#pragma unroll
+    for (int k = 0; k < kNV; k++) acc[k] = 0.0;
+    auto issue = [&](int atom, int b) {
+        const int nrow = min(in_cnt[atom], in_cap);
+        const uint32_t bytes = (uint32_t)max(16, (nrow * 4 + 15) & ~15);
+        umma::fence_smem_async();               // earlier reads of this buffer before the async write
+        bulk_row(bufs + (size_t)b * in_cap, in_list + (size_t)atom * in_cap, bytes, &mb[b]);
+    };
+    const int stride = nblk * W;
+    int i = blk * W + w;
+    uint32_t ph0 = 0, ph1 = 0;
+    int cur = 0;
+    bool pending = false;                       // a copy into buffer cur ^ 1 may be in flight
+    if (i < na && lane == 0) issue(i, 0);
+    for (; i < na; i += stride) {
+        const int inext = i + stride;
+        if (inext < na && lane == 0) issue(inext, cur ^ 1);
+        pending = inext < na;
+        const bool ok = umma::mbar_wait(&mb[cur], cur ? ph1 : ph0);
+        if (cur) ph1 ^= 1; else ph0 ^= 1;
+        if (!__all_sync(kFull, ok)) {
+            if (lane == 0 && atomicCAS(&err->code, FMD_OK, FMD_ERR_CUDA) == FMD_OK) {
+                err->where = K_LJ; err->index = i; err->value = 0;
+            }
+            break;
+        }
+        const int* row = bufs + (size_t)cur * in_cap;
+        const int tot = min(in_cnt[i], in_cap);
+        const double px = pos[3 * i], py = pos[3 * i + 1], pz = pos[3 * i + 2];
+        double fx = 0.0, fy = 0.0, fz = 0.0;
+        for (int b = lane; b < tot; b += 32 * U) {
+            int jc[U];
+            double cx[U], cy[U], cz[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) jc[u] = b + 32 * u < tot ? row[b + 32 * u] : -1;
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int j = jc[u] < 0 ? i : jc[u];
+                cx[u] = pos[3 * j]; cy[u] = pos[3 * j + 1]; cz[u] = pos[3 * j + 2];
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                if (jc[u] < 0) continue;
+                double dx = __dsub_rn(cx[u], px), dy = __dsub_rn(cy[u], py), dz = __dsub_rn(cz[u], pz);
+                if (diag) {
+                    dx = mimg1(dx, h[0], hi[0]);
+                    dy = mimg1(dy, h[4], hi[4]);
+                    dz = mimg1(dz, h[8], hi[8]);
+                } else {
+                    mimg(dx, dy, dz, hi, h);
+                }
+                if (jc[u] > i) lj_pair<FULL_VIRIAL, F32, true>(dx, dy, dz, p, pf, fx, fy, fz, acc);
+                else lj_pair<FULL_VIRIAL, F32, false>(dx, dy, dz, p, pf, fx, fy, fz, acc);
+            }
+        }
+        fx = warp_sum(fx); fy = warp_sum(fy); fz = warp_sum(fz);
+        if (lane == 0) {
+            F[3 * i] = Facc[3 * i] + fx;
+            F[3 * i + 1] = Facc[3 * i + 1] + fy;
+            F[3 * i + 2] = Facc[3 * i + 2] + fz;
+            if (Facc != F) { Facc[3 * i] = 0.0; Facc[3 * i + 1] = 0.0; Facc[3 * i + 2] = 0.0; }
+        }
+        __syncwarp();                           // buffer cur is reused two atoms on
+        cur ^= 1;
+        pending = false;
+    }
+    // after an early exit, the copy issued for the next atom may still be in flight
+    if (pending) umma::mbar_wait(&mb[cur ^ 1], (cur ^ 1) ? ph1 : ph0);
+    block_sum_store<kNV>(acc, sm, part + (size_t)blk * kNV);
+}
+
+template <bool FULL_VIRIAL, bool F32, int U, int NT>
+__global__ void __launch_bounds__(NT)
+k_lj_gather_staged(const double* __restrict__ pos, const double* __restrict__ hh, const int* __restrict__ in_cnt,
+                   const int* __restrict__ in_list, int in_cap, int na, double* __restrict__ F,
+                   double* __restrict__ Facc, LJP p, double* __restrict__ part, DevErr* err) {
+    extern __shared__ __align__(128) unsigned char dsm[];
+    __shared__ double sm[32 * kNV];
+    __shared__ double s_hh[18];
+    lj_gather_staged_body<FULL_VIRIAL, F32, U, NT>(pos, hh, in_cnt, in_list, in_cap, na, F, Facc, p, part, err,
+                                                   blockIdx.x, gridDim.x, dsm, sm, s_hh);
+}
+
+// Replica batch, rows staged (all replicas share the row stride in_cap).
+template <bool FULL_VIRIAL, bool F32, int U, int NT>
+__global__ void __launch_bounds__(NT)
+k_b_lj_gather_staged(const StepArrays* __restrict__ As, const int* __restrict__ off, int R, int ff) {
+    extern __shared__ __align__(128) unsigned char dsm[];
+    __shared__ double sm[32 * kNV];
+    __shared__ double s_hh[18];
+    const int r = batch_rep(off, R, blockIdx.x);
+    const StepArrays& a = As[r];
+    const LJP p = lj_params_dev(ff);
+    lj_gather_staged_body<FULL_VIRIAL, F32, U, NT>(a.pos, a.S->h, a.in_cnt, a.in_list, a.in_cap, a.n, a.F, a.Facc, p,
+                                                   a.part_f2, a.err, blockIdx.x - off[r], off[r + 1] - off[r], dsm,
+                                                   sm, s_hh);
 }
 
 // Replica batch: the same gather over every replica in one launch; block b
@@ -584,7 +720,7 @@ k_b_lj_gather(const StepArrays* __restrict__ As, const int* __restrict__ off, in
     const int r = batch_rep(off, R, blockIdx.x);
     const StepArrays& a = As[r];
     const LJP p = lj_params_dev(ff);
-    lj_gather_body<FULL_VIRIAL, F32, U, false>(a.pos, a.S->h, a.cnt_a, a.list_a, a.cap_a, a.in_cnt, a.in_list, a.in_cap,
+    lj_gather_body<FULL_VIRIAL, F32, U, false>(a.pos, a.S->h, a.in_cnt, a.in_list, a.in_cap,
                                         a.n, a.F, a.Facc, p, a.part_f2, blockIdx.x - off[r], off[r + 1] - off[r], sm,
                                         s_hh);
 }
@@ -655,17 +791,60 @@ int lj_dispatch(bool launch, const double* pos, const double* hh, const int* cnt
                 double* part, cudaStream_t st) {
     const int nb = std::min(kLJMaxBlocks, lj_occupancy<FV, F32, U, PIPE, NT>() * kSMs);
     if (launch)
-        k_lj_gather<FV, F32, U, PIPE, NT><<<nb, NT, 0, st>>>(pos, hh, cnt, list, cap, in_cnt, in_list, in_cap, na,
-                                                             F, Facc, p, part);
+        k_lj_gather<FV, F32, U, PIPE, NT><<<nb, NT, 0, st>>>(pos, hh, in_cnt, in_list, in_cap, na, F, Facc, p,
+                                                             part);
     return nb;
 }
 
-// Launches (launch == true) or sizes the gather of one shape; returns its grid.
+size_t staged_smem(int threads, int in_cap) {
+    return (size_t)(threads / 32) * 2 * (in_cap * sizeof(int) + sizeof(uint64_t));
+}
+
+// Staged variant: grid from the occupancy at its dynamic shared memory.
+template <bool FV, bool F32, int U, int NT>
+int lj_dispatch_staged(bool launch, const double* pos, const double* hh, const int* in_cnt, const int* in_list,
+                       int in_cap, int na, double* F, double* Facc, const LJP& p, double* part, DevErr* err,
+                       cudaStream_t st) {
+    static std::map<int, int> occ;                 // in_cap -> resident blocks per SM
+    const size_t smem = staged_smem(NT, in_cap);
+    auto it = occ.find(in_cap);
+    if (it == occ.end()) {
+        cudaFuncSetAttribute(k_lj_gather_staged<FV, F32, U, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             200 * 1024);
+        int b = 0;
+        if (smem > 200 * 1024 ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_lj_gather_staged<FV, F32, U, NT>, NT, smem) !=
+                cudaSuccess)
+            b = 0;
+        it = occ.emplace(in_cap, b).first;
+    }
+    if (it->second < 1) return 0;
+    const int nb = std::min(kLJMaxBlocks, it->second * kSMs);
+    if (launch)
+        k_lj_gather_staged<FV, F32, U, NT><<<nb, NT, smem, st>>>(pos, hh, in_cnt, in_list, in_cap, na, F, Facc, p,
+                                                                 part, err);
+    return nb;
+}
+
+// Launches (launch == true) or sizes the gather of one shape; returns its grid
+// (0: the shape cannot run with this row stride).
 int lj_select(bool launch, int ff, int precision, const LJShape& sh, const double* pos, const double* hh,
               const int* cnt, const int* list, int cap, const int* in_cnt, const int* in_list, int in_cap, int na,
-              double* F, double* Facc, double* part, cudaStream_t st) {
+              double* F, double* Facc, double* part, cudaStream_t st, DevErr* err = nullptr) {
     const LJP p = lj_params(ff);
     const bool fv = ff == FMD_FF_AIREBO, f32 = precision == FMD_PREC_FP32_PAIR;
+    if (sh.pipe == 2) {
+        if (in_cap % 4 != 0 || (launch && err == nullptr)) return 0;
+#define FMD_LJS(FV, F32, U, NT) \
+    return lj_dispatch_staged<FV, F32, U, NT>(launch, pos, hh, in_cnt, in_list, in_cap, na, F, Facc, p, part, err, st)
+#define FMD_LJS_NT(FV, F32, U) if (sh.threads == 128) { FMD_LJS(FV, F32, U, 128); } else { FMD_LJS(FV, F32, U, 256); }
+#define FMD_LJS_U(FV, F32) if (sh.unroll == 2) { FMD_LJS_NT(FV, F32, 2) } else { FMD_LJS_NT(FV, F32, 4) }
+        if (fv) { if (f32) { FMD_LJS_U(true, true) } else { FMD_LJS_U(true, false) } }
+        else { if (f32) { FMD_LJS_U(false, true) } else { FMD_LJS_U(false, false) } }
+#undef FMD_LJS_U
+#undef FMD_LJS_NT
+#undef FMD_LJS
+    }
 #define FMD_LJ_CALL(FV, F32, U, PIPE, NT) \
     return lj_dispatch<FV, F32, U, PIPE, NT>(launch, pos, hh, cnt, list, cap, in_cnt, in_list, in_cap, na, F, Facc, p, part, st)
 #define FMD_LJ_NT(FV, F32, U, PIPE) \
@@ -682,21 +861,45 @@ int lj_select(bool launch, int ff, int precision, const LJShape& sh, const doubl
 
 }  // namespace
 
-int lj_gather_blocks(int ff, int precision, const LJShape& sh) {
-    return lj_select(false, ff, precision, sh, nullptr, nullptr, nullptr, nullptr, 0, nullptr, nullptr, 0, 0, nullptr,
-                     nullptr, nullptr, nullptr);
+int lj_gather_blocks(int ff, int precision, const LJShape& sh, int in_cap) {
+    return lj_select(false, ff, precision, sh, nullptr, nullptr, nullptr, nullptr, 0, nullptr, nullptr, in_cap, 0,
+                     nullptr, nullptr, nullptr, nullptr);
 }
 
 cudaError_t lj_gather_launch(int ff, const double* pos, const double* hh, const int* cnt, const int* list,
                              int cap, const int* in_cnt, const int* in_list, int in_cap, int na, double* F,
-                             double* Facc, double* part, cudaStream_t st, int precision, const LJShape& sh) {
-    lj_select(true, ff, precision, sh, pos, hh, cnt, list, cap, in_cnt, in_list, in_cap, na, F, Facc, part, st);
+                             double* Facc, double* part, cudaStream_t st, int precision, const LJShape& sh,
+                             DevErr* err) {
+    if (lj_select(true, ff, precision, sh, pos, hh, cnt, list, cap, in_cnt, in_list, in_cap, na, F, Facc, part, st,
+                  err) == 0)
+        return cudaErrorInvalidConfiguration;
     return cudaGetLastError();
 }
 
 cudaError_t batch_lj_launch(const StepArrays* As, const int* off, int R, int nblocks, int ff, int precision,
-                            int threads, int unroll, cudaStream_t st) {
+                            int threads, int unroll, cudaStream_t st, int staged_in_cap) {
     const bool fv = ff == FMD_FF_AIREBO, f32 = precision == FMD_PREC_FP32_PAIR;
+    if (staged_in_cap > 0) {
+        const size_t smem = staged_smem(threads, staged_in_cap);
+#define FMD_BLS(FV, F32, U, NT)                                                                               \
+    {                                                                                                         \
+        static bool attr = false;                                                                             \
+        if (!attr) {                                                                                          \
+            cudaFuncSetAttribute(k_b_lj_gather_staged<FV, F32, U, NT>,                                        \
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);                    \
+            attr = true;                                                                                      \
+        }                                                                                                     \
+        k_b_lj_gather_staged<FV, F32, U, NT><<<nblocks, NT, smem, st>>>(As, off, R, ff);                      \
+    }
+#define FMD_BLS_NT(FV, F32, U) if (threads == 128) FMD_BLS(FV, F32, U, 128) else FMD_BLS(FV, F32, U, 256)
+#define FMD_BLS_U(FV, F32) if (unroll == 2) { FMD_BLS_NT(FV, F32, 2) } else { FMD_BLS_NT(FV, F32, 4) }
+        if (fv) { if (f32) { FMD_BLS_U(true, true) } else { FMD_BLS_U(true, false) } }
+        else { if (f32) { FMD_BLS_U(false, true) } else { FMD_BLS_U(false, false) } }
+#undef FMD_BLS_U
+#undef FMD_BLS_NT
+#undef FMD_BLS
+        return cudaGetLastError();
+    }
 #define FMD_BLJ(FV, F32, U, NT) k_b_lj_gather<FV, F32, U, NT><<<nblocks, NT, 0, st>>>(As, off, R, ff)
 #define FMD_BLJ_NT(FV, F32, U) if (threads == 128) FMD_BLJ(FV, F32, U, 128); else FMD_BLJ(FV, F32, U, 256)
 #define FMD_BLJ_U(FV, F32) if (unroll == 2) { FMD_BLJ_NT(FV, F32, 2); } else { FMD_BLJ_NT(FV, F32, 4); }

@@ -36,6 +36,7 @@ constexpr int kSideStreams = 8;     // parallel branches of a rebuild
 
 struct Tune {
     int lj_threads = 256, lj_unroll = 4, lj_apb = 16;   // apb: atoms per block
+    int lj_staged = 0;                                   // rows staged in shared memory
     int f1_threads = 128, f1_tpb = 512;                  // tpb: terms per block
     double lj_ms = 0, f1_ms = 0;
 };
@@ -86,6 +87,7 @@ struct fmd_batch {
         bd.nblk_f1 = off[2 * (R + 1) + R];
         bd.lj_threads = t.lj_threads;
         bd.lj_unroll = t.lj_unroll;
+        bd.lj_staged_in_cap = t.lj_staged ? sys[0]->arr.in_cap : 0;
         bd.f1_threads = t.f1_threads;
         return ctx->sync_check("batch offsets");
     }
@@ -136,18 +138,24 @@ struct fmd_batch {
         Tune best = tune;
         best.lj_ms = 1e30;
         cudaStream_t st = ctx->stream;
-        for (int nt : {128, 256})
-            for (int u : {2, 4})
-                for (int apb : {8, 16, 32, 64}) {
-                    Tune t = best;
-                    t.lj_threads = nt; t.lj_unroll = u; t.lj_apb = apb;
-                    int rc = set_offsets(t);
-                    if (rc) return rc;
-                    const double ms = time_ms(3, [&]() {
-                        return batch_lj_launch(dA, bd.off_lj, R, bd.nblk_lj, bd.ff, bd.precision, nt, u, st);
-                    });
-                    if (ms < best.lj_ms) { best = t; best.lj_ms = ms; }
-                }
+        // staged rows need one row stride (16-byte multiple) across replicas
+        bool can_stage = sys[0]->arr.in_cap % 4 == 0;
+        for (System* s : sys) can_stage = can_stage && s->arr.in_cap == sys[0]->arr.in_cap;
+        for (int staged : {0, 1})
+            for (int nt : {128, 256})
+                for (int u : {2, 4})
+                    for (int apb : {8, 16, 32, 64}) {
+                        if (staged && !can_stage) continue;
+                        Tune t = best;
+                        t.lj_threads = nt; t.lj_unroll = u; t.lj_apb = apb; t.lj_staged = staged;
+                        int rc = set_offsets(t);
+                        if (rc) return rc;
+                        const int icap = staged ? sys[0]->arr.in_cap : 0;
+                        const double ms = time_ms(3, [&]() {
+                            return batch_lj_launch(dA, bd.off_lj, R, bd.nblk_lj, bd.ff, bd.precision, nt, u, st, icap);
+                        });
+                        if (ms < best.lj_ms) { best = t; best.lj_ms = ms; }
+                    }
         if (bd.kind == FMD_SYS_MM) {
             best.f1_ms = 1e30;
             Tune b2 = best;
@@ -321,6 +329,7 @@ extern "C" int fmd_batch_get_tuning(fmd_batch* b, fmd_batch_tuning* t) {
     t->lj_threads = b->tune.lj_threads;
     t->lj_unroll = b->tune.lj_unroll;
     t->lj_atoms_per_block = b->tune.lj_apb;
+    t->lj_staged = b->tune.lj_staged;
     t->bonded_threads = b->tune.f1_threads;
     t->bonded_terms_per_block = b->tune.f1_tpb;
     t->lj_ms = b->tune.lj_ms;

@@ -51,7 +51,9 @@ enum ListMode { LIST_SYM = 0, LIST_INTRA = 1, LIST_HALF = 2 };
 cudaError_t nlist_build(const CellList& cl, int mode, const double* pos, const int* mol_id, int n,
                         const double* hh, double rc2, int cap, int* cnt, int* list, int* dropped,
                         DevErr* err, cudaStream_t st, const int* gate = nullptr);
-// Incoming (transposed) entries of a half list, sorted ascending per row.
+// Full rows of a half list for the LJ gather: row j (stride in_cap) is the
+// incoming entries i < j (ascending, at most in_cap - cap) then row j itself;
+// in_cnt[j] = their total.
 cudaError_t nlist_transpose(const int* cnt, const int* list, int cap, int n, int* in_cnt,
                             int* in_list, int in_cap, DevErr* err, cudaStream_t st, const int* gate = nullptr);
 size_t nlist_bitmap_smem(int n, int* warps_per_block);
@@ -85,17 +87,21 @@ cudaError_t rebo_slots_launch(const double* pos, const double* hh, const int* cn
 // FMD_PREC_FP64 (the reference's arithmetic) or FMD_PREC_FP32_PAIR (pair
 // algebra in FP32, FP64 minimum image, cutoff test and accumulation).
 // shape: threads per block (128/256), list entries in flight per lane (2/4)
-// and software pipelining; the grid is one full wave of the instantiation
-// (resident blocks per SM x SMs, at most kLJMaxBlocks) and writes that many
-// partial records -- lj_gather_blocks returns it.
+// and the row feed (pipe 0: loads as used, 1: software-pipelined loads,
+// 2: rows staged in shared memory by bulk asynchronous copies, needs
+// in_cap % 4 == 0 and an error word); the grid is one full wave of the
+// instantiation (resident blocks per SM x SMs, at most kLJMaxBlocks) and
+// writes that many partial records -- lj_gather_blocks returns it (0: the
+// shape cannot run with this row stride).
 struct LJShape {
     int threads = 256, unroll = 4, pipe = 0;
 };
-int lj_gather_blocks(int ff, int precision, const LJShape& shape);
+int lj_gather_blocks(int ff, int precision, const LJShape& shape, int in_cap);
 cudaError_t lj_gather_launch(int ff, const double* pos, const double* hh, const int* cnt,
                              const int* list, int cap, const int* in_cnt, const int* in_list,
                              int in_cap, int na, double* F, double* Facc, double* part,
-                             cudaStream_t st, int precision = FMD_PREC_FP64, const LJShape& shape = LJShape{});
+                             cudaStream_t st, int precision = FMD_PREC_FP64, const LJShape& shape = LJShape{},
+                             DevErr* err = nullptr);
 // Rigid site-site LJ (a5-a6): writes F, T; per-block {E, W9} partials (grid n).
 cudaError_t rigid_launch(int precision, const double* pos, const double* qv, const double* body,
                          const double* hh, const int* cnt, const int* list, int cap, int n,

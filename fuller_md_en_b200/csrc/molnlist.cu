@@ -187,13 +187,15 @@ k_mol_rows(const double* __restrict__ pos, const double* __restrict__ hh, int n,
     }
 }
 
-// Incoming rows of the half list: for atom j, the atoms i < j of lower
+// Full rows for the LJ gather: for atom j, the atoms i < j of lower
 // neighbour molecules whose row holds j (the FP64 test from i's side, and j
-// within row i's first `cap` accepted entries); one warp per atom.
+// within row i's first `cap` accepted entries), at most in_cap - cap of them,
+// followed by j's own row; one warp per atom.
 __global__ void __launch_bounds__(256)
 k_mol_incoming(const double* __restrict__ pos, const double* __restrict__ hh, int n, const int* __restrict__ off,
                const int* __restrict__ amol, const int* __restrict__ npart, const int* __restrict__ part, int pmax,
-               double rc2, int cap, const int* __restrict__ list, const int* __restrict__ tot,
+               double rc2, int cap, const int* __restrict__ cnt, const int* __restrict__ list,
+               const int* __restrict__ tot,
                int* __restrict__ in_cnt, int* __restrict__ in_list, int in_cap, DevErr* err,
                const int* __restrict__ flag) {
     if (flag[0] == 0) return;
@@ -218,13 +220,16 @@ k_mol_incoming(const double* __restrict__ pos, const double* __restrict__ hh, in
                 if (ok && tot[i] > cap) ok = j <= list[(size_t)i * cap + cap - 1];
                 const unsigned m = __ballot_sync(kFull, ok);
                 const int k = emitted + __popc(m & ((1u << lane) - 1u));
-                if (ok && k < in_cap) row[k] = i;
+                if (ok && k < in_cap - cap) row[k] = i;
                 emitted += __popc(m);
             }
         }
+        const int kept = emitted < in_cap - cap ? emitted : in_cap - cap;
+        const int mo = cnt[j];
+        for (int k = lane; k < mo; k += 32) row[kept + k] = list[(size_t)j * cap + k];
         if (lane == 0) {
-            in_cnt[j] = emitted < in_cap ? emitted : in_cap;
-            if (emitted > in_cap && atomicCAS(&err->code, FMD_OK, FMD_ERR_CAPACITY) == FMD_OK) {
+            in_cnt[j] = kept + mo;
+            if (emitted > in_cap - cap && atomicCAS(&err->code, FMD_OK, FMD_ERR_CAPACITY) == FMD_OK) {
                 err->where = K_TRANSPOSE; err->index = j; err->value = emitted;
             }
         }
@@ -309,7 +314,7 @@ cudaError_t mol_rows_half(const MolLists& m, const double* pos, const double* hh
     k_mol_rows<0><<<kRowBlocksMol, 256, 0, st>>>(pos, hh, m.n, m.off, m.amol, m.npart, m.part, m.pmax, rc2, cap, cnt,
                                                  list, m.tot, dropped, m.flag);
     k_mol_incoming<<<kRowBlocksMol, 256, 0, st>>>(pos, hh, m.n, m.off, m.amol, m.npart, m.part, m.pmax, rc2, cap,
-                                                  list, m.tot, in_cnt, in_list, in_cap, err, m.flag);
+                                                  cnt, list, m.tot, in_cnt, in_list, in_cap, err, m.flag);
     return cudaGetLastError();
 }
 

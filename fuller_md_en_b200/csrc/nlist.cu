@@ -271,7 +271,10 @@ k_nlist(const GridDev* __restrict__ g, const int* __restrict__ cell_start,
     }
 }
 
-// Scatter half-list entries (i -> j) into row j of the incoming list.
+// Full rows for the LJ gather: row j (stride in_cap) holds the incoming
+// entries i < j of the half list (at most in_cap - cap, ascending) followed
+// by j's own half-list row.
+// Scatter half-list entries (i -> j) into row j.
 __global__ void k_transpose_scatter(const int* __restrict__ cnt, const int* __restrict__ list, int cap,
                                     int n, int* __restrict__ in_cnt, int* __restrict__ in_list,
                                     int in_cap, DevErr* err, const int* __restrict__ gate) {
@@ -283,17 +286,18 @@ __global__ void k_transpose_scatter(const int* __restrict__ cnt, const int* __re
     for (int k = lane; k < m; k += 32) {
         const int j = list[(size_t)i * cap + k];
         const int slot = atomicAdd(&in_cnt[j], 1);
-        if (slot < in_cap) in_list[(size_t)j * in_cap + slot] = i;
+        if (slot < in_cap - cap) in_list[(size_t)j * in_cap + slot] = i;
         else if (atomicCAS(&err->code, FMD_OK, FMD_ERR_CAPACITY) == FMD_OK) {
             err->where = K_TRANSPOSE; err->index = j; err->value = slot + 1;
         }
     }
 }
 
-// Sorts each incoming row ascending through the bitmap.
+// Sorts each incoming row ascending through the bitmap, then appends the
+// atom's own half-list row.
 __global__ void __launch_bounds__(256)
 k_transpose_sort(int n, int* __restrict__ in_cnt, int* __restrict__ in_list, int in_cap, int words,
-                 const int* __restrict__ gate) {
+                 const int* __restrict__ cnt, const int* __restrict__ list, int cap, const int* __restrict__ gate) {
     if (gate && *gate) return;
     extern __shared__ unsigned bm_all[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
@@ -302,7 +306,7 @@ k_transpose_sort(int n, int* __restrict__ in_cnt, int* __restrict__ in_list, int
     __syncwarp();
     for (int j = blockIdx.x * wpb + wib; j < n; j += gridDim.x * wpb) {
         int m = in_cnt[j];
-        m = m < in_cap ? m : in_cap;
+        m = m < in_cap - cap ? m : in_cap - cap;
         int* row = in_list + (size_t)j * in_cap;
         int lo = INT_MAX, hi = -1;
         for (int k = lane; k < m; k += 32) {
@@ -317,8 +321,10 @@ k_transpose_sort(int n, int* __restrict__ in_cnt, int* __restrict__ in_list, int
             hi = max(hi, __shfl_xor_sync(kFull, hi, o));
         }
         __syncwarp();
-        if (m > 0) bitmap_emit(bm, lo >> 5, hi >> 5, row, in_cap, lane);
-        if (lane == 0) in_cnt[j] = m;
+        if (m > 0) bitmap_emit(bm, lo >> 5, hi >> 5, row, in_cap - cap, lane);
+        const int mo = cnt[j];
+        for (int k = lane; k < mo; k += 32) row[m + k] = list[(size_t)j * cap + k];
+        if (lane == 0) in_cnt[j] = m + mo;
         __syncwarp();
     }
 }
@@ -452,7 +458,7 @@ cudaError_t nlist_transpose(const int* cnt, const int* list, int cap, int n, int
     }
     int blocks = (n + wpb - 1) / wpb;
     if (blocks > kSMs * 16) blocks = kSMs * 16;
-    k_transpose_sort<<<blocks, 32 * wpb, smem, st>>>(n, in_cnt, in_list, in_cap, (n + 31) / 32, gate);
+    k_transpose_sort<<<blocks, 32 * wpb, smem, st>>>(n, in_cnt, in_list, in_cap, (n + 31) / 32, cnt, list, cap, gate);
     return cudaGetLastError();
 }
 

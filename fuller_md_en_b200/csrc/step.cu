@@ -463,13 +463,13 @@ cudaError_t enqueue_forces(const StepArrays& a, cudaStream_t st, bool judge) {
         else e = rebo_launch(a.pos, hh, a.cnt_b, a.list_b, a.cap_b, a.n, a.Facc, a.part_f1, st);
         if (e != cudaSuccess) return e;
         e = lj_gather_launch(FMD_FF_AIREBO, a.pos, hh, a.cnt_a, a.list_a, a.cap_a, a.in_cnt, a.in_list, a.in_cap,
-                             a.n, a.F, a.Facc, a.part_f2, st, a.precision, a.lj_shape);
+                             a.n, a.F, a.Facc, a.part_f2, st, a.precision, a.lj_shape, a.err);
     } else {
         if ((e = mm_bonded_launch(a.topo, a.pos, hh, a.Facc, a.part_f1, st)) != cudaSuccess) return e;
         if (a.has_charge)
             if ((e = mm_coulomb_launch(a.pos, hh, a.charge, a.mol_id, a.n, a.Facc, a.part_f3, st)) != cudaSuccess) return e;
         e = lj_gather_launch(FMD_FF_MM, a.pos, hh, a.cnt_a, a.list_a, a.cap_a, a.in_cnt, a.in_list, a.in_cap,
-                             a.n, a.F, a.Facc, a.part_f2, st, a.precision, a.lj_shape);
+                             a.n, a.F, a.Facc, a.part_f2, st, a.precision, a.lj_shape, a.err);
     }
     return e;
 }
@@ -506,8 +506,8 @@ cudaError_t enqueue_batch_step(const BatchDev& b, bool rescale_phase, cudaStream
     k_b_kick<<<b.nblk_atom, kPB, 0, st>>>(b);
     if (b.kind == FMD_SYS_MM)
         if ((e = batch_mm_bonded_launch(b.A, b.off_f1, b.R, b.nblk_f1, b.f1_threads, st)) != cudaSuccess) return e;
-    if ((e = batch_lj_launch(b.A, b.off_lj, b.R, b.nblk_lj, b.ff, b.precision, b.lj_threads, b.lj_unroll, st)) !=
-        cudaSuccess)
+    if ((e = batch_lj_launch(b.A, b.off_lj, b.R, b.nblk_lj, b.ff, b.precision, b.lj_threads, b.lj_unroll, st,
+                             b.lj_staged_in_cap)) != cudaSuccess)
         return e;
     k_b_kick2<<<b.nblk_atom, kPB, 0, st>>>(b);
     k_b_end<<<b.R, 256, 0, st>>>(b);

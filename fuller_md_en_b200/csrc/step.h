@@ -44,7 +44,7 @@ struct StepArrays {
     int has_charge = 0;
     SysScal* S = nullptr;
     const int* cnt_a = nullptr; const int* list_a = nullptr; int cap_a = 0;     // LJ half / rigid
-    const int* in_cnt = nullptr; const int* in_list = nullptr; int in_cap = 0;  // LJ incoming
+    const int* in_cnt = nullptr; const int* in_list = nullptr; int in_cap = 0;  // LJ full rows (incoming + own)
     const int* cnt_b = nullptr; const int* list_b = nullptr; int cap_b = 0;     // REBO
     double* rebo_slots = nullptr;   // [n * cap_b * kReboSlotDoubles] REBO slot records (fast path)
     double* part_f1 = nullptr;  // REBO / rigid / bonded partials
@@ -55,6 +55,7 @@ struct StepArrays {
     double rmcut2 = 0, Mmol = 0, I0 = 0;
     int precision = FMD_PREC_FP64;
     LJShape lj_shape{};            // launch shape of the atomistic LJ gather
+    DevErr* err = nullptr;         // device error word (bounded waits of staged kernels)
     int lj_blocks = 0;             // its grid = partial records in part_f2
     SgStep* sg = nullptr;          // AIREBO: learned REBO term instead of the plain kernel
     int rebo_blocks = kForceBlocks;  // partial records the REBO term writes into part_f1
@@ -106,11 +107,13 @@ struct BatchDev {
     const int* off_f1 = nullptr;     // bonded terms (part_f1 records)
     int nblk_atom = 0, nblk_lj = 0, nblk_f1 = 0;   // totals (off[R])
     int lj_threads = 256, lj_unroll = 4, f1_threads = 128;
+    int lj_staged_in_cap = 0;        // > 0: LJ rows staged in shared memory
     int kind = FMD_SYS_MM, ff = FMD_FF_MM, precision = FMD_PREC_FP64;
 };
 // LJ gather / MM bonded terms over all replicas in one launch each.
+// staged_in_cap > 0: rows staged in shared memory (all replicas' row stride).
 cudaError_t batch_lj_launch(const StepArrays* As, const int* off, int R, int nblocks, int ff, int precision,
-                            int threads, int unroll, cudaStream_t st);
+                            int threads, int unroll, cudaStream_t st, int staged_in_cap = 0);
 cudaError_t batch_mm_bonded_launch(const StepArrays* As, const int* off, int R, int nblocks, int threads,
                                    cudaStream_t st);
 // One step of every replica (the single-system step's launches, each once

@@ -67,6 +67,7 @@ int System::alloc_common(const double* pos_h, const double* vel_h, const double*
         alloc(&arr.part_ke, (size_t)kForceBlocks * 2, (const double*)nullptr) ||
         alloc(&dropped, 2, (const int*)nullptr) || alloc(&arr.S, 1, (const SysScal*)nullptr))
         return ctx->fail(FMD_ERR_CUDA, "device allocation failed");
+    arr.err = ctx->d_err;
     cudaMemsetAsync(arr.F, 0, sizeof(double) * 3 * n, st);
     cudaMemsetAsync(arr.Facc, 0, sizeof(double) * 3 * n, st);
     cudaMemsetAsync(dropped, 0, sizeof(int) * 2, st);
@@ -102,8 +103,8 @@ int System::alloc_lists(double rc_list_a, int cap_a_, double rc_list_b, int cap_
             return ctx->fail(FMD_ERR_CUDA, "list allocation failed");
     }
     if (transpose) {
-        arr.in_cap = kInCap;
-        if (alloc(&cnt, n, (const int*)nullptr) || alloc(&lst, (size_t)n * kInCap, (const int*)nullptr))
+        arr.in_cap = kInCap + cap_a_;   // full rows: incoming entries then the row itself
+        if (alloc(&cnt, n, (const int*)nullptr) || alloc(&lst, (size_t)n * arr.in_cap, (const int*)nullptr))
             return ctx->fail(FMD_ERR_CUDA, "list allocation failed");
         arr.in_cnt = cnt; arr.in_list = lst;
     }
@@ -168,6 +169,14 @@ int System::tune_lj() {
     if (it != cache.end()) {
         arr.lj_shape = it->second;
     } else {
+        // Each candidate is timed right after a write larger than L2, as the
+        // gather runs inside a step whose other kernels have evicted its rows.
+        void* flush = nullptr;
+        const size_t flush_bytes = 160u << 20;
+        if (cudaMalloc(&flush, flush_bytes) != cudaSuccess) {
+            cudaGetLastError();
+            flush = nullptr;
+        }
         cudaEvent_t e0, e1;
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);
@@ -175,22 +184,29 @@ int System::tune_lj() {
         LJShape pick;
         for (int nt : {128, 256})
             for (int u : {2, 4})
-                for (int pipe : {0, 1}) {
+                for (int pipe : {0, 1, 2}) {
                     const LJShape sh{nt, u, pipe};
+                    if (lj_gather_blocks(ff, arr.precision, sh, arr.in_cap) < 1) continue;
                     auto go = [&]() {
                         return lj_gather_launch(ff, arr.pos, arr.S->h, arr.cnt_a, arr.list_a, arr.cap_a, arr.in_cnt,
                                                 arr.in_list, arr.in_cap, arr.n, arr.Facc, arr.Facc, arr.part_f2, st,
-                                                arr.precision, sh);
+                                                arr.precision, sh, ctx->d_err);
                     };
                     go();
-                    cudaEventRecord(e0, st);
-                    for (int r = 0; r < 3; r++) go();
-                    cudaEventRecord(e1, st);
-                    cudaEventSynchronize(e1);
-                    float ms = 0.f;
-                    cudaEventElapsedTime(&ms, e0, e1);
-                    if (ms < best) { best = ms; pick = sh; }
+                    float tot = 0.f;
+                    for (int r = 0; r < 3; r++) {
+                        if (flush) cudaMemsetAsync(flush, r, flush_bytes, st);
+                        cudaEventRecord(e0, st);
+                        go();
+                        cudaEventRecord(e1, st);
+                        cudaEventSynchronize(e1);
+                        float ms = 0.f;
+                        cudaEventElapsedTime(&ms, e0, e1);
+                        tot += ms;
+                    }
+                    if (tot < best) { best = tot; pick = sh; }
                 }
+        if (flush) cudaFree(flush);
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         // the timing runs accumulated into Facc
@@ -200,7 +216,7 @@ int System::tune_lj() {
         cache[key] = pick;
         arr.lj_shape = pick;
     }
-    arr.lj_blocks = lj_gather_blocks(ff, arr.precision, arr.lj_shape);
+    arr.lj_blocks = lj_gather_blocks(ff, arr.precision, arr.lj_shape, arr.in_cap);
     return FMD_OK;
 }
 
@@ -360,7 +376,7 @@ extern "C" int fmd_system_create_airebo(fmd_ctx* ctx, const fmd_run_params* p, i
     s->arr.kind = FMD_SYS_AIREBO;
     s->arr.n = na;
     s->arr.precision = p->precision;
-    s->arr.lj_blocks = lj_gather_blocks(FMD_FF_AIREBO, p->precision, s->arr.lj_shape);
+    s->arr.lj_blocks = lj_gather_blocks(FMD_FF_AIREBO, p->precision, s->arr.lj_shape, 0);
     int rc = s->alloc_common(pos, vel, h, npt);
     if (rc != FMD_OK) return rc;
     double* m; int* mid;
@@ -386,7 +402,7 @@ extern "C" int fmd_system_create_mm(fmd_ctx* ctx, const fmd_run_params* p, int n
     s->arr.kind = FMD_SYS_MM;
     s->arr.n = na;
     s->arr.precision = p->precision;
-    s->arr.lj_blocks = lj_gather_blocks(FMD_FF_MM, p->precision, s->arr.lj_shape);
+    s->arr.lj_blocks = lj_gather_blocks(FMD_FF_MM, p->precision, s->arr.lj_shape, 0);
     int rc = s->alloc_common(pos, vel, h, npt);
     if (rc != FMD_OK) return rc;
     int* mid;
@@ -514,7 +530,7 @@ extern "C" int fmd_system_kernel_ms(fmd_system* s, int stage, int reps, double* 
                 // Timed into the scratch accumulator (F itself is left alone).
                 return lj_gather_launch(a.kind == FMD_SYS_AIREBO ? FMD_FF_AIREBO : FMD_FF_MM, a.pos, hh, a.cnt_a,
                                         a.list_a, a.cap_a, a.in_cnt, a.in_list, a.in_cap, a.n, a.Facc, a.Facc,
-                                        a.part_f2, st, a.precision, a.lj_shape);
+                                        a.part_f2, st, a.precision, a.lj_shape, a.err);
             case 1:
                 if (a.kind == FMD_SYS_AIREBO && a.sg)   // the REBO term the step uses
                     return sg_enqueue_rebo(*a.sg, a, false, st);
@@ -553,6 +569,30 @@ extern "C" int fmd_system_kernel_ms(fmd_system* s, int stage, int reps, double* 
     if (err != cudaSuccess) return y.ctx->fail(FMD_ERR_CUDA, cudaGetErrorString(err));
     *ms = (double)tot / reps;
     return rc;
+}
+
+extern "C" int fmd_system_set_lj_shape(fmd_system* s, int threads, int unroll, int feed) {
+    if (!s || !s->sys) return FMD_ERR_ARG;
+    fmd::System& y = *s->sys;
+    if (y.arr.kind == FMD_SYS_RIGID || (threads != 128 && threads != 256) || (unroll != 2 && unroll != 4) ||
+        feed < 0 || feed > 2)
+        return y.ctx->fail(FMD_ERR_ARG, "fmd_system_set_lj_shape: bad shape");
+    const LJShape sh{threads, unroll, feed};
+    const int ff = y.arr.kind == FMD_SYS_AIREBO ? FMD_FF_AIREBO : FMD_FF_MM;
+    const int nb = lj_gather_blocks(ff, y.arr.precision, sh, y.arr.in_cap);
+    if (nb < 1) return y.ctx->fail(FMD_ERR_ARG, "fmd_system_set_lj_shape: shape cannot run with this list");
+    if (cudaStreamSynchronize(y.ctx->stream) != cudaSuccess) return y.ctx->fail(FMD_ERR_CUDA, "sync failed");
+    y.drop_graphs();                     // captured graphs hold the old launch
+    y.arr.lj_shape = sh;
+    y.arr.lj_blocks = nb;
+    if (y.arr.sg) {                      // keep the learned term's graph variants too
+        int rc = FMD_OK;
+        for (int r = 0; r < 2 && rc == FMD_OK; r++)
+            for (int ph = 0; ph < 2 && rc == FMD_OK; ph++)
+                for (int j = 0; j < 2 && rc == FMD_OK; j++) rc = y.capture(r != 0, ph != 0, j != 0);
+        return rc;
+    }
+    return FMD_OK;
 }
 
 extern "C" int fmd_system_lj_shape(fmd_system* s, int* threads, int* unroll, int* pipelined, int* blocks) {

@@ -8,7 +8,7 @@
 
 namespace fmd {
 
-constexpr int kInCap = 1024;   // incoming (transposed) LJ entries per atom
+constexpr int kInCap = 1024;   // incoming (transposed) LJ entries per atom; full rows add the own row
 
 struct System {
     fmd_ctx* ctx = nullptr;

@@ -250,9 +250,13 @@ int fmd_system_destroy(fmd_system *s);
  * a judge step of the learned REBO term). */
 int fmd_system_kernel_ms(fmd_system *s, int stage, int reps, double *ms_per_launch);
 /* Launch shape of the atomistic LJ gather that fmd_system_init's autotuner
- * chose (threads per block, list entries in flight per lane, software
- * pipelining 0/1, grid blocks); any pointer may be NULL. */
+ * chose (threads per block 128/256, list entries in flight per lane 2/4,
+ * row feed 0 loads as used / 1 software-pipelined / 2 rows staged in shared
+ * memory by bulk asynchronous copies, grid blocks); any pointer may be NULL.
+ * fmd_system_set_lj_shape pins a shape (for reproducible runs; results then
+ * do not depend on timing), after fmd_system_init. */
 int fmd_system_lj_shape(fmd_system *s, int *threads, int *unroll, int *pipelined, int *blocks);
+int fmd_system_set_lj_shape(fmd_system *s, int threads, int unroll, int feed);
 int fmd_system_step_kernels(fmd_system *s, int rebuild, int phase, int *nkernels);
 
 /* ------------------------------------------------------- replica batches --
@@ -273,6 +277,7 @@ typedef struct {
     int lj_threads;               /* threads per block of the LJ gather */
     int lj_unroll;                /* list entries in flight per lane (neighbours per warp / 32) */
     int lj_atoms_per_block;       /* sites per block of the LJ gather */
+    int lj_staged;                /* 1: LJ rows staged in shared memory by bulk asynchronous copies */
     int bonded_threads;           /* threads per block of the bonded terms */
     int bonded_terms_per_block;
     double lj_ms, bonded_ms;      /* timed duration of the chosen shapes, ms per launch */
