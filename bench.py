@@ -125,7 +125,8 @@ def make_system(ctx, rank: int, precision=None):
     says otherwise."""
     from fuller_md_en_b200 import RunConfig, System, crystal
     from fuller_md_en_b200._lib import FMD_PREC_FP64
-    s = crystal.atomistic(NC, jitter=JITTER, seed=SEED + rank, T=T_K)
+    from fuller_md_en_b200.replicas import replica_seed
+    s = crystal.atomistic(NC, jitter=JITTER, seed=replica_seed(SEED, rank), T=T_K)
     na = s["pos"].size // 3
     cfg = RunConfig(dt=DT, T=T_K, Pe=P_GPA, nsteps=10 ** 6, nlup=NLUP, gavg_from=1, gavg_to=10 ** 6, nc=NC,
                     nmol=s["nmol"], use_graphs=1,
@@ -206,11 +207,9 @@ def run_ours(args, ws, rank, local):
     obs = sysd.run(K + 1, K + 1)               # one more step: observables sanity
     if not math.isfinite(obs.E[0]):
         raise RuntimeError("non-finite energy in the benchmark run")
-    if ws > 1:
-        t = torch.tensor([ms_total], device=f"cuda:{local}")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_total = float(t.item())
-    value = ws * na * K / (ms_total / 1e3)
+    from fuller_md_en_b200.replicas import job_throughput, max_over_ranks
+    ms_total = max_over_ranks(ms_total, device=f"cuda:{local}")
+    value = job_throughput(na, K, ms_total, ws)
 
     # ---------------- roofline of the dominant kernel ----------------
     stages = {"lj_gather": sysd.kernel_ms(0, 20), "rebo": sysd.kernel_ms(1, 20),

@@ -118,6 +118,7 @@ _SIGS = {
     "fmd_system_averages": (c_int, [c_void_p, POINTER(Avg)]),
     "fmd_system_download": (c_int, [c_void_p, _dp, _dp, _dp, _dp, _dp, POINTER(NPT)]),
     "fmd_system_lists": (c_int, [c_void_p, _ip, _ip, _ip, _ip]),
+    "fmd_system_virial": (c_int, [c_void_p, _dp, _dp]),
     "fmd_system_destroy": (c_int, [c_void_p]),
     "fmd_system_kernel_ms": (c_int, [c_void_p, c_int, c_int, POINTER(c_double)]),
     "fmd_system_step_kernels": (c_int, [c_void_p, c_int, c_int, POINTER(c_int)]),

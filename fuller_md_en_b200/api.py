@@ -398,6 +398,13 @@ class System:
                                                      _i(lb) if lb is not None else None), "fmd_system_lists")
         return ca, la, cb, lb
 
+    def virial(self):
+        """(W9 of the last force evaluation, current kinetic energy)."""
+        W = np.zeros(9)
+        ke = ctypes.c_double(0)
+        self.ctx.check(self.ctx.lib.fmd_system_virial(self.h, _d(W), ctypes.byref(ke)), "fmd_system_virial")
+        return W, ke.value
+
     def kernel_ms(self, stage: int, reps: int = 20) -> float:
         """Mean duration (ms) of one launch of a stage, CUDA events on the context stream."""
         ms = ctypes.c_double(0)

@@ -571,6 +571,19 @@ extern "C" int fmd_system_kernel_ms(fmd_system* s, int stage, int reps, double* 
     return rc;
 }
 
+extern "C" int fmd_system_virial(fmd_system* s, double* W9, double* KE) {
+    if (!s || !s->sys) return FMD_ERR_ARG;
+    fmd::System& y = *s->sys;
+    SysScal h;
+    if (cudaMemcpyAsync(&h, y.arr.S, sizeof(h), cudaMemcpyDeviceToHost, y.ctx->stream) != cudaSuccess)
+        return y.ctx->fail(FMD_ERR_CUDA, "fmd_system_virial: copy failed");
+    const int rc = y.ctx->sync_check("fmd_system_virial");
+    if (rc != FMD_OK) return rc;
+    if (W9) std::memcpy(W9, h.W9, sizeof(double) * 9);
+    if (KE) *KE = h.KE;
+    return FMD_OK;
+}
+
 extern "C" int fmd_system_set_lj_shape(fmd_system* s, int threads, int unroll, int feed) {
     if (!s || !s->sys) return FMD_ERR_ARG;
     fmd::System& y = *s->sys;

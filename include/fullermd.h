@@ -234,6 +234,9 @@ int fmd_system_averages(fmd_system *s, fmd_avg *avg);
 /* Copies the state to host arrays (any may be NULL). */
 int fmd_system_download(fmd_system *s, double *pos, double *vel, double *qv, double *omg,
                         double *h, fmd_npt *npt);
+/* Virial tensor W9 of the last force evaluation and the current kinetic
+ * energy (eV; rigid: translational + rotational); either may be NULL. */
+int fmd_system_virial(fmd_system *s, double *W9, double *KE);
 /* Current neighbour lists (reference layout) for inspection. */
 int fmd_system_lists(fmd_system *s, int *cnt_a, int *list_a, int *cnt_b, int *list_b);
 int fmd_system_destroy(fmd_system *s);
