@@ -249,6 +249,11 @@ def run_ours(args, ws, rank, local):
     if not args.no_batch:
         batch_res = run_batch(args, ctx, stream, flush, ws, rank)
 
+    # ---------------- rigid-body LJ, C60 FCC nc=10 (240,000 sites) ----------------
+    rigid_res = None
+    if not args.no_rigid:
+        rigid_res = run_rigid(args, ctx, stream, flush, ws, rank, local)
+
     # ---------------- end to end through the public API ----------------
     e2e = None
     if rank == 0 or ws > 1:
@@ -300,8 +305,64 @@ def run_ours(args, ws, rank, local):
         "e2e": e2e,
         "surrogate": sg_res,
         "batch": batch_res,
+        "rigid": rigid_res,
     }
     return res
+
+
+def run_rigid(args, ctx, stream, flush, ws, rank, local):
+    """C60 FCC nc=10 as rigid bodies: 4,000 molecules x 60 sites = 240,000
+    sites, 300 K, 1 GPa, dt 1 fs, molecule lists every 25 steps, FP32 site-pair
+    arithmetic with FP64 per-molecule sums and FP64 integrator."""
+    from fuller_md_en_b200 import RunConfig, System, crystal
+    from fuller_md_en_b200._lib import FMD_PREC_FP32_PAIR
+    from fuller_md_en_b200.replicas import job_throughput, max_over_ranks, replica_seed
+    s = crystal.rigid(10, seed=replica_seed(SEED, rank))
+    n = s["n"]
+    rmcut = 3.0 * 3.431 + 2 * s["Rmol"] + 1.0
+    cfg = RunConfig(dt=1.0, T=300.0, Pe=1.0, nsteps=10 ** 6, nlup=25, gavg_from=1, gavg_to=10 ** 6, nc=10, nmol=n,
+                    precision=FMD_PREC_FP32_PAIR)
+    sysd = System.rigid(ctx, cfg, 60, s["body"], s["I0"], s["Mmol"], rmcut, s["pos"], s["vel"], s["qv"], s["omg"],
+                        s["h"], crystal.npt_rigid(300.0, 1.0, n))
+    sysd.init()
+    K = args.steps
+    step_ms = timed_steps(ctx, stream, sysd, K, flush)
+    obs = sysd.run(K + 1, K + 1)
+    if not math.isfinite(obs.E[0]):
+        raise RuntimeError("non-finite energy in the rigid benchmark run")
+    pair_ms = sysd.kernel_ms(0, 10)
+    sysd.close()
+    ms = max_over_ranks(float(sum(step_ms)), device=f"cuda:{local}")
+    sites = n * 60
+    out = {"value": job_throughput(sites, K, ms, ws), "unit": "site-steps/s", "ms_per_step": ms / K,
+           "workload": "rigid-body LJ, C60 FCC nc=10: 4,000 molecules / 240,000 sites, 300 K, 1 GPa, dt 1 fs, "
+                       "molecule lists every 25 steps, FP32 site pairs with FP64 sums and integrator",
+           "site_pair_kernel_ms": pair_ms}
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = rigid_reference_sample(s, n, rmcut)
+    return out
+
+
+def rigid_reference_sample(s, n, rmcut, K=3):
+    """The reference's own rigid step (oracle/_ref, OpenMP build, all host
+    threads) on global steps 1..K of the same crystal, molecule list built once."""
+    from fuller_md_en_b200 import crystal
+    from oracle.fmd_oracle import Ref, ref_available
+    if not ref_available():
+        return None
+    R = Ref(omp=True)
+    st = dict(pos=s["pos"].copy(), vel=s["vel"].copy(), qv=s["qv"].copy(), omg=s["omg"].copy(), h=s["h"].copy(),
+              hi=crystal.inv9(s["h"]), npt=crystal.npt_rigid(300.0, 1.0, n))
+    c, l = R.lj_nlist(st["pos"], st["h"], st["hi"], n, rmcut)
+    e, F, T, W = R.lj_forces(st["pos"], st["qv"], s["body"], st["h"], st["hi"], c, l, n, 60, rmcut * rmcut)
+    st.update(F=F, T=T, W9=W)
+    t0 = time.perf_counter()
+    for _ in range(K):
+        R.lj_step(st, s["body"], s["I0"], s["Mmol"], 60, rmcut * rmcut, 1.0, c, l)
+    dt = (time.perf_counter() - t0) / K
+    cores = os.cpu_count() or 1
+    return {"value": n * 60 / dt, "unit": "site-steps/s", "cores": cores, "kind": "reference",
+            "sample": f"{K} steps of the reference's step_npt (OpenMP build, {cores} threads), {dt * 1e3:.0f} ms/step"}
 
 
 def run_batch(args, ctx, stream, flush, ws, rank):
@@ -495,6 +556,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-surrogate", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-rigid", action="store_true")
     ap.add_argument("--sg-train-steps", type=int, default=6000)
     args = ap.parse_args()
     if args.warmup < 3:

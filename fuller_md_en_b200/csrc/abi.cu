@@ -128,7 +128,7 @@ namespace {
 enum Slot {
     S_POS = 0, S_HH, S_MOL, S_CNT, S_LIST, S_CNT2, S_LIST2, S_INCNT, S_INLIST, S_DROP,
     S_F, S_FACC, S_T, S_QV, S_BODY, S_VEL, S_OMG, S_MASS, S_PART1, S_PART2, S_PART3, S_PARTKE,
-    S_SCAL, S_CHARGE, S_RSLOT, S_TOPO0
+    S_SCAL, S_CHARGE, S_RSLOT, S_RLAB, S_TOPO0
 };
 
 template <class T>
@@ -398,6 +398,7 @@ extern "C" int fmd_lj_rigid_forces(fmd_ctx* ctx, const double* pos, const double
     StepArrays a;
     a.precision = ctx->precision;
     a.kind = FMD_SYS_RIGID; a.n = n; a.natom = natom; a.rmcut2 = rmcut2; a.precision = precision;
+    if (up<double>(ctx, S_RLAB, nullptr, (size_t)n * natom * kRigidLabDoubles, &a.rigid_lab)) return FMD_ERR_CUDA;
     double *dpos, *dq, *db, *dF, *dT;
     int *dc, *dl;
     int rc = up(ctx, S_POS, pos, 3 * (size_t)n, &dpos);
@@ -597,6 +598,7 @@ extern "C" int fmd_rigid_step(fmd_ctx* ctx, double* pos, double* vel, double* qv
     StepArrays a;
     a.precision = ctx->precision;
     a.kind = FMD_SYS_RIGID; a.n = n; a.natom = natom; a.rmcut2 = rmcut2; a.Mmol = Mmol; a.I0 = I0;
+    if (up<double>(ctx, S_RLAB, nullptr, (size_t)n * natom * kRigidLabDoubles, &a.rigid_lab)) return FMD_ERR_CUDA;
     a.precision = precision;
     double *dpos, *dvel, *dq, *dw, *dF, *dT, *db;
     int *dc, *dl;

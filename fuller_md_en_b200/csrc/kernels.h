@@ -103,10 +103,15 @@ cudaError_t lj_gather_launch(int ff, const double* pos, const double* hh, const 
                              cudaStream_t st, int precision = FMD_PREC_FP64, const LJShape& shape = LJShape{},
                              DevErr* err = nullptr);
 // Rigid site-site LJ (a5-a6): writes F, T; per-block {E, W9} partials (grid n).
+// lab (may be null): scratch of n * natom * 4 doubles for the lab-frame sites;
+// with it (and natom <= 64) the warp-per-neighbour kernel runs, in launch
+// shape 0 (4 warps per molecule), 1 (4 warps, registers capped for 4 blocks
+// per SM) or 2 (8 warps, capped for 2 blocks per SM).
+constexpr int kRigidLabDoubles = 4;   // per site
 cudaError_t rigid_launch(int precision, const double* pos, const double* qv, const double* body,
                          const double* hh, const int* cnt, const int* list, int cap, int n,
                          int natom, double rmcut2, double* F, double* T, double* part,
-                         cudaStream_t st);
+                         cudaStream_t st, double* lab = nullptr, int shape = 0);
 int rigid_grid(int n);
 
 // MM bonded terms (a10-a13): atomics into Facc; partials {E_b,E_a,E_d,E_i, W00,W11,W22}

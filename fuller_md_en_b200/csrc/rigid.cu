@@ -16,6 +16,7 @@
 //   FMD_PREC_FP32_PAIR  COM image and cutoff skip in FP64, site offsets and
 //                       pair arithmetic in FP32, per-neighbour FP32 sums folded
 //                       into FP64 per-molecule accumulators.
+#include <algorithm>
 #include <cmath>
 #include "kernels.h"
 #include "geom.cuh"
@@ -206,17 +207,195 @@ k_rigid(const double* __restrict__ pos, const double* __restrict__ qv, const dou
     }
 }
 
+// ---------------------------------------------------------------------------
+// Warp-per-neighbour variant.  k_rigid_lab writes every molecule's lab-frame
+// sites once per step (the reference computes the whole lab frame first too,
+// LJ:276-291).  In k_rigid_w one CTA owns molecule i; each warp takes one
+// listed neighbour j at a time, copies j's sites from the lab array into its
+// own shared-memory slice with coalesced 16/32-byte loads, and lane l handles
+// sites l and l + 32 of i against all sites of j -- no block-wide barrier in
+// the neighbour loop.  Per-neighbour partial sums stay in the pair precision
+// and are folded into FP64 per-molecule accumulators; the CTA reduces them
+// in a fixed order.
+template <class P>
+__global__ void __launch_bounds__(256)
+k_rigid_lab(const double* __restrict__ qv, const double* __restrict__ body, int n, int natom,
+            Site<P>* __restrict__ lab) {
+    const long long tot = (long long)n * natom;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t / natom), a = (int)(t % natom);
+        double R[9];
+        quat_rot(qv + 4 * i, R);
+        const double bx = body[3 * a], by = body[3 * a + 1], bz = body[3 * a + 2];
+        Site<P> s;
+        s.x = (P)dot3_rn(R[0], R[1], R[2], bx, by, bz);
+        s.y = (P)dot3_rn(R[3], R[4], R[5], bx, by, bz);
+        s.z = (P)dot3_rn(R[6], R[7], R[8], bx, by, bz);
+        s.pad = 0;
+        lab[t] = s;
+    }
+}
+
+// W warps per molecule; MINB resident blocks per SM requested from the
+// compiler (a register cap: 0 leaves the register count free).
+template <class P, int W, int MINB>
+__global__ void __launch_bounds__(32 * W, MINB)
+k_rigid_w(const double* __restrict__ pos, const Site<P>* __restrict__ lab, const double* __restrict__ hh,
+          const int* __restrict__ cnt, const int* __restrict__ list, int cap, int n, int natom, double rmcut2,
+          RigidConst rc, double* __restrict__ F, double* __restrict__ T, double* __restrict__ part) {
+    constexpr int kRigidWarps = W;
+    __shared__ Site<P> lab_i[2 * 32];
+    __shared__ Site<P> lab_j[kRigidWarps][2 * 32];
+    __shared__ double sm[32 * 16];
+    __shared__ double s_hh[18];
+    const int i = blockIdx.x;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (threadIdx.x < 18) s_hh[threadIdx.x] = hh[threadIdx.x];
+    for (int a = threadIdx.x; a < natom; a += blockDim.x) lab_i[a] = lab[(size_t)i * natom + a];
+    __syncthreads();
+    const double* h = s_hh;
+    const double* hi = s_hh + 9;
+    const double pix = pos[3 * i], piy = pos[3 * i + 1], piz = pos[3 * i + 2];
+    const int a0 = lane, a1 = lane + 32;
+    const bool v0 = a0 < natom, v1 = a1 < natom;
+    const Site<P> r0 = lab_i[v0 ? a0 : 0], r1 = lab_i[v1 ? a1 : 0];
+    double acc[16];   // F(3) T(3) W(9) E
+#pragma unroll
+    for (int k = 0; k < 16; k++) acc[k] = 0.0;
+    const float sig2 = (float)rc.sig2, sig2_lo = (float)(rc.sig2 - (double)(float)rc.sig2);
+    const float rcut2f = (float)rc.rcut2, c24f = (float)rc.c24, c4f = (float)rc.c4;
+    const int nn = cnt[i];
+    Site<P>* sj = lab_j[w];
+    for (int k = w; k < nn; k += kRigidWarps) {
+        const int j = list[(size_t)i * cap + k];
+        double mx = __dsub_rn(pos[3 * j], pix), my = __dsub_rn(pos[3 * j + 1], piy), mz = __dsub_rn(pos[3 * j + 2], piz);
+        mimg(mx, my, mz, hi, h);
+        if (norm2_rn(mx, my, mz) > rmcut2) continue;             // warp-uniform (LJ:320)
+        __syncwarp();
+        if (v0) sj[a0] = lab[(size_t)j * natom + a0];
+        if (v1) sj[a1] = lab[(size_t)j * natom + a1];
+        __syncwarp();
+        // per-neighbour partial sums for sites a0 and a1
+        P f[2][3] = {{0, 0, 0}, {0, 0, 0}}, wv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, e = 0;
+        if constexpr (sizeof(P) == 8) {
+            for (int b = 0; b < natom; b++) {
+                const Site<P> rb = sj[b];
+#pragma unroll
+                for (int s = 0; s < 2; s++) {
+                    const Site<P>& ra = s ? r1 : r0;
+                    if (!(s ? v1 : v0)) continue;
+                    // FP64: reference order ((dm + r_b) - r_a) for every decision (LJ:330-336)
+                    const double dx = __dsub_rn(__dadd_rn(mx, rb.x), ra.x);
+                    const double dy = __dsub_rn(__dadd_rn(my, rb.y), ra.y);
+                    const double dz = __dsub_rn(__dadd_rn(mz, rb.z), ra.z);
+                    double r2 = norm2_rn(dx, dy, dz);
+                    if (r2 < rc.rcut2) {
+                        if (r2 < 0.25) r2 = 0.25;
+                        const double ri2 = 1.0 / r2, s2 = rc.sig2 * ri2, s6 = s2 * s2 * s2, s12 = s6 * s6;
+                        const double fm = rc.c24 * (2.0 * s12 - s6) * ri2;
+                        const double fx = fm * dx, fy = fm * dy, fz = fm * dz;
+                        f[s][0] -= fx; f[s][1] -= fy; f[s][2] -= fz;
+                        e += 0.5 * (rc.c4 * (s12 - s6) - rc.vshift);
+                        wv[0] += 0.5 * dx * fx; wv[1] += 0.5 * dx * fy; wv[2] += 0.5 * dx * fz;
+                        wv[3] += 0.5 * dy * fx; wv[4] += 0.5 * dy * fy; wv[5] += 0.5 * dy * fz;
+                        wv[6] += 0.5 * dz * fx; wv[7] += 0.5 * dz * fy; wv[8] += 0.5 * dz * fz;
+                    }
+                }
+            }
+        } else {
+            // COM image split into FP32 head + tail so each pair distance keeps
+            // ~1e-7 relative accuracy; the small site difference goes first.
+            const float mxh = (float)mx, myh = (float)my, mzh = (float)mz;
+            const float mxl = (float)(mx - (double)mxh), myl = (float)(my - (double)myh), mzl = (float)(mz - (double)mzh);
+            float eterm = 0.f;
+            int npair = 0;
+            for (int b = 0; b < natom; b++) {
+                const Site<P> rb = sj[b];
+#pragma unroll
+                for (int s = 0; s < 2; s++) {
+                    const Site<P>& ra = s ? r1 : r0;
+                    if (!(s ? v1 : v0)) continue;
+                    const float dx = (mxh + (rb.x - ra.x)) + mxl;
+                    const float dy = (myh + (rb.y - ra.y)) + myl;
+                    const float dz = (mzh + (rb.z - ra.z)) + mzl;
+                    float r2 = dx * dx + dy * dy + dz * dz;
+                    if (r2 < rcut2f) {
+                        r2 = fmaxf(r2, 0.25f);
+                        const float ri2 = 1.0f / r2, s2 = fmaf(sig2, ri2, sig2_lo * ri2), s6 = s2 * s2 * s2,
+                                    s12 = s6 * s6;
+                        const float fm = c24f * (2.0f * s12 - s6) * ri2;
+                        const float fx = fm * dx, fy = fm * dy, fz = fm * dz;
+                        f[s][0] -= fx; f[s][1] -= fy; f[s][2] -= fz;
+                        eterm += c4f * (s12 - s6);
+                        npair++;
+                        wv[0] += dx * fx; wv[1] += dx * fy; wv[2] += dx * fz;
+                        wv[3] += dy * fx; wv[4] += dy * fy; wv[5] += dy * fz;
+                        wv[6] += dz * fx; wv[7] += dz * fy; wv[8] += dz * fz;
+                    }
+                }
+            }
+            // energy and virial halved for the symmetric list (LJ:339-341); the
+            // shift in FP64 once per neighbour
+            e = 0.5f * eterm;
+            acc[15] -= 0.5 * rc.vshift * npair;
+#pragma unroll
+            for (int q = 0; q < 9; q++) wv[q] *= 0.5f;
+        }
+#pragma unroll
+        for (int s = 0; s < 2; s++) {
+            if (!(s ? v1 : v0)) continue;
+            const Site<P>& ra = s ? r1 : r0;
+            const double fx = (double)f[s][0], fy = (double)f[s][1], fz = (double)f[s][2];
+            const double rx = (double)ra.x, ry = (double)ra.y, rz = (double)ra.z;
+            acc[0] += fx; acc[1] += fy; acc[2] += fz;
+            // torque -= r_a x f with f the force on i's site (LJ:337)
+            acc[3] += ry * fz - rz * fy;
+            acc[4] += rz * fx - rx * fz;
+            acc[5] += rx * fy - ry * fx;
+        }
+#pragma unroll
+        for (int q = 0; q < 9; q++) acc[6 + q] += (double)wv[q];
+        acc[15] += (double)e;
+    }
+    double tot[16];
+    block_sum_store<16>(acc, sm, tot);
+    if (threadIdx.x == 0) {
+        F[3 * i] = tot[0]; F[3 * i + 1] = tot[1]; F[3 * i + 2] = tot[2];
+        T[3 * i] = tot[3]; T[3 * i + 1] = tot[4]; T[3 * i + 2] = tot[5];
+        double* o = part + (size_t)i * kNV;
+        o[0] = tot[15];
+#pragma unroll
+        for (int q = 0; q < 9; q++) o[1 + q] = tot[6 + q];
+    }
+}
+
 }  // namespace
 
 int rigid_grid(int n) { return n; }
 
 cudaError_t rigid_launch(int precision, const double* pos, const double* qv, const double* body,
                          const double* hh, const int* cnt, const int* list, int cap, int n, int natom,
-                         double rmcut2, double* F, double* T, double* part, cudaStream_t st) {
+                         double rmcut2, double* F, double* T, double* part, cudaStream_t st, double* lab,
+                         int shape) {
     if (n <= 0) return cudaSuccess;
     if (natom < 1 || natom > kMaxSites) return cudaErrorInvalidValue;
-    const int ts = ((natom + 31) / 32) * 32;
     const RigidConst rc = rigid_const();
+    if (lab != nullptr && natom <= 64) {
+        const int lb = (int)std::min<long long>(((long long)n * natom + 255) / 256, kSMs * 16);
+#define FMD_RW(P, W, MB) \
+    k_rigid_w<P, W, MB><<<n, 32 * W, 0, st>>>(pos, reinterpret_cast<const Site<P>*>(lab), hh, cnt, list, cap, n, natom, \
+                                              rmcut2, rc, F, T, part)
+        if (precision == FMD_PREC_FP32_PAIR) {
+            k_rigid_lab<float><<<lb, 256, 0, st>>>(qv, body, n, natom, reinterpret_cast<Site<float>*>(lab));
+            if (shape == 1) FMD_RW(float, 4, 4); else if (shape == 2) FMD_RW(float, 8, 2); else FMD_RW(float, 4, 1);
+        } else {
+            k_rigid_lab<double><<<lb, 256, 0, st>>>(qv, body, n, natom, reinterpret_cast<Site<double>*>(lab));
+            if (shape == 1) FMD_RW(double, 4, 4); else if (shape == 2) FMD_RW(double, 8, 2); else FMD_RW(double, 4, 1);
+        }
+#undef FMD_RW
+        return cudaGetLastError();
+    }
+    const int ts = ((natom + 31) / 32) * 32;
     if (precision == FMD_PREC_FP32_PAIR)
         k_rigid<float><<<n, 2 * ts, 0, st>>>(pos, qv, body, hh, cnt, list, cap, n, natom, ts, rmcut2, rc, F, T, part);
     else

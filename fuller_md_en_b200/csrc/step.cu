@@ -454,7 +454,7 @@ cudaError_t enqueue_forces(const StepArrays& a, cudaStream_t st, bool judge) {
     const double* hh = a.S->h;
     if (a.kind == FMD_SYS_RIGID) {
         e = rigid_launch(a.precision, a.pos, a.qv, a.body, hh, a.cnt_a, a.list_a, a.cap_a, a.n, a.natom,
-                         a.rmcut2, a.F, a.T, a.part_f1, st);
+                         a.rmcut2, a.F, a.T, a.part_f1, st, a.rigid_lab, a.rigid_shape);
     } else if (a.kind == FMD_SYS_AIREBO) {
         if (a.sg) e = sg_enqueue_rebo(*a.sg, a, judge, st);
         else if (a.rebo_slots)

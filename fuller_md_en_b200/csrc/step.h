@@ -53,6 +53,8 @@ struct StepArrays {
     double* part_ke = nullptr;  // kinetic partials
     MMTopoDev topo{};
     double rmcut2 = 0, Mmol = 0, I0 = 0;
+    double* rigid_lab = nullptr;   // [n * natom * kRigidLabDoubles] lab-frame sites (rigid)
+    int rigid_shape = 0;           // launch shape of the rigid pair kernel (rigid_launch)
     int precision = FMD_PREC_FP64;
     LJShape lj_shape{};            // launch shape of the atomistic LJ gather
     DevErr* err = nullptr;         // device error word (bounded waits of staged kernels)

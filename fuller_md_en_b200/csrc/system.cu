@@ -220,6 +220,47 @@ int System::tune_lj() {
     return FMD_OK;
 }
 
+// Launch shape of the rigid pair kernel, timed on this system's own list at
+// set-up (the pair kernel writes F, T and partials only, which the first
+// force evaluation below recomputes); cached per (device, molecules, sites,
+// precision).
+int System::tune_rigid() {
+    static std::map<std::tuple<int, int, int, int>, int> cache;
+    const auto key = std::make_tuple(ctx->device, arr.n, arr.natom, arr.precision);
+    auto it = cache.find(key);
+    if (it != cache.end()) {
+        arr.rigid_shape = it->second;
+        return FMD_OK;
+    }
+    cudaStream_t st = ctx->stream;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float best = 1e30f;
+    int pick = 0;
+    for (int shape : {0, 1, 2}) {
+        auto go = [&]() {
+            return rigid_launch(arr.precision, arr.pos, arr.qv, arr.body, arr.S->h, arr.cnt_a, arr.list_a, arr.cap_a,
+                                arr.n, arr.natom, arr.rmcut2, arr.F, arr.T, arr.part_f1, st, arr.rigid_lab, shape);
+        };
+        go();
+        cudaEventRecord(e0, st);
+        for (int r = 0; r < 3; r++) go();
+        cudaEventRecord(e1, st);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best) { best = ms; pick = shape; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    const int rc = ctx->sync_check("rigid launch-shape tuning");
+    if (rc != FMD_OK) return rc;
+    cache[key] = pick;
+    arr.rigid_shape = pick;
+    return FMD_OK;
+}
+
 int System::init() {
     cudaStream_t st = ctx->stream;
     // Pre-loop order of the reference: lists from the unwrapped positions,
@@ -228,6 +269,9 @@ int System::init() {
     if (apply_pbc_launch(arr.pos, arr.n, arr.S->h, st) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "apply_pbc failed");
     if (arr.kind != FMD_SYS_RIGID) {
         const int rc = tune_lj();
+        if (rc != FMD_OK) return rc;
+    } else {
+        const int rc = tune_rigid();
         if (rc != FMD_OK) return rc;
     }
     if (enqueue_forces(arr, st) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "force launch failed");
@@ -357,6 +401,10 @@ extern "C" int fmd_system_create_rigid(fmd_ctx* ctx, const fmd_run_params* p, in
         return ctx->fail(FMD_ERR_CUDA, "device allocation failed");
     cudaMemsetAsync(T, 0, sizeof(double) * 3 * n, ctx->stream);
     s->arr.body = bd; s->arr.qv = q; s->arr.omg = w; s->arr.T = T;
+    double* lab;
+    if (s->alloc(&lab, (size_t)n * natom * kRigidLabDoubles, (const double*)nullptr))
+        return ctx->fail(FMD_ERR_CUDA, "device allocation failed");
+    s->arr.rigid_lab = lab;
     // The list radius is rmcut+3 (LJ:259); the force kernel skips pairs
     // beyond rmcut (LJ:320).
     if ((rc = s->alloc_lists(rmc, max_neigh, 0.0, 0, false)) != FMD_OK) return rc;
@@ -526,7 +574,7 @@ extern "C" int fmd_system_kernel_ms(fmd_system* s, int stage, int reps, double* 
             case 0:
                 if (a.kind == FMD_SYS_RIGID)
                     return rigid_launch(a.precision, a.pos, a.qv, a.body, hh, a.cnt_a, a.list_a, a.cap_a, a.n,
-                                        a.natom, a.rmcut2, a.F, a.T, a.part_f1, st);
+                                        a.natom, a.rmcut2, a.F, a.T, a.part_f1, st, a.rigid_lab, a.rigid_shape);
                 // Timed into the scratch accumulator (F itself is left alone).
                 return lj_gather_launch(a.kind == FMD_SYS_AIREBO ? FMD_FF_AIREBO : FMD_FF_MM, a.pos, hh, a.cnt_a,
                                         a.list_a, a.cap_a, a.in_cnt, a.in_list, a.in_cap, a.n, a.Facc, a.Facc,
@@ -539,7 +587,7 @@ extern "C" int fmd_system_kernel_ms(fmd_system* s, int stage, int reps, double* 
                                              a.part_f1, kForceBlocks, nullptr, 0, st);
                 if (a.kind == FMD_SYS_MM) return mm_bonded_launch(a.topo, a.pos, hh, a.Facc, a.part_f1, st);
                 return rigid_launch(a.precision, a.pos, a.qv, a.body, hh, a.cnt_a, a.list_a, a.cap_a, a.n, a.natom,
-                                    a.rmcut2, a.F, a.T, a.part_f1, st);
+                                    a.rmcut2, a.F, a.T, a.part_f1, st, a.rigid_lab, a.rigid_shape);
             case 2:
                 return y.enqueue_rebuild(st);
             default:

@@ -36,6 +36,7 @@ struct System {
     bool judge_step(int g) const { return arr.sg && arr.sg->judge_every > 0 && g % arr.sg->judge_every == 0; }
     int init();
     int tune_lj();
+    int tune_rigid();
     int capture(bool rebuild, bool phase, bool judge = false);
     void drop_graphs();
     int use_surrogate(fmd_sg* model, int judge_every, double rmse_max);
