@@ -272,8 +272,24 @@ k_rigid_w(const double* __restrict__ pos, const Site<P>* __restrict__ lab, const
         mimg(mx, my, mz, hi, h);
         if (norm2_rn(mx, my, mz) > rmcut2) continue;             // warp-uniform (LJ:320)
         __syncwarp();
-        if (v0) sj[a0] = lab[(size_t)j * natom + a0];
-        if (v1) sj[a1] = lab[(size_t)j * natom + a1];
+        if constexpr (sizeof(P) == 8) {
+            if (v0) sj[a0] = lab[(size_t)j * natom + a0];
+            if (v1) sj[a1] = lab[(size_t)j * natom + a1];
+        } else {
+            // FP32 pairs: j's sites moved by the COM image m in FP64 and rounded
+            // once, so each pair distance is one subtraction; the rounding error
+            // is independent per site (not shared by the whole molecule pair).
+#pragma unroll
+            for (int s = 0; s < 2; s++) {
+                const int b = s ? a1 : a0;
+                if (!(s ? v1 : v0)) continue;
+                const Site<P> q = lab[(size_t)j * natom + b];
+                Site<P> t;
+                t.x = (float)((double)q.x + mx); t.y = (float)((double)q.y + my); t.z = (float)((double)q.z + mz);
+                t.pad = 0.f;
+                sj[b] = t;
+            }
+        }
         __syncwarp();
         // per-neighbour partial sums for sites a0 and a1
         P f[2][3] = {{0, 0, 0}, {0, 0, 0}}, wv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, e = 0;
@@ -303,11 +319,8 @@ k_rigid_w(const double* __restrict__ pos, const Site<P>* __restrict__ lab, const
                 }
             }
         } else {
-            // COM image split into FP32 head + tail so each pair distance keeps
-            // ~1e-7 relative accuracy; the small site difference goes first.
-            const float mxh = (float)mx, myh = (float)my, mzh = (float)mz;
-            const float mxl = (float)(mx - (double)mxh), myl = (float)(my - (double)myh), mzl = (float)(mz - (double)mzh);
             float eterm = 0.f;
+            float wxx = 0.f, wyy = 0.f, wzz = 0.f, wxy = 0.f, wxz = 0.f, wyz = 0.f;
             int npair = 0;
             for (int b = 0; b < natom; b++) {
                 const Site<P> rb = sj[b];
@@ -315,25 +328,25 @@ k_rigid_w(const double* __restrict__ pos, const Site<P>* __restrict__ lab, const
                 for (int s = 0; s < 2; s++) {
                     const Site<P>& ra = s ? r1 : r0;
                     if (!(s ? v1 : v0)) continue;
-                    const float dx = (mxh + (rb.x - ra.x)) + mxl;
-                    const float dy = (myh + (rb.y - ra.y)) + myl;
-                    const float dz = (mzh + (rb.z - ra.z)) + mzl;
-                    float r2 = dx * dx + dy * dy + dz * dz;
+                    const float dx = rb.x - ra.x, dy = rb.y - ra.y, dz = rb.z - ra.z;
+                    float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
                     if (r2 < rcut2f) {
                         r2 = fmaxf(r2, 0.25f);
                         const float ri2 = 1.0f / r2, s2 = fmaf(sig2, ri2, sig2_lo * ri2), s6 = s2 * s2 * s2,
                                     s12 = s6 * s6;
-                        const float fm = c24f * (2.0f * s12 - s6) * ri2;
+                        const float fm = c24f * fmaf(2.0f, s12, -s6) * ri2;
                         const float fx = fm * dx, fy = fm * dy, fz = fm * dz;
                         f[s][0] -= fx; f[s][1] -= fy; f[s][2] -= fz;
-                        eterm += c4f * (s12 - s6);
+                        eterm = fmaf(c4f, s12 - s6, eterm);
                         npair++;
-                        wv[0] += dx * fx; wv[1] += dx * fy; wv[2] += dx * fz;
-                        wv[3] += dy * fx; wv[4] += dy * fy; wv[5] += dy * fz;
-                        wv[6] += dz * fx; wv[7] += dz * fy; wv[8] += dz * fz;
+                        // fm d (x) d is symmetric: six components
+                        wxx = fmaf(dx, fx, wxx); wyy = fmaf(dy, fy, wyy); wzz = fmaf(dz, fz, wzz);
+                        wxy = fmaf(dx, fy, wxy); wxz = fmaf(dx, fz, wxz); wyz = fmaf(dy, fz, wyz);
                     }
                 }
             }
+            wv[0] = wxx; wv[4] = wyy; wv[8] = wzz;
+            wv[1] = wv[3] = wxy; wv[2] = wv[6] = wxz; wv[5] = wv[7] = wyz;
             // energy and virial halved for the symmetric list (LJ:339-341); the
             // shift in FP64 once per neighbour
             e = 0.5f * eterm;
