@@ -23,6 +23,7 @@
 #include "rebo_fn.cuh"
 #include "step.h"
 #include "umma.cuh"
+#include "pdl.cuh"
 
 namespace fmd {
 namespace {
@@ -168,6 +169,7 @@ __global__ void __launch_bounds__(256)
 k_rebo_slots(const double* __restrict__ pos, const double* __restrict__ hh, const int* __restrict__ cnt,
              const int* __restrict__ list, int cap, int na, Slot* __restrict__ sl,
              const int* __restrict__ gate, int want) {
+    FMD_PDL_WAIT();
     if (gate != nullptr && *gate != want) return;
     __shared__ double s_hh[18];
     if (threadIdx.x < 18) s_hh[threadIdx.x] = hh[threadIdx.x];
@@ -272,6 +274,7 @@ __device__ __forceinline__ double three_body_coeff(double gs, double b, double f
 __global__ void __launch_bounds__(256)
 k_rebo_bo(const Slot* __restrict__ sl, const int* __restrict__ cnt, const int* __restrict__ list, int cap, int na,
           SlotBO* __restrict__ bo, const int* __restrict__ gate, int want) {
+    FMD_PDL_WAIT();
     if (gate != nullptr && *gate != want) return;
     const long long tot = (long long)na * cap;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x) {
@@ -334,6 +337,7 @@ __global__ void __launch_bounds__(256)
 k_rebo_force(const Slot* __restrict__ sl, const SlotBO* __restrict__ bo, const int* __restrict__ cnt,
              const int* __restrict__ list, int cap, int na, double* __restrict__ F, double* __restrict__ part,
              const int* __restrict__ gate, int want) {
+    FMD_PDL_WAIT();
     if (gate != nullptr && *gate != want) return;
     __shared__ double sm[32 * kNV];
     double acc[kNV];
@@ -567,6 +571,7 @@ __global__ void __launch_bounds__(NT)
 k_lj_gather(const double* __restrict__ pos, const double* __restrict__ hh, const int* __restrict__ in_cnt,
             const int* __restrict__ in_list, int in_cap, int na, double* __restrict__ F,
             double* __restrict__ Facc, LJP p, double* __restrict__ part) {
+    FMD_PDL_WAIT();
     __shared__ double sm[32 * kNV];
     __shared__ double s_hh[18];
     lj_gather_body<FULL_VIRIAL, F32, U, PIPE>(pos, hh, in_cnt, in_list, in_cap, na, F, Facc, p, part, blockIdx.x,
@@ -688,6 +693,7 @@ __global__ void __launch_bounds__(NT)
 k_lj_gather_staged(const double* __restrict__ pos, const double* __restrict__ hh, const int* __restrict__ in_cnt,
                    const int* __restrict__ in_list, int in_cap, int na, double* __restrict__ F,
                    double* __restrict__ Facc, LJP p, double* __restrict__ part, DevErr* err) {
+    FMD_PDL_WAIT();
     extern __shared__ __align__(128) unsigned char dsm[];
     __shared__ double sm[32 * kNV];
     __shared__ double s_hh[18];
@@ -764,9 +770,16 @@ cudaError_t rebo_slots_launch(const double* pos, const double* hh, const int* cn
                               int want, cudaStream_t st) {
     Slot* sl = reinterpret_cast<Slot*>(slots);
     SlotBO* bo = reinterpret_cast<SlotBO*>(slots + (size_t)na * cap * 8);
-    k_rebo_slots<<<kForceBlocks, 256, 0, st>>>(pos, hh, cnt, list, cap, na, sl, gate, want);
-    k_rebo_bo<<<kForceBlocks, 256, 0, st>>>(sl, cnt, list, cap, na, bo, gate, want);
-    k_rebo_force<<<nblocks, 256, 0, st>>>(sl, bo, cnt, list, cap, na, F, part, gate, want);
+    cudaError_t e;
+    if ((e = launch_pdl(k_rebo_slots, dim3(kForceBlocks), dim3(256), 0, st, pos, hh, cnt, list, cap, na, sl, gate,
+                        want)) != cudaSuccess)
+        return e;
+    if ((e = launch_pdl(k_rebo_bo, dim3(kForceBlocks), dim3(256), 0, st, (const Slot*)sl, cnt, list, cap, na, bo, gate,
+                        want)) != cudaSuccess)
+        return e;
+    if ((e = launch_pdl(k_rebo_force, dim3(nblocks), dim3(256), 0, st, (const Slot*)sl, (const SlotBO*)bo, cnt, list,
+                        cap, na, F, part, gate, want)) != cudaSuccess)
+        return e;
     return cudaGetLastError();
 }
 
@@ -791,8 +804,8 @@ int lj_dispatch(bool launch, const double* pos, const double* hh, const int* cnt
                 double* part, cudaStream_t st) {
     const int nb = std::min(kLJMaxBlocks, lj_occupancy<FV, F32, U, PIPE, NT>() * kSMs);
     if (launch)
-        k_lj_gather<FV, F32, U, PIPE, NT><<<nb, NT, 0, st>>>(pos, hh, in_cnt, in_list, in_cap, na, F, Facc, p,
-                                                             part);
+        launch_pdl(k_lj_gather<FV, F32, U, PIPE, NT>, dim3(nb), dim3(NT), 0, st, pos, hh, in_cnt, in_list, in_cap, na,
+                   F, Facc, p, part);
     return nb;
 }
 
@@ -821,8 +834,8 @@ int lj_dispatch_staged(bool launch, const double* pos, const double* hh, const i
     if (it->second < 1) return 0;
     const int nb = std::min(kLJMaxBlocks, it->second * kSMs);
     if (launch)
-        k_lj_gather_staged<FV, F32, U, NT><<<nb, NT, smem, st>>>(pos, hh, in_cnt, in_list, in_cap, na, F, Facc, p,
-                                                                 part, err);
+        launch_pdl(k_lj_gather_staged<FV, F32, U, NT>, dim3(nb), dim3(NT), smem, st, pos, hh, in_cnt, in_list, in_cap,
+                   na, F, Facc, p, part, err);
     return nb;
 }
 

@@ -24,6 +24,7 @@
 #include "step.h"
 #include "geom.cuh"
 #include "sg_host.h"
+#include "pdl.cuh"
 
 namespace fmd {
 namespace {
@@ -88,6 +89,7 @@ __device__ void begin_body(SysScal* S, int kind, const StepParams& p) {
 namespace {
 
 __global__ void k_begin(SysScal* S, int kind, StepParams p) {
+    FMD_PDL_WAIT();
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     begin_body(S, kind, p);
 }
@@ -180,9 +182,13 @@ __device__ void kick2_body(const StepArrays& a, double dt, int blk, int nblk, do
 
 namespace {
 
-__global__ void __launch_bounds__(kPB) k_kick(StepArrays a, double dt) { kick_body(a, dt, blockIdx.x, gridDim.x); }
+__global__ void __launch_bounds__(kPB) k_kick(StepArrays a, double dt) {
+    FMD_PDL_WAIT();
+    kick_body(a, dt, blockIdx.x, gridDim.x);
+}
 
 __global__ void __launch_bounds__(kPB) k_kick2(StepArrays a, double dt) {
+    FMD_PDL_WAIT();
     __shared__ double sm[32 * 2];
     kick2_body(a, dt, blockIdx.x, gridDim.x, sm);
 }
@@ -234,6 +240,7 @@ __device__ void rescale_body(const StepArrays& a, int blk, int nblk, double* sm)
 namespace {
 
 __global__ void __launch_bounds__(kPB) k_rescale(StepArrays a) {
+    FMD_PDL_WAIT();
     __shared__ double sm[32 * 2];
     rescale_body(a, blockIdx.x, gridDim.x, sm);
 }
@@ -383,11 +390,13 @@ __device__ void rescale_end_body(const StepArrays& a, const StepParams& p, int n
 namespace {
 
 __global__ void __launch_bounds__(kRedThreads) k_end(StepArrays a, StepParams p, int nblk_f1, int nblk_ke) {
+    FMD_PDL_WAIT();
     __shared__ double sm[32 * kRedFields];
     end_body(a, p, nblk_f1, nblk_ke, a.lj_blocks, sm);
 }
 
 __global__ void __launch_bounds__(kRedThreads) k_rescale_end(StepArrays a, StepParams p, int nblk_ke) {
+    FMD_PDL_WAIT();
     __shared__ double sm[32 * kRedFields];
     rescale_end_body(a, p, nblk_ke, sm);
 }
@@ -488,14 +497,19 @@ cudaError_t enqueue_ke(const StepArrays& a, cudaStream_t st) {
 cudaError_t enqueue_step(const StepArrays& a, const StepParams& p, bool rescale_phase, cudaStream_t st,
                          bool judge) {
     cudaError_t e;
-    k_begin<<<1, 32, 0, st>>>(a.S, a.kind, p);
-    k_kick<<<kForceBlocks, kPB, 0, st>>>(a, p.dt);
+    // programmatic dependent launches: each kernel's launch overlaps the
+    // previous one's tail (pdl.cuh)
+    if ((e = launch_pdl(k_begin, dim3(1), dim3(32), 0, st, a.S, a.kind, p)) != cudaSuccess) return e;
+    if ((e = launch_pdl(k_kick, dim3(kForceBlocks), dim3(kPB), 0, st, a, p.dt)) != cudaSuccess) return e;
     if ((e = enqueue_forces(a, st, judge)) != cudaSuccess) return e;
-    k_kick2<<<kForceBlocks, kPB, 0, st>>>(a, p.dt);
-    k_end<<<1, kRedThreads, 0, st>>>(a, p, force_partial_blocks(a), kForceBlocks);
+    if ((e = launch_pdl(k_kick2, dim3(kForceBlocks), dim3(kPB), 0, st, a, p.dt)) != cudaSuccess) return e;
+    if ((e = launch_pdl(k_end, dim3(1), dim3(kRedThreads), 0, st, a, p, force_partial_blocks(a), kForceBlocks)) !=
+        cudaSuccess)
+        return e;
     if (rescale_phase && p.schedule) {
-        k_rescale<<<kForceBlocks, kPB, 0, st>>>(a);
-        k_rescale_end<<<1, kRedThreads, 0, st>>>(a, p, kForceBlocks);
+        if ((e = launch_pdl(k_rescale, dim3(kForceBlocks), dim3(kPB), 0, st, a)) != cudaSuccess) return e;
+        if ((e = launch_pdl(k_rescale_end, dim3(1), dim3(kRedThreads), 0, st, a, p, kForceBlocks)) != cudaSuccess)
+            return e;
     }
     return cudaGetLastError();
 }
