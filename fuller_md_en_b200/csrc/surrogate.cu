@@ -30,22 +30,45 @@ namespace {
 using namespace rebo;
 using namespace dev;
 
-__global__ void k_sg_count(const double* __restrict__ pos, const double* __restrict__ hh,
-                           const int* __restrict__ cnt, const int* __restrict__ list, int cap, int na,
-                           int* __restrict__ acnt, const int* __restrict__ gate) {
+// Rows of each atom (bonds kept by the row rule), and their exclusive scan
+// within each block of 256 atoms (block totals in bsum); one atom per thread.
+constexpr int kScanBlock = 256;
+
+__global__ void __launch_bounds__(kScanBlock)
+k_sg_count(const double* __restrict__ pos, const double* __restrict__ hh, const int* __restrict__ cnt,
+           const int* __restrict__ list, int cap, int na, int* __restrict__ acnt, const int* __restrict__ gate,
+           int* __restrict__ aoff, int* __restrict__ bsum) {
+    __shared__ int wsum[kScanBlock / 32];
     double h[9], hi[9];
     load_cell(hh, h, hi);
     // A set gate (the plain kernel has taken over) leaves every atom without rows.
     const bool off = gate != nullptr && *gate != 0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < na; i += gridDim.x * blockDim.x) {
-        int c = 0;
-        for (int jn = 0; jn < (off ? 0 : cnt[i]); jn++) {
+    const int i = blockIdx.x * kScanBlock + threadIdx.x;
+    int c = 0;
+    if (i < na && !off) {
+        for (int jn = 0; jn < cnt[i]; jn++) {
             double x, y, z;
             bond_vec(pos, i, list[(size_t)i * cap + jn], h, hi, x, y, z);
             c += bond_kept(sqrt(norm2_rn(x, y, z)));
         }
-        acnt[i] = c;
     }
+    if (i < na) acnt[i] = c;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) wsum[wid] = incl;
+    __syncthreads();
+    int before = 0, total = 0;
+    for (int k = 0; k < kScanBlock / 32; k++) {
+        if (k < wid) before += wsum[k];
+        total += wsum[k];
+    }
+    if (i < na) aoff[i] = before + incl - c;          // block-local exclusive offset
+    if (threadIdx.x == 0) bsum[blockIdx.x] = total;
 }
 
 // Exclusive scan of acnt[0..na) into aoff[0..na]; one block of 1024 threads.
@@ -73,13 +96,20 @@ __global__ void __launch_bounds__(1024) k_sg_scan(const int* __restrict__ acnt, 
 
 __global__ void k_sg_rows(const double* __restrict__ pos, const double* __restrict__ hh,
                           const int* __restrict__ cnt, const int* __restrict__ list, int cap, int na,
-                          const int* __restrict__ aoff, int* __restrict__ row_i, int* __restrict__ row_s,
-                          int* __restrict__ rowid, const int* __restrict__ gate) {
+                          int* __restrict__ aoff, int* __restrict__ row_i, int* __restrict__ row_s,
+                          int* __restrict__ rowid, const int* __restrict__ gate, const int* __restrict__ boff) {
+    // global offsets: block-local offset + the block's scanned total
+    const int i = blockIdx.x * kScanBlock + threadIdx.x;
+    const int nblk = (na + kScanBlock - 1) / kScanBlock;
+    if (i == 0) aoff[na] = boff[nblk];
+    if (i >= na) return;
+    const int r0 = aoff[i] + boff[blockIdx.x];
+    aoff[i] = r0;
     if (gate != nullptr && *gate != 0) return;
     double h[9], hi[9];
     load_cell(hh, h, hi);
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < na; i += gridDim.x * blockDim.x) {
-        int r = aoff[i];
+    {
+        int r = r0;
         for (int jn = 0; jn < cap; jn++) {
             int id = -1;
             if (jn < cnt[i]) {
@@ -161,22 +191,26 @@ __global__ void k_sg_desc(const double* __restrict__ pos, const double* __restri
 }
 
 // ------------------------------------------------------------------ network
-constexpr int kMlpThreads = 256;
+// 16 warps: four per TMEM lane quadrant, each owning 32 of the 128 columns,
+// so the epilogues (TMEM -> SiLU -> BF16 tile) run on 512 threads.
+constexpr int kMlpThreads = 512;
+constexpr int kColGroups = kMlpThreads / 128;      // column groups per row
+constexpr int kColsPerThread = H / kColGroups;      // 32
 // dynamic shared memory map (bytes)
 constexpr int SM_W1 = 0, SM_W2 = SM_W1 + H * D * 2, SM_W3 = SM_W2 + H * H * 2, SM_X = SM_W3 + H * H * 2,
               SM_ACT = SM_X + TILE * D * 2, SM_W4 = SM_ACT + TILE * H * 2, SM_RED = SM_W4 + H * 4,
-              SM_TOTAL = SM_RED + 2 * TILE * 4;
+              SM_TOTAL = SM_RED + kColGroups * TILE * 4;
 // TMEM columns
 constexpr uint32_t TM_Z1 = 0, TM_Z2 = 128, TM_Z3 = 256, TM_T = 384;
 
 // Epilogue writing one 128 x 128 BF16 operand tile from TMEM: each thread
-// owns row q and 64 columns [c0, c0+64).  kind 0: h = SiLU(z), column 127
+// owns row q and kColsPerThread columns from c0.  kind 0: h = SiLU(z), column 127
 // held at 1.  kind 1: g = t * SiLU'(z) (z from a second TMEM region),
 // column 127 held at 0.
 template <int KIND>
 __device__ __forceinline__ void epi_tile(uint32_t ta, uint32_t tz, unsigned char* act, int q, int c0) {
 #pragma unroll 1
-    for (int cc = 0; cc < 64; cc += 16) {
+    for (int cc = 0; cc < kColsPerThread; cc += 16) {
         float v[16];
         umma::tmem_ld16(ta + c0 + cc, v);
         if (KIND == 1) {
@@ -212,7 +246,7 @@ k_sg_mlp(const uint16_t* __restrict__ img, const float* __restrict__ vec, const 
     __shared__ uint32_t tbase;
     const int t = threadIdx.x, w = t >> 5, lane = t & 31;
     const int q = 32 * (w & 3) + lane;          // tile row owned by this thread
-    const int c0 = 64 * (w >> 2);               // first of its 64 columns
+    const int c0 = kColsPerThread * (w >> 2);   // first of its columns
     const int R = *nrows;
     const int ntiles = (R + TILE - 1) / TILE;
     if ((int)blockIdx.x >= ntiles) return;      // uniform per block; nothing allocated yet
@@ -271,7 +305,7 @@ k_sg_mlp(const uint16_t* __restrict__ img, const float* __restrict__ vec, const 
         {   // output layer and g3 = bs * w4 * SiLU'(z3)
             float y = 0.f;
 #pragma unroll 1
-            for (int cc = 0; cc < 64; cc += 16) {
+            for (int cc = 0; cc < kColsPerThread; cc += 16) {
                 float z[16];
                 umma::tmem_ld16(tl + TM_Z3 + c0 + cc, z);
                 float g[16];
@@ -298,7 +332,12 @@ k_sg_mlp(const uint16_t* __restrict__ img, const float* __restrict__ vec, const 
         to_mma();
         {
             const int row = tile * TILE + q;
-            if (c0 == 0 && row < R) bout[row] = b0 + bs * (red[q] + red[TILE + q]);
+            if (c0 == 0 && row < R) {
+                float y = 0.f;
+#pragma unroll
+                for (int g = 0; g < kColGroups; g++) y += red[g * TILE + q];
+                bout[row] = b0 + bs * y;
+            }
         }
         if (t == 0) issue(tm + TM_T, sA, H, false, sW3, H, true, H, H / 16, &mbar);   // t2 = g3 W3^T
         SG_WAIT();
@@ -310,7 +349,7 @@ k_sg_mlp(const uint16_t* __restrict__ img, const float* __restrict__ vec, const 
         to_mma();
         if (t == 0) issue(tm + TM_T, sA, H, false, sW1, D, true, D, H / 16, &mbar);   // gx = g1 W1^T
         SG_WAIT();
-        {
+        if ((w >> 2) < D / 16) {                // gx has D = 32 columns: two groups of 16
             const int row = tile * TILE + q;
             const int cg = 16 * (w >> 2);
             float v[16];
@@ -483,6 +522,8 @@ cudaError_t work_alloc(Work& w, int na, int cap) {
     A((void**)&w.gx, sizeof(float) * (size_t)rcap * D);
     A((void**)&w.part, sizeof(double) * (size_t)kRowBlocks * kNV);
     A((void**)&w.err, sizeof(int) * 4);
+    A((void**)&w.bsum, sizeof(int) * ((size_t)na / 256 + 2));
+    A((void**)&w.boff, sizeof(int) * ((size_t)na / 256 + 3));
     if (e == cudaSuccess) e = cudaMemset(w.err, 0, sizeof(int) * 4);
     if (e != cudaSuccess) {
         work_free(w);
@@ -497,6 +538,7 @@ cudaError_t work_alloc(Work& w, int na, int cap) {
 void work_free(Work& w) {
     cudaFree(w.acnt); cudaFree(w.aoff); cudaFree(w.row_i); cudaFree(w.row_s); cudaFree(w.rowid);
     cudaFree(w.partner); cudaFree(w.X); cudaFree(w.b); cudaFree(w.gx); cudaFree(w.part); cudaFree(w.err);
+    cudaFree(w.bsum); cudaFree(w.boff);
     w = Work{};
 }
 
@@ -509,10 +551,10 @@ cudaError_t build_rows(Work& w, const float* vec, const double* pos, const doubl
                        const int* list, int cap, int na, cudaStream_t st, const int* gate) {
     if (na > w.na_cap || cap != w.cap) return cudaErrorInvalidValue;
     w.na_used = na;
-    const int nb = (na + 255) / 256;
-    k_sg_count<<<nb, 256, 0, st>>>(pos, hh, cnt, list, cap, na, w.acnt, gate);
-    k_sg_scan<<<1, 1024, 0, st>>>(w.acnt, na, w.aoff);
-    k_sg_rows<<<nb, 256, 0, st>>>(pos, hh, cnt, list, cap, na, w.aoff, w.row_i, w.row_s, w.rowid, gate);
+    const int nb = (na + kScanBlock - 1) / kScanBlock;
+    k_sg_count<<<nb, kScanBlock, 0, st>>>(pos, hh, cnt, list, cap, na, w.acnt, gate, w.aoff, w.bsum);
+    k_sg_scan<<<1, 1024, 0, st>>>(w.bsum, nb, w.boff);
+    k_sg_rows<<<nb, kScanBlock, 0, st>>>(pos, hh, cnt, list, cap, na, w.aoff, w.row_i, w.row_s, w.rowid, gate, w.boff);
     k_sg_desc<<<kRowBlocks, 128, 0, st>>>(pos, hh, cnt, list, cap, na, w.aoff, w.row_i, w.row_s, w.rowid, vec,
                                           w.r_cap, w.X, w.partner, w.err);
     return cudaGetLastError();

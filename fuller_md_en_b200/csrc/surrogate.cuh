@@ -49,6 +49,8 @@ struct Work {
     float* gx = nullptr;      // [r_cap * D] db/dx_n
     double* part = nullptr;   // per-block {E, W9}
     int* err = nullptr;       // [4] kernel status words
+    int* bsum = nullptr;      // [na / 256 + 1] rows per block of 256 atoms
+    int* boff = nullptr;      // [na / 256 + 2] their exclusive scan
 };
 
 cudaError_t work_alloc(Work& w, int na, int cap);
