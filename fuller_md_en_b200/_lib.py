@@ -7,7 +7,7 @@ usable, every call raises.
 from __future__ import annotations
 
 import ctypes
-from ctypes import POINTER, c_char_p, c_double, c_float, c_int, c_void_p
+from ctypes import POINTER, c_char_p, c_double, c_float, c_int, c_longlong, c_void_p
 from pathlib import Path
 
 LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libfullermd_cuda.so"
@@ -124,6 +124,9 @@ _SIGS = {
     "fmd_system_step_kernels": (c_int, [c_void_p, c_int, c_int, POINTER(c_int)]),
     "fmd_system_lj_shape": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int), POINTER(c_int), POINTER(c_int)]),
     "fmd_system_set_lj_shape": (c_int, [c_void_p, c_int, c_int, c_int]),
+    "fmd_system_set_lj_prune": (c_int, [c_void_p, c_double]),
+    "fmd_system_forces": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "fmd_system_lj_prune": (c_int, [c_void_p, POINTER(c_double), POINTER(c_longlong), POINTER(c_longlong)]),
     "fmd_umma_selftest": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, POINTER(c_float)]),
     "fmd_sg_nparams": (c_int, []),
     "fmd_sg_create": (c_int, [c_void_p, _dp, POINTER(c_void_p)]),

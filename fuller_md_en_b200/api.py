@@ -10,6 +10,7 @@ MM = src/fuller_LJ_npt_mmmd_serial_omp_acc.cpp.
 from __future__ import annotations
 
 import ctypes
+import weakref
 from dataclasses import dataclass
 from typing import Optional
 
@@ -67,6 +68,12 @@ class Context:
             raise FmdError(rc, f"fmd_ctx_create(device={device}) failed: "
                            f"{self.lib.fmd_status_string(rc).decode()}")
         self.h = h
+        self._owned = []          # weak references to handles made on this context
+
+    def adopt(self, obj) -> None:
+        """Registers a handle (system, batch, model, dataset) that must be
+        released before the context itself."""
+        self._owned.append(weakref.ref(obj))
 
     def check(self, rc: int, what: str) -> None:
         if rc != 0:
@@ -89,6 +96,13 @@ class Context:
 
     def close(self) -> None:
         if self.h:
+            # handles made on this context go first, newest first (a batch
+            # before its systems); they hold the context's stream
+            for r in reversed(self._owned):
+                o = r()
+                if o is not None:
+                    o.close()
+            self._owned.clear()
             self.lib.fmd_ctx_destroy(self.h)
             self.h = None
 
@@ -323,6 +337,7 @@ class System:
 
     def __init__(self, ctx: Context, handle: ctypes.c_void_p, n: int, kind: int):
         self.ctx, self.h, self.n, self.kind = ctx, handle, n, kind
+        ctx.adopt(self)
 
     @classmethod
     def airebo(cls, ctx: Context, cfg: RunConfig, pos, vel, mass, mol_id, h, npt) -> "System":
@@ -389,6 +404,15 @@ class System:
                                                         ctypes.byref(npt)), "fmd_system_download")
         return {"pos": pos, "vel": vel, "qv": qv, "omg": omg, "h": h, "npt": npt_to_array(npt)}
 
+    def forces(self):
+        """(F of the last force evaluation, torques or None, energies E[8])."""
+        n = self.n
+        F, E = np.zeros(3 * n), np.zeros(8)
+        T = np.zeros(3 * n) if self.kind == _lib.FMD_SYS_RIGID else None
+        self.ctx.check(self.ctx.lib.fmd_system_forces(self.h, _d(F), _d(T) if T is not None else None, _d(E)),
+                       "fmd_system_forces")
+        return F, T, E
+
     def lists(self, cap_a: int, cap_b: int = 0):
         n = self.n
         ca, la = np.zeros(n, np.int32), np.zeros(n * cap_a, np.int32)
@@ -426,6 +450,20 @@ class System:
     def set_lj_shape(self, threads: int, unroll: int, feed: int) -> None:
         """Pins the LJ gather's launch shape (feed 0 plain, 1 pipelined, 2 staged rows)."""
         self.ctx.check(self.ctx.lib.fmd_system_set_lj_shape(self.h, threads, unroll, feed), "fmd_system_set_lj_shape")
+
+    def set_lj_prune(self, delta: float) -> None:
+        """Buffer (A) of the pruned LJ gather rows beyond the cutoff; 0 turns
+        pruning off (the full rows every step).  Default 0.5."""
+        self.ctx.check(self.ctx.lib.fmd_system_set_lj_prune(self.h, float(delta)), "fmd_system_set_lj_prune")
+
+    def lj_prune(self) -> dict:
+        """{'delta', 'evaluations': force evaluations since set-up, 'prunes':
+        those that walked the full rows and pruned them}."""
+        d = ctypes.c_double(0)
+        n = [ctypes.c_longlong(0), ctypes.c_longlong(0)]
+        self.ctx.check(self.ctx.lib.fmd_system_lj_prune(self.h, ctypes.byref(d), ctypes.byref(n[0]),
+                                                        ctypes.byref(n[1])), "fmd_system_lj_prune")
+        return {"delta": d.value, "evaluations": n[0].value, "prunes": n[1].value}
 
     def use_surrogate(self, model, judge_every: int = 100, rmse_max: float = 0.025) -> None:
         """Learned REBO term from `model` (a surrogate.Surrogate, or None for
@@ -469,6 +507,7 @@ class Batch:
         ctx.check(ctx.lib.fmd_batch_create(ctx.h, len(self.systems), arr, int(autotune), ctypes.byref(out)),
                   "fmd_batch_create")
         self.h = out
+        ctx.adopt(self)
 
     def enqueue(self, first: int, last: int) -> None:
         self.ctx.check(self.ctx.lib.fmd_batch_enqueue(self.h, first, last), "fmd_batch_enqueue")

@@ -20,6 +20,7 @@
 #include <map>
 #include "kernels.h"
 #include "geom.cuh"
+#include "ljpair.cuh"
 #include "rebo_fn.cuh"
 #include "step.h"
 #include "umma.cuh"
@@ -382,99 +383,7 @@ k_rebo_force(const Slot* __restrict__ sl, const SlotBO* __restrict__ bo, const i
     block_sum_store<kNV>(acc, sm, part + (size_t)blockIdx.x * kNV);
 }
 
-struct LJP {
-    double sig2, c4, c24, rc2, vshift;
-};
-
-// Reference constants, computed with the reference's expressions.
-__host__ __device__ LJP lj_params_dev(int ff) {
-    LJP p;
-    if (ff == FMD_FF_AIREBO) {  // AI:119-124
-        const double sig = 3.40, eps = 2.84e-3, rc = 3.0 * sig;
-        const double sr = sig / rc, sr2 = sr * sr, sr6 = sr2 * sr2 * sr2;
-        p.sig2 = sig * sig; p.c4 = 4 * eps; p.c24 = 24 * eps; p.rc2 = rc * rc;
-        p.vshift = 4 * eps * (sr6 * sr6 - sr6);
-    } else {                    // MM:113-116
-        const double sig = 3.431, eps = 2.635e-3, rc = 3.0 * sig;
-        const double sr = 1.0 / 3.0, sr2 = sr * sr, sr6 = sr2 * sr2 * sr2;
-        p.sig2 = sig * sig; p.c4 = 4 * eps; p.c24 = 24 * eps; p.rc2 = rc * rc;
-        p.vshift = 4.0 * eps * (sr6 * sr6 - sr6);
-    }
-    return p;
-}
 LJP lj_params(int ff) { return lj_params_dev(ff); }
-
-// One component of the minimum image for a diagonal cell.  With zero
-// off-diagonals the reference's s = hi0*dx + hi1*dy + hi2*dz and
-// d = h0*s0 + h1*s1 + h2*s2 reduce exactly to these products (adding +-0
-// changes nothing), so this is bitwise the reference's mimg.
-// For |s| < 1.5 (always so for wrapped positions) round(s), half away from
-// zero, is one of -1, 0, 1 and two comparisons give it exactly.
-__device__ __forceinline__ double mimg1(double d, double hii, double hii_inv) {
-    double s = __dmul_rn(hii_inv, d);
-    double r = s >= 0.5 ? 1.0 : (s <= -0.5 ? -1.0 : 0.0);
-    if (!(fabs(s) < 1.5)) r = round(s);
-    s = __dsub_rn(s, r);
-    return __dmul_rn(hii, s);
-}
-
-// 1/x for x in the FP32 normal range: the FP32 hardware reciprocal (relative
-// error ~2^-23) refined by one Newton-Raphson step y + y (1 - x y), which
-// squares the error (~1e-14), in place of a full IEEE division.
-__device__ __forceinline__ double rcp_nr(double x) {
-    float yf;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"((float)x));
-    const double y = (double)yf;
-    return fma(y, fma(-x, y, 1.0), y);
-}
-
-// FP32 copies of the pair constants (FP32-pair precision).  sigma^2 is kept
-// as a head + tail pair: its FP32 rounding would scale every s^6 by the same
-// factor, a bias that the near-cancelling repulsive and attractive virial
-// sums amplify about tenfold; c4 and c24 scale both parts alike and stay single.
-struct LJF {
-    float sig2, sig2_lo, c4, c24;
-};
-
-// One listed pair seen from atom i: d = r_j - r_i after the minimum image.
-// The cutoff test is the reference's FP64 one in both precisions, so both
-// modes interact through exactly the reference's pair set.  FP64: the
-// reference's arithmetic (AI:447-466).  FP32: the pair algebra (1/r^2, s^6,
-// s^12, fm) in FP32; the minimum image, r^2, the force, energy and virial
-// accumulation stay FP64.  COUNT: this side counts energy and virial.
-template <bool FULL_VIRIAL, bool F32, bool COUNT>
-__device__ __forceinline__ void lj_pair(double dx, double dy, double dz, const LJP& p, const LJF& pf,
-                                        double& fx, double& fy, double& fz, double* acc) {
-    double r2 = norm2_rn(dx, dy, dz);
-    if (r2 > p.rc2) return;
-    if (r2 < 0.25) r2 = 0.25;
-    double fm, e = 0.0;
-    if (F32) {
-        const float ri2 = __frcp_rn((float)r2);
-        const float s2 = fmaf(pf.sig2, ri2, pf.sig2_lo * ri2), s6 = s2 * s2 * s2, s12 = s6 * s6;
-        fm = (double)(pf.c24 * (2.f * s12 - s6) * ri2);
-        if (COUNT) e = (double)(pf.c4 * (s12 - s6)) - p.vshift;
-    } else {
-        const double ri2 = rcp_nr(r2), s2 = p.sig2 * ri2, s6 = s2 * s2 * s2, s12 = s6 * s6;
-        fm = p.c24 * (2 * s12 - s6) * ri2;
-        if (COUNT) e = p.c4 * (s12 - s6) - p.vshift;
-    }
-    fx -= fm * dx; fy -= fm * dy; fz -= fm * dz;
-    if (COUNT) {
-        acc[0] += e;
-        if (FULL_VIRIAL) {
-            const double d[3] = {dx, dy, dz};
-#pragma unroll
-            for (int a = 0; a < 3; a++)
-#pragma unroll
-                for (int b = 0; b < 3; b++) acc[1 + a * 3 + b] += d[a] * fm * d[b];
-        } else {
-            acc[1] += dx * fm * dx;
-            acc[5] += dy * fm * dy;
-            acc[9] += dz * fm * dz;
-        }
-    }
-}
 
 // Entries per lane in flight (U): the index loads of U entries are issued
 // together, then their positions, then the pair arithmetic, so one warp has
@@ -498,6 +407,63 @@ __device__ __forceinline__ void lj_fetch(const double* __restrict__ pos, const i
     }
 }
 
+// Pair terms of one chunk (U entries per lane; jc < 0: none) seen from atom i.
+// A pruning gather (po.cnt set) also appends the chunk's entries with
+// r^2 <= po.r2 to prow in row order (entry b0 + 32 u + lane, u then lane
+// ascending); every lane of the warp must call this.
+template <bool FULL_VIRIAL, bool F32, int U>
+__device__ __forceinline__ void lj_chunk(const int (&jc)[U], const double (&cx)[U], const double (&cy)[U],
+                                         const double (&cz)[U], int i, double px, double py, double pz,
+                                         const double* h, const double* hi, bool diag, const LJP& p, const LJF& pf,
+                                         double& fx, double& fy, double& fz, double* acc, const LJPruneOut& po,
+                                         int* __restrict__ prow, int& pc, int lane) {
+    bool keep[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+        keep[u] = false;
+        if (jc[u] < 0) continue;
+        double dx = __dsub_rn(cx[u], px), dy = __dsub_rn(cy[u], py), dz = __dsub_rn(cz[u], pz);
+        if (diag) {
+            dx = mimg1(dx, h[0], hi[0]);
+            dy = mimg1(dy, h[4], hi[4]);
+            dz = mimg1(dz, h[8], hi[8]);
+        } else {
+            mimg(dx, dy, dz, hi, h);
+        }
+        if (po.cnt) keep[u] = norm2_rn(dx, dy, dz) <= po.r2;
+        if (jc[u] > i) lj_pair<FULL_VIRIAL, F32, true>(dx, dy, dz, p, pf, fx, fy, fz, acc);
+        else lj_pair<FULL_VIRIAL, F32, false>(dx, dy, dz, p, pf, fx, fy, fz, acc);
+    }
+    if (po.cnt) {
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const unsigned m = __ballot_sync(kFull, keep[u]);
+            if (keep[u]) prow[pc + __popc(m & ((1u << lane) - 1u))] = jc[u];
+            pc += __popc(m);
+        }
+    }
+}
+
+// End of atom i's row: F[i] = Facc[i] + the warp's sum (Facc cleared), and for
+// a pruning gather the pruned row's length and i's fractional position.
+__device__ __forceinline__ void lj_atom_done(int i, double fx, double fy, double fz, double px, double py,
+                                             double pz, const double* hi, double* __restrict__ F,
+                                             double* __restrict__ Facc, const LJPruneOut& po, int pc, int lane) {
+    fx = warp_sum(fx); fy = warp_sum(fy); fz = warp_sum(fz);
+    if (lane == 0) {
+        F[3 * i] = Facc[3 * i] + fx;
+        F[3 * i + 1] = Facc[3 * i + 1] + fy;
+        F[3 * i + 2] = Facc[3 * i + 2] + fz;
+        if (Facc != F) { Facc[3 * i] = 0.0; Facc[3 * i + 1] = 0.0; Facc[3 * i + 2] = 0.0; }
+        if (po.cnt) {
+            po.cnt[i] = pc;
+            po.sb[3 * i] = hi[0] * px + hi[1] * py + hi[2] * pz;
+            po.sb[3 * i + 1] = hi[3] * px + hi[4] * py + hi[5] * pz;
+            po.sb[3 * i + 2] = hi[6] * px + hi[7] * py + hi[8] * pz;
+        }
+    }
+}
+
 // One gather pass over atoms blk, blk + nblk, ... (in warps) of one system;
 // per-block {E, W9} into part[blk].  sm: 32 * kNV doubles, s_hh: 18.
 // Row i of the full list (in_list, stride in_cap, in_cnt[i] entries) is the
@@ -509,7 +475,8 @@ __device__ __forceinline__ void lj_gather_body(const double* __restrict__ pos, c
                                                const int* __restrict__ in_cnt, const int* __restrict__ in_list,
                                                int in_cap, int na, double* __restrict__ F,
                                                double* __restrict__ Facc, const LJP& p, double* __restrict__ part,
-                                               int blk, int nblk, double* sm, double* s_hh) {
+                                               int blk, int nblk, double* sm, double* s_hh,
+                                               const LJPruneOut& po) {
     if (threadIdx.x < 18) s_hh[threadIdx.x] = hh[threadIdx.x];
     __syncthreads();
     const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
@@ -527,41 +494,25 @@ __device__ __forceinline__ void lj_gather_body(const double* __restrict__ pos, c
         double fx = 0.0, fy = 0.0, fz = 0.0;
         const int tot = min(in_cnt[i], in_cap);
         const int* row = in_list + (size_t)i * in_cap;
+        int* prow = po.cnt ? po.list + (size_t)i * in_cap : nullptr;
+        int pc = 0;
         int jj[U];
         double qx[U], qy[U], qz[U];
-        if (PIPE && lane < tot) lj_fetch<U>(pos, row, tot, lane, i, jj, qx, qy, qz);
-        for (int b = lane; b < tot; b += 32 * U) {
+        if (PIPE && tot > 0) lj_fetch<U>(pos, row, tot, lane, i, jj, qx, qy, qz);
+        for (int b0 = 0; b0 < tot; b0 += 32 * U) {       // uniform over the warp
             int jc[U];
             double cx[U], cy[U], cz[U];
             if (PIPE) {
 #pragma unroll
                 for (int u = 0; u < U; u++) { jc[u] = jj[u]; cx[u] = qx[u]; cy[u] = qy[u]; cz[u] = qz[u]; }
-                if (b + 32 * U < tot) lj_fetch<U>(pos, row, tot, b + 32 * U, i, jj, qx, qy, qz);
+                if (b0 + 32 * U < tot) lj_fetch<U>(pos, row, tot, b0 + 32 * U + lane, i, jj, qx, qy, qz);
             } else {
-                lj_fetch<U>(pos, row, tot, b, i, jc, cx, cy, cz);
+                lj_fetch<U>(pos, row, tot, b0 + lane, i, jc, cx, cy, cz);
             }
-#pragma unroll
-            for (int u = 0; u < U; u++) {
-                if (jc[u] < 0) continue;
-                double dx = __dsub_rn(cx[u], px), dy = __dsub_rn(cy[u], py), dz = __dsub_rn(cz[u], pz);
-                if (diag) {
-                    dx = mimg1(dx, h[0], hi[0]);
-                    dy = mimg1(dy, h[4], hi[4]);
-                    dz = mimg1(dz, h[8], hi[8]);
-                } else {
-                    mimg(dx, dy, dz, hi, h);
-                }
-                if (jc[u] > i) lj_pair<FULL_VIRIAL, F32, true>(dx, dy, dz, p, pf, fx, fy, fz, acc);
-                else lj_pair<FULL_VIRIAL, F32, false>(dx, dy, dz, p, pf, fx, fy, fz, acc);
-            }
+            lj_chunk<FULL_VIRIAL, F32, U>(jc, cx, cy, cz, i, px, py, pz, h, hi, diag, p, pf, fx, fy, fz, acc, po,
+                                          prow, pc, lane);
         }
-        fx = warp_sum(fx); fy = warp_sum(fy); fz = warp_sum(fz);
-        if (lane == 0) {
-            F[3 * i] = Facc[3 * i] + fx;
-            F[3 * i + 1] = Facc[3 * i + 1] + fy;
-            F[3 * i + 2] = Facc[3 * i + 2] + fz;
-            if (Facc != F) { Facc[3 * i] = 0.0; Facc[3 * i + 1] = 0.0; Facc[3 * i + 2] = 0.0; }
-        }
+        lj_atom_done(i, fx, fy, fz, px, py, pz, hi, F, Facc, po, pc, lane);
     }
     block_sum_store<kNV>(acc, sm, part + (size_t)blk * kNV);
 }
@@ -570,12 +521,14 @@ template <bool FULL_VIRIAL, bool F32, int U, bool PIPE, int NT>
 __global__ void __launch_bounds__(NT)
 k_lj_gather(const double* __restrict__ pos, const double* __restrict__ hh, const int* __restrict__ in_cnt,
             const int* __restrict__ in_list, int in_cap, int na, double* __restrict__ F,
-            double* __restrict__ Facc, LJP p, double* __restrict__ part) {
+            double* __restrict__ Facc, LJP p, double* __restrict__ part, const int* __restrict__ gate, int want,
+            LJPruneOut po) {
     FMD_PDL_WAIT();
+    if (gate && *gate != want) return;
     __shared__ double sm[32 * kNV];
     __shared__ double s_hh[18];
     lj_gather_body<FULL_VIRIAL, F32, U, PIPE>(pos, hh, in_cnt, in_list, in_cap, na, F, Facc, p, part, blockIdx.x,
-                                              gridDim.x, sm, s_hh);
+                                              gridDim.x, sm, s_hh, po);
 }
 
 // Row-staged gather: each warp copies its next atom's full row into a
@@ -600,7 +553,8 @@ __device__ __forceinline__ void lj_gather_staged_body(const double* __restrict__
                                                       int in_cap, int na, double* __restrict__ F,
                                                       double* __restrict__ Facc, const LJP& p,
                                                       double* __restrict__ part, DevErr* err, int blk, int nblk,
-                                                      unsigned char* dsm, double* sm, double* s_hh) {
+                                                      unsigned char* dsm, double* sm, double* s_hh,
+                                                      const LJPruneOut& po) {
     constexpr int W = NT / 32;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     int* bufs = reinterpret_cast<int*>(dsm) + (size_t)w * 2 * in_cap;
@@ -647,7 +601,10 @@ __device__ __forceinline__ void lj_gather_staged_body(const double* __restrict__
         const int tot = min(in_cnt[i], in_cap);
         const double px = pos[3 * i], py = pos[3 * i + 1], pz = pos[3 * i + 2];
         double fx = 0.0, fy = 0.0, fz = 0.0;
-        for (int b = lane; b < tot; b += 32 * U) {
+        int* prow = po.cnt ? po.list + (size_t)i * in_cap : nullptr;
+        int pc = 0;
+        for (int b0 = 0; b0 < tot; b0 += 32 * U) {       // uniform over the warp
+            const int b = b0 + lane;
             int jc[U];
             double cx[U], cy[U], cz[U];
 #pragma unroll
@@ -657,28 +614,10 @@ __device__ __forceinline__ void lj_gather_staged_body(const double* __restrict__
                 const int j = jc[u] < 0 ? i : jc[u];
                 cx[u] = pos[3 * j]; cy[u] = pos[3 * j + 1]; cz[u] = pos[3 * j + 2];
             }
-#pragma unroll
-            for (int u = 0; u < U; u++) {
-                if (jc[u] < 0) continue;
-                double dx = __dsub_rn(cx[u], px), dy = __dsub_rn(cy[u], py), dz = __dsub_rn(cz[u], pz);
-                if (diag) {
-                    dx = mimg1(dx, h[0], hi[0]);
-                    dy = mimg1(dy, h[4], hi[4]);
-                    dz = mimg1(dz, h[8], hi[8]);
-                } else {
-                    mimg(dx, dy, dz, hi, h);
-                }
-                if (jc[u] > i) lj_pair<FULL_VIRIAL, F32, true>(dx, dy, dz, p, pf, fx, fy, fz, acc);
-                else lj_pair<FULL_VIRIAL, F32, false>(dx, dy, dz, p, pf, fx, fy, fz, acc);
-            }
+            lj_chunk<FULL_VIRIAL, F32, U>(jc, cx, cy, cz, i, px, py, pz, h, hi, diag, p, pf, fx, fy, fz, acc, po,
+                                          prow, pc, lane);
         }
-        fx = warp_sum(fx); fy = warp_sum(fy); fz = warp_sum(fz);
-        if (lane == 0) {
-            F[3 * i] = Facc[3 * i] + fx;
-            F[3 * i + 1] = Facc[3 * i + 1] + fy;
-            F[3 * i + 2] = Facc[3 * i + 2] + fz;
-            if (Facc != F) { Facc[3 * i] = 0.0; Facc[3 * i + 1] = 0.0; Facc[3 * i + 2] = 0.0; }
-        }
+        lj_atom_done(i, fx, fy, fz, px, py, pz, hi, F, Facc, po, pc, lane);
         __syncwarp();                           // buffer cur is reused two atoms on
         cur ^= 1;
         pending = false;
@@ -692,13 +631,15 @@ template <bool FULL_VIRIAL, bool F32, int U, int NT>
 __global__ void __launch_bounds__(NT)
 k_lj_gather_staged(const double* __restrict__ pos, const double* __restrict__ hh, const int* __restrict__ in_cnt,
                    const int* __restrict__ in_list, int in_cap, int na, double* __restrict__ F,
-                   double* __restrict__ Facc, LJP p, double* __restrict__ part, DevErr* err) {
+                   double* __restrict__ Facc, LJP p, double* __restrict__ part, DevErr* err,
+                   const int* __restrict__ gate, int want, LJPruneOut po) {
     FMD_PDL_WAIT();
+    if (gate && *gate != want) return;
     extern __shared__ __align__(128) unsigned char dsm[];
     __shared__ double sm[32 * kNV];
     __shared__ double s_hh[18];
     lj_gather_staged_body<FULL_VIRIAL, F32, U, NT>(pos, hh, in_cnt, in_list, in_cap, na, F, Facc, p, part, err,
-                                                   blockIdx.x, gridDim.x, dsm, sm, s_hh);
+                                                   blockIdx.x, gridDim.x, dsm, sm, s_hh, po);
 }
 
 // Replica batch, rows staged (all replicas share the row stride in_cap).
@@ -713,7 +654,7 @@ k_b_lj_gather_staged(const StepArrays* __restrict__ As, const int* __restrict__ 
     const LJP p = lj_params_dev(ff);
     lj_gather_staged_body<FULL_VIRIAL, F32, U, NT>(a.pos, a.S->h, a.in_cnt, a.in_list, a.in_cap, a.n, a.F, a.Facc, p,
                                                    a.part_f2, a.err, blockIdx.x - off[r], off[r + 1] - off[r], dsm,
-                                                   sm, s_hh);
+                                                   sm, s_hh, LJPruneOut{});
 }
 
 // Replica batch: the same gather over every replica in one launch; block b
@@ -728,7 +669,7 @@ k_b_lj_gather(const StepArrays* __restrict__ As, const int* __restrict__ off, in
     const LJP p = lj_params_dev(ff);
     lj_gather_body<FULL_VIRIAL, F32, U, false>(a.pos, a.S->h, a.in_cnt, a.in_list, a.in_cap,
                                         a.n, a.F, a.Facc, p, a.part_f2, blockIdx.x - off[r], off[r + 1] - off[r], sm,
-                                        s_hh);
+                                        s_hh, LJPruneOut{});
 }
 
 __global__ void k_reduce(const double* __restrict__ part, int nblk, int nv, double* __restrict__ out) {
@@ -801,11 +742,11 @@ int lj_occupancy() {
 template <bool FV, bool F32, int U, bool PIPE, int NT>
 int lj_dispatch(bool launch, const double* pos, const double* hh, const int* cnt, const int* list, int cap,
                 const int* in_cnt, const int* in_list, int in_cap, int na, double* F, double* Facc, const LJP& p,
-                double* part, cudaStream_t st) {
+                double* part, cudaStream_t st, const int* gate, int want, const LJPruneOut& po) {
     const int nb = std::min(kLJMaxBlocks, lj_occupancy<FV, F32, U, PIPE, NT>() * kSMs);
     if (launch)
         launch_pdl(k_lj_gather<FV, F32, U, PIPE, NT>, dim3(nb), dim3(NT), 0, st, pos, hh, in_cnt, in_list, in_cap, na,
-                   F, Facc, p, part);
+                   F, Facc, p, part, gate, want, po);
     return nb;
 }
 
@@ -817,7 +758,7 @@ size_t staged_smem(int threads, int in_cap) {
 template <bool FV, bool F32, int U, int NT>
 int lj_dispatch_staged(bool launch, const double* pos, const double* hh, const int* in_cnt, const int* in_list,
                        int in_cap, int na, double* F, double* Facc, const LJP& p, double* part, DevErr* err,
-                       cudaStream_t st) {
+                       cudaStream_t st, const int* gate, int want, const LJPruneOut& po) {
     static std::map<int, int> occ;                 // in_cap -> resident blocks per SM
     const size_t smem = staged_smem(NT, in_cap);
     auto it = occ.find(in_cap);
@@ -835,7 +776,7 @@ int lj_dispatch_staged(bool launch, const double* pos, const double* hh, const i
     const int nb = std::min(kLJMaxBlocks, it->second * kSMs);
     if (launch)
         launch_pdl(k_lj_gather_staged<FV, F32, U, NT>, dim3(nb), dim3(NT), smem, st, pos, hh, in_cnt, in_list, in_cap,
-                   na, F, Facc, p, part, err);
+                   na, F, Facc, p, part, err, gate, want, po);
     return nb;
 }
 
@@ -843,13 +784,15 @@ int lj_dispatch_staged(bool launch, const double* pos, const double* hh, const i
 // (0: the shape cannot run with this row stride).
 int lj_select(bool launch, int ff, int precision, const LJShape& sh, const double* pos, const double* hh,
               const int* cnt, const int* list, int cap, const int* in_cnt, const int* in_list, int in_cap, int na,
-              double* F, double* Facc, double* part, cudaStream_t st, DevErr* err = nullptr) {
+              double* F, double* Facc, double* part, cudaStream_t st, DevErr* err = nullptr,
+              const int* gate = nullptr, int want = 0, const LJPruneOut& po = LJPruneOut{}) {
     const LJP p = lj_params(ff);
     const bool fv = ff == FMD_FF_AIREBO, f32 = precision == FMD_PREC_FP32_PAIR;
     if (sh.pipe == 2) {
         if (in_cap % 4 != 0 || (launch && err == nullptr)) return 0;
 #define FMD_LJS(FV, F32, U, NT) \
-    return lj_dispatch_staged<FV, F32, U, NT>(launch, pos, hh, in_cnt, in_list, in_cap, na, F, Facc, p, part, err, st)
+    return lj_dispatch_staged<FV, F32, U, NT>(launch, pos, hh, in_cnt, in_list, in_cap, na, F, Facc, p, part, err, st, \
+                                              gate, want, po)
 #define FMD_LJS_NT(FV, F32, U) if (sh.threads == 128) { FMD_LJS(FV, F32, U, 128); } else { FMD_LJS(FV, F32, U, 256); }
 #define FMD_LJS_U(FV, F32) if (sh.unroll == 2) { FMD_LJS_NT(FV, F32, 2) } else { FMD_LJS_NT(FV, F32, 4) }
         if (fv) { if (f32) { FMD_LJS_U(true, true) } else { FMD_LJS_U(true, false) } }
@@ -859,7 +802,8 @@ int lj_select(bool launch, int ff, int precision, const LJShape& sh, const doubl
 #undef FMD_LJS
     }
 #define FMD_LJ_CALL(FV, F32, U, PIPE, NT) \
-    return lj_dispatch<FV, F32, U, PIPE, NT>(launch, pos, hh, cnt, list, cap, in_cnt, in_list, in_cap, na, F, Facc, p, part, st)
+    return lj_dispatch<FV, F32, U, PIPE, NT>(launch, pos, hh, cnt, list, cap, in_cnt, in_list, in_cap, na, F, Facc, p, \
+                                             part, st, gate, want, po)
 #define FMD_LJ_NT(FV, F32, U, PIPE) \
     if (sh.threads == 128) { FMD_LJ_CALL(FV, F32, U, PIPE, 128); } else { FMD_LJ_CALL(FV, F32, U, PIPE, 256); }
 #define FMD_LJ_PIPE(FV, F32, U) if (sh.pipe) { FMD_LJ_NT(FV, F32, U, true) } else { FMD_LJ_NT(FV, F32, U, false) }
@@ -882,9 +826,9 @@ int lj_gather_blocks(int ff, int precision, const LJShape& sh, int in_cap) {
 cudaError_t lj_gather_launch(int ff, const double* pos, const double* hh, const int* cnt, const int* list,
                              int cap, const int* in_cnt, const int* in_list, int in_cap, int na, double* F,
                              double* Facc, double* part, cudaStream_t st, int precision, const LJShape& sh,
-                             DevErr* err) {
+                             DevErr* err, const int* gate, int want, const LJPruneOut& po) {
     if (lj_select(true, ff, precision, sh, pos, hh, cnt, list, cap, in_cnt, in_list, in_cap, na, F, Facc, part, st,
-                  err) == 0)
+                  err, gate, want, po) == 0)
         return cudaErrorInvalidConfiguration;
     return cudaGetLastError();
 }

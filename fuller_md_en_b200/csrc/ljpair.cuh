@@ -1,0 +1,107 @@
+// ljpair.cuh -- the shifted 12-6 LJ pair of the AIREBO and MM programs
+// (AI:119-124, 441-446; MM:113-116), the exact diagonal-cell minimum image
+// and the FP64 reciprocal shared by the list gather (airebo.cu) and the
+// molecule-tile kernel (ljtile.cu).
+#pragma once
+#include <cmath>
+#include "geom.cuh"
+#include "kernels.h"
+
+namespace fmd {
+namespace {
+
+struct LJP {
+    double sig2, c4, c24, rc2, vshift;
+};
+
+// Reference constants, computed with the reference's expressions.
+__host__ __device__ inline LJP lj_params_dev(int ff) {
+    LJP p;
+    if (ff == FMD_FF_AIREBO) {  // AI:119-124
+        const double sig = 3.40, eps = 2.84e-3, rc = 3.0 * sig;
+        const double sr = sig / rc, sr2 = sr * sr, sr6 = sr2 * sr2 * sr2;
+        p.sig2 = sig * sig; p.c4 = 4 * eps; p.c24 = 24 * eps; p.rc2 = rc * rc;
+        p.vshift = 4 * eps * (sr6 * sr6 - sr6);
+    } else {                    // MM:113-116
+        const double sig = 3.431, eps = 2.635e-3, rc = 3.0 * sig;
+        const double sr = 1.0 / 3.0, sr2 = sr * sr, sr6 = sr2 * sr2 * sr2;
+        p.sig2 = sig * sig; p.c4 = 4 * eps; p.c24 = 24 * eps; p.rc2 = rc * rc;
+        p.vshift = 4.0 * eps * (sr6 * sr6 - sr6);
+    }
+    return p;
+}
+
+// One component of the minimum image for a diagonal cell.  With zero
+// off-diagonals the reference's s = hi0*dx + hi1*dy + hi2*dz and
+// d = h0*s0 + h1*s1 + h2*s2 reduce exactly to these products (adding +-0
+// changes nothing), so this is bitwise the reference's mimg.
+// For |s| < 1.5 (always so for wrapped positions) round(s), half away from
+// zero, is one of -1, 0, 1 and two comparisons give it exactly.
+__device__ __forceinline__ double mimg1(double d, double hii, double hii_inv) {
+    double s = __dmul_rn(hii_inv, d);
+    double r = s >= 0.5 ? 1.0 : (s <= -0.5 ? -1.0 : 0.0);
+    if (!(fabs(s) < 1.5)) r = round(s);
+    s = __dsub_rn(s, r);
+    return __dmul_rn(hii, s);
+}
+
+// 1/x for x in the FP32 normal range: the FP32 hardware reciprocal (relative
+// error ~2^-23) refined by one Newton-Raphson step y + y (1 - x y), which
+// squares the error (~1e-14), in place of a full IEEE division.
+__device__ __forceinline__ double rcp_nr(double x) {
+    float yf;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"((float)x));
+    const double y = (double)yf;
+    return fma(y, fma(-x, y, 1.0), y);
+}
+
+// FP32 copies of the pair constants (FP32-pair precision).  sigma^2 is kept
+// as a head + tail pair: its FP32 rounding would scale every s^6 by the same
+// factor, a bias that the near-cancelling repulsive and attractive virial
+// sums amplify about tenfold; c4 and c24 scale both parts alike and stay single.
+struct LJF {
+    float sig2, sig2_lo, c4, c24;
+};
+
+// One listed pair seen from atom i: d = r_j - r_i after the minimum image.
+// The cutoff test is the reference's FP64 one in both precisions, so both
+// modes interact through exactly the reference's pair set.  FP64: the
+// reference's arithmetic (AI:447-466).  FP32: the pair algebra (1/r^2, s^6,
+// s^12, fm) in FP32; the minimum image, r^2, the force, energy and virial
+// accumulation stay FP64.  COUNT: this side counts energy and virial.
+template <bool FULL_VIRIAL, bool F32, bool COUNT>
+__device__ __forceinline__ void lj_pair(double dx, double dy, double dz, const LJP& p, const LJF& pf,
+                                        double& fx, double& fy, double& fz, double* acc) {
+    double r2 = norm2_rn(dx, dy, dz);
+    if (r2 > p.rc2) return;
+    if (r2 < 0.25) r2 = 0.25;
+    double fm, e = 0.0;
+    if (F32) {
+        const float ri2 = __frcp_rn((float)r2);
+        const float s2 = fmaf(pf.sig2, ri2, pf.sig2_lo * ri2), s6 = s2 * s2 * s2, s12 = s6 * s6;
+        fm = (double)(pf.c24 * (2.f * s12 - s6) * ri2);
+        if (COUNT) e = (double)(pf.c4 * (s12 - s6)) - p.vshift;
+    } else {
+        const double ri2 = rcp_nr(r2), s2 = p.sig2 * ri2, s6 = s2 * s2 * s2, s12 = s6 * s6;
+        fm = p.c24 * (2 * s12 - s6) * ri2;
+        if (COUNT) e = p.c4 * (s12 - s6) - p.vshift;
+    }
+    fx -= fm * dx; fy -= fm * dy; fz -= fm * dz;
+    if (COUNT) {
+        acc[0] += e;
+        if (FULL_VIRIAL) {
+            const double d[3] = {dx, dy, dz};
+#pragma unroll
+            for (int a = 0; a < 3; a++)
+#pragma unroll
+                for (int b = 0; b < 3; b++) acc[1 + a * 3 + b] += d[a] * fm * d[b];
+        } else {
+            acc[1] += dx * fm * dx;
+            acc[5] += dy * fm * dy;
+            acc[9] += dz * fm * dz;
+        }
+    }
+}
+
+}  // namespace
+}  // namespace fmd

@@ -1,0 +1,112 @@
+// ljprune.cu -- dynamic pruning of the LJ gather's full rows.
+//
+// The reference takes a listed pair when r <= LJ_RCUT at the current step
+// (AI:441, MM:745); its list holds pairs within LJ_RCUT + 2 at the last build,
+// rows cut after MAX_LJ_NEIGH entries (AI:263-272, MM:337-346).  The gather's
+// full rows (airebo.cu) hold exactly those pairs.  A pruning gather walks them,
+// and besides the forces writes each row's entries with r <= LJ_RCUT + delta
+// now, in row order, so the pruned rows are a sub-sequence of the full rows
+// and keep their truncation.  Later steps gather the pruned rows.
+//
+// Exactness.  With a diagonal cell at the prune and now, the reference's
+// minimum image is the nearest image per axis.  For fractional positions s,
+// prune cell h_p, current cell h, u = max_i |h (s_i - s_i,p)| (nearest image)
+// and k = max_a |h_aa - h_p,aa| / h_p,aa, an entry at distance > rc + delta at
+// the prune is now farther than (1 - k)(rc + delta) - 2u.  While
+// k (rc + delta) + 2u < delta (less a rounding margin) every entry dropped by
+// the prune is still beyond the cutoff, so the pruned rows yield exactly the
+// pairs of the full rows: the same pair terms, summed in the same relative
+// order (only their lane assignment changes).  The drift raises u
+// (kick_body), the decision runs on the device before the gathers, and both
+// gathers sit in the step's graph, each returning at once unless the flag
+// selects it.  A list build marks the next evaluation as a prune.
+#include <cmath>
+
+#include "geom.cuh"
+#include "ljprune.h"
+#include "pdl.cuh"
+
+namespace fmd {
+namespace {
+
+constexpr unsigned long long kPruneMark = 0x7F7F7F7F7F7F7F7Full;   // ~1.4e306 A: forces a prune
+
+__device__ __forceinline__ bool diag9(const double* h) {
+    return h[1] == 0.0 && h[2] == 0.0 && h[3] == 0.0 && h[5] == 0.0 && h[6] == 0.0 && h[7] == 0.0;
+}
+
+__global__ void k_prune_decide(unsigned long long* __restrict__ words, const double* __restrict__ hh,
+                               double* __restrict__ hb, int* __restrict__ flag,
+                               unsigned long long* __restrict__ stats, double delta, double rc) {
+    FMD_PDL_WAIT();
+    if (threadIdx.x != 0) return;
+    const double u = __longlong_as_double((long long)*words);
+    double k = 0.0;
+    for (int a = 0; a < 3; a++) k = fmax(k, fabs(hh[4 * a] - hb[4 * a]) / fabs(hb[4 * a]));
+    const bool keep = diag9(hh) && diag9(hb) && k * (rc + delta) + 2.0 * u < delta - 1e-6;
+    *flag = keep ? 0 : 1;
+    stats[0] += 1ull;
+    if (!keep) {
+        *words = 0ull;
+        for (int q = 0; q < 9; q++) hb[q] = hh[q];
+        stats[1] += 1ull;
+    }
+}
+
+__global__ void k_prune_mark(unsigned long long* words) { *words = kPruneMark; }
+
+}  // namespace
+
+cudaError_t lj_prune_alloc(LJPrune& p, int n, int stride, double rc, double delta) {
+    p = LJPrune();
+    cudaError_t e = cudaSuccess;
+    auto A = [&](void** q, size_t bytes) {
+        if (e == cudaSuccess) e = cudaMalloc(q, bytes);
+        if (e == cudaSuccess) e = cudaMemset(*q, 0, bytes);
+    };
+    A((void**)&p.cnt, sizeof(int) * n);
+    A((void**)&p.list, sizeof(int) * (size_t)n * stride);
+    A((void**)&p.sb, sizeof(double) * 3 * n);
+    A((void**)&p.hb, sizeof(double) * 9);
+    A((void**)&p.words, sizeof(unsigned long long));
+    A((void**)&p.flag, sizeof(int));
+    A((void**)&p.stats, sizeof(unsigned long long) * 2);
+    if (e == cudaSuccess) e = cudaMemset(p.words, 0x7F, sizeof(unsigned long long));
+    if (e != cudaSuccess) {
+        lj_prune_free(p);
+        return e;
+    }
+    p.n = n;
+    p.stride = stride;
+    p.rc = rc;
+    p.delta = delta;
+    p.ok = true;
+    return cudaSuccess;
+}
+
+void lj_prune_free(LJPrune& p) {
+    cudaFree(p.cnt); cudaFree(p.list); cudaFree(p.sb); cudaFree(p.hb); cudaFree(p.words); cudaFree(p.flag);
+    cudaFree(p.stats);
+    p = LJPrune();
+}
+
+cudaError_t lj_prune_mark(const LJPrune& p, cudaStream_t st) {
+    k_prune_mark<<<1, 1, 0, st>>>(p.words);
+    return cudaGetLastError();
+}
+
+cudaError_t lj_prune_decide(const LJPrune& p, const double* hh, cudaStream_t st) {
+    return launch_pdl(k_prune_decide, dim3(1), dim3(32), 0, st, p.words, hh, p.hb, p.flag, p.stats, p.delta, p.rc);
+}
+
+LJPruneOut lj_prune_out(const LJPrune& p) {
+    LJPruneOut o;
+    o.cnt = p.cnt;
+    o.list = p.list;
+    o.sb = p.sb;
+    const double r = p.rc + p.delta;
+    o.r2 = r * r;
+    return o;
+}
+
+}  // namespace fmd

@@ -8,10 +8,9 @@
 // atoms of the higher-numbered neighbour molecules in ascending order: the row
 // comes out sorted without a bitmap, its first `cap` entries are the
 // reference's truncation, and the candidates of one molecule are contiguous
-// in memory (coalesced loads).  The incoming (transposed) rows of the LJ
-// gather come out of the same walk over lower-numbered molecules, keeping
-// (i, j) when it passes the same FP64 test and sits inside row i's first
-// `cap` entries.  Intramolecular (REBO) rows walk the atom's own molecule.
+// in memory (coalesced loads).  The LJ gather's full rows are the transpose of
+// these rows (nlist_transpose, nlist.cu), whichever builder made them.
+// Intramolecular (REBO) rows walk the atom's own molecule.
 //
 // Candidate molecules: a centre c and radius R per molecule, and molecule
 // pairs with |c_A - c_B| <= rc + R_A + R_B (minimum image).  For a diagonal
@@ -29,6 +28,8 @@
 
 namespace fmd {
 namespace {
+
+constexpr double kScreenMax = 2048.0;   // coordinate and cell-edge bound of the FP32 screen (A)
 
 __device__ __forceinline__ bool diag_cell(const double* h, const double* hi) {
     return h[1] == 0.0 && h[2] == 0.0 && h[3] == 0.0 && h[5] == 0.0 && h[6] == 0.0 && h[7] == 0.0 &&
@@ -61,11 +62,12 @@ __device__ __forceinline__ bool pair_in(const double* __restrict__ pos, int i, i
 }
 
 // Centre (mean of the minimum images relative to the first atom) and radius
-// (largest minimum-image distance of an atom from the centre) per molecule;
-// one warp per molecule.  Resets the partner-overflow flag.
+// (largest minimum-image distance of an atom from the centre) per molecule,
+// and the FP32 copy of the positions; one warp per molecule.  Resets the
+// partner-overflow flag.
 __global__ void k_mol_centre(const double* __restrict__ pos, const double* __restrict__ hh,
                              const int* __restrict__ off, int M, double* __restrict__ cen, double* __restrict__ rad,
-                             int* __restrict__ flag) {
+                             float4* __restrict__ pos32, int* __restrict__ flag) {
     const double* h = hh;
     const double* hi = hh + 9;
     const int lane = threadIdx.x & 31;
@@ -76,6 +78,9 @@ __global__ void k_mol_centre(const double* __restrict__ pos, const double* __res
     double sx = 0.0, sy = 0.0, sz = 0.0;
     for (int a = a0 + lane; a < a1; a += 32) {
         double dx = pos[3 * a] - pos[3 * a0], dy = pos[3 * a + 1] - pos[3 * a0 + 1], dz = pos[3 * a + 2] - pos[3 * a0 + 2];
+        const double x = pos[3 * a], y = pos[3 * a + 1], z = pos[3 * a + 2];
+        const bool small = fabs(x) < kScreenMax && fabs(y) < kScreenMax && fabs(z) < kScreenMax;
+        pos32[a] = make_float4((float)x, (float)y, (float)z, small ? 1.0f : 0.0f);
         mimg(dx, dy, dz, hi, h);
         sx += dx; sy += dy; sz += dz;
     }
@@ -133,15 +138,57 @@ __global__ void k_mol_decide(const double* __restrict__ hh, int* __restrict__ fl
     if (threadIdx.x == 0) flag[0] = (diag_cell(hh, hh + 9) && flag[1] == 0) ? 1 : 0;
 }
 
+// FP32 screen of the reference's test r^2 < rc2 (diagonal cell): positions
+// rounded to FP32 (error <= 2^-24 * 2048 = 1.2e-4 A per coordinate when
+// |x| < kScreenMax; <= 4e-6 A below 128 A), difference and nearest image in
+// FP32 (rintf, as the FP64 image for |d| well below half the cell), so r^2 at
+// r ~ 12 A is off by less than 0.016 A^2 (1e-3 A^2 below 128 A).  Outside a
+// band of +-kScreenBand around rc2 its verdict is the FP64 one; inside, the
+// FP64 test decides.  Used when half the narrowest cell edge exceeds the list
+// radius by 1 A (no candidate near the radius sits near a half-cell image
+// switch), every edge is below kScreenMax, and both atoms lie within
+// +-kScreenMax (pos32.w = 1).
+constexpr float kScreenBand = 0.05f;
+struct Screen {
+    bool on = false;
+    float L[3], Li[3], lo2, hi2;
+};
+
+__device__ __forceinline__ Screen make_screen(const double* h, const double* hi, bool diag, double rc2) {
+    Screen sc;
+    const double rc = sqrt(rc2);
+    sc.on = diag && 0.5 * fmin(fabs(h[0]), fmin(fabs(h[4]), fabs(h[8]))) > rc + 1.0 &&
+            fmax(fabs(h[0]), fmax(fabs(h[4]), fabs(h[8]))) < kScreenMax;
+    for (int a = 0; a < 3; a++) { sc.L[a] = (float)h[4 * a]; sc.Li[a] = (float)hi[4 * a]; }
+    sc.lo2 = (float)rc2 - kScreenBand;
+    sc.hi2 = (float)rc2 + kScreenBand;
+    return sc;
+}
+
 // Emits the accepted candidates j = c0 .. c1-1 (ascending) of the row being
 // built; `emitted` counts every accepted candidate, entries past `cap` are
 // not stored.
-__device__ __forceinline__ void emit_range(const double* __restrict__ pos, int i, int c0, int c1, const double* h,
-                                           const double* hi, bool diag, double rc2, bool intra, int cap,
-                                           int* __restrict__ row, int& emitted, int lane) {
+__device__ __forceinline__ void emit_range(const double* __restrict__ pos, const float4* __restrict__ pos32, int i,
+                                           int c0, int c1, const double* h, const double* hi, bool diag, double rc2,
+                                           const Screen& sc, bool intra, int cap, int* __restrict__ row,
+                                           int& emitted, int lane) {
+    const float4 pi = sc.on ? pos32[i] : make_float4(0.f, 0.f, 0.f, 0.f);
     for (int b = c0; b < c1; b += 32) {
         const int j = b + lane;
-        const bool ok = j < c1 && (!intra || j != i) && pair_in(pos, i, j, h, hi, diag, rc2);
+        bool ok = j < c1 && (!intra || j != i);
+        if (ok) {
+            const float4 q = sc.on ? pos32[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+            if (sc.on && pi.w != 0.0f && q.w != 0.0f) {
+                float dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
+                dx = fmaf(-sc.L[0], rintf(dx * sc.Li[0]), dx);
+                dy = fmaf(-sc.L[1], rintf(dy * sc.Li[1]), dy);
+                dz = fmaf(-sc.L[2], rintf(dz * sc.Li[2]), dz);
+                const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                ok = r2 < sc.lo2 ? true : (r2 > sc.hi2 ? false : pair_in(pos, i, j, h, hi, diag, rc2));
+            } else {
+                ok = pair_in(pos, i, j, h, hi, diag, rc2);
+            }
+        }
         const unsigned m = __ballot_sync(kFull, ok);
         const int k = emitted + __popc(m & ((1u << lane) - 1u));
         if (ok && k < cap) row[k] = j;
@@ -155,7 +202,7 @@ template <int MODE>
 __global__ void __launch_bounds__(256)
 k_mol_rows(const double* __restrict__ pos, const double* __restrict__ hh, int n, const int* __restrict__ off,
            const int* __restrict__ amol, const int* __restrict__ npart, const int* __restrict__ part, int pmax,
-           double rc2, int cap, int* __restrict__ cnt, int* __restrict__ list, int* __restrict__ tot,
+           const float4* __restrict__ pos32, double rc2, int cap, int* __restrict__ cnt, int* __restrict__ list,
            int* __restrict__ dropped, const int* __restrict__ flag) {
     if (MODE == 0 && flag[0] == 0) return;
     __shared__ double s_hh[18];
@@ -164,74 +211,27 @@ k_mol_rows(const double* __restrict__ pos, const double* __restrict__ hh, int n,
     const double* h = s_hh;
     const double* hi = s_hh + 9;
     const bool diag = diag_cell(h, hi);
+    // intramolecular rows are short: no screen
+    Screen sc = make_screen(h, hi, diag, rc2);
+    if (MODE == 1) sc.on = false;
     const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
     for (int i = blockIdx.x * wpb + (threadIdx.x >> 5); i < n; i += gridDim.x * wpb) {
         const int A = amol[i];
         int* row = list + (size_t)i * cap;
         int emitted = 0;
         if (MODE == 1) {
-            emit_range(pos, i, off[A], off[A + 1], h, hi, diag, rc2, true, cap, row, emitted, lane);
+            emit_range(pos, pos32, i, off[A], off[A + 1], h, hi, diag, rc2, sc, true, cap, row, emitted, lane);
         } else {
             const int np = npart[A];
             for (int p = 0; p < np; p++) {
                 const int B = part[(size_t)A * pmax + p];
                 if (B < A) continue;
-                emit_range(pos, i, off[B], off[B + 1], h, hi, diag, rc2, false, cap, row, emitted, lane);
+                emit_range(pos, pos32, i, off[B], off[B + 1], h, hi, diag, rc2, sc, false, cap, row, emitted, lane);
             }
         }
         if (lane == 0) {
             cnt[i] = emitted < cap ? emitted : cap;
-            if (tot) tot[i] = emitted;
             if (emitted > cap && dropped) atomicAdd(dropped, emitted - cap);
-        }
-    }
-}
-
-// Full rows for the LJ gather: for atom j, the atoms i < j of lower
-// neighbour molecules whose row holds j (the FP64 test from i's side, and j
-// within row i's first `cap` accepted entries), at most in_cap - cap of them,
-// followed by j's own row; one warp per atom.
-__global__ void __launch_bounds__(256)
-k_mol_incoming(const double* __restrict__ pos, const double* __restrict__ hh, int n, const int* __restrict__ off,
-               const int* __restrict__ amol, const int* __restrict__ npart, const int* __restrict__ part, int pmax,
-               double rc2, int cap, const int* __restrict__ cnt, const int* __restrict__ list,
-               const int* __restrict__ tot,
-               int* __restrict__ in_cnt, int* __restrict__ in_list, int in_cap, DevErr* err,
-               const int* __restrict__ flag) {
-    if (flag[0] == 0) return;
-    __shared__ double s_hh[18];
-    if (threadIdx.x < 18) s_hh[threadIdx.x] = hh[threadIdx.x];
-    __syncthreads();
-    const double* h = s_hh;
-    const double* hi = s_hh + 9;
-    const bool diag = diag_cell(h, hi);
-    const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
-    for (int j = blockIdx.x * wpb + (threadIdx.x >> 5); j < n; j += gridDim.x * wpb) {
-        const int B = amol[j];
-        int* row = in_list + (size_t)j * in_cap;
-        int emitted = 0;
-        const int np = npart[B];
-        for (int p = 0; p < np; p++) {
-            const int A = part[(size_t)B * pmax + p];
-            if (A > B) break;                      // partners are ascending
-            for (int b = off[A]; b < off[A + 1]; b += 32) {
-                const int i = b + lane;
-                bool ok = i < off[A + 1] && pair_in(pos, i, j, h, hi, diag, rc2);
-                if (ok && tot[i] > cap) ok = j <= list[(size_t)i * cap + cap - 1];
-                const unsigned m = __ballot_sync(kFull, ok);
-                const int k = emitted + __popc(m & ((1u << lane) - 1u));
-                if (ok && k < in_cap - cap) row[k] = i;
-                emitted += __popc(m);
-            }
-        }
-        const int kept = emitted < in_cap - cap ? emitted : in_cap - cap;
-        const int mo = cnt[j];
-        for (int k = lane; k < mo; k += 32) row[kept + k] = list[(size_t)j * cap + k];
-        if (lane == 0) {
-            in_cnt[j] = kept + mo;
-            if (emitted > in_cap - cap && atomicCAS(&err->code, FMD_OK, FMD_ERR_CAPACITY) == FMD_OK) {
-                err->where = K_TRANSPOSE; err->index = j; err->value = emitted;
-            }
         }
     }
 }
@@ -262,6 +262,7 @@ cudaError_t mol_lists_alloc(MolLists& m, int n, const int* mol_id_host) {
         for (int k = off[a]; k < off[a + 1]; k++) amol[k] = a;
     m.M = M;
     m.pmax = std::min(M, kMolPartners);
+    for (int a = 0; a < M; a++) m.max_atoms = std::max(m.max_atoms, off[a + 1] - off[a]);
     cudaError_t e;
     auto A = [&](void** p, size_t bytes) {
         if (e == cudaSuccess) e = cudaMalloc(p, bytes);
@@ -271,9 +272,9 @@ cudaError_t mol_lists_alloc(MolLists& m, int n, const int* mol_id_host) {
     A((void**)&m.amol, sizeof(int) * n);
     A((void**)&m.cen, sizeof(double) * 3 * M);
     A((void**)&m.rad, sizeof(double) * M);
+    A((void**)&m.pos32, sizeof(float4) * n);
     A((void**)&m.npart, sizeof(int) * M);
     A((void**)&m.part, sizeof(int) * (size_t)M * m.pmax);
-    A((void**)&m.tot, sizeof(int) * n);
     A((void**)&m.flag, sizeof(int) * 2);
     if (e == cudaSuccess) e = cudaMemcpy(m.off, off.data(), sizeof(int) * (M + 1), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(m.amol, amol.data(), sizeof(int) * n, cudaMemcpyHostToDevice);
@@ -288,14 +289,14 @@ cudaError_t mol_lists_alloc(MolLists& m, int n, const int* mol_id_host) {
 }
 
 void mol_lists_free(MolLists& m) {
-    cudaFree(m.off); cudaFree(m.amol); cudaFree(m.cen); cudaFree(m.rad); cudaFree(m.npart); cudaFree(m.part);
-    cudaFree(m.tot); cudaFree(m.flag);
+    cudaFree(m.off); cudaFree(m.amol); cudaFree(m.cen); cudaFree(m.rad); cudaFree(m.pos32); cudaFree(m.npart); cudaFree(m.part);
+    cudaFree(m.flag);
     m = MolLists();
 }
 
 cudaError_t mol_partners(MolLists& m, const double* pos, const double* hh, double rc, cudaStream_t st) {
     const int wblocks = (m.M * 32 + 255) / 256;
-    k_mol_centre<<<wblocks, 256, 0, st>>>(pos, hh, m.off, m.M, m.cen, m.rad, m.flag);
+    k_mol_centre<<<wblocks, 256, 0, st>>>(pos, hh, m.off, m.M, m.cen, m.rad, m.pos32, m.flag);
     k_mol_pairs<<<wblocks, 256, 0, st>>>(hh, m.M, m.cen, m.rad, rc, m.pmax, m.npart, m.part, m.flag);
     k_mol_decide<<<1, 32, 0, st>>>(hh, m.flag);
     return cudaGetLastError();
@@ -303,18 +304,15 @@ cudaError_t mol_partners(MolLists& m, const double* pos, const double* hh, doubl
 
 cudaError_t mol_rows_intra(const MolLists& m, const double* pos, const double* hh, double rc2, int cap, int* cnt,
                            int* list, int* dropped, cudaStream_t st) {
-    k_mol_rows<1><<<kRowBlocksMol, 256, 0, st>>>(pos, hh, m.n, m.off, m.amol, m.npart, m.part, m.pmax, rc2, cap, cnt,
-                                                 list, nullptr, dropped, m.flag);
+    k_mol_rows<1><<<kRowBlocksMol, 256, 0, st>>>(pos, hh, m.n, m.off, m.amol, m.npart, m.part, m.pmax, m.pos32, rc2,
+                                                 cap, cnt, list, dropped, m.flag);
     return cudaGetLastError();
 }
 
 cudaError_t mol_rows_half(const MolLists& m, const double* pos, const double* hh, double rc2, int cap, int* cnt,
-                          int* list, int* in_cnt, int* in_list, int in_cap, int* dropped, DevErr* err,
-                          cudaStream_t st) {
-    k_mol_rows<0><<<kRowBlocksMol, 256, 0, st>>>(pos, hh, m.n, m.off, m.amol, m.npart, m.part, m.pmax, rc2, cap, cnt,
-                                                 list, m.tot, dropped, m.flag);
-    k_mol_incoming<<<kRowBlocksMol, 256, 0, st>>>(pos, hh, m.n, m.off, m.amol, m.npart, m.part, m.pmax, rc2, cap,
-                                                  cnt, list, m.tot, in_cnt, in_list, in_cap, err, m.flag);
+                          int* list, int* dropped, cudaStream_t st) {
+    k_mol_rows<0><<<kRowBlocksMol, 256, 0, st>>>(pos, hh, m.n, m.off, m.amol, m.npart, m.part, m.pmax, m.pos32, rc2,
+                                                 cap, cnt, list, dropped, m.flag);
     return cudaGetLastError();
 }
 

@@ -15,13 +15,14 @@ constexpr int kMolPartners = 256;   // partner molecules per molecule (table wid
 struct MolLists {
     bool ok = false;          // molecules are contiguous index ranges
     int n = 0, M = 0, pmax = 0;
+    int max_atoms = 0;        // atoms of the largest molecule
     int* off = nullptr;       // [M + 1] first atom of each molecule
     int* amol = nullptr;      // [n] molecule of each atom
     double* cen = nullptr;    // [3 M] centres
     double* rad = nullptr;    // [M] radii
+    float4* pos32 = nullptr;  // [n] positions of the build rounded to FP32 (w unused), for the prefilter
     int* npart = nullptr;     // [M] partner count
     int* part = nullptr;      // [M * pmax] partners, ascending
-    int* tot = nullptr;       // [n] accepted half-list partners before truncation
     int* flag = nullptr;      // [2] {molecule path valid, partner overflow}
 };
 
@@ -34,9 +35,8 @@ cudaError_t mol_partners(MolLists& m, const double* pos, const double* hh, doubl
 // Intramolecular rows (always valid for contiguous molecules).
 cudaError_t mol_rows_intra(const MolLists& m, const double* pos, const double* hh, double rc2, int cap, int* cnt,
                            int* list, int* dropped, cudaStream_t st);
-// Half-list rows and their incoming rows; no-ops unless flag[0] is set.
+// Half-list rows (the reference's truncation at cap); no-ops unless flag[0] is set.
 cudaError_t mol_rows_half(const MolLists& m, const double* pos, const double* hh, double rc2, int cap, int* cnt,
-                          int* list, int* in_cnt, int* in_list, int in_cap, int* dropped, DevErr* err,
-                          cudaStream_t st);
+                          int* list, int* dropped, cudaStream_t st);
 
 }  // namespace fmd

@@ -22,6 +22,7 @@
 // with -fmad=false so they round like the reference's host code.
 #include <cmath>
 #include "step.h"
+#include "ljprune.h"
 #include "geom.cuh"
 #include "sg_host.h"
 #include "pdl.cuh"
@@ -118,6 +119,7 @@ __device__ void kick_body(const StepArrays& a, double dt, int blk, int nblk) {
     const double* h = S->h;
     const bool rigid = a.kind == FMD_SYS_RIGID;
     const double cF = rigid ? kConv / a.Mmol : kConv / kMC, cT = rigid ? kConv / a.I0 : 0.0;
+    double u2 = 0.0;   // largest squared displacement since the last LJ prune
     for (int i = blk * blockDim.x + threadIdx.x; i < a.n; i += nblk * blockDim.x) {
         const double mi = (a.mass != nullptr) ? kConv / a.mass[i] : cF;
         double v[3], p[3];
@@ -137,6 +139,14 @@ __device__ void kick_body(const StepArrays& a, double dt, int blk, int nblk) {
         a.pos[3 * i] = h[0] * sx + h[1] * sy + h[2] * sz;
         a.pos[3 * i + 1] = h[3] * sx + h[4] * sy + h[5] * sz;
         a.pos[3 * i + 2] = h[6] * sx + h[7] * sy + h[8] * sz;
+        if (a.prune_sb) {
+            // nearest-image fractional displacement, measured in the new cell
+            double ex = sx - a.prune_sb[3 * i], ey = sy - a.prune_sb[3 * i + 1], ez = sz - a.prune_sb[3 * i + 2];
+            ex -= rint(ex); ey -= rint(ey); ez -= rint(ez);
+            const double ux = h[0] * ex + h[1] * ey + h[2] * ez, uy = h[3] * ex + h[4] * ey + h[5] * ez,
+                         uz = h[6] * ex + h[7] * ey + h[8] * ez;
+            u2 = fmax(u2, ux * ux + uy * uy + uz * uz);
+        }
         if (rigid) {
             double w[3];
             for (int c = 0; c < 3; c++) {
@@ -145,6 +155,12 @@ __device__ void kick_body(const StepArrays& a, double dt, int blk, int nblk) {
             }
             quat_step(a.qv + 4 * i, w[0], w[1], w[2], dt);               // LJ:503-508
         }
+    }
+    if (a.prune_sb) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) u2 = fmax(u2, __shfl_xor_sync(kFull, u2, o));
+        if ((threadIdx.x & 31) == 0 && u2 > 0.0)
+            atomicMax(a.prune_umax, (unsigned long long)__double_as_longlong(sqrt(u2) * (1.0 + 1e-12)));
     }
 }
 
@@ -458,6 +474,25 @@ int force_partial_blocks(const StepArrays& a) {
     return a.kind == FMD_SYS_RIGID ? rigid_grid(a.n) : (a.kind == FMD_SYS_AIREBO ? a.rebo_blocks : kForceBlocks);
 }
 
+// LJ term of an atomistic system: the gather over the full rows, or with
+// pruned rows the decision, then a pruning gather over the full rows and a
+// gather over the pruned rows, each returning at once unless selected.
+cudaError_t enqueue_lj(const StepArrays& a, int ff, cudaStream_t st) {
+    const double* hh = a.S->h;
+    if (!a.prune || a.prune->delta <= 0.0)
+        return lj_gather_launch(ff, a.pos, hh, a.cnt_a, a.list_a, a.cap_a, a.in_cnt, a.in_list, a.in_cap, a.n, a.F,
+                                a.Facc, a.part_f2, st, a.precision, a.lj_shape, a.err);
+    const LJPrune& q = *a.prune;
+    cudaError_t e;
+    if ((e = lj_prune_decide(q, hh, st)) != cudaSuccess) return e;
+    if ((e = lj_gather_launch(ff, a.pos, hh, a.cnt_a, a.list_a, a.cap_a, a.in_cnt, a.in_list, a.in_cap, a.n, a.F,
+                              a.Facc, a.part_f2, st, a.precision, a.lj_shape, a.err, q.flag, 1, lj_prune_out(q))) !=
+        cudaSuccess)
+        return e;
+    return lj_gather_launch(ff, a.pos, hh, a.cnt_a, a.list_a, a.cap_a, q.cnt, q.list, a.in_cap, a.n, a.F, a.Facc,
+                            a.part_f2, st, a.precision, a.lj_shape, a.err, q.flag, 0);
+}
+
 cudaError_t enqueue_forces(const StepArrays& a, cudaStream_t st, bool judge) {
     cudaError_t e = cudaSuccess;
     const double* hh = a.S->h;
@@ -471,14 +506,12 @@ cudaError_t enqueue_forces(const StepArrays& a, cudaStream_t st, bool judge) {
                                   kForceBlocks, nullptr, 0, st);
         else e = rebo_launch(a.pos, hh, a.cnt_b, a.list_b, a.cap_b, a.n, a.Facc, a.part_f1, st);
         if (e != cudaSuccess) return e;
-        e = lj_gather_launch(FMD_FF_AIREBO, a.pos, hh, a.cnt_a, a.list_a, a.cap_a, a.in_cnt, a.in_list, a.in_cap,
-                             a.n, a.F, a.Facc, a.part_f2, st, a.precision, a.lj_shape, a.err);
+        e = enqueue_lj(a, FMD_FF_AIREBO, st);
     } else {
         if ((e = mm_bonded_launch(a.topo, a.pos, hh, a.Facc, a.part_f1, st)) != cudaSuccess) return e;
         if (a.has_charge)
             if ((e = mm_coulomb_launch(a.pos, hh, a.charge, a.mol_id, a.n, a.Facc, a.part_f3, st)) != cudaSuccess) return e;
-        e = lj_gather_launch(FMD_FF_MM, a.pos, hh, a.cnt_a, a.list_a, a.cap_a, a.in_cnt, a.in_list, a.in_cap,
-                             a.n, a.F, a.Facc, a.part_f2, st, a.precision, a.lj_shape, a.err);
+        e = enqueue_lj(a, FMD_FF_MM, st);
     }
     return e;
 }

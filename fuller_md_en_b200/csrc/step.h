@@ -29,6 +29,7 @@ struct SysScal {
 };
 
 struct SgStep;   // learned REBO term of a system (sg_host.h)
+struct LJPrune;  // pruned LJ rows of a system (ljprune.h)
 
 // Device pointers and sizes of one step.
 struct StepArrays {
@@ -61,6 +62,12 @@ struct StepArrays {
     int lj_blocks = 0;             // its grid = partial records in part_f2
     SgStep* sg = nullptr;          // AIREBO: learned REBO term instead of the plain kernel
     int rebo_blocks = kForceBlocks;  // partial records the REBO term writes into part_f1
+    // Pruned LJ rows (AIREBO, MM): host descriptor (nullptr: full rows every
+    // step), and the fractional positions of the last prune and the
+    // displacement word the drift raises.
+    const LJPrune* prune = nullptr;
+    const double* prune_sb = nullptr;
+    unsigned long long* prune_umax = nullptr;
 };
 
 struct StepParams {
@@ -73,6 +80,8 @@ struct StepParams {
 // judge: AIREBO with a learned REBO term also runs the plain REBO kernel and
 // compares the two (sg_step.cu).
 cudaError_t enqueue_forces(const StepArrays& a, cudaStream_t st, bool judge = false);
+// The LJ term alone (ff: FMD_FF_AIREBO / FMD_FF_MM): F = Facc + LJ, Facc zeroed.
+cudaError_t enqueue_lj(const StepArrays& a, int ff, cudaStream_t st);
 // Reduces the force partials into S->W9 / S->E (one small kernel).
 cudaError_t enqueue_force_reduce(const StepArrays& a, cudaStream_t st);
 // Recomputes S->KE (and kt, kr) from the velocities.

@@ -46,6 +46,8 @@ void System::release() {
     owned.clear();
     cells_free(cells_a);
     cells_free(cells_b);
+    lj_prune_free(prune);
+    arr.prune = nullptr; arr.prune_sb = nullptr; arr.prune_umax = nullptr;
     mol_lists_free(mol);
 }
 
@@ -112,6 +114,16 @@ int System::alloc_lists(double rc_list_a, int cap_a_, double rc_list_b, int cap_
 }
 
 // Rebuild of every list this kind uses, as the driver does at gstep % nlup == 0.
+int System::alloc_prune(double rc_lj) {
+    if (!arr.in_list) return FMD_OK;
+    if (lj_prune_alloc(prune, arr.n, arr.in_cap, rc_lj, kPruneDelta) != cudaSuccess)
+        return ctx->fail(FMD_ERR_CUDA, "device allocation failed");
+    arr.prune = &prune;
+    arr.prune_sb = prune.sb;
+    arr.prune_umax = prune.words;
+    return FMD_OK;
+}
+
 cudaError_t System::enqueue_rebuild(cudaStream_t st) {
     cudaError_t e;
     double* hh = arr.S->h;
@@ -147,12 +159,13 @@ cudaError_t System::enqueue_rebuild(cudaStream_t st) {
     if ((e = nlist_build(cells_a, LIST_HALF, arr.pos, arr.mol_id, arr.n, hh, rc2_a, arr.cap_a, cnt_a, list_a,
                          dropped, ctx->d_err, st, gate)) != cudaSuccess)
         return e;
-    if ((e = nlist_transpose(arr.cnt_a, arr.list_a, arr.cap_a, arr.n, const_cast<int*>(arr.in_cnt),
-                             const_cast<int*>(arr.in_list), arr.in_cap, ctx->d_err, st, gate)) != cudaSuccess)
+    if (mol.ok && (e = mol_rows_half(mol, arr.pos, hh, rc2_a, arr.cap_a, cnt_a, list_a, dropped, st)) != cudaSuccess)
         return e;
-    if (mol.ok)
-        return mol_rows_half(mol, arr.pos, hh, rc2_a, arr.cap_a, cnt_a, list_a, const_cast<int*>(arr.in_cnt),
-                             const_cast<int*>(arr.in_list), arr.in_cap, dropped, ctx->d_err, st);
+    // the gather's full rows from whichever half list was built
+    if ((e = nlist_transpose(arr.cnt_a, arr.list_a, arr.cap_a, arr.n, const_cast<int*>(arr.in_cnt),
+                             const_cast<int*>(arr.in_list), arr.in_cap, ctx->d_err, st)) != cudaSuccess)
+        return e;
+    if (prune.ok) return lj_prune_mark(prune, st);     // new rows: the next evaluation prunes them
     return cudaSuccess;
 }
 
@@ -434,6 +447,7 @@ extern "C" int fmd_system_create_airebo(fmd_ctx* ctx, const fmd_run_params* p, i
     const double rebo_rcut = 2.0 + 0.3;         // AI:116
     if ((rc = s->alloc_lists(lj_rcut + 2.0, 400, rebo_rcut, 12, true)) != FMD_OK) return rc;
     if (fmd::mol_lists_alloc(s->mol, na, mol_id) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "list allocation failed");
+    if ((rc = s->alloc_prune(lj_rcut)) != FMD_OK) return rc;
     out[0] = new fmd_system{std::move(s)};
     return FMD_OK;
 }
@@ -469,6 +483,7 @@ extern "C" int fmd_system_create_mm(fmd_ctx* ctx, const fmd_run_params* p, int n
     const double rcut = 3.0 * 3.431;            // MM:114
     if ((rc = s->alloc_lists(rcut + 2.0, 400, 0.0, 0, true)) != FMD_OK) return rc;
     if (fmd::mol_lists_alloc(s->mol, na, mol_id) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "list allocation failed");
+    if ((rc = s->alloc_prune(rcut)) != FMD_OK) return rc;
     out[0] = new fmd_system{std::move(s)};
     return FMD_OK;
 }
@@ -549,6 +564,17 @@ extern "C" int fmd_system_download(fmd_system* s, double* pos, double* vel, doub
     return y.ctx->sync_check("system download");
 }
 
+extern "C" int fmd_system_forces(fmd_system* s, double* F, double* T, double* E) {
+    if (!s || !s->sys) return FMD_ERR_ARG;
+    fmd::System& y = *s->sys;
+    cudaStream_t st = y.ctx->stream;
+    const size_t n = y.arr.n;
+    if (F) cudaMemcpyAsync(F, y.arr.F, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, st);
+    if (T && y.arr.T) cudaMemcpyAsync(T, y.arr.T, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, st);
+    if (E) cudaMemcpyAsync(E, y.arr.S->E, sizeof(double) * 8, cudaMemcpyDeviceToHost, st);
+    return y.ctx->sync_check("system forces");
+}
+
 extern "C" int fmd_system_lists(fmd_system* s, int* cnt_a, int* list_a, int* cnt_b, int* list_b) {
     if (!s) return FMD_ERR_ARG;
     fmd::System& y = *s->sys;
@@ -563,7 +589,7 @@ extern "C" int fmd_system_lists(fmd_system* s, int* cnt_a, int* list_a, int* cnt
 }
 
 extern "C" int fmd_system_kernel_ms(fmd_system* s, int stage, int reps, double* ms) {
-    if (!s || !ms || reps < 1 || stage < 0 || stage > 3) return FMD_ERR_ARG;
+    if (!s || !ms || reps < 1 || stage < 0 || stage > 4) return FMD_ERR_ARG;
     fmd::System& y = *s->sys;
     if (!y.initialized) return y.ctx->fail(FMD_ERR_STATE, "kernel timing before init");
     cudaStream_t st = y.ctx->stream;
@@ -590,6 +616,12 @@ extern "C" int fmd_system_kernel_ms(fmd_system* s, int stage, int reps, double* 
                                     a.rmcut2, a.F, a.T, a.part_f1, st, a.rigid_lab, a.rigid_shape);
             case 2:
                 return y.enqueue_rebuild(st);
+            case 4:
+                // the gather over the pruned rows of the last prune, into the scratch accumulator
+                if (!a.prune) return cudaErrorInvalidValue;
+                return lj_gather_launch(a.kind == FMD_SYS_AIREBO ? FMD_FF_AIREBO : FMD_FF_MM, a.pos, hh, a.cnt_a,
+                                        a.list_a, a.cap_a, a.prune->cnt, a.prune->list, a.in_cap, a.n, a.Facc,
+                                        a.Facc, a.part_f2, st, a.precision, a.lj_shape, a.err);
             default:
                 return enqueue_forces(a, st);
         }
@@ -653,6 +685,46 @@ extern "C" int fmd_system_set_lj_shape(fmd_system* s, int threads, int unroll, i
                 for (int j = 0; j < 2 && rc == FMD_OK; j++) rc = y.capture(r != 0, ph != 0, j != 0);
         return rc;
     }
+    return FMD_OK;
+}
+
+extern "C" int fmd_system_set_lj_prune(fmd_system* s, double delta) {
+    if (!s || !s->sys) return FMD_ERR_ARG;
+    fmd::System& y = *s->sys;
+    if (!(delta >= 0.0 && delta <= 10.0))
+        return y.ctx->fail(FMD_ERR_ARG, "fmd_system_set_lj_prune: delta must lie in [0, 10] A");
+    if (!y.prune.ok) {
+        if (delta == 0.0) return FMD_OK;
+        return y.ctx->fail(FMD_ERR_ARG, "fmd_system_set_lj_prune: the system has no LJ gather rows");
+    }
+    if (y.prune.delta == delta) return FMD_OK;
+    if (cudaStreamSynchronize(y.ctx->stream) != cudaSuccess) return y.ctx->fail(FMD_ERR_CUDA, "sync failed");
+    y.drop_graphs();                     // captured graphs hold the old launches
+    y.prune.delta = delta;
+    if (lj_prune_mark(y.prune, y.ctx->stream) != cudaSuccess) return y.ctx->fail(FMD_ERR_CUDA, "prune mark failed");
+    if (y.initialized && y.p.use_graphs) {
+        int rc = FMD_OK;
+        const int nj = y.arr.sg ? 2 : 1;
+        for (int r = 0; r < 2 && rc == FMD_OK; r++)
+            for (int ph = 0; ph < 2 && rc == FMD_OK; ph++)
+                for (int j = 0; j < nj && rc == FMD_OK; j++) rc = y.capture(r != 0, ph != 0, j != 0);
+        return rc;
+    }
+    return FMD_OK;
+}
+
+extern "C" int fmd_system_lj_prune(fmd_system* s, double* delta, long long* evaluations, long long* prunes) {
+    if (!s || !s->sys) return FMD_ERR_ARG;
+    fmd::System& y = *s->sys;
+    if (delta) *delta = y.prune.ok ? y.prune.delta : 0.0;
+    unsigned long long st[2] = {0ull, 0ull};
+    if (y.prune.ok && (evaluations || prunes)) {
+        if (cudaStreamSynchronize(y.ctx->stream) != cudaSuccess ||
+            cudaMemcpy(st, y.prune.stats, sizeof(st), cudaMemcpyDeviceToHost) != cudaSuccess)
+            return y.ctx->fail(FMD_ERR_CUDA, "fmd_system_lj_prune: read failed");
+    }
+    if (evaluations) *evaluations = (long long)st[0];
+    if (prunes) *prunes = (long long)st[1];
     return FMD_OK;
 }
 

@@ -2,6 +2,7 @@
 #pragma once
 #include <memory>
 #include <vector>
+#include "ljprune.h"
 #include "molnlist.h"
 #include "sg_host.h"
 #include "step.h"
@@ -9,6 +10,7 @@
 namespace fmd {
 
 constexpr int kInCap = 1024;   // incoming (transposed) LJ entries per atom; full rows add the own row
+constexpr double kPruneDelta = 0.5;   // default buffer of the pruned LJ rows beyond the cutoff (A)
 
 struct System {
     fmd_ctx* ctx = nullptr;
@@ -17,6 +19,7 @@ struct System {
     StepArrays arr{};
     CellList cells_a, cells_b;
     MolLists mol;                      // molecule-wise list builder (contiguous molecules)
+    LJPrune prune;                     // pruned LJ rows (AIREBO, MM; prune.ok false: full rows only)
     double rc_a = 0, rc2_a = 0, rc_b = 0, rc2_b = 0;
     double h0[9] = {0};
     int* dropped = nullptr;            // device: {list a, list b} overflow counts
@@ -29,6 +32,7 @@ struct System {
     template <class T> cudaError_t alloc(T** p, size_t count, const T* src);
     int alloc_common(const double* pos, const double* vel, const double* h, const fmd_npt* npt);
     int alloc_lists(double rc_list_a, int cap_a, double rc_list_b, int cap_b, bool transpose);
+    int alloc_prune(double rc_lj);
     int upload_topology(const fmd_mm_topology* t);
     cudaError_t enqueue_rebuild(cudaStream_t st);
     cudaError_t enqueue_variant(bool rebuild, bool phase, cudaStream_t st, bool judge = false);

@@ -73,6 +73,7 @@ class Surrogate:
         v = flatten(P)
         rc = self.lib.fmd_sg_create(ctx.h, v.ctypes.data_as(_lib._dp), ctypes.byref(self.h))
         ctx.check(rc, "fmd_sg_create")
+        ctx.adopt(self)
 
     def close(self):
         if self.h:
@@ -176,6 +177,7 @@ class Dataset:
         self.ctx = ctx
         self.h = ctypes.c_void_p()
         ctx.check(self.lib.fmd_sg_data_create(ctx.h, ctypes.byref(self.h)), "fmd_sg_data_create")
+        ctx.adopt(self)
 
     def __len__(self) -> int:
         return int(self.lib.fmd_sg_data_count(self.h))

@@ -234,6 +234,11 @@ int fmd_system_averages(fmd_system *s, fmd_avg *avg);
 /* Copies the state to host arrays (any may be NULL). */
 int fmd_system_download(fmd_system *s, double *pos, double *vel, double *qv, double *omg,
                         double *h, fmd_npt *npt);
+/* Forces (3 n doubles; rigid systems: centre-of-mass forces) of the last force
+ * evaluation, torques (rigid only, 3 n) and its energies E[8] in the program's
+ * grouping (AIREBO: total, REBO, LJ; MM: bond, angle, dihedral, improper, LJ,
+ * Coulomb, total; rigid: LJ); any pointer may be null. */
+int fmd_system_forces(fmd_system *s, double *F, double *T, double *E);
 /* Virial tensor W9 of the last force evaluation and the current kinetic
  * energy (eV; rigid: translational + rotational); either may be NULL. */
 int fmd_system_virial(fmd_system *s, double *W9, double *KE);
@@ -246,7 +251,9 @@ int fmd_system_destroy(fmd_system *s);
  * and returns the mean duration per launch in milliseconds; stages:
  *   0 the pair kernel (rigid site-site LJ, or the atomistic LJ gather),
  *   1 the second force kernel (REBO, or MM bonded), 2 a full list rebuild,
- *   3 one complete step (eager launches).
+ *   3 the whole force evaluation of a step (eager launches),
+ *   4 the atomistic LJ gather over the pruned rows of the last prune (see
+ *     fmd_system_set_lj_prune).
  * The force stages leave F in place (they recompute the current forces).
  * fmd_system_step_kernels returns the number of kernel launches of one step
  * of each variant (list rebuild or not; phase bit 0: cold/warm phase, bit 1:
@@ -259,6 +266,18 @@ int fmd_system_kernel_ms(fmd_system *s, int stage, int reps, double *ms_per_laun
  * fmd_system_set_lj_shape pins a shape (for reproducible runs; results then
  * do not depend on timing), after fmd_system_init. */
 int fmd_system_lj_shape(fmd_system *s, int *threads, int *unroll, int *pipelined, int *blocks);
+/* Pruned rows of the atomistic LJ gather (AIREBO, MM; the reference walks
+ * its whole list every step, AI:435-470, MM:729-760).  After each list build,
+ * and whenever the largest atom displacement u and the largest relative
+ * cell-edge change k since the last prune reach k (rc + delta) + 2 u >= delta,
+ * the gather walks the full rows and keeps each row's entries within
+ * rc + delta, in row order; other steps walk those rows.  Every pair within
+ * the cutoff stays in them, so the pairs and pair terms are the full rows'
+ * (on non-diagonal cells every step prunes).  delta in A: 0 = off, default
+ * 0.5.  fmd_system_lj_prune reports delta and the numbers of force
+ * evaluations and of prunes among them since set-up. */
+int fmd_system_set_lj_prune(fmd_system *s, double delta);
+int fmd_system_lj_prune(fmd_system *s, double *delta, long long *evaluations, long long *prunes);
 int fmd_system_set_lj_shape(fmd_system *s, int threads, int unroll, int feed);
 int fmd_system_step_kernels(fmd_system *s, int rebuild, int phase, int *nkernels);
 
