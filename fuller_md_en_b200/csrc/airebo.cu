@@ -169,15 +169,16 @@ struct Slot {
 __global__ void __launch_bounds__(256)
 k_rebo_slots(const double* __restrict__ pos, const double* __restrict__ hh, const int* __restrict__ cnt,
              const int* __restrict__ list, int cap, int na, Slot* __restrict__ sl,
-             const int* __restrict__ gate, int want) {
+             const int* __restrict__ gate, int want, const int* __restrict__ ids) {
     FMD_PDL_WAIT();
     if (gate != nullptr && *gate != want) return;
     __shared__ double s_hh[18];
     if (threadIdx.x < 18) s_hh[threadIdx.x] = hh[threadIdx.x];
     __syncthreads();
-    const long long tot = (long long)na * cap;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(t / cap), jn = (int)(t % cap);
+    const int tot = ids ? ids[0] : na * cap;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < tot; k += gridDim.x * blockDim.x) {
+        const int t = ids ? ids[1 + k] : k;
+        const int i = t / cap, jn = t - i * cap;
         if (jn >= cnt[i]) continue;
         double x, y, z;
         bond_vec(pos, i, list[t], s_hh, s_hh + 9, x, y, z);
@@ -274,12 +275,13 @@ __device__ __forceinline__ double three_body_coeff(double gs, double b, double f
 
 __global__ void __launch_bounds__(256)
 k_rebo_bo(const Slot* __restrict__ sl, const int* __restrict__ cnt, const int* __restrict__ list, int cap, int na,
-          SlotBO* __restrict__ bo, const int* __restrict__ gate, int want) {
+          SlotBO* __restrict__ bo, const int* __restrict__ gate, int want, const int* __restrict__ ids) {
     FMD_PDL_WAIT();
     if (gate != nullptr && *gate != want) return;
-    const long long tot = (long long)na * cap;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x) {
-        const int c = (int)(t / cap), jn = (int)(t % cap);
+    const int tot = ids ? ids[0] : na * cap;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < tot; k += gridDim.x * blockDim.x) {
+        const int t = ids ? ids[1 + k] : k;
+        const int c = t / cap, jn = t - c * cap;
         const int m = cnt[c];
         if (jn >= m) continue;
         const Slot q = sl[t];
@@ -337,16 +339,17 @@ __device__ __forceinline__ void three_body_sl(double* __restrict__ F, const Slot
 __global__ void __launch_bounds__(256)
 k_rebo_force(const Slot* __restrict__ sl, const SlotBO* __restrict__ bo, const int* __restrict__ cnt,
              const int* __restrict__ list, int cap, int na, double* __restrict__ F, double* __restrict__ part,
-             const int* __restrict__ gate, int want) {
+             const int* __restrict__ gate, int want, const int* __restrict__ ids) {
     FMD_PDL_WAIT();
     if (gate != nullptr && *gate != want) return;
     __shared__ double sm[32 * kNV];
     double acc[kNV];
 #pragma unroll
     for (int k = 0; k < kNV; k++) acc[k] = 0.0;
-    const long long tot = (long long)na * cap;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(t / cap), jn = (int)(t % cap);
+    const int tot = ids ? ids[0] : na * cap;
+    for (int kk = blockIdx.x * blockDim.x + threadIdx.x; kk < tot; kk += gridDim.x * blockDim.x) {
+        const int t = ids ? ids[1 + kk] : kk;
+        const int i = t / cap, jn = t - i * cap;
         const int m = cnt[i];
         if (jn >= m) continue;
         const SlotBO o = bo[t];
@@ -708,19 +711,92 @@ cudaError_t rebo_launch_gated(const double* pos, const double* hh, const int* cn
 
 cudaError_t rebo_slots_launch(const double* pos, const double* hh, const int* cnt, const int* list, int cap,
                               int na, double* slots, double* F, double* part, int nblocks, const int* gate,
-                              int want, cudaStream_t st) {
+                              int want, cudaStream_t st, const int* ids) {
     Slot* sl = reinterpret_cast<Slot*>(slots);
     SlotBO* bo = reinterpret_cast<SlotBO*>(slots + (size_t)na * cap * 8);
     cudaError_t e;
     if ((e = launch_pdl(k_rebo_slots, dim3(kForceBlocks), dim3(256), 0, st, pos, hh, cnt, list, cap, na, sl, gate,
-                        want)) != cudaSuccess)
+                        want, ids)) != cudaSuccess)
         return e;
     if ((e = launch_pdl(k_rebo_bo, dim3(kForceBlocks), dim3(256), 0, st, (const Slot*)sl, cnt, list, cap, na, bo, gate,
-                        want)) != cudaSuccess)
+                        want, ids)) != cudaSuccess)
         return e;
     if ((e = launch_pdl(k_rebo_force, dim3(nblocks), dim3(256), 0, st, (const Slot*)sl, (const SlotBO*)bo, cnt, list,
-                        cap, na, F, part, gate, want)) != cudaSuccess)
+                        cap, na, F, part, gate, want, ids)) != cudaSuccess)
         return e;
+    return cudaGetLastError();
+}
+
+namespace {
+
+// Occupied slots of a REBO list in atom-major order: per 1024-atom block the
+// slot count, then each block's offset (sum of the earlier blocks) and an
+// in-block exclusive scan place atom i's slots i * cap + jn, jn < cnt[i].
+constexpr int kIdsBlock = 1024;
+
+__global__ void __launch_bounds__(kIdsBlock) k_ids_count(const int* __restrict__ cnt, int cap, int n,
+                                                          int* __restrict__ bsum) {
+    __shared__ int sw[kIdsBlock / 32];
+    const int i = blockIdx.x * kIdsBlock + threadIdx.x;
+    int v = i < n ? min(cnt[i], cap) : 0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    if ((threadIdx.x & 31) == 0) sw[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        int u = sw[threadIdx.x];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) u += __shfl_xor_sync(kFull, u, o);
+        if (threadIdx.x == 0) bsum[blockIdx.x] = u;
+    }
+}
+
+__global__ void __launch_bounds__(kIdsBlock) k_ids_emit(const int* __restrict__ cnt, int cap, int n,
+                                                         const int* __restrict__ bsum, int* __restrict__ ids) {
+    __shared__ int sw[kIdsBlock / 32];
+    __shared__ int s_base;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (w == 0) {                                  // offset of this block
+        int b = 0;
+        for (int k = lane; k < (int)blockIdx.x; k += 32) b += bsum[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) b += __shfl_xor_sync(kFull, b, o);
+        if (lane == 0) s_base = b;
+    }
+    const int i = blockIdx.x * kIdsBlock + threadIdx.x;
+    const int m = i < n ? min(cnt[i], cap) : 0;
+    int x = m;                                     // inclusive warp scan
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(kFull, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) sw[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int y = sw[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int z = __shfl_up_sync(kFull, y, o);
+            if (lane >= o) y += z;
+        }
+        sw[lane] = y;                              // inclusive over warps
+    }
+    __syncthreads();
+    const int off = s_base + (w > 0 ? sw[w - 1] : 0) + x - m;
+    for (int jn = 0; jn < m; jn++) ids[1 + off + jn] = i * cap + jn;
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == kIdsBlock - 1) ids[0] = off + m;
+}
+
+}  // namespace
+
+int rebo_ids_scratch(int n) { return (n + kIdsBlock - 1) / kIdsBlock; }
+
+cudaError_t rebo_ids_build(const int* cnt, int cap, int n, int* ids, int* bsum, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    const int nb = rebo_ids_scratch(n);
+    k_ids_count<<<nb, kIdsBlock, 0, st>>>(cnt, cap, n, bsum);
+    k_ids_emit<<<nb, kIdsBlock, 0, st>>>(cnt, cap, n, bsum, ids);
     return cudaGetLastError();
 }
 

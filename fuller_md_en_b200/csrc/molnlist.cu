@@ -236,6 +236,98 @@ k_mol_rows(const double* __restrict__ pos, const double* __restrict__ hh, int n,
     }
 }
 
+// Half-list rows when every molecule has S atoms: atom i's candidates are the
+// atoms of its partner molecules above its own, ascending, i.e. candidate k
+// is atom k mod S of the (k div S)-th such partner.  The partners' first atoms
+// go to shared memory once per atom, and the warp walks the candidates as one
+// sequence, 32 * kFlatU at a time, so each lane has kFlatU candidate loads in
+// flight instead of a dependent partner lookup per molecule.  Same test, order
+// and truncation as k_mol_rows<0>.  k div S is (k + 0.5) * fl(1/S) truncated:
+// the quotient's fractional part stays 0.5/S from an integer, and the FP32
+// product's relative error (<= 2^-23) cannot cross that for k < 4e6.
+constexpr int kFlatU = 4;
+constexpr int kFlatWarps = 8;
+
+__global__ void __launch_bounds__(32 * kFlatWarps)
+k_mol_half_flat(const double* __restrict__ pos, const double* __restrict__ hh, int n, const int* __restrict__ off,
+                const int* __restrict__ amol, const int* __restrict__ npart, const int* __restrict__ part, int pmax,
+                int S, const float4* __restrict__ pos32, double rc2, int cap, int* __restrict__ cnt,
+                int* __restrict__ list, int* __restrict__ dropped, const int* __restrict__ flag) {
+    if (flag[0] == 0) return;
+    __shared__ double s_hh[18];
+    __shared__ int s_start[kFlatWarps][kMolPartners];
+    if (threadIdx.x < 18) s_hh[threadIdx.x] = hh[threadIdx.x];
+    __syncthreads();
+    const double* h = s_hh;
+    const double* hi = s_hh + 9;
+    const bool diag = diag_cell(h, hi);
+    const Screen sc = make_screen(h, hi, diag, rc2);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned below = (1u << lane) - 1u;
+    int* st = s_start[w];
+    const float invS = 1.0f / (float)S;
+    for (int i = blockIdx.x * kFlatWarps + w; i < n; i += gridDim.x * kFlatWarps) {
+        const int A = amol[i];
+        const int np = npart[A];
+        const int* pa = part + (size_t)A * pmax;
+        int nup = 0;
+        for (int q0 = 0; q0 < np; q0 += 32) {
+            const int q = q0 + lane;
+            const int B = q < np ? pa[q] : -1;
+            const bool up = B > A;
+            const unsigned m = __ballot_sync(kFull, up);
+            if (up) st[nup + __popc(m & below)] = off[B];
+            nup += __popc(m);
+        }
+        __syncwarp();
+        const int ncand = nup * S;
+        const float4 pi = pos32[i];
+        const bool screen = sc.on && pi.w != 0.0f;
+        int* row = list + (size_t)i * cap;
+        int emitted = 0;
+        for (int k0 = 0; k0 < ncand; k0 += 32 * kFlatU) {
+            int jj[kFlatU];
+            float4 q[kFlatU];
+#pragma unroll
+            for (int u = 0; u < kFlatU; u++) {
+                const int k = k0 + 32 * u + lane;
+                jj[u] = -1;
+                if (k < ncand) {
+                    const int pk = (int)(((float)k + 0.5f) * invS);
+                    jj[u] = st[pk] + (k - pk * S);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kFlatU; u++) q[u] = jj[u] >= 0 ? pos32[jj[u]] : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+            for (int u = 0; u < kFlatU; u++) {
+                bool ok = jj[u] >= 0;
+                if (ok) {
+                    if (screen && q[u].w != 0.0f) {
+                        float dx = q[u].x - pi.x, dy = q[u].y - pi.y, dz = q[u].z - pi.z;
+                        dx = fmaf(-sc.L[0], rintf(dx * sc.Li[0]), dx);
+                        dy = fmaf(-sc.L[1], rintf(dy * sc.Li[1]), dy);
+                        dz = fmaf(-sc.L[2], rintf(dz * sc.Li[2]), dz);
+                        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                        ok = r2 < sc.lo2 ? true : (r2 > sc.hi2 ? false : pair_in(pos, i, jj[u], h, hi, diag, rc2));
+                    } else {
+                        ok = pair_in(pos, i, jj[u], h, hi, diag, rc2);
+                    }
+                }
+                const unsigned m = __ballot_sync(kFull, ok);
+                const int kk = emitted + __popc(m & below);
+                if (ok && kk < cap) row[kk] = jj[u];
+                emitted += __popc(m);
+            }
+        }
+        __syncwarp();                              // st is refilled for the next atom
+        if (lane == 0) {
+            cnt[i] = emitted < cap ? emitted : cap;
+            if (emitted > cap && dropped) atomicAdd(dropped, emitted - cap);
+        }
+    }
+}
+
 constexpr int kRowBlocksMol = kSMs * 8;
 
 }  // namespace
@@ -263,6 +355,9 @@ cudaError_t mol_lists_alloc(MolLists& m, int n, const int* mol_id_host) {
     m.M = M;
     m.pmax = std::min(M, kMolPartners);
     for (int a = 0; a < M; a++) m.max_atoms = std::max(m.max_atoms, off[a + 1] - off[a]);
+    m.usize = m.max_atoms;
+    for (int a = 0; a < M; a++)
+        if (off[a + 1] - off[a] != m.usize) m.usize = 0;
     cudaError_t e;
     auto A = [&](void** p, size_t bytes) {
         if (e == cudaSuccess) e = cudaMalloc(p, bytes);
@@ -311,6 +406,12 @@ cudaError_t mol_rows_intra(const MolLists& m, const double* pos, const double* h
 
 cudaError_t mol_rows_half(const MolLists& m, const double* pos, const double* hh, double rc2, int cap, int* cnt,
                           int* list, int* dropped, cudaStream_t st) {
+    if (m.usize > 0) {
+        k_mol_half_flat<<<kRowBlocksMol, 32 * kFlatWarps, 0, st>>>(pos, hh, m.n, m.off, m.amol, m.npart, m.part,
+                                                                   m.pmax, m.usize, m.pos32, rc2, cap, cnt, list,
+                                                                   dropped, m.flag);
+        return cudaGetLastError();
+    }
     k_mol_rows<0><<<kRowBlocksMol, 256, 0, st>>>(pos, hh, m.n, m.off, m.amol, m.npart, m.part, m.pmax, m.pos32, rc2,
                                                  cap, cnt, list, dropped, m.flag);
     return cudaGetLastError();

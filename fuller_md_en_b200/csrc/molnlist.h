@@ -16,6 +16,7 @@ struct MolLists {
     bool ok = false;          // molecules are contiguous index ranges
     int n = 0, M = 0, pmax = 0;
     int max_atoms = 0;        // atoms of the largest molecule
+    int usize = 0;            // atoms of every molecule when all have the same count, else 0
     int* off = nullptr;       // [M + 1] first atom of each molecule
     int* amol = nullptr;      // [n] molecule of each atom
     double* cen = nullptr;    // [3 M] centres

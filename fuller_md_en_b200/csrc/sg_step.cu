@@ -63,11 +63,11 @@ cudaError_t sg_enqueue_rebo(SgStep& g, const StepArrays& a, bool judge, cudaStre
                                     a.part_f1, st, off);
     if (e != cudaSuccess) return e;
     e = rebo_slots_launch(a.pos, hh, a.cnt_b, a.list_b, a.cap_b, a.n, a.rebo_slots, a.Facc, a.part_f1,
-                          sg::kRowBlocks, off, 1, st);
+                          sg::kRowBlocks, off, 1, st, a.rebo_ids);
     if (e != cudaSuccess || !judge) return e;
     if ((e = cudaMemsetAsync(g.Fj, 0, sizeof(double) * 3 * (size_t)a.n, st)) != cudaSuccess) return e;
     e = rebo_slots_launch(a.pos, hh, a.cnt_b, a.list_b, a.cap_b, a.n, a.rebo_slots, g.Fj, g.part_j, sg::kRowBlocks,
-                          off, 0, st);
+                          off, 0, st, a.rebo_ids);
     if (e != cudaSuccess) return e;
     k_sg_judge<<<1, kJudgeThreads, 0, st>>>(a.S, a.Facc, g.Fj, g.part_j, a.part_f1, 3 * a.n, sg::kRowBlocks,
                                             g.rmse_max);

@@ -103,6 +103,12 @@ int System::alloc_lists(double rc_list_a, int cap_a_, double rc_list_b, int cap_
         if (cells_alloc(cells_b, n, h0, rc_b) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "cell allocation failed");
         if (alloc(&arr.rebo_slots, (size_t)n * cap_b_ * kReboSlotDoubles, (const double*)nullptr))
             return ctx->fail(FMD_ERR_CUDA, "list allocation failed");
+        int* ids;
+        if (alloc(&ids, 1 + (size_t)n * cap_b_, (const int*)nullptr) ||
+            alloc(&rebo_bsum, (size_t)rebo_ids_scratch(n), (const int*)nullptr))
+            return ctx->fail(FMD_ERR_CUDA, "list allocation failed");
+        cudaMemsetAsync(ids, 0, sizeof(int), ctx->stream);
+        arr.rebo_ids = ids;
     }
     if (transpose) {
         arr.in_cap = kInCap + cap_a_;   // full rows: incoming entries then the row itself
@@ -147,6 +153,10 @@ cudaError_t System::enqueue_rebuild(cudaStream_t st) {
                                  ctx->d_err, st)) != cudaSuccess)
                 return e;
         }
+        if (arr.rebo_ids &&
+            (e = rebo_ids_build(arr.cnt_b, arr.cap_b, arr.n, const_cast<int*>(arr.rebo_ids), rebo_bsum, st)) !=
+                cudaSuccess)
+            return e;
     }
     // Half list: the molecule path when valid for this rebuild (decided on
     // the device), else the cell-grid path; both are in the graph, gated.
@@ -610,7 +620,7 @@ extern "C" int fmd_system_kernel_ms(fmd_system* s, int stage, int reps, double* 
                     return sg_enqueue_rebo(*a.sg, a, false, st);
                 if (a.kind == FMD_SYS_AIREBO)
                     return rebo_slots_launch(a.pos, hh, a.cnt_b, a.list_b, a.cap_b, a.n, a.rebo_slots, a.Facc,
-                                             a.part_f1, kForceBlocks, nullptr, 0, st);
+                                             a.part_f1, kForceBlocks, nullptr, 0, st, a.rebo_ids);
                 if (a.kind == FMD_SYS_MM) return mm_bonded_launch(a.topo, a.pos, hh, a.Facc, a.part_f1, st);
                 return rigid_launch(a.precision, a.pos, a.qv, a.body, hh, a.cnt_a, a.list_a, a.cap_a, a.n, a.natom,
                                     a.rmcut2, a.F, a.T, a.part_f1, st, a.rigid_lab, a.rigid_shape);

@@ -23,6 +23,7 @@ struct System {
     double rc_a = 0, rc2_a = 0, rc_b = 0, rc2_b = 0;
     double h0[9] = {0};
     int* dropped = nullptr;            // device: {list a, list b} overflow counts
+    int* rebo_bsum = nullptr;          // device scratch of the REBO slot index build
     bool initialized = false;
     // one graph per {rebuild, cold/warm phase, judge of the learned REBO term}
     cudaGraphExec_t graphs[2][2][2] = {};
