@@ -413,6 +413,12 @@ class System:
                        "fmd_system_forces")
         return F, T, E
 
+    def lj_rows(self):
+        """(full LJ gather row lengths of the last build, pruned row lengths of the last prune)."""
+        full, pruned = np.zeros(self.n, np.int32), np.zeros(self.n, np.int32)
+        self.ctx.check(self.ctx.lib.fmd_system_lj_rows(self.h, _i(full), _i(pruned)), "fmd_system_lj_rows")
+        return full, pruned
+
     def lists(self, cap_a: int, cap_b: int = 0):
         n = self.n
         ca, la = np.zeros(n, np.int32), np.zeros(n * cap_a, np.int32)

@@ -15,8 +15,8 @@
 // the prune is now farther than (1 - k)(rc + delta) - 2u.  While
 // k (rc + delta) + 2u < delta (less a rounding margin) every entry dropped by
 // the prune is still beyond the cutoff, so the pruned rows yield exactly the
-// pairs of the full rows: the same pair terms, summed in the same relative
-// order (only their lane assignment changes).  The drift raises u
+// pairs of the full rows and the same pair terms; only the lanes that add
+// them, and so the rounding of the sums, change.  The drift raises u
 // (kick_body), the decision runs on the device before the gathers, and both
 // gathers sit in the step's graph, each returning at once unless the flag
 // selects it.  A list build marks the next evaluation as a prune.
@@ -60,17 +60,18 @@ __global__ void k_prune_mark(unsigned long long* words) { *words = kPruneMark; }
 cudaError_t lj_prune_alloc(LJPrune& p, int n, int stride, double rc, double delta) {
     p = LJPrune();
     cudaError_t e = cudaSuccess;
-    auto A = [&](void** q, size_t bytes) {
+    auto A = [&](void** q, size_t bytes, bool zero) {
         if (e == cudaSuccess) e = cudaMalloc(q, bytes);
-        if (e == cudaSuccess) e = cudaMemset(*q, 0, bytes);
+        if (e == cudaSuccess && zero) e = cudaMemset(*q, 0, bytes);
     };
-    A((void**)&p.cnt, sizeof(int) * n);
-    A((void**)&p.list, sizeof(int) * (size_t)n * stride);
-    A((void**)&p.sb, sizeof(double) * 3 * n);
-    A((void**)&p.hb, sizeof(double) * 9);
-    A((void**)&p.words, sizeof(unsigned long long));
-    A((void**)&p.flag, sizeof(int));
-    A((void**)&p.stats, sizeof(unsigned long long) * 2);
+    // the rows are written by the first evaluation (a prune) before any read
+    A((void**)&p.cnt, sizeof(int) * n, true);
+    A((void**)&p.list, sizeof(int) * (size_t)n * stride, false);
+    A((void**)&p.sb, sizeof(double) * 3 * n, true);
+    A((void**)&p.hb, sizeof(double) * 9, true);
+    A((void**)&p.words, sizeof(unsigned long long), true);
+    A((void**)&p.flag, sizeof(int), true);
+    A((void**)&p.stats, sizeof(unsigned long long) * 2, true);
     if (e == cudaSuccess) e = cudaMemset(p.words, 0x7F, sizeof(unsigned long long));
     if (e != cudaSuccess) {
         lj_prune_free(p);

@@ -6,6 +6,8 @@
 #include <cmath>
 #include <cstddef>
 #include <cstring>
+#include <cstdio>
+#include <cstdlib>
 #include <map>
 #include <memory>
 #include <tuple>
@@ -186,6 +188,20 @@ cudaError_t System::enqueue_rebuild(cudaStream_t st) {
 int System::tune_lj() {
     static std::map<std::tuple<int, int, int, int, int>, LJShape> cache;
     const int ff = arr.kind == FMD_SYS_AIREBO ? FMD_FF_AIREBO : FMD_FF_MM;
+    // FMD_LJ_SHAPE="threads,unroll,feed" pins the shape (no trial launches),
+    // for reproducible runs and profiler captures.
+    if (const char* env = std::getenv("FMD_LJ_SHAPE")) {
+        LJShape sh;
+        if (std::sscanf(env, "%d,%d,%d", &sh.threads, &sh.unroll, &sh.pipe) == 3 &&
+            (sh.threads == 128 || sh.threads == 256) && (sh.unroll == 2 || sh.unroll == 4) && sh.pipe >= 0 &&
+            sh.pipe <= 2 && lj_gather_blocks(ff, arr.precision, sh, arr.in_cap) > 0) {
+            arr.lj_shape = sh;
+            arr.lj_blocks = lj_gather_blocks(ff, arr.precision, sh, arr.in_cap);
+            return FMD_OK;
+        }
+        return ctx->fail(FMD_ERR_ARG, "FMD_LJ_SHAPE: expected threads,unroll,feed with threads 128|256, "
+                                      "unroll 2|4, feed 0..2");
+    }
     const auto key = std::make_tuple(ctx->device, arr.kind, arr.n, arr.cap_a, arr.precision);
     cudaStream_t st = ctx->stream;
     auto it = cache.find(key);
@@ -583,6 +599,16 @@ extern "C" int fmd_system_forces(fmd_system* s, double* F, double* T, double* E)
     if (T && y.arr.T) cudaMemcpyAsync(T, y.arr.T, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, st);
     if (E) cudaMemcpyAsync(E, y.arr.S->E, sizeof(double) * 8, cudaMemcpyDeviceToHost, st);
     return y.ctx->sync_check("system forces");
+}
+
+extern "C" int fmd_system_lj_rows(fmd_system* s, int* full_cnt, int* pruned_cnt) {
+    if (!s || !s->sys) return FMD_ERR_ARG;
+    fmd::System& y = *s->sys;
+    cudaStream_t st = y.ctx->stream;
+    const size_t n = y.arr.n;
+    if (full_cnt && y.arr.in_cnt) cudaMemcpyAsync(full_cnt, y.arr.in_cnt, sizeof(int) * n, cudaMemcpyDeviceToHost, st);
+    if (pruned_cnt && y.prune.ok) cudaMemcpyAsync(pruned_cnt, y.prune.cnt, sizeof(int) * n, cudaMemcpyDeviceToHost, st);
+    return y.ctx->sync_check("system LJ rows");
 }
 
 extern "C" int fmd_system_lists(fmd_system* s, int* cnt_a, int* list_a, int* cnt_b, int* list_b) {

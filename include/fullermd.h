@@ -244,6 +244,10 @@ int fmd_system_forces(fmd_system *s, double *F, double *T, double *E);
 int fmd_system_virial(fmd_system *s, double *W9, double *KE);
 /* Current neighbour lists (reference layout) for inspection. */
 int fmd_system_lists(fmd_system *s, int *cnt_a, int *list_a, int *cnt_b, int *list_b);
+/* Row lengths of the atomistic LJ gather (n ints each, either may be NULL):
+ * the full rows (incoming entries + the reference row) of the last list build
+ * and the pruned rows of the last prune (see fmd_system_set_lj_prune). */
+int fmd_system_lj_rows(fmd_system *s, int *full_cnt, int *pruned_cnt);
 int fmd_system_destroy(fmd_system *s);
 
 /* Measurement helpers (no reference counterpart).  fmd_system_kernel_ms
