@@ -328,7 +328,23 @@ __device__ __forceinline__ void three_body_sl(double* __restrict__ F, const Slot
     atomic_add3(F, c, fcx, fcy, fcz);
 }
 
-// Forces, one thread per directed slot i -> j.  The reference enumerates
+// Sum of (x, y, z) over the lanes of this lane's segment, left in the segment's
+// lowest lane.  Segments are runs of consecutive lanes (seg: this lane's
+// segment as a lane mask, span: the longest segment of the warp); lane L ends
+// with the sum over L .. its segment's last lane, so the lowest lane holds
+// the whole sum.  Fixed order.
+__device__ __forceinline__ void seg_sum3(double& x, double& y, double& z, unsigned seg, int lane, int span) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        if (o >= span) break;                          // uniform over the warp
+        const double wx = __shfl_down_sync(kFull, x, o);
+        const double wy = __shfl_down_sync(kFull, y, o);
+        const double wz = __shfl_down_sync(kFull, z, o);
+        if (lane + o < 32 && ((seg >> (lane + o)) & 1u)) { x += wx; y += wy; z += wz; }
+    }
+}
+
+// Forces, one lane per directed slot i -> j.  The reference enumerates
 // bonds from the row of the lower index (AI:288) and evaluates the three-body
 // blocks of both ends from their own rows.  Here the slot i -> j does the
 // three-body block of centre i, and for j > i also the pair term; when the
@@ -336,6 +352,13 @@ __device__ __forceinline__ void three_body_sl(double* __restrict__ F, const Slot
 // slot (j > i) also computes b_ji and centre j's block from j's row, and a
 // slot with j < i whose partner is missing does nothing (the reference never
 // visits that bond).
+//
+// The slots of one centre sit in consecutive lanes (atom-major slot order),
+// and at step kn of the three-body loop every one of them pushes a force onto
+// the same neighbour list[i][kn]: the lanes of the centre sum it first
+// (seg_sum) and one lane adds it, and the reactions on the centre and its
+// pair-term forces go out as one sum per centre, so a centre with m bonds
+// issues about m + 1 + m/2 atomic triples instead of m^2 + m/2.
 __global__ void __launch_bounds__(256)
 k_rebo_force(const Slot* __restrict__ sl, const SlotBO* __restrict__ bo, const int* __restrict__ cnt,
              const int* __restrict__ list, int cap, int na, double* __restrict__ F, double* __restrict__ part,
@@ -346,42 +369,90 @@ k_rebo_force(const Slot* __restrict__ sl, const SlotBO* __restrict__ bo, const i
     double acc[kNV];
 #pragma unroll
     for (int k = 0; k < kNV; k++) acc[k] = 0.0;
+    const int lane = threadIdx.x & 31;
     const int tot = ids ? ids[0] : na * cap;
-    for (int kk = blockIdx.x * blockDim.x + threadIdx.x; kk < tot; kk += gridDim.x * blockDim.x) {
-        const int t = ids ? ids[1 + kk] : kk;
+    // warp-uniform loop: the shuffles below need every lane
+    for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < tot; base += gridDim.x * blockDim.x) {
+        const int kk = base + lane;
+        bool valid = kk < tot;
+        const int t = valid ? (ids ? ids[1 + kk] : kk) : 0;
         const int i = t / cap, jn = t - i * cap;
-        const int m = cnt[i];
-        if (jn >= m) continue;
-        const SlotBO o = bo[t];
-        if (o.ok == 0.0) continue;
-        const int j = list[t];
-        const int mj = cnt[j];
-        int pn = -1;                          // partner slot j -> i
-        for (int kn = 0; kn < mj; kn++)
-            if (list[(size_t)j * cap + kn] == i) { pn = kn; break; }
-        if (j < i && pn < 0) continue;
-        const Slot q = sl[t];
-        three_body_sl(F, sl, list, cap, i, m, j, q.dx, q.dy, q.dz, q.rinv, o.coeff);
-        if (j < i) continue;
-        double bji;
-        if (pn >= 0) {
-            bji = bo[(size_t)j * cap + pn].b;
-        } else {
-            const double gji = bo_sum_sl(sl, list, cap, j, mj, i, -q.dx, -q.dy, -q.dz, q.rinv);
-            bji = 1.0 / sqrt(1.0 + gji);
-            three_body_sl(F, sl, list, cap, j, mj, i, -q.dx, -q.dy, -q.dz, q.rinv,
-                          three_body_coeff(gji, bji, q.fc, o.va));
+        const int m = valid ? cnt[i] : 0;
+        valid = valid && jn < m;
+        bool ok = false;
+        SlotBO o;
+        o.b = o.g = o.coeff = o.vr = o.dvr = o.va = o.dva = o.ok = 0.0;
+        if (valid) {
+            o = bo[t];
+            ok = o.ok != 0.0;
         }
-        const double bbar = 0.5 * (o.b + bji);
-        acc[0] += q.fc * (o.vr - bbar * o.va);
-        const double fpair = (q.dfc * (o.vr - bbar * o.va) + q.fc * (o.dvr - bbar * o.dva)) * q.rinv;
-        atomic_add3(F, i, fpair * q.dx, fpair * q.dy, fpair * q.dz);
-        atomic_add3(F, j, -fpair * q.dx, -fpair * q.dy, -fpair * q.dz);
-        const double d[3] = {q.dx, q.dy, q.dz};
+        int j = -1, pn = -1, mj = 0;
+        if (ok) {
+            j = list[t];
+            mj = cnt[j];
+            for (int kn = 0; kn < mj; kn++)   // partner slot j -> i
+                if (list[(size_t)j * cap + kn] == i) { pn = kn; break; }
+            if (j < i && pn < 0) ok = false;
+        }
+        Slot q;
+        q.dx = q.dy = q.dz = q.r = q.rinv = q.fc = q.dfc = q.pad = 0.0;
+        if (ok) q = sl[t];
+        // lanes of one centre (a lane that is not a slot is alone)
+        const unsigned seg = __match_any_sync(kFull, valid ? i : -1 - lane);
+        const bool lead = lane == __ffs(seg) - 1;
+        const int span = __reduce_max_sync(kFull, (unsigned)__popc(seg));
+        double fcx = 0.0, fcy = 0.0, fcz = 0.0;      // force on the centre i from this slot
+        // three-body block of centre i for the bond i -> j (AI:368-419)
+        const bool tb = ok && o.coeff != 0.0;
+        const double ux = q.dx * q.rinv, uy = q.dy * q.rinv, uz = q.dz * q.rinv;
+        const int mseg = __reduce_max_sync(kFull, valid ? m : 0);
+        for (int kn = 0; kn < mseg; kn++) {
+            double fx = 0.0, fy = 0.0, fz = 0.0;
+            int kt = -1;
+            if (valid && kn < m) {
+                const size_t off = (size_t)i * cap + kn;
+                kt = list[off];
+                if (tb && kt != j) {
+                    const Slot r = sl[off];
+                    if (!(r.fc < 1e-15)) {
+                        const double rx = r.dx * r.rinv, ry = r.dy * r.rinv, rz = r.dz * r.rinv;
+                        const double ct = clamp1((q.dx * r.dx + q.dy * r.dy + q.dz * r.dz) * (q.rinv * r.rinv));
+                        double gv, dgv;
+                        ang_g_dg(ct, gv, dgv);
+                        const double a1 = o.coeff * r.dfc * gv, a2 = o.coeff * r.fc * dgv;
+                        fx = a1 * rx + a2 * ((ux - ct * rx) * r.rinv);
+                        fy = a1 * ry + a2 * ((uy - ct * ry) * r.rinv);
+                        fz = a1 * rz + a2 * ((uz - ct * rz) * r.rinv);
+                        fcx -= fx; fcy -= fy; fcz -= fz;
+                    }
+                }
+            }
+            seg_sum3(fx, fy, fz, seg, lane, span);
+            if (lead && kt >= 0 && (fx != 0.0 || fy != 0.0 || fz != 0.0)) atomic_add3(F, kt, fx, fy, fz);
+        }
+        if (ok && j > i) {
+            double bji;
+            if (pn >= 0) {
+                bji = bo[(size_t)j * cap + pn].b;
+            } else {
+                const double gji = bo_sum_sl(sl, list, cap, j, mj, i, -q.dx, -q.dy, -q.dz, q.rinv);
+                bji = 1.0 / sqrt(1.0 + gji);
+                three_body_sl(F, sl, list, cap, j, mj, i, -q.dx, -q.dy, -q.dz, q.rinv,
+                              three_body_coeff(gji, bji, q.fc, o.va));
+            }
+            const double bbar = 0.5 * (o.b + bji);
+            acc[0] += q.fc * (o.vr - bbar * o.va);
+            const double fpair = (q.dfc * (o.vr - bbar * o.va) + q.fc * (o.dvr - bbar * o.dva)) * q.rinv;
+            fcx += fpair * q.dx; fcy += fpair * q.dy; fcz += fpair * q.dz;
+            atomic_add3(F, j, -fpair * q.dx, -fpair * q.dy, -fpair * q.dz);
+            const double d[3] = {q.dx, q.dy, q.dz};
 #pragma unroll
-        for (int a = 0; a < 3; a++)
+            for (int a = 0; a < 3; a++)
 #pragma unroll
-            for (int b = 0; b < 3; b++) acc[1 + a * 3 + b] -= d[a] * fpair * d[b];
+                for (int b = 0; b < 3; b++) acc[1 + a * 3 + b] -= d[a] * fpair * d[b];
+        }
+        seg_sum3(fcx, fcy, fcz, seg, lane, span);
+        if (lead && valid && (fcx != 0.0 || fcy != 0.0 || fcz != 0.0)) atomic_add3(F, i, fcx, fcy, fcz);
     }
     block_sum_store<kNV>(acc, sm, part + (size_t)blockIdx.x * kNV);
 }
