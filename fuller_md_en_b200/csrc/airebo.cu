@@ -588,6 +588,7 @@ __device__ __forceinline__ void lj_gather_body(const double* __restrict__ pos, c
         }
         lj_atom_done(i, fx, fy, fz, px, py, pz, hi, F, Facc, po, pc, lane);
     }
+    lj_virial_mirror<FULL_VIRIAL>(acc);
     block_sum_store<kNV>(acc, sm, part + (size_t)blk * kNV);
 }
 
@@ -698,6 +699,7 @@ __device__ __forceinline__ void lj_gather_staged_body(const double* __restrict__
     }
     // after an early exit, the copy issued for the next atom may still be in flight
     if (pending) umma::mbar_wait(&mb[cur ^ 1], (cur ^ 1) ? ph1 : ph0);
+    lj_virial_mirror<FULL_VIRIAL>(acc);
     block_sum_store<kNV>(acc, sm, part + (size_t)blk * kNV);
 }
 

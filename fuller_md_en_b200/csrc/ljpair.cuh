@@ -69,6 +69,10 @@ struct LJF {
 // reference's arithmetic (AI:447-466).  FP32: the pair algebra (1/r^2, s^6,
 // s^12, fm) in FP32; the minimum image, r^2, the force, energy and virial
 // accumulation stay FP64.  COUNT: this side counts energy and virial.
+// FULL_VIRIAL (AIREBO's vir9, AI:455-466): the pair tensor d fm d^T is
+// symmetric, so only its six distinct entries are accumulated, in acc[1],
+// acc[2], acc[3], acc[5], acc[6], acc[9] (row-major W at acc[1..9]);
+// lj_virial_mirror fills the lower triangle before the block sum.
 template <bool FULL_VIRIAL, bool F32, bool COUNT>
 __device__ __forceinline__ void lj_pair(double dx, double dy, double dz, const LJP& p, const LJF& pf,
                                         double& fx, double& fy, double& fz, double* acc) {
@@ -86,21 +90,28 @@ __device__ __forceinline__ void lj_pair(double dx, double dy, double dz, const L
         fm = p.c24 * (2 * s12 - s6) * ri2;
         if (COUNT) e = p.c4 * (s12 - s6) - p.vshift;
     }
+    if (COUNT && FULL_VIRIAL) {
+        const double gx = fm * dx, gy = fm * dy, gz = fm * dz;
+        fx -= gx; fy -= gy; fz -= gz;
+        acc[0] += e;
+        acc[1] += dx * gx; acc[2] += dx * gy; acc[3] += dx * gz;
+        acc[5] += dy * gy; acc[6] += dy * gz;
+        acc[9] += dz * gz;
+        return;
+    }
     fx -= fm * dx; fy -= fm * dy; fz -= fm * dz;
     if (COUNT) {
         acc[0] += e;
-        if (FULL_VIRIAL) {
-            const double d[3] = {dx, dy, dz};
-#pragma unroll
-            for (int a = 0; a < 3; a++)
-#pragma unroll
-                for (int b = 0; b < 3; b++) acc[1 + a * 3 + b] += d[a] * fm * d[b];
-        } else {
-            acc[1] += dx * fm * dx;
-            acc[5] += dy * fm * dy;
-            acc[9] += dz * fm * dz;
-        }
+        acc[1] += dx * fm * dx;
+        acc[5] += dy * fm * dy;
+        acc[9] += dz * fm * dz;
     }
+}
+
+// Lower triangle of the symmetric virial accumulated by lj_pair<true, ...>.
+template <bool FULL_VIRIAL>
+__device__ __forceinline__ void lj_virial_mirror(double* acc) {
+    if (FULL_VIRIAL) { acc[4] = acc[2]; acc[7] = acc[3]; acc[8] = acc[6]; }
 }
 
 }  // namespace
