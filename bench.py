@@ -222,7 +222,7 @@ def run_ours(args, ws, rank, local):
                 "lj_prune_fraction": prune["prunes"] / max(1, prune["evaluations"]), "rebo": stages["rebo"],
                 "list_rebuild": stages["list_rebuild"] / NLUP}
     full_bytes, lj_bytes, n_full, n_pruned = list_bytes(sysd, na)
-    lj_shape = sysd.lj_shape()
+    lj_shape = {"full_rows": sysd.lj_shape(), "pruned_rows": sysd.lj_shape_pruned()}
     peak, peak_src = peaks()
     achieved = lj_bytes / (stages["lj_gather_pruned"] / 1e3) / 1e9
     traffic = None

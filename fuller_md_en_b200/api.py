@@ -453,6 +453,13 @@ class System:
         self.ctx.check(self.ctx.lib.fmd_system_lj_shape(self.h, *[ctypes.byref(x) for x in v]), "fmd_system_lj_shape")
         return dict(zip(("threads", "unroll", "pipelined", "blocks"), (x.value for x in v)))
 
+    def lj_shape_pruned(self) -> dict:
+        """Launch shape of the LJ gather over the pruned rows (tuned on them at init)."""
+        v = [ctypes.c_int(0) for _ in range(3)]
+        self.ctx.check(self.ctx.lib.fmd_system_lj_shape_pruned(self.h, *[ctypes.byref(x) for x in v]),
+                       "fmd_system_lj_shape_pruned")
+        return dict(zip(("threads", "unroll", "feed"), (x.value for x in v)))
+
     def set_lj_shape(self, threads: int, unroll: int, feed: int) -> None:
         """Pins the LJ gather's launch shape (feed 0 plain, 1 pipelined, 2 staged rows)."""
         self.ctx.check(self.ctx.lib.fmd_system_set_lj_shape(self.h, threads, unroll, feed), "fmd_system_set_lj_shape")

@@ -102,7 +102,8 @@ int rebo_ids_scratch(int n);
 // the whole grid returns at once unless *gate == want.  po.cnt non-null: a
 // pruning gather, which also writes per atom i the entries of its row with
 // r^2 <= po.r2 now, in row order, to po.list + i * in_cap (po.cnt[i] of them)
-// and its fractional position to po.sb (ljprune.cu).
+// and its fractional position to po.sb (ljprune.cu).  nrec > grid: the
+// records grid .. nrec-1 are written as zeros.
 struct LJShape {
     int threads = 256, unroll = 4, pipe = 0;
 };
@@ -118,7 +119,7 @@ cudaError_t lj_gather_launch(int ff, const double* pos, const double* hh, const 
                              int in_cap, int na, double* F, double* Facc, double* part,
                              cudaStream_t st, int precision = FMD_PREC_FP64, const LJShape& shape = LJShape{},
                              DevErr* err = nullptr, const int* gate = nullptr, int want = 0,
-                             const LJPruneOut& po = LJPruneOut{});
+                             const LJPruneOut& po = LJPruneOut{}, int nrec = 0);
 // Rigid site-site LJ (a5-a6): writes F, T; per-block {E, W9} partials (grid n).
 // lab (may be null): scratch of n * natom * 4 doubles for the lab-frame sites;
 // with it (and natom <= 64) the warp-per-neighbour kernel runs, in launch

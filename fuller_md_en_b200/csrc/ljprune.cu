@@ -57,12 +57,12 @@ __global__ void k_prune_mark(unsigned long long* words) { *words = kPruneMark; }
 
 }  // namespace
 
-cudaError_t lj_prune_alloc(LJPrune& p, int n, int stride, double rc, double delta) {
+cudaError_t lj_prune_alloc(LJPrune& p, int n, int stride, double rc, double delta, cudaStream_t st) {
     p = LJPrune();
     cudaError_t e = cudaSuccess;
     auto A = [&](void** q, size_t bytes, bool zero) {
         if (e == cudaSuccess) e = cudaMalloc(q, bytes);
-        if (e == cudaSuccess && zero) e = cudaMemset(*q, 0, bytes);
+        if (e == cudaSuccess && zero) e = cudaMemsetAsync(*q, 0, bytes, st);
     };
     // the rows are written by the first evaluation (a prune) before any read
     A((void**)&p.cnt, sizeof(int) * n, true);
@@ -72,7 +72,7 @@ cudaError_t lj_prune_alloc(LJPrune& p, int n, int stride, double rc, double delt
     A((void**)&p.words, sizeof(unsigned long long), true);
     A((void**)&p.flag, sizeof(int), true);
     A((void**)&p.stats, sizeof(unsigned long long) * 2, true);
-    if (e == cudaSuccess) e = cudaMemset(p.words, 0x7F, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemsetAsync(p.words, 0x7F, sizeof(unsigned long long), st);
     if (e != cudaSuccess) {
         lj_prune_free(p);
         return e;

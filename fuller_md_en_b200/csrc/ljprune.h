@@ -25,7 +25,9 @@ struct LJPrune {
     unsigned long long* stats = nullptr;  // [2] {force evaluations, prune evaluations}
 };
 
-cudaError_t lj_prune_alloc(LJPrune& p, int n, int stride, double rc, double delta);
+// The small arrays are cleared on st; the row buffer is written by the first
+// evaluation (a prune) before any read.
+cudaError_t lj_prune_alloc(LJPrune& p, int n, int stride, double rc, double delta, cudaStream_t st);
 void lj_prune_free(LJPrune& p);
 // After a list build (and at set-up): the next evaluation prunes.
 cudaError_t lj_prune_mark(const LJPrune& p, cudaStream_t st);

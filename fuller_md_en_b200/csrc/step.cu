@@ -481,16 +481,17 @@ cudaError_t enqueue_lj(const StepArrays& a, int ff, cudaStream_t st) {
     const double* hh = a.S->h;
     if (!a.prune || a.prune->delta <= 0.0)
         return lj_gather_launch(ff, a.pos, hh, a.cnt_a, a.list_a, a.cap_a, a.in_cnt, a.in_list, a.in_cap, a.n, a.F,
-                                a.Facc, a.part_f2, st, a.precision, a.lj_shape, a.err);
+                                a.Facc, a.part_f2, st, a.precision, a.lj_shape, a.err, nullptr, 0, LJPruneOut{},
+                                a.lj_blocks);
     const LJPrune& q = *a.prune;
     cudaError_t e;
     if ((e = lj_prune_decide(q, hh, st)) != cudaSuccess) return e;
     if ((e = lj_gather_launch(ff, a.pos, hh, a.cnt_a, a.list_a, a.cap_a, a.in_cnt, a.in_list, a.in_cap, a.n, a.F,
-                              a.Facc, a.part_f2, st, a.precision, a.lj_shape, a.err, q.flag, 1, lj_prune_out(q))) !=
-        cudaSuccess)
+                              a.Facc, a.part_f2, st, a.precision, a.lj_shape, a.err, q.flag, 1, lj_prune_out(q),
+                              a.lj_blocks)) != cudaSuccess)
         return e;
     return lj_gather_launch(ff, a.pos, hh, a.cnt_a, a.list_a, a.cap_a, q.cnt, q.list, a.in_cap, a.n, a.F, a.Facc,
-                            a.part_f2, st, a.precision, a.lj_shape, a.err, q.flag, 0);
+                            a.part_f2, st, a.precision, a.lj_shape_p, a.err, q.flag, 0, LJPruneOut{}, a.lj_blocks);
 }
 
 cudaError_t enqueue_forces(const StepArrays& a, cudaStream_t st, bool judge) {

@@ -58,9 +58,10 @@ struct StepArrays {
     double* rigid_lab = nullptr;   // [n * natom * kRigidLabDoubles] lab-frame sites (rigid)
     int rigid_shape = 0;           // launch shape of the rigid pair kernel (rigid_launch)
     int precision = FMD_PREC_FP64;
-    LJShape lj_shape{};            // launch shape of the atomistic LJ gather
+    LJShape lj_shape{};            // launch shape of the atomistic LJ gather over the full rows
+    LJShape lj_shape_p{};          // ... and over the pruned rows
     DevErr* err = nullptr;         // device error word (bounded waits of staged kernels)
-    int lj_blocks = 0;             // its grid = partial records in part_f2
+    int lj_blocks = 0;             // partial records in part_f2: the larger grid of the two gathers
     SgStep* sg = nullptr;          // AIREBO: learned REBO term instead of the plain kernel
     int rebo_blocks = kForceBlocks;  // partial records the REBO term writes into part_f1
     // Pruned LJ rows (AIREBO, MM): host descriptor (nullptr: full rows every

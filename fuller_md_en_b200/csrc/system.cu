@@ -124,7 +124,7 @@ int System::alloc_lists(double rc_list_a, int cap_a_, double rc_list_b, int cap_
 // Rebuild of every list this kind uses, as the driver does at gstep % nlup == 0.
 int System::alloc_prune(double rc_lj) {
     if (!arr.in_list) return FMD_OK;
-    if (lj_prune_alloc(prune, arr.n, arr.in_cap, rc_lj, kPruneDelta) != cudaSuccess)
+    if (lj_prune_alloc(prune, arr.n, arr.in_cap, rc_lj, kPruneDelta, ctx->stream) != cudaSuccess)
         return ctx->fail(FMD_ERR_CUDA, "device allocation failed");
     arr.prune = &prune;
     arr.prune_sb = prune.sb;
@@ -185,77 +185,120 @@ cudaError_t System::enqueue_rebuild(cudaStream_t st) {
 // block, list entries in flight per lane, software pipelining) is timed on
 // this system's own lists at set-up and the fastest kept; the choice is
 // cached per (device, kind, atoms, list width, precision) for the process.
+// Times every launch shape of the atomistic LJ gather over the rows
+// (rcnt, rlist; stride in_cap) and returns the fastest.  Each candidate is
+// timed right after a write larger than L2, as the gather runs inside a step
+// whose other kernels have evicted its rows; the runs accumulate into the
+// scratch accumulator, which is cleared afterwards.
+LJShape System::pick_lj_shape(const int* rcnt, const int* rlist, int& rc) {
+    const int ff = arr.kind == FMD_SYS_AIREBO ? FMD_FF_AIREBO : FMD_FF_MM;
+    cudaStream_t st = ctx->stream;
+    void* flush = nullptr;
+    const size_t flush_bytes = 160u << 20;
+    if (cudaMalloc(&flush, flush_bytes) != cudaSuccess) {
+        cudaGetLastError();
+        flush = nullptr;
+    }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float best = 1e30f;
+    LJShape pick;
+    for (int nt : {128, 256})
+        for (int u : {2, 4})
+            for (int pipe : {0, 1, 2}) {
+                const LJShape sh{nt, u, pipe};
+                if (lj_gather_blocks(ff, arr.precision, sh, arr.in_cap) < 1) continue;
+                auto go = [&]() {
+                    return lj_gather_launch(ff, arr.pos, arr.S->h, arr.cnt_a, arr.list_a, arr.cap_a, rcnt, rlist,
+                                            arr.in_cap, arr.n, arr.Facc, arr.Facc, arr.part_f2, st, arr.precision,
+                                            sh, ctx->d_err);
+                };
+                go();
+                float tot = 0.f;
+                for (int r = 0; r < 3; r++) {
+                    if (flush) cudaMemsetAsync(flush, r, flush_bytes, st);
+                    cudaEventRecord(e0, st);
+                    go();
+                    cudaEventRecord(e1, st);
+                    cudaEventSynchronize(e1);
+                    float ms = 0.f;
+                    cudaEventElapsedTime(&ms, e0, e1);
+                    tot += ms;
+                }
+                if (tot < best) { best = tot; pick = sh; }
+            }
+    if (flush) cudaFree(flush);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaMemsetAsync(arr.Facc, 0, sizeof(double) * 3 * (size_t)arr.n, st);
+    rc = ctx->sync_check("LJ launch-shape tuning");
+    return pick;
+}
+
+// Partial records of the LJ term: the larger grid of the two gathers (the
+// smaller one zero-fills the rest).
+void System::set_lj_blocks() {
+    const int ff = arr.kind == FMD_SYS_AIREBO ? FMD_FF_AIREBO : FMD_FF_MM;
+    arr.lj_blocks = std::max(lj_gather_blocks(ff, arr.precision, arr.lj_shape, arr.in_cap),
+                             lj_gather_blocks(ff, arr.precision, arr.lj_shape_p, arr.in_cap));
+}
+
+// Launch shape of the atomistic LJ gather over the full rows: every candidate
+// (threads per block, list entries in flight per lane, row feed) is timed on
+// this system's own rows at set-up and the fastest kept; the choice is cached
+// per (device, kind, atoms, list width, precision) for the process.  The
+// gather over the pruned rows is tuned the same way once those rows exist
+// (tune_lj_pruned).
 int System::tune_lj() {
     static std::map<std::tuple<int, int, int, int, int>, LJShape> cache;
     const int ff = arr.kind == FMD_SYS_AIREBO ? FMD_FF_AIREBO : FMD_FF_MM;
-    // FMD_LJ_SHAPE="threads,unroll,feed" pins the shape (no trial launches),
-    // for reproducible runs and profiler captures.
+    // FMD_LJ_SHAPE="threads,unroll,feed" pins the shape of both gathers (no
+    // trial launches), for reproducible runs and profiler captures.
     if (const char* env = std::getenv("FMD_LJ_SHAPE")) {
         LJShape sh;
         if (std::sscanf(env, "%d,%d,%d", &sh.threads, &sh.unroll, &sh.pipe) == 3 &&
             (sh.threads == 128 || sh.threads == 256) && (sh.unroll == 2 || sh.unroll == 4) && sh.pipe >= 0 &&
             sh.pipe <= 2 && lj_gather_blocks(ff, arr.precision, sh, arr.in_cap) > 0) {
             arr.lj_shape = sh;
-            arr.lj_blocks = lj_gather_blocks(ff, arr.precision, sh, arr.in_cap);
+            arr.lj_shape_p = sh;
+            set_lj_blocks();
             return FMD_OK;
         }
         return ctx->fail(FMD_ERR_ARG, "FMD_LJ_SHAPE: expected threads,unroll,feed with threads 128|256, "
                                       "unroll 2|4, feed 0..2");
     }
     const auto key = std::make_tuple(ctx->device, arr.kind, arr.n, arr.cap_a, arr.precision);
-    cudaStream_t st = ctx->stream;
     auto it = cache.find(key);
     if (it != cache.end()) {
         arr.lj_shape = it->second;
     } else {
-        // Each candidate is timed right after a write larger than L2, as the
-        // gather runs inside a step whose other kernels have evicted its rows.
-        void* flush = nullptr;
-        const size_t flush_bytes = 160u << 20;
-        if (cudaMalloc(&flush, flush_bytes) != cudaSuccess) {
-            cudaGetLastError();
-            flush = nullptr;
-        }
-        cudaEvent_t e0, e1;
-        cudaEventCreate(&e0);
-        cudaEventCreate(&e1);
-        float best = 1e30f;
-        LJShape pick;
-        for (int nt : {128, 256})
-            for (int u : {2, 4})
-                for (int pipe : {0, 1, 2}) {
-                    const LJShape sh{nt, u, pipe};
-                    if (lj_gather_blocks(ff, arr.precision, sh, arr.in_cap) < 1) continue;
-                    auto go = [&]() {
-                        return lj_gather_launch(ff, arr.pos, arr.S->h, arr.cnt_a, arr.list_a, arr.cap_a, arr.in_cnt,
-                                                arr.in_list, arr.in_cap, arr.n, arr.Facc, arr.Facc, arr.part_f2, st,
-                                                arr.precision, sh, ctx->d_err);
-                    };
-                    go();
-                    float tot = 0.f;
-                    for (int r = 0; r < 3; r++) {
-                        if (flush) cudaMemsetAsync(flush, r, flush_bytes, st);
-                        cudaEventRecord(e0, st);
-                        go();
-                        cudaEventRecord(e1, st);
-                        cudaEventSynchronize(e1);
-                        float ms = 0.f;
-                        cudaEventElapsedTime(&ms, e0, e1);
-                        tot += ms;
-                    }
-                    if (tot < best) { best = tot; pick = sh; }
-                }
-        if (flush) cudaFree(flush);
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
-        // the timing runs accumulated into Facc
-        cudaMemsetAsync(arr.Facc, 0, sizeof(double) * 3 * (size_t)arr.n, st);
-        const int rc = ctx->sync_check("LJ launch-shape tuning");
+        int rc = FMD_OK;
+        const LJShape pick = pick_lj_shape(arr.in_cnt, arr.in_list, rc);
         if (rc != FMD_OK) return rc;
         cache[key] = pick;
         arr.lj_shape = pick;
     }
-    arr.lj_blocks = lj_gather_blocks(ff, arr.precision, arr.lj_shape, arr.in_cap);
+    arr.lj_shape_p = arr.lj_shape;
+    set_lj_blocks();
+    return FMD_OK;
+}
+
+int System::tune_lj_pruned() {
+    static std::map<std::tuple<int, int, int, int, int>, LJShape> cache;
+    if (!prune.ok || prune.delta <= 0.0 || std::getenv("FMD_LJ_SHAPE")) return FMD_OK;
+    const auto key = std::make_tuple(ctx->device, arr.kind, arr.n, arr.cap_a, arr.precision);
+    auto it = cache.find(key);
+    if (it != cache.end()) {
+        arr.lj_shape_p = it->second;
+    } else {
+        int rc = FMD_OK;
+        const LJShape pick = pick_lj_shape(prune.cnt, prune.list, rc);
+        if (rc != FMD_OK) return rc;
+        cache[key] = pick;
+        arr.lj_shape_p = pick;
+    }
+    set_lj_blocks();
     return FMD_OK;
 }
 
@@ -318,6 +361,8 @@ int System::init() {
     if (enqueue_ke(arr, st) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "kinetic launch failed");
     int rc = ctx->sync_check("system init");
     if (rc != FMD_OK) return rc;
+    // the first evaluation pruned the LJ rows: tune the gather over them
+    if (arr.kind != FMD_SYS_RIGID && (rc = tune_lj_pruned()) != FMD_OK) return rc;
     initialized = true;
     // Capture the four step variants now, so no host-side capture ever sits
     // between two steps of a run.
@@ -657,7 +702,7 @@ extern "C" int fmd_system_kernel_ms(fmd_system* s, int stage, int reps, double* 
                 if (!a.prune) return cudaErrorInvalidValue;
                 return lj_gather_launch(a.kind == FMD_SYS_AIREBO ? FMD_FF_AIREBO : FMD_FF_MM, a.pos, hh, a.cnt_a,
                                         a.list_a, a.cap_a, a.prune->cnt, a.prune->list, a.in_cap, a.n, a.Facc,
-                                        a.Facc, a.part_f2, st, a.precision, a.lj_shape, a.err);
+                                        a.Facc, a.part_f2, st, a.precision, a.lj_shape_p, a.err);
             default:
                 return enqueue_forces(a, st);
         }
@@ -713,6 +758,7 @@ extern "C" int fmd_system_set_lj_shape(fmd_system* s, int threads, int unroll, i
     if (cudaStreamSynchronize(y.ctx->stream) != cudaSuccess) return y.ctx->fail(FMD_ERR_CUDA, "sync failed");
     y.drop_graphs();                     // captured graphs hold the old launch
     y.arr.lj_shape = sh;
+    y.arr.lj_shape_p = sh;
     y.arr.lj_blocks = nb;
     if (y.arr.sg) {                      // keep the learned term's graph variants too
         int rc = FMD_OK;
@@ -761,6 +807,15 @@ extern "C" int fmd_system_lj_prune(fmd_system* s, double* delta, long long* eval
     }
     if (evaluations) *evaluations = (long long)st[0];
     if (prunes) *prunes = (long long)st[1];
+    return FMD_OK;
+}
+
+extern "C" int fmd_system_lj_shape_pruned(fmd_system* s, int* threads, int* unroll, int* feed) {
+    if (!s || !s->sys) return FMD_ERR_ARG;
+    const StepArrays& a = s->sys->arr;
+    if (threads) *threads = a.lj_shape_p.threads;
+    if (unroll) *unroll = a.lj_shape_p.unroll;
+    if (feed) *feed = a.lj_shape_p.pipe;
     return FMD_OK;
 }
 

@@ -41,6 +41,9 @@ struct System {
     bool judge_step(int g) const { return arr.sg && arr.sg->judge_every > 0 && g % arr.sg->judge_every == 0; }
     int init();
     int tune_lj();
+    int tune_lj_pruned();
+    LJShape pick_lj_shape(const int* rcnt, const int* rlist, int& rc);
+    void set_lj_blocks();
     int tune_rigid();
     int capture(bool rebuild, bool phase, bool judge = false);
     void drop_graphs();

@@ -270,6 +270,9 @@ int fmd_system_kernel_ms(fmd_system *s, int stage, int reps, double *ms_per_laun
  * fmd_system_set_lj_shape pins a shape (for reproducible runs; results then
  * do not depend on timing), after fmd_system_init. */
 int fmd_system_lj_shape(fmd_system *s, int *threads, int *unroll, int *pipelined, int *blocks);
+/* Launch shape of the gather over the pruned rows, tuned separately on those
+ * rows at set-up (the same shape when pinned by FMD_LJ_SHAPE or set_lj_shape). */
+int fmd_system_lj_shape_pruned(fmd_system *s, int *threads, int *unroll, int *feed);
 /* Pruned rows of the atomistic LJ gather (AIREBO, MM; the reference walks
  * its whole list every step, AI:435-470, MM:729-760).  After each list build,
  * and whenever the largest atom displacement u and the largest relative
