@@ -199,14 +199,16 @@ __device__ __forceinline__ void ang_g_dg(double x, double& g, double& dg) {
     dg = G_A0 * 2.0 * c2 * hh * inv * inv;
 }
 
-// Sum over centre c's other slots of f_c G(cos) for the bond c -> skip whose
-// vector is s*(bx,by,bz) with s = +-1 (AI:301-309).
-__device__ __forceinline__ double bo_sum_sl(const Slot* __restrict__ sl, const int* __restrict__ list, int cap,
-                                            int c, int m, int skip, double bx, double by, double bz, double rbinv) {
+// Sum over centre c's other slots of f_c G(cos) for the bond in slot skip_kn
+// of c's row (-1: the bond is not in c's row) whose vector is s*(bx,by,bz)
+// with s = +-1 (AI:301-309).  Rows hold no atom twice, so skipping the slot is
+// skipping the bonded atom.
+__device__ __forceinline__ double bo_sum_sl(const Slot* __restrict__ sl, int cap, int c, int m, int skip_kn,
+                                            double bx, double by, double bz, double rbinv) {
     double gs = 0.0;
     for (int kn = 0; kn < m; kn++) {
         const size_t o = (size_t)c * cap + kn;
-        if (list[o] == skip) continue;
+        if (kn == skip_kn) continue;
         const Slot q = sl[o];
         if (q.fc < 1e-15) continue;
         const double ct = clamp1((bx * q.dx + by * q.dy + bz * q.dz) * (rbinv * q.rinv));
@@ -289,7 +291,7 @@ k_rebo_bo(const Slot* __restrict__ sl, const int* __restrict__ cnt, const int* _
         o.ok = 0.0;
         // the reference's bond gate (AI:292-296)
         if (q.r <= DMAX_CC && !(q.fc < 1e-15 && q.dfc == 0)) {
-            const double g = bo_sum_sl(sl, list, cap, c, m, list[t], q.dx, q.dy, q.dz, q.rinv);
+            const double g = bo_sum_sl(sl, cap, c, m, jn, q.dx, q.dy, q.dz, q.rinv);
             o.g = g;
             o.b = 1.0 / sqrt(1.0 + g);
             rebo_pair_fn(q.r, q.rinv, o.vr, o.dvr, o.va, o.dva);
@@ -390,8 +392,12 @@ k_rebo_force(const Slot* __restrict__ sl, const SlotBO* __restrict__ bo, const i
         if (ok) {
             j = list[t];
             mj = cnt[j];
-            for (int kn = 0; kn < mj; kn++)   // partner slot j -> i
-                if (list[(size_t)j * cap + kn] == i) { pn = kn; break; }
+            if (ids) {
+                pn = ids[1 + (size_t)na * cap + t];   // partner slot j -> i of the last build
+            } else {
+                for (int kn = 0; kn < mj; kn++)
+                    if (list[(size_t)j * cap + kn] == i) { pn = kn; break; }
+            }
             if (j < i && pn < 0) ok = false;
         }
         Slot q;
@@ -435,7 +441,7 @@ k_rebo_force(const Slot* __restrict__ sl, const SlotBO* __restrict__ bo, const i
             if (pn >= 0) {
                 bji = bo[(size_t)j * cap + pn].b;
             } else {
-                const double gji = bo_sum_sl(sl, list, cap, j, mj, i, -q.dx, -q.dy, -q.dz, q.rinv);
+                const double gji = bo_sum_sl(sl, cap, j, mj, -1, -q.dx, -q.dy, -q.dz, q.rinv);
                 bji = 1.0 / sqrt(1.0 + gji);
                 three_body_sl(F, sl, list, cap, j, mj, i, -q.dx, -q.dy, -q.dz, q.rinv,
                               three_body_coeff(gji, bji, q.fc, o.va));
@@ -870,15 +876,34 @@ __global__ void __launch_bounds__(kIdsBlock) k_ids_emit(const int* __restrict__ 
     if (blockIdx.x == gridDim.x - 1 && threadIdx.x == kIdsBlock - 1) ids[0] = off + m;
 }
 
+// Partner slot of every occupied slot i -> j: the position of i in j's row,
+// -1 when j's row lacks i (rows cut at cap); written after the slot ids.
+__global__ void k_ids_partner(const int* __restrict__ cnt, const int* __restrict__ list, int cap, int n,
+                              int* __restrict__ ids) {
+    const int tot = ids[0];
+    int* pslot = ids + 1 + (size_t)n * cap;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < tot; k += gridDim.x * blockDim.x) {
+        const int t = ids[1 + k];
+        const int i = t / cap;
+        const int j = list[t];
+        const int mj = min(cnt[j], cap);
+        int pn = -1;
+        for (int kn = 0; kn < mj; kn++)
+            if (list[(size_t)j * cap + kn] == i) { pn = kn; break; }
+        pslot[t] = pn;
+    }
+}
+
 }  // namespace
 
 int rebo_ids_scratch(int n) { return (n + kIdsBlock - 1) / kIdsBlock; }
 
-cudaError_t rebo_ids_build(const int* cnt, int cap, int n, int* ids, int* bsum, cudaStream_t st) {
+cudaError_t rebo_ids_build(const int* cnt, const int* list, int cap, int n, int* ids, int* bsum, cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
     const int nb = rebo_ids_scratch(n);
     k_ids_count<<<nb, kIdsBlock, 0, st>>>(cnt, cap, n, bsum);
     k_ids_emit<<<nb, kIdsBlock, 0, st>>>(cnt, cap, n, bsum, ids);
+    k_ids_partner<<<kForceBlocks, 256, 0, st>>>(cnt, list, cap, n, ids);
     return cudaGetLastError();
 }
 

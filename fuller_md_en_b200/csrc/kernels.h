@@ -80,13 +80,14 @@ cudaError_t rebo_launch_gated(const double* pos, const double* hh, const int* cn
 // as rebo_launch_gated (gate may be null).
 constexpr int kReboSlotDoubles = 16;
 // ids (may be null): the occupied slots in atom-major order, ids[0] their
-// number and ids[1 + k] the slot i * cap + jn (rebo_ids_build); threads then
-// walk only those instead of every slot of every row.
+// number and ids[1 + k] the slot i * cap + jn, then at ids[1 + na * cap + t]
+// the partner slot of slot t (i's position in j's row, -1 if absent)
+// (rebo_ids_build); threads then walk only the occupied slots.
 cudaError_t rebo_slots_launch(const double* pos, const double* hh, const int* cnt, const int* list, int cap,
                               int na, double* slots, double* F, double* part, int nblocks, const int* gate,
                               int want, cudaStream_t st, const int* ids = nullptr);
-// Builds ids (1 + n * cap ints) from the list counts; bsum: rebo_ids_scratch(n) ints.
-cudaError_t rebo_ids_build(const int* cnt, int cap, int n, int* ids, int* bsum, cudaStream_t st);
+// Builds ids (1 + 2 n cap ints) from the list; bsum: rebo_ids_scratch(n) ints.
+cudaError_t rebo_ids_build(const int* cnt, const int* list, int cap, int n, int* ids, int* bsum, cudaStream_t st);
 int rebo_ids_scratch(int n);
 // Half-list LJ gather (a8, a14): F[i] = Facc[i] + LJ(i); Facc[i] zeroed
 // (unless Facc == F).  ff: FMD_FF_AIREBO / FMD_FF_MM.  precision:

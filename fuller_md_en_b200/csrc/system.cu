@@ -106,7 +106,7 @@ int System::alloc_lists(double rc_list_a, int cap_a_, double rc_list_b, int cap_
         if (alloc(&arr.rebo_slots, (size_t)n * cap_b_ * kReboSlotDoubles, (const double*)nullptr))
             return ctx->fail(FMD_ERR_CUDA, "list allocation failed");
         int* ids;
-        if (alloc(&ids, 1 + (size_t)n * cap_b_, (const int*)nullptr) ||
+        if (alloc(&ids, 1 + 2 * (size_t)n * cap_b_, (const int*)nullptr) ||
             alloc(&rebo_bsum, (size_t)rebo_ids_scratch(n), (const int*)nullptr))
             return ctx->fail(FMD_ERR_CUDA, "list allocation failed");
         cudaMemsetAsync(ids, 0, sizeof(int), ctx->stream);
@@ -156,7 +156,8 @@ cudaError_t System::enqueue_rebuild(cudaStream_t st) {
                 return e;
         }
         if (arr.rebo_ids &&
-            (e = rebo_ids_build(arr.cnt_b, arr.cap_b, arr.n, const_cast<int*>(arr.rebo_ids), rebo_bsum, st)) !=
+            (e = rebo_ids_build(arr.cnt_b, arr.list_b, arr.cap_b, arr.n, const_cast<int*>(arr.rebo_ids), rebo_bsum,
+                                st)) !=
                 cudaSuccess)
             return e;
     }
