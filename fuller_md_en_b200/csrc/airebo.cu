@@ -494,7 +494,8 @@ __device__ __forceinline__ void lj_fetch(const double* __restrict__ pos, const i
 template <bool FULL_VIRIAL, bool F32, int U>
 __device__ __forceinline__ void lj_chunk(const int (&jc)[U], const double (&cx)[U], const double (&cy)[U],
                                          const double (&cz)[U], int i, double px, double py, double pz,
-                                         const double* h, const double* hi, bool diag, const LJP& p, const LJF& pf,
+                                         const double* h, const double* hi, bool diag, bool wide, const LJP& p,
+                                         const LJF& pf,
                                          double& fx, double& fy, double& fz, double* acc, const LJPruneOut& po,
                                          int* __restrict__ prow, int& pc, int lane) {
     bool keep[U];
@@ -503,7 +504,11 @@ __device__ __forceinline__ void lj_chunk(const int (&jc)[U], const double (&cx)[
         keep[u] = false;
         if (jc[u] < 0) continue;
         double dx = __dsub_rn(cx[u], px), dy = __dsub_rn(cy[u], py), dz = __dsub_rn(cz[u], pz);
-        if (diag) {
+        if (wide) {
+            dx = mimg1_rint(dx, h[0], hi[0]);
+            dy = mimg1_rint(dy, h[4], hi[4]);
+            dz = mimg1_rint(dz, h[8], hi[8]);
+        } else if (diag) {
             dx = mimg1(dx, h[0], hi[0]);
             dy = mimg1(dy, h[4], hi[4]);
             dz = mimg1(dz, h[8], hi[8]);
@@ -565,6 +570,8 @@ __device__ __forceinline__ void lj_gather_body(const double* __restrict__ pos, c
     // Diagonal cell (FCC/BCC boxes under the diagonal barostat): uniform branch.
     const bool diag = h[1] == 0.0 && h[2] == 0.0 && h[3] == 0.0 && h[5] == 0.0 && h[6] == 0.0 && h[7] == 0.0 &&
                       hi[1] == 0.0 && hi[2] == 0.0 && hi[3] == 0.0 && hi[5] == 0.0 && hi[6] == 0.0 && hi[7] == 0.0;
+    // half the narrowest edge beyond the cutoff: the one-instruction image (mimg1_rint)
+    const bool wide = diag && 0.25 * fmin(h[0] * h[0], fmin(h[4] * h[4], h[8] * h[8])) > p.rc2 * (1.0 + 1e-9);
     const LJF pf{(float)p.sig2, (float)(p.sig2 - (double)(float)p.sig2), (float)p.c4, (float)p.c24};
     double acc[kNV];
 #pragma unroll
@@ -589,7 +596,7 @@ __device__ __forceinline__ void lj_gather_body(const double* __restrict__ pos, c
             } else {
                 lj_fetch<U>(pos, row, tot, b0 + lane, i, jc, cx, cy, cz);
             }
-            lj_chunk<FULL_VIRIAL, F32, U>(jc, cx, cy, cz, i, px, py, pz, h, hi, diag, p, pf, fx, fy, fz, acc, po,
+            lj_chunk<FULL_VIRIAL, F32, U>(jc, cx, cy, cz, i, px, py, pz, h, hi, diag, wide, p, pf, fx, fy, fz, acc, po,
                                           prow, pc, lane);
         }
         lj_atom_done(i, fx, fy, fz, px, py, pz, hi, F, Facc, po, pc, lane);
@@ -658,6 +665,8 @@ __device__ __forceinline__ void lj_gather_staged_body(const double* __restrict__
     const double* hi = s_hh + 9;
     const bool diag = h[1] == 0.0 && h[2] == 0.0 && h[3] == 0.0 && h[5] == 0.0 && h[6] == 0.0 && h[7] == 0.0 &&
                       hi[1] == 0.0 && hi[2] == 0.0 && hi[3] == 0.0 && hi[5] == 0.0 && hi[6] == 0.0 && hi[7] == 0.0;
+    // half the narrowest edge beyond the cutoff: the one-instruction image (mimg1_rint)
+    const bool wide = diag && 0.25 * fmin(h[0] * h[0], fmin(h[4] * h[4], h[8] * h[8])) > p.rc2 * (1.0 + 1e-9);
     const LJF pf{(float)p.sig2, (float)(p.sig2 - (double)(float)p.sig2), (float)p.c4, (float)p.c24};
     double acc[kNV];
 #pragma unroll
@@ -703,7 +712,7 @@ __device__ __forceinline__ void lj_gather_staged_body(const double* __restrict__
                 const int j = jc[u] < 0 ? i : jc[u];
                 cx[u] = pos[3 * j]; cy[u] = pos[3 * j + 1]; cz[u] = pos[3 * j + 2];
             }
-            lj_chunk<FULL_VIRIAL, F32, U>(jc, cx, cy, cz, i, px, py, pz, h, hi, diag, p, pf, fx, fy, fz, acc, po,
+            lj_chunk<FULL_VIRIAL, F32, U>(jc, cx, cy, cz, i, px, py, pz, h, hi, diag, wide, p, pf, fx, fy, fz, acc, po,
                                           prow, pc, lane);
         }
         lj_atom_done(i, fx, fy, fz, px, py, pz, hi, F, Facc, po, pc, lane);

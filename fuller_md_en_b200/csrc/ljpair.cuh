@@ -45,6 +45,17 @@ __device__ __forceinline__ double mimg1(double d, double hii, double hii_inv) {
     return __dmul_rn(hii, s);
 }
 
+// The same image by one rounding instruction: rint (half to even) and the
+// reference's round (half away from zero) differ only where s is a
+// half-integer, and there both images lie half a cell edge away along this
+// axis, so |d| and r^2 are the same under either and the pair is beyond the
+// cutoff whenever half the narrowest edge exceeds it -- the only case this is
+// used in.  Every other pair gets the identical image and d bit for bit.
+__device__ __forceinline__ double mimg1_rint(double d, double hii, double hii_inv) {
+    const double s = __dmul_rn(hii_inv, d);
+    return __dmul_rn(hii, __dsub_rn(s, rint(s)));
+}
+
 // 1/x for x in the FP32 normal range: the FP32 hardware reciprocal (relative
 // error ~2^-23) refined by one Newton-Raphson step y + y (1 - x y), which
 // squares the error (~1e-14), in place of a full IEEE division.
