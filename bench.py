@@ -234,32 +234,10 @@ def run_ours(args, ws, rank, local):
     launches = sum(n_reb if (1 + k) % NLUP == 0 else n_prod for k in range(K))
     sysd.close()
 
-    # ---------------- the same steps with FP32 pair arithmetic ----------------
-    from fuller_md_en_b200._lib import FMD_PREC_FP32_PAIR
-    _, _, cfg32, _ = make_system(ctx, rank, precision=FMD_PREC_FP32_PAIR)
-    sys32 = System.airebo(ctx, cfg32, s["pos"], s["vel"], s["mass"], s["mol_id"], s["h"], npt)
-    sys32.init()
-    ms32 = float(sum(timed_steps(ctx, stream, sys32, K, flush)))
-    lj32_ms = sys32.kernel_ms(0, 20)
-    sys32.close()
-    value32 = ws * na * K / (ms32 / 1e3)
-
-    # ---------------- learned surrogate on the same workload ----------------
-    sg_res = None
-    if not args.no_surrogate:
-        sg_res = run_surrogate(args, ctx, stream, s, na, cfg, npt, flush, ws, local, value)
-
-    # ---------------- batched MM replicas (uneven sizes, one launch per phase) ----------------
-    batch_res = None
-    if not args.no_batch:
-        batch_res = run_batch(args, ctx, stream, flush, ws, rank)
-
-    # ---------------- rigid-body LJ, C60 FCC nc=10 (240,000 sites) ----------------
-    rigid_res = None
-    if not args.no_rigid:
-        rigid_res = run_rigid(args, ctx, stream, flush, ws, rank, local)
-
     # ---------------- end to end through the public API ----------------
+    # Measured before the legs that run the reference's OpenMP build on the
+    # host: its worker threads keep spinning on every core for a while after
+    # each parallel region and would slow this wall-clock window's host side.
     e2e = None
     if rank == 0 or ws > 1:
         from fuller_md_en_b200 import System as Sys
@@ -289,6 +267,31 @@ def run_ours(args, ws, rank, local):
                "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K, "wall_parts": e2e_parts,
                "note": "wall clock: state upload, init (lists + first forces), K steps in chunks of "
                        f"{prn} with observables read back per chunk, state download"}
+    # ---------------- the same steps with FP32 pair arithmetic ----------------
+    from fuller_md_en_b200._lib import FMD_PREC_FP32_PAIR
+    _, _, cfg32, _ = make_system(ctx, rank, precision=FMD_PREC_FP32_PAIR)
+    sys32 = System.airebo(ctx, cfg32, s["pos"], s["vel"], s["mass"], s["mol_id"], s["h"], npt)
+    sys32.init()
+    ms32 = float(sum(timed_steps(ctx, stream, sys32, K, flush)))
+    lj32_ms = sys32.kernel_ms(0, 20)
+    sys32.close()
+    value32 = ws * na * K / (ms32 / 1e3)
+
+    # ---------------- learned surrogate on the same workload ----------------
+    sg_res = None
+    if not args.no_surrogate:
+        sg_res = run_surrogate(args, ctx, stream, s, na, cfg, npt, flush, ws, local, value)
+
+    # ---------------- batched MM replicas (uneven sizes, one launch per phase) ----------------
+    batch_res = None
+    if not args.no_batch:
+        batch_res = run_batch(args, ctx, stream, flush, ws, rank)
+
+    # ---------------- rigid-body LJ, C60 FCC nc=10 (240,000 sites) ----------------
+    rigid_res = None
+    if not args.no_rigid:
+        rigid_res = run_rigid(args, ctx, stream, flush, ws, rank, local)
+
     ctx.close()
     del flush
     res = {

@@ -21,6 +21,7 @@
 #include "kernels.h"
 #include "geom.cuh"
 #include "ljpair.cuh"
+#include "ljprune.cuh"
 #include "rebo_fn.cuh"
 #include "step.h"
 #include "umma.cuh"
@@ -605,8 +606,19 @@ __device__ __forceinline__ void lj_gather_body(const double* __restrict__ pos, c
     block_sum_store<kNV>(acc, sm, part + (size_t)blk * kNV);
 }
 
-// Records gridDim.x .. nrec-1 of part are zero: the two gathers of a pruned
-// system may run on different grids and write one record count.
+// The rows of this evaluation: with po.words set, the full rows and pruned-
+// row output when a prune is due, else the pruned rows (po.cnt, po.list) and
+// no output; every block decides on the same inputs.
+__device__ __forceinline__ void lj_rows_select(const double* hh, const int*& rcnt, const int*& rlist,
+                                               LJPruneOut& po) {
+    if (!po.words || lj_prune_needed(po.words, hh, po.hb, po.delta, po.rc)) return;
+    rcnt = po.cnt;
+    rlist = po.list;
+    po.cnt = nullptr;
+}
+
+// Records gridDim.x .. nrec-1 of part are zero: the gathers of one system
+// may run on different grids and write one record count.
 __device__ __forceinline__ void lj_zero_records(double* __restrict__ part, int nrec) {
     if (threadIdx.x < kNV)
         for (int r = gridDim.x + blockIdx.x; r < nrec; r += gridDim.x) part[(size_t)r * kNV + threadIdx.x] = 0.0;
@@ -616,13 +628,14 @@ template <bool FULL_VIRIAL, bool F32, int U, bool PIPE, int NT>
 __global__ void __launch_bounds__(NT)
 k_lj_gather(const double* __restrict__ pos, const double* __restrict__ hh, const int* __restrict__ in_cnt,
             const int* __restrict__ in_list, int in_cap, int na, double* __restrict__ F,
-            double* __restrict__ Facc, LJP p, double* __restrict__ part, const int* __restrict__ gate, int want,
-            LJPruneOut po, int nrec) {
+            double* __restrict__ Facc, LJP p, double* __restrict__ part, LJPruneOut po, int nrec) {
     FMD_PDL_WAIT();
-    if (gate && *gate != want) return;
     __shared__ double sm[32 * kNV];
     __shared__ double s_hh[18];
-    lj_gather_body<FULL_VIRIAL, F32, U, PIPE>(pos, hh, in_cnt, in_list, in_cap, na, F, Facc, p, part, blockIdx.x,
+    const int* rcnt = in_cnt;
+    const int* rlist = in_list;
+    lj_rows_select(hh, rcnt, rlist, po);
+    lj_gather_body<FULL_VIRIAL, F32, U, PIPE>(pos, hh, rcnt, rlist, in_cap, na, F, Facc, p, part, blockIdx.x,
                                               gridDim.x, sm, s_hh, po);
     lj_zero_records(part, nrec);
 }
@@ -731,13 +744,15 @@ __global__ void __launch_bounds__(NT)
 k_lj_gather_staged(const double* __restrict__ pos, const double* __restrict__ hh, const int* __restrict__ in_cnt,
                    const int* __restrict__ in_list, int in_cap, int na, double* __restrict__ F,
                    double* __restrict__ Facc, LJP p, double* __restrict__ part, DevErr* err,
-                   const int* __restrict__ gate, int want, LJPruneOut po, int nrec) {
+                   LJPruneOut po, int nrec) {
     FMD_PDL_WAIT();
-    if (gate && *gate != want) return;
     extern __shared__ __align__(128) unsigned char dsm[];
     __shared__ double sm[32 * kNV];
     __shared__ double s_hh[18];
-    lj_gather_staged_body<FULL_VIRIAL, F32, U, NT>(pos, hh, in_cnt, in_list, in_cap, na, F, Facc, p, part, err,
+    const int* rcnt = in_cnt;
+    const int* rlist = in_list;
+    lj_rows_select(hh, rcnt, rlist, po);
+    lj_gather_staged_body<FULL_VIRIAL, F32, U, NT>(pos, hh, rcnt, rlist, in_cap, na, F, Facc, p, part, err,
                                                    blockIdx.x, gridDim.x, dsm, sm, s_hh, po);
     lj_zero_records(part, nrec);
 }
@@ -934,11 +949,11 @@ int lj_occupancy() {
 template <bool FV, bool F32, int U, bool PIPE, int NT>
 int lj_dispatch(bool launch, const double* pos, const double* hh, const int* cnt, const int* list, int cap,
                 const int* in_cnt, const int* in_list, int in_cap, int na, double* F, double* Facc, const LJP& p,
-                double* part, cudaStream_t st, const int* gate, int want, const LJPruneOut& po, int nrec) {
+                double* part, cudaStream_t st, const LJPruneOut& po, int nrec) {
     const int nb = std::min(kLJMaxBlocks, lj_occupancy<FV, F32, U, PIPE, NT>() * kSMs);
     if (launch)
         launch_pdl(k_lj_gather<FV, F32, U, PIPE, NT>, dim3(nb), dim3(NT), 0, st, pos, hh, in_cnt, in_list, in_cap, na,
-                   F, Facc, p, part, gate, want, po, nrec);
+                   F, Facc, p, part, po, nrec);
     return nb;
 }
 
@@ -950,7 +965,7 @@ size_t staged_smem(int threads, int in_cap) {
 template <bool FV, bool F32, int U, int NT>
 int lj_dispatch_staged(bool launch, const double* pos, const double* hh, const int* in_cnt, const int* in_list,
                        int in_cap, int na, double* F, double* Facc, const LJP& p, double* part, DevErr* err,
-                       cudaStream_t st, const int* gate, int want, const LJPruneOut& po, int nrec) {
+                       cudaStream_t st, const LJPruneOut& po, int nrec) {
     static std::map<int, int> occ;                 // in_cap -> resident blocks per SM
     const size_t smem = staged_smem(NT, in_cap);
     auto it = occ.find(in_cap);
@@ -968,7 +983,7 @@ int lj_dispatch_staged(bool launch, const double* pos, const double* hh, const i
     const int nb = std::min(kLJMaxBlocks, it->second * kSMs);
     if (launch)
         launch_pdl(k_lj_gather_staged<FV, F32, U, NT>, dim3(nb), dim3(NT), smem, st, pos, hh, in_cnt, in_list, in_cap,
-                   na, F, Facc, p, part, err, gate, want, po, nrec);
+                   na, F, Facc, p, part, err, po, nrec);
     return nb;
 }
 
@@ -977,14 +992,14 @@ int lj_dispatch_staged(bool launch, const double* pos, const double* hh, const i
 int lj_select(bool launch, int ff, int precision, const LJShape& sh, const double* pos, const double* hh,
               const int* cnt, const int* list, int cap, const int* in_cnt, const int* in_list, int in_cap, int na,
               double* F, double* Facc, double* part, cudaStream_t st, DevErr* err = nullptr,
-              const int* gate = nullptr, int want = 0, const LJPruneOut& po = LJPruneOut{}, int nrec = 0) {
+              const LJPruneOut& po = LJPruneOut{}, int nrec = 0) {
     const LJP p = lj_params(ff);
     const bool fv = ff == FMD_FF_AIREBO, f32 = precision == FMD_PREC_FP32_PAIR;
     if (sh.pipe == 2) {
         if (in_cap % 4 != 0 || (launch && err == nullptr)) return 0;
 #define FMD_LJS(FV, F32, U, NT) \
     return lj_dispatch_staged<FV, F32, U, NT>(launch, pos, hh, in_cnt, in_list, in_cap, na, F, Facc, p, part, err, st, \
-                                              gate, want, po, nrec)
+                                              po, nrec)
 #define FMD_LJS_NT(FV, F32, U) if (sh.threads == 128) { FMD_LJS(FV, F32, U, 128); } else { FMD_LJS(FV, F32, U, 256); }
 #define FMD_LJS_U(FV, F32) if (sh.unroll == 2) { FMD_LJS_NT(FV, F32, 2) } else { FMD_LJS_NT(FV, F32, 4) }
         if (fv) { if (f32) { FMD_LJS_U(true, true) } else { FMD_LJS_U(true, false) } }
@@ -995,7 +1010,7 @@ int lj_select(bool launch, int ff, int precision, const LJShape& sh, const doubl
     }
 #define FMD_LJ_CALL(FV, F32, U, PIPE, NT) \
     return lj_dispatch<FV, F32, U, PIPE, NT>(launch, pos, hh, cnt, list, cap, in_cnt, in_list, in_cap, na, F, Facc, p, \
-                                             part, st, gate, want, po, nrec)
+                                             part, st, po, nrec)
 #define FMD_LJ_NT(FV, F32, U, PIPE) \
     if (sh.threads == 128) { FMD_LJ_CALL(FV, F32, U, PIPE, 128); } else { FMD_LJ_CALL(FV, F32, U, PIPE, 256); }
 #define FMD_LJ_PIPE(FV, F32, U) if (sh.pipe) { FMD_LJ_NT(FV, F32, U, true) } else { FMD_LJ_NT(FV, F32, U, false) }
@@ -1018,9 +1033,9 @@ int lj_gather_blocks(int ff, int precision, const LJShape& sh, int in_cap) {
 cudaError_t lj_gather_launch(int ff, const double* pos, const double* hh, const int* cnt, const int* list,
                              int cap, const int* in_cnt, const int* in_list, int in_cap, int na, double* F,
                              double* Facc, double* part, cudaStream_t st, int precision, const LJShape& sh,
-                             DevErr* err, const int* gate, int want, const LJPruneOut& po, int nrec) {
+                             DevErr* err, const LJPruneOut& po, int nrec) {
     if (lj_select(true, ff, precision, sh, pos, hh, cnt, list, cap, in_cnt, in_list, in_cap, na, F, Facc, part, st,
-                  err, gate, want, po, nrec) == 0)
+                  err, po, nrec) == 0)
         return cudaErrorInvalidConfiguration;
     return cudaGetLastError();
 }

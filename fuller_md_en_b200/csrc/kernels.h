@@ -99,12 +99,13 @@ int rebo_ids_scratch(int n);
 // in_cap % 4 == 0 and an error word); the grid is one full wave of the
 // instantiation (resident blocks per SM x SMs, at most kLJMaxBlocks) and
 // writes that many partial records -- lj_gather_blocks returns it (0: the
-// shape cannot run with this row stride).  gate (device int, may be null):
-// the whole grid returns at once unless *gate == want.  po.cnt non-null: a
-// pruning gather, which also writes per atom i the entries of its row with
+// shape cannot run with this row stride).  po.cnt non-null: a pruning
+// gather, which also writes per atom i the entries of its row with
 // r^2 <= po.r2 now, in row order, to po.list + i * in_cap (po.cnt[i] of them)
-// and its fractional position to po.sb (ljprune.cu).  nrec > grid: the
-// records grid .. nrec-1 are written as zeros.
+// and its fractional position to po.sb (ljprune.cu); with po.words also set
+// the gather first decides (lj_prune_needed) and walks the pruned rows
+// instead when no prune is due.  nrec > grid: the records grid .. nrec-1 are
+// written as zeros.
 struct LJShape {
     int threads = 256, unroll = 4, pipe = 0;
 };
@@ -113,14 +114,18 @@ struct LJPruneOut {
     int* list = nullptr;
     double* sb = nullptr;
     double r2 = 0.0;
+    // with words set, the gather decides per evaluation (lj_prune_needed):
+    // full rows plus pruned-row output, or the pruned rows (cnt, list) as input
+    const unsigned long long* words = nullptr;
+    const double* hb = nullptr;
+    double delta = 0.0, rc = 0.0;
 };
 int lj_gather_blocks(int ff, int precision, const LJShape& shape, int in_cap);
 cudaError_t lj_gather_launch(int ff, const double* pos, const double* hh, const int* cnt,
                              const int* list, int cap, const int* in_cnt, const int* in_list,
                              int in_cap, int na, double* F, double* Facc, double* part,
                              cudaStream_t st, int precision = FMD_PREC_FP64, const LJShape& shape = LJShape{},
-                             DevErr* err = nullptr, const int* gate = nullptr, int want = 0,
-                             const LJPruneOut& po = LJPruneOut{}, int nrec = 0);
+                             DevErr* err = nullptr, const LJPruneOut& po = LJPruneOut{}, int nrec = 0);
 // Rigid site-site LJ (a5-a6): writes F, T; per-block {E, W9} partials (grid n).
 // lab (may be null): scratch of n * natom * 4 doubles for the lab-frame sites;
 // with it (and natom <= 64) the warp-per-neighbour kernel runs, in launch

@@ -17,41 +17,18 @@
 // the prune is still beyond the cutoff, so the pruned rows yield exactly the
 // pairs of the full rows and the same pair terms; only the lanes that add
 // them, and so the rounding of the sums, change.  The drift raises u
-// (kick_body), the decision runs on the device before the gathers, and both
-// gathers sit in the step's graph, each returning at once unless the flag
-// selects it.  A list build marks the next evaluation as a prune.
+// (kick_body); each block of the gather evaluates the condition
+// (lj_prune_needed) and walks either the full rows, writing pruned ones, or
+// the pruned rows; the step's reduction kernel then restarts the bound when
+// the evaluation pruned.  A list build marks the next evaluation as a prune.
 #include <cmath>
 
-#include "geom.cuh"
 #include "ljprune.h"
-#include "pdl.cuh"
 
 namespace fmd {
 namespace {
 
 constexpr unsigned long long kPruneMark = 0x7F7F7F7F7F7F7F7Full;   // ~1.4e306 A: forces a prune
-
-__device__ __forceinline__ bool diag9(const double* h) {
-    return h[1] == 0.0 && h[2] == 0.0 && h[3] == 0.0 && h[5] == 0.0 && h[6] == 0.0 && h[7] == 0.0;
-}
-
-__global__ void k_prune_decide(unsigned long long* __restrict__ words, const double* __restrict__ hh,
-                               double* __restrict__ hb, int* __restrict__ flag,
-                               unsigned long long* __restrict__ stats, double delta, double rc) {
-    FMD_PDL_WAIT();
-    if (threadIdx.x != 0) return;
-    const double u = __longlong_as_double((long long)*words);
-    double k = 0.0;
-    for (int a = 0; a < 3; a++) k = fmax(k, fabs(hh[4 * a] - hb[4 * a]) / fabs(hb[4 * a]));
-    const bool keep = diag9(hh) && diag9(hb) && k * (rc + delta) + 2.0 * u < delta - 1e-6;
-    *flag = keep ? 0 : 1;
-    stats[0] += 1ull;
-    if (!keep) {
-        *words = 0ull;
-        for (int q = 0; q < 9; q++) hb[q] = hh[q];
-        stats[1] += 1ull;
-    }
-}
 
 __global__ void k_prune_mark(unsigned long long* words) { *words = kPruneMark; }
 
@@ -70,7 +47,6 @@ cudaError_t lj_prune_alloc(LJPrune& p, int n, int stride, double rc, double delt
     A((void**)&p.sb, sizeof(double) * 3 * n, true);
     A((void**)&p.hb, sizeof(double) * 9, true);
     A((void**)&p.words, sizeof(unsigned long long), true);
-    A((void**)&p.flag, sizeof(int), true);
     A((void**)&p.stats, sizeof(unsigned long long) * 2, true);
     if (e == cudaSuccess) e = cudaMemsetAsync(p.words, 0x7F, sizeof(unsigned long long), st);
     if (e != cudaSuccess) {
@@ -86,18 +62,13 @@ cudaError_t lj_prune_alloc(LJPrune& p, int n, int stride, double rc, double delt
 }
 
 void lj_prune_free(LJPrune& p) {
-    cudaFree(p.cnt); cudaFree(p.list); cudaFree(p.sb); cudaFree(p.hb); cudaFree(p.words); cudaFree(p.flag);
-    cudaFree(p.stats);
+    cudaFree(p.cnt); cudaFree(p.list); cudaFree(p.sb); cudaFree(p.hb); cudaFree(p.words); cudaFree(p.stats);
     p = LJPrune();
 }
 
 cudaError_t lj_prune_mark(const LJPrune& p, cudaStream_t st) {
     k_prune_mark<<<1, 1, 0, st>>>(p.words);
     return cudaGetLastError();
-}
-
-cudaError_t lj_prune_decide(const LJPrune& p, const double* hh, cudaStream_t st) {
-    return launch_pdl(k_prune_decide, dim3(1), dim3(32), 0, st, p.words, hh, p.hb, p.flag, p.stats, p.delta, p.rc);
 }
 
 LJPruneOut lj_prune_out(const LJPrune& p) {
@@ -107,6 +78,10 @@ LJPruneOut lj_prune_out(const LJPrune& p) {
     o.sb = p.sb;
     const double r = p.rc + p.delta;
     o.r2 = r * r;
+    o.words = p.words;
+    o.hb = p.hb;
+    o.delta = p.delta;
+    o.rc = p.rc;
     return o;
 }
 

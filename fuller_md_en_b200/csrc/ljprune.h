@@ -21,7 +21,6 @@ struct LJPrune {
     double* sb = nullptr;         // [3 n] fractional positions at the last prune
     double* hb = nullptr;         // [9] cell at the last prune
     unsigned long long* words = nullptr;  // [1] bits of the largest displacement since the last prune
-    int* flag = nullptr;          // [1] 1: this evaluation gathers the full rows and prunes
     unsigned long long* stats = nullptr;  // [2] {force evaluations, prune evaluations}
 };
 
@@ -31,11 +30,7 @@ cudaError_t lj_prune_alloc(LJPrune& p, int n, int stride, double rc, double delt
 void lj_prune_free(LJPrune& p);
 // After a list build (and at set-up): the next evaluation prunes.
 cudaError_t lj_prune_mark(const LJPrune& p, cudaStream_t st);
-// Before the gathers of each evaluation: flag = 1 when the pruned rows may
-// miss a pair now within the cutoff (then the displacement and cell snapshot
-// restart from this step).
-cudaError_t lj_prune_decide(const LJPrune& p, const double* hh, cudaStream_t st);
-// Output block of a pruning gather.
+// Output and decision block of the gather (lj_gather_launch's po).
 LJPruneOut lj_prune_out(const LJPrune& p);
 
 }  // namespace fmd

@@ -23,6 +23,7 @@
 #include <cmath>
 #include "step.h"
 #include "ljprune.h"
+#include "ljprune.cuh"
 #include "geom.cuh"
 #include "sg_host.h"
 #include "pdl.cuh"
@@ -358,11 +359,27 @@ __device__ void record(SysScal* S, int kind, const StepParams& p) {
 
 }  // namespace
 
+// After the LJ gather of a force evaluation (thread 0 of its reduction): when
+// that gather pruned (the same decision on the same inputs), the displacement
+// bound restarts from this step's positions and cell; counts evaluations and
+// prunes.
+__device__ void lj_prune_commit(const StepArrays& a) {
+    if (!a.prune_hb || !(a.prune_delta > 0.0)) return;
+    const double* hh = a.S->h;
+    if (lj_prune_needed(a.prune_umax, hh, a.prune_hb, a.prune_delta, a.prune_rc)) {
+        *a.prune_umax = 0ull;
+        for (int q = 0; q < 9; q++) a.prune_hb[q] = hh[q];
+        a.prune_stats[1] += 1ull;
+    }
+    a.prune_stats[0] += 1ull;
+}
+
 __device__ void end_body(const StepArrays& a, const StepParams& p, int nblk_f1, int nblk_ke, int nblk_f2,
                          double* sm) {
     double t[kRedFields];
     reduce_all(a, nblk_f1, nblk_ke, true, true, sm, t, nblk_f2);
     if (threadIdx.x != 0) return;
+    lj_prune_commit(a);
     forces_from_sums(a, t);
     kinetic_from_sums(a, t);
     SysScal* S = a.S;
@@ -465,7 +482,10 @@ __global__ void __launch_bounds__(kRedThreads) k_force_final(StepArrays a, int n
     __shared__ double sm[32 * kRedFields];
     double t[kRedFields];
     reduce_all(a, nblk_f1, 0, true, false, sm, t, a.lj_blocks);
-    if (threadIdx.x == 0) forces_from_sums(a, t);
+    if (threadIdx.x == 0) {
+        forces_from_sums(a, t);
+        lj_prune_commit(a);
+    }
 }
 
 }  // namespace
@@ -475,23 +495,19 @@ int force_partial_blocks(const StepArrays& a) {
 }
 
 // LJ term of an atomistic system: the gather over the full rows, or with
-// pruned rows the decision, then a pruning gather over the full rows and a
-// gather over the pruned rows, each returning at once unless selected.
+// pruned rows the gather that decides per evaluation between pruning the full
+// rows and walking the pruned ones.
 cudaError_t enqueue_lj(const StepArrays& a, int ff, cudaStream_t st) {
     const double* hh = a.S->h;
     if (!a.prune || a.prune->delta <= 0.0)
         return lj_gather_launch(ff, a.pos, hh, a.cnt_a, a.list_a, a.cap_a, a.in_cnt, a.in_list, a.in_cap, a.n, a.F,
-                                a.Facc, a.part_f2, st, a.precision, a.lj_shape, a.err, nullptr, 0, LJPruneOut{},
-                                a.lj_blocks);
-    const LJPrune& q = *a.prune;
-    cudaError_t e;
-    if ((e = lj_prune_decide(q, hh, st)) != cudaSuccess) return e;
-    if ((e = lj_gather_launch(ff, a.pos, hh, a.cnt_a, a.list_a, a.cap_a, a.in_cnt, a.in_list, a.in_cap, a.n, a.F,
-                              a.Facc, a.part_f2, st, a.precision, a.lj_shape, a.err, q.flag, 1, lj_prune_out(q),
-                              a.lj_blocks)) != cudaSuccess)
-        return e;
-    return lj_gather_launch(ff, a.pos, hh, a.cnt_a, a.list_a, a.cap_a, q.cnt, q.list, a.in_cap, a.n, a.F, a.Facc,
-                            a.part_f2, st, a.precision, a.lj_shape_p, a.err, q.flag, 0, LJPruneOut{}, a.lj_blocks);
+                                a.Facc, a.part_f2, st, a.precision, a.lj_shape, a.err, LJPruneOut{}, a.lj_blocks);
+    // one launch: each block decides whether this evaluation prunes (full
+    // rows, pruned rows written) or walks the pruned rows; the step's
+    // reduction then restarts the displacement bound (lj_prune_commit)
+    return lj_gather_launch(ff, a.pos, hh, a.cnt_a, a.list_a, a.cap_a, a.in_cnt, a.in_list, a.in_cap, a.n, a.F,
+                            a.Facc, a.part_f2, st, a.precision, a.lj_shape_p, a.err, lj_prune_out(*a.prune),
+                            a.lj_blocks);
 }
 
 cudaError_t enqueue_forces(const StepArrays& a, cudaStream_t st, bool judge) {

@@ -70,6 +70,9 @@ struct StepArrays {
     const LJPrune* prune = nullptr;
     const double* prune_sb = nullptr;
     unsigned long long* prune_umax = nullptr;
+    double* prune_hb = nullptr;                 // cell of the last prune
+    unsigned long long* prune_stats = nullptr;  // {evaluations, prunes}
+    double prune_delta = 0.0, prune_rc = 0.0;   // buffer (0: off) and LJ cutoff
 };
 
 struct StepParams {

@@ -49,7 +49,8 @@ void System::release() {
     cells_free(cells_a);
     cells_free(cells_b);
     lj_prune_free(prune);
-    arr.prune = nullptr; arr.prune_sb = nullptr; arr.prune_umax = nullptr;
+    arr.prune = nullptr; arr.prune_sb = nullptr; arr.prune_umax = nullptr; arr.prune_hb = nullptr;
+    arr.prune_stats = nullptr; arr.prune_delta = 0.0;
     mol_lists_free(mol);
 }
 
@@ -129,6 +130,10 @@ int System::alloc_prune(double rc_lj) {
     arr.prune = &prune;
     arr.prune_sb = prune.sb;
     arr.prune_umax = prune.words;
+    arr.prune_hb = prune.hb;
+    arr.prune_stats = prune.stats;
+    arr.prune_delta = prune.delta;
+    arr.prune_rc = prune.rc;
     return FMD_OK;
 }
 
@@ -784,6 +789,7 @@ extern "C" int fmd_system_set_lj_prune(fmd_system* s, double delta) {
     if (cudaStreamSynchronize(y.ctx->stream) != cudaSuccess) return y.ctx->fail(FMD_ERR_CUDA, "sync failed");
     y.drop_graphs();                     // captured graphs hold the old launches
     y.prune.delta = delta;
+    y.arr.prune_delta = delta;
     if (lj_prune_mark(y.prune, y.ctx->stream) != cudaSuccess) return y.ctx->fail(FMD_ERR_CUDA, "prune mark failed");
     if (y.initialized && y.p.use_graphs) {
         int rc = FMD_OK;
