@@ -179,6 +179,7 @@ k_rebo_slots(const double* __restrict__ pos, const double* __restrict__ hh, cons
     const int tot = ids ? ids[0] : na * cap;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < tot; k += gridDim.x * blockDim.x) {
         const int t = ids ? ids[1 + k] : k;
+        if (t < 0) continue;
         const int i = t / cap, jn = t - i * cap;
         if (jn >= cnt[i]) continue;
         double x, y, z;
@@ -284,6 +285,7 @@ k_rebo_bo(const Slot* __restrict__ sl, const int* __restrict__ cnt, const int* _
     const int tot = ids ? ids[0] : na * cap;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < tot; k += gridDim.x * blockDim.x) {
         const int t = ids ? ids[1 + k] : k;
+        if (t < 0) continue;
         const int c = t / cap, jn = t - c * cap;
         const int m = cnt[c];
         if (jn >= m) continue;
@@ -300,6 +302,77 @@ k_rebo_bo(const Slot* __restrict__ sl, const int* __restrict__ cnt, const int* _
             o.ok = 1.0;
         }
         bo[t] = o;
+    }
+}
+
+// Slot geometry and bond order in one pass over the warp-aligned slot index
+// (the slots of one centre are consecutive lanes of one warp): each lane
+// computes its own slot's record (as k_rebo_slots), then takes the other
+// slots' vectors from their lanes by shuffles and sums f_c G(cos) in slot
+// order (as bo_sum_sl), so the bond order needs no slot-record reads and
+// both records come out bit for bit as the two-kernel path writes them.
+__global__ void __launch_bounds__(256)
+k_rebo_geo_bo(const double* __restrict__ pos, const double* __restrict__ hh, const int* __restrict__ cnt,
+              const int* __restrict__ list, int cap, Slot* __restrict__ sl, SlotBO* __restrict__ bo,
+              const int* __restrict__ gate, int want, const int* __restrict__ ids) {
+    FMD_PDL_WAIT();
+    if (gate != nullptr && *gate != want) return;
+    __shared__ double s_hh[18];
+    if (threadIdx.x < 18) s_hh[threadIdx.x] = hh[threadIdx.x];
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int tot = ids[0];
+    for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < tot; base += gridDim.x * blockDim.x) {
+        const int k = base + lane;
+        int t = k < tot ? ids[1 + k] : -1;
+        const bool valid = t >= 0;
+        if (!valid) t = 0;
+        const int c = t / cap, jn = t - c * cap;
+        const int m = valid ? cnt[c] : 0;
+        Slot q;
+        q.dx = q.dy = q.dz = q.r = q.fc = q.dfc = q.pad = 0.0;
+        q.rinv = 0.0;
+        if (valid) {
+            double x, y, z;
+            bond_vec(pos, c, list[t], s_hh, s_hh + 9, x, y, z);
+            const double r = sqrt(norm2_rn(x, y, z));
+            q.dx = x; q.dy = y; q.dz = z; q.r = r; q.rinv = 1.0 / r;
+            // r > DMAX_CC is skipped by every use (AI:304, 370); f_c = 0 there.
+            q.fc = r > DMAX_CC ? 0.0 : sw_fc(r);
+            q.dfc = r > DMAX_CC ? 0.0 : sw_dfc(r);
+            sl[t] = q;
+        }
+        const unsigned seg = __match_any_sync(kFull, valid ? c : -1 - lane);
+        const int s0 = __ffs(seg) - 1;
+        const int span = (int)__reduce_max_sync(kFull, (unsigned)m);
+        // the reference's bond gate (AI:292-296)
+        const bool need = valid && q.r <= DMAX_CC && !(q.fc < 1e-15 && q.dfc == 0);
+        double gs = 0.0;
+        for (int kn = 0; kn < span; kn++) {
+            const int src = s0 + (kn < m ? kn : 0);
+            const double kx = __shfl_sync(kFull, q.dx, src), ky = __shfl_sync(kFull, q.dy, src),
+                         kz = __shfl_sync(kFull, q.dz, src), kri = __shfl_sync(kFull, q.rinv, src),
+                         kfc = __shfl_sync(kFull, q.fc, src);
+            if (need && kn < m && kn != jn && !(kfc < 1e-15)) {
+                const double ct = clamp1((q.dx * kx + q.dy * ky + q.dz * kz) * (q.rinv * kri));
+                double g, dg;
+                ang_g_dg(ct, g, dg);
+                gs += kfc * g;
+            }
+        }
+        if (valid) {
+            SlotBO o;
+            o.b = o.g = o.coeff = o.vr = o.dvr = o.va = o.dva = 0.0;
+            o.ok = 0.0;
+            if (need) {
+                o.g = gs;
+                o.b = 1.0 / sqrt(1.0 + gs);
+                rebo_pair_fn(q.r, q.rinv, o.vr, o.dvr, o.va, o.dva);
+                o.coeff = three_body_coeff(gs, o.b, q.fc, o.va);
+                o.ok = 1.0;
+            }
+            bo[t] = o;
+        }
     }
 }
 
@@ -378,7 +451,8 @@ k_rebo_force(const Slot* __restrict__ sl, const SlotBO* __restrict__ bo, const i
     for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < tot; base += gridDim.x * blockDim.x) {
         const int kk = base + lane;
         bool valid = kk < tot;
-        const int t = valid ? (ids ? ids[1 + kk] : kk) : 0;
+        int t = valid ? (ids ? ids[1 + kk] : kk) : 0;
+        if (t < 0) { valid = false; t = 0; }            // padding lane of the slot index
         const int i = t / cap, jn = t - i * cap;
         const int m = valid ? cnt[i] : 0;
         valid = valid && jn < m;
@@ -394,7 +468,7 @@ k_rebo_force(const Slot* __restrict__ sl, const SlotBO* __restrict__ bo, const i
             j = list[t];
             mj = cnt[j];
             if (ids) {
-                pn = ids[1 + (size_t)na * cap + t];   // partner slot j -> i of the last build
+                pn = ids[1 + (size_t)kIdsLanes * na + t];   // partner slot j -> i of the last build
             } else {
                 for (int kn = 0; kn < mj; kn++)
                     if (list[(size_t)j * cap + kn] == i) { pn = kn; break; }
@@ -827,12 +901,18 @@ cudaError_t rebo_slots_launch(const double* pos, const double* hh, const int* cn
     Slot* sl = reinterpret_cast<Slot*>(slots);
     SlotBO* bo = reinterpret_cast<SlotBO*>(slots + (size_t)na * cap * 8);
     cudaError_t e;
-    if ((e = launch_pdl(k_rebo_slots, dim3(kForceBlocks), dim3(256), 0, st, pos, hh, cnt, list, cap, na, sl, gate,
-                        want, ids)) != cudaSuccess)
-        return e;
-    if ((e = launch_pdl(k_rebo_bo, dim3(kForceBlocks), dim3(256), 0, st, (const Slot*)sl, cnt, list, cap, na, bo, gate,
-                        want, ids)) != cudaSuccess)
-        return e;
+    if (ids) {
+        if ((e = launch_pdl(k_rebo_geo_bo, dim3(kForceBlocks), dim3(256), 0, st, pos, hh, cnt, list, cap, sl, bo,
+                            gate, want, ids)) != cudaSuccess)
+            return e;
+    } else {
+        if ((e = launch_pdl(k_rebo_slots, dim3(kForceBlocks), dim3(256), 0, st, pos, hh, cnt, list, cap, na, sl, gate,
+                            want, ids)) != cudaSuccess)
+            return e;
+        if ((e = launch_pdl(k_rebo_bo, dim3(kForceBlocks), dim3(256), 0, st, (const Slot*)sl, cnt, list, cap, na, bo,
+                            gate, want, ids)) != cudaSuccess)
+            return e;
+    }
     if ((e = launch_pdl(k_rebo_force, dim3(nblocks), dim3(256), 0, st, (const Slot*)sl, (const SlotBO*)bo, cnt, list,
                         cap, na, F, part, gate, want, ids)) != cudaSuccess)
         return e;
@@ -841,31 +921,37 @@ cudaError_t rebo_slots_launch(const double* pos, const double* hh, const int* cn
 
 namespace {
 
-// Occupied slots of a REBO list in atom-major order: per 1024-atom block the
-// slot count, then each block's offset (sum of the earlier blocks) and an
-// in-block exclusive scan place atom i's slots i * cap + jn, jn < cnt[i].
+// Occupied slots of a REBO list in atom-major order, packed into 32-lane
+// bins so that no atom's slots straddle a warp: per 1024-atom block one thread
+// places the atoms one after another, starting a new bin when an atom's slots
+// would cross one (cap <= 32), and the block's length is rounded up to whole
+// bins; a scan of the block lengths then places the blocks.  Unused lanes hold
+// -1.  Layout: ids[0] = padded length P, ids[1 .. P] slot ids or -1, then at
+// ids[1 + 32 n + t] the partner slot of slot t.
 constexpr int kIdsBlock = 1024;
 
 __global__ void __launch_bounds__(kIdsBlock) k_ids_count(const int* __restrict__ cnt, int cap, int n,
-                                                          int* __restrict__ bsum) {
-    __shared__ int sw[kIdsBlock / 32];
+                                                          int* __restrict__ bsum, int* __restrict__ istart) {
+    __shared__ int sm_cnt[kIdsBlock];
     const int i = blockIdx.x * kIdsBlock + threadIdx.x;
-    int v = i < n ? min(cnt[i], cap) : 0;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
-    if ((threadIdx.x & 31) == 0) sw[threadIdx.x >> 5] = v;
+    sm_cnt[threadIdx.x] = i < n ? min(cnt[i], cap) : 0;
     __syncthreads();
-    if (threadIdx.x < 32) {
-        int u = sw[threadIdx.x];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) u += __shfl_xor_sync(kFull, u, o);
-        if (threadIdx.x == 0) bsum[blockIdx.x] = u;
+    if (threadIdx.x == 0) {
+        int pos = 0;
+        const int na = min(kIdsBlock, n - (int)blockIdx.x * kIdsBlock);
+        for (int k = 0; k < na; k++) {
+            const int m = sm_cnt[k];
+            if ((pos & 31) + m > 32) pos = (pos + 31) & ~31;
+            istart[blockIdx.x * kIdsBlock + k] = pos;
+            pos += m;
+        }
+        bsum[blockIdx.x] = (pos + 31) & ~31;
     }
 }
 
 __global__ void __launch_bounds__(kIdsBlock) k_ids_emit(const int* __restrict__ cnt, int cap, int n,
-                                                         const int* __restrict__ bsum, int* __restrict__ ids) {
-    __shared__ int sw[kIdsBlock / 32];
+                                                         const int* __restrict__ bsum,
+                                                         const int* __restrict__ istart, int* __restrict__ ids) {
     __shared__ int s_base;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     if (w == 0) {                                  // offset of this block
@@ -875,39 +961,27 @@ __global__ void __launch_bounds__(kIdsBlock) k_ids_emit(const int* __restrict__ 
         for (int o = 16; o > 0; o >>= 1) b += __shfl_xor_sync(kFull, b, o);
         if (lane == 0) s_base = b;
     }
+    __syncthreads();
+    const int base = s_base, len = bsum[blockIdx.x];
+    for (int k = threadIdx.x; k < len; k += kIdsBlock) ids[1 + base + k] = -1;
+    __syncthreads();
     const int i = blockIdx.x * kIdsBlock + threadIdx.x;
-    const int m = i < n ? min(cnt[i], cap) : 0;
-    int x = m;                                     // inclusive warp scan
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(kFull, x, o);
-        if (lane >= o) x += y;
+    if (i < n) {
+        const int m = min(cnt[i], cap), off = base + istart[i];
+        for (int jn = 0; jn < m; jn++) ids[1 + off + jn] = i * cap + jn;
     }
-    if (lane == 31) sw[w] = x;
-    __syncthreads();
-    if (w == 0) {
-        int y = sw[lane];
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int z = __shfl_up_sync(kFull, y, o);
-            if (lane >= o) y += z;
-        }
-        sw[lane] = y;                              // inclusive over warps
-    }
-    __syncthreads();
-    const int off = s_base + (w > 0 ? sw[w - 1] : 0) + x - m;
-    for (int jn = 0; jn < m; jn++) ids[1 + off + jn] = i * cap + jn;
-    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == kIdsBlock - 1) ids[0] = off + m;
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) ids[0] = base + len;
 }
 
 // Partner slot of every occupied slot i -> j: the position of i in j's row,
-// -1 when j's row lacks i (rows cut at cap); written after the slot ids.
+// -1 when j's row lacks i (rows cut at cap).
 __global__ void k_ids_partner(const int* __restrict__ cnt, const int* __restrict__ list, int cap, int n,
                               int* __restrict__ ids) {
     const int tot = ids[0];
-    int* pslot = ids + 1 + (size_t)n * cap;
+    int* pslot = ids + 1 + (size_t)kIdsLanes * n;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < tot; k += gridDim.x * blockDim.x) {
         const int t = ids[1 + k];
+        if (t < 0) continue;
         const int i = t / cap;
         const int j = list[t];
         const int mj = min(cnt[j], cap);
@@ -920,13 +994,16 @@ __global__ void k_ids_partner(const int* __restrict__ cnt, const int* __restrict
 
 }  // namespace
 
-int rebo_ids_scratch(int n) { return (n + kIdsBlock - 1) / kIdsBlock; }
+int rebo_ids_scratch(int n) { return (n + kIdsBlock - 1) / kIdsBlock + n; }
 
-cudaError_t rebo_ids_build(const int* cnt, const int* list, int cap, int n, int* ids, int* bsum, cudaStream_t st) {
+cudaError_t rebo_ids_build(const int* cnt, const int* list, int cap, int n, int* ids, int* scratch, cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
-    const int nb = rebo_ids_scratch(n);
-    k_ids_count<<<nb, kIdsBlock, 0, st>>>(cnt, cap, n, bsum);
-    k_ids_emit<<<nb, kIdsBlock, 0, st>>>(cnt, cap, n, bsum, ids);
+    if (cap > 32) return cudaErrorInvalidValue;
+    const int nb = (n + kIdsBlock - 1) / kIdsBlock;
+    int* bsum = scratch;
+    int* istart = scratch + nb;
+    k_ids_count<<<nb, kIdsBlock, 0, st>>>(cnt, cap, n, bsum, istart);
+    k_ids_emit<<<nb, kIdsBlock, 0, st>>>(cnt, cap, n, bsum, istart, ids);
     k_ids_partner<<<kForceBlocks, 256, 0, st>>>(cnt, list, cap, n, ids);
     return cudaGetLastError();
 }

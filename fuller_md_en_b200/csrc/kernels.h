@@ -79,15 +79,20 @@ cudaError_t rebo_launch_gated(const double* pos, const double* hh, const int* cn
 // na * cap bond-order records; device scratch owned by the caller); otherwise
 // as rebo_launch_gated (gate may be null).
 constexpr int kReboSlotDoubles = 16;
-// ids (may be null): the occupied slots in atom-major order, ids[0] their
-// number and ids[1 + k] the slot i * cap + jn, then at ids[1 + na * cap + t]
-// the partner slot of slot t (i's position in j's row, -1 if absent)
-// (rebo_ids_build); threads then walk only the occupied slots.
+// ids (may be null): the occupied slots in atom-major order packed into
+// 32-lane bins (no atom's slots cross a bin; unused lanes -1), ids[0] the
+// padded length and ids[1 + k] the slot i * cap + jn, then at
+// ids[1 + kIdsLanes * na + t] the partner slot of slot t (i's position in j's
+// row, -1 if absent) (rebo_ids_build); lanes then walk only occupied slots,
+// and the slots of one atom share a warp.
 cudaError_t rebo_slots_launch(const double* pos, const double* hh, const int* cnt, const int* list, int cap,
                               int na, double* slots, double* F, double* part, int nblocks, const int* gate,
                               int want, cudaStream_t st, const int* ids = nullptr);
-// Builds ids (1 + 2 n cap ints) from the list; bsum: rebo_ids_scratch(n) ints.
-cudaError_t rebo_ids_build(const int* cnt, const int* list, int cap, int n, int* ids, int* bsum, cudaStream_t st);
+// Builds ids (1 + kIdsLanes n + n cap ints) from the list (cap <= 32);
+// scratch: rebo_ids_scratch(n) ints.
+constexpr int kIdsLanes = 32;
+cudaError_t rebo_ids_build(const int* cnt, const int* list, int cap, int n, int* ids, int* scratch,
+                           cudaStream_t st);
 int rebo_ids_scratch(int n);
 // Half-list LJ gather (a8, a14): F[i] = Facc[i] + LJ(i); Facc[i] zeroed
 // (unless Facc == F).  ff: FMD_FF_AIREBO / FMD_FF_MM.  precision:

@@ -48,7 +48,7 @@ struct StepArrays {
     const int* in_cnt = nullptr; const int* in_list = nullptr; int in_cap = 0;  // LJ full rows (incoming + own)
     const int* cnt_b = nullptr; const int* list_b = nullptr; int cap_b = 0;     // REBO
     double* rebo_slots = nullptr;   // [n * cap_b * kReboSlotDoubles] REBO slot records (fast path)
-    const int* rebo_ids = nullptr;  // [1 + 2 n cap_b] occupied REBO slots and partner slots of the last build
+    const int* rebo_ids = nullptr;  // occupied REBO slots (warp-aligned) and partner slots of the last build
     double* part_f1 = nullptr;  // REBO / rigid / bonded partials
     double* part_f2 = nullptr;  // LJ partials
     double* part_f3 = nullptr;  // Coulomb partials

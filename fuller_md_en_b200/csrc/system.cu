@@ -107,7 +107,7 @@ int System::alloc_lists(double rc_list_a, int cap_a_, double rc_list_b, int cap_
         if (alloc(&arr.rebo_slots, (size_t)n * cap_b_ * kReboSlotDoubles, (const double*)nullptr))
             return ctx->fail(FMD_ERR_CUDA, "list allocation failed");
         int* ids;
-        if (alloc(&ids, 1 + 2 * (size_t)n * cap_b_, (const int*)nullptr) ||
+        if (alloc(&ids, 1 + (size_t)kIdsLanes * n + (size_t)n * cap_b_, (const int*)nullptr) ||
             alloc(&rebo_bsum, (size_t)rebo_ids_scratch(n), (const int*)nullptr))
             return ctx->fail(FMD_ERR_CUDA, "list allocation failed");
         cudaMemsetAsync(ids, 0, sizeof(int), ctx->stream);
