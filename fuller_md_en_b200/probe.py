@@ -8,10 +8,12 @@ builds the benchmark system (C60 FCC nc=5, 30,000 atoms, jitter 0.01 A,
 untimed launch first, then the timed ones, then the current forces are
 recomputed).  FMD_LJ_SHAPE pins the LJ gather's launch shape (threads,
 entries per lane, row feed) so the launch sequence does not depend on the
-autotuner: with --steps 0 and --reps 1, the LJ gather launches are set-up
-(full rows, then pruned rows gated off), the untimed and the timed launch
-of the stage, then the recomputation's two; a profiler capturing the
-gather's launch 4 sees the timed, warm launch on the benchmark state.
+autotuner: with --steps 0 and --reps 1, the LJ gather launches are set-up's
+(one, pruning the full rows), the untimed and the timed launch of the stage,
+then the recomputation's; a profiler capturing the gather's launch 3 sees
+the timed, warm launch on the benchmark state.  For --stage rebo the REBO
+kernels launch twice per force evaluation (geometry + bond order, forces):
+set-up, one per step, then the untimed and the timed evaluation.
 Prints one JSON line.
 """
 from __future__ import annotations
