@@ -94,6 +94,8 @@ extern "C" int fmd_ctx_destroy(fmd_ctx* ctx) {
     if (!ctx) return FMD_OK;
     cudaStreamSynchronize(ctx->stream);
     for (auto& b : ctx->scratch) if (b.p) cudaFree(b.p);
+    for (auto& b : ctx->mem_cache) cudaFree(b.second);
+    ctx->mem_cache.clear();
     if (ctx->d_err) cudaFree(ctx->d_err);
     if (ctx->h_err) cudaFreeHost(ctx->h_err);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);

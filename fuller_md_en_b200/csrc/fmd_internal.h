@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <cstddef>
 #include <cstdint>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -66,6 +67,24 @@ struct fmd_ctx {
     double* h_scalars = nullptr;
     // pair arithmetic of the atomistic LJ terms in host-pointer calls (fmd_precision)
     int precision = FMD_PREC_FP64;
+    // Device blocks released by systems of this context, by size: the next
+    // system of the same size takes them instead of mapping fresh memory
+    // (cudaMalloc of a few hundred MB costs milliseconds and varies with the
+    // process's allocation history).  Freed with the context.
+    std::multimap<size_t, void*> mem_cache;
+    cudaError_t dev_alloc(void** p, size_t bytes) {
+        auto it = mem_cache.find(bytes);
+        if (it != mem_cache.end()) {
+            *p = it->second;
+            mem_cache.erase(it);
+            return cudaSuccess;
+        }
+        return cudaMalloc(p, bytes);
+    }
+    // The caller has synchronised every stream that used the block.
+    void dev_release(void* p, size_t bytes) {
+        if (p) mem_cache.emplace(bytes, p);
+    }
 
     int fail(int code, const std::string& m) {
         last_code = code;

@@ -34,36 +34,13 @@ __global__ void k_prune_mark(unsigned long long* words) { *words = kPruneMark; }
 
 }  // namespace
 
-cudaError_t lj_prune_alloc(LJPrune& p, int n, int stride, double rc, double delta, cudaStream_t st) {
-    p = LJPrune();
-    cudaError_t e = cudaSuccess;
-    auto A = [&](void** q, size_t bytes, bool zero) {
-        if (e == cudaSuccess) e = cudaMalloc(q, bytes);
-        if (e == cudaSuccess && zero) e = cudaMemsetAsync(*q, 0, bytes, st);
-    };
-    // the rows are written by the first evaluation (a prune) before any read
-    A((void**)&p.cnt, sizeof(int) * n, true);
-    A((void**)&p.list, sizeof(int) * (size_t)n * stride, false);
-    A((void**)&p.sb, sizeof(double) * 3 * n, true);
-    A((void**)&p.hb, sizeof(double) * 9, true);
-    A((void**)&p.words, sizeof(unsigned long long), true);
-    A((void**)&p.stats, sizeof(unsigned long long) * 2, true);
+cudaError_t lj_prune_clear(const LJPrune& p, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(p.cnt, 0, sizeof(int) * p.n, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(p.sb, 0, sizeof(double) * 3 * p.n, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(p.hb, 0, sizeof(double) * 9, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(p.stats, 0, sizeof(unsigned long long) * 2, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(p.words, 0x7F, sizeof(unsigned long long), st);
-    if (e != cudaSuccess) {
-        lj_prune_free(p);
-        return e;
-    }
-    p.n = n;
-    p.stride = stride;
-    p.rc = rc;
-    p.delta = delta;
-    p.ok = true;
-    return cudaSuccess;
-}
-
-void lj_prune_free(LJPrune& p) {
-    cudaFree(p.cnt); cudaFree(p.list); cudaFree(p.sb); cudaFree(p.hb); cudaFree(p.words); cudaFree(p.stats);
-    p = LJPrune();
+    return e;
 }
 
 cudaError_t lj_prune_mark(const LJPrune& p, cudaStream_t st) {

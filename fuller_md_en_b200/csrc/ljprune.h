@@ -24,10 +24,10 @@ struct LJPrune {
     unsigned long long* stats = nullptr;  // [2] {force evaluations, prune evaluations}
 };
 
-// The small arrays are cleared on st; the row buffer is written by the first
-// evaluation (a prune) before any read.
-cudaError_t lj_prune_alloc(LJPrune& p, int n, int stride, double rc, double delta, cudaStream_t st);
-void lj_prune_free(LJPrune& p);
+// Clears the counters, snapshot and cell on st and marks the first
+// evaluation as a prune (the arrays are owned by the system; the row buffer
+// is written by that prune before any read).
+cudaError_t lj_prune_clear(const LJPrune& p, cudaStream_t st);
 // After a list build (and at set-up): the next evaluation prunes.
 cudaError_t lj_prune_mark(const LJPrune& p, cudaStream_t st);
 // Output and decision block of the gather (lj_gather_launch's po).

@@ -21,14 +21,8 @@ namespace fmd {
 
 namespace {
 template <class T>
-cudaError_t dalloc(T** p, size_t count) {
-    return cudaMalloc((void**)p, sizeof(T) * (count > 0 ? count : 1));
-}
-template <class T>
-cudaError_t dupload(T** p, const T* src, size_t count, cudaStream_t st) {
-    cudaError_t e = dalloc(p, count);
-    if (e != cudaSuccess || src == nullptr || count == 0) return e;
-    return cudaMemcpyAsync(*p, src, sizeof(T) * count, cudaMemcpyHostToDevice, st);
+size_t dbytes(size_t count) {
+    return sizeof(T) * (count > 0 ? count : 1);
 }
 }  // namespace
 
@@ -44,11 +38,17 @@ void System::release() {
     if (sg) sg::work_free(sg->work);
     sg.reset();
     arr.sg = nullptr;
-    for (void* p : owned) cudaFree(p);
+    if (ctx) {
+        // every stream that used these blocks has finished with them
+        cudaStreamSynchronize(ctx->stream);
+        for (auto& b : owned) ctx->dev_release(b.first, b.second);
+    } else {
+        for (auto& b : owned) cudaFree(b.first);
+    }
     owned.clear();
     cells_free(cells_a);
     cells_free(cells_b);
-    lj_prune_free(prune);
+    prune = LJPrune();                  // its arrays are among the owned blocks
     arr.prune = nullptr; arr.prune_sb = nullptr; arr.prune_umax = nullptr; arr.prune_hb = nullptr;
     arr.prune_stats = nullptr; arr.prune_delta = 0.0;
     mol_lists_free(mol);
@@ -56,9 +56,12 @@ void System::release() {
 
 template <class T>
 cudaError_t System::alloc(T** p, size_t count, const T* src) {
-    cudaError_t e = dupload(p, src, count, ctx->stream);
-    if (e == cudaSuccess) owned.push_back((void*)*p);
-    return e;
+    const size_t bytes = dbytes<T>(count);
+    cudaError_t e = ctx->dev_alloc((void**)p, bytes);
+    if (e != cudaSuccess) return e;
+    owned.emplace_back((void*)*p, bytes);
+    if (src == nullptr || count == 0) return cudaSuccess;
+    return cudaMemcpyAsync(*p, src, sizeof(T) * count, cudaMemcpyHostToDevice, ctx->stream);
 }
 
 int System::alloc_common(const double* pos_h, const double* vel_h, const double* h_h, const fmd_npt* npt_h) {
@@ -125,8 +128,20 @@ int System::alloc_lists(double rc_list_a, int cap_a_, double rc_list_b, int cap_
 // Rebuild of every list this kind uses, as the driver does at gstep % nlup == 0.
 int System::alloc_prune(double rc_lj) {
     if (!arr.in_list) return FMD_OK;
-    if (lj_prune_alloc(prune, arr.n, arr.in_cap, rc_lj, kPruneDelta, ctx->stream) != cudaSuccess)
+    const int n = arr.n;
+    LJPrune q;
+    if (alloc(&q.cnt, n, (const int*)nullptr) || alloc(&q.list, (size_t)n * arr.in_cap, (const int*)nullptr) ||
+        alloc(&q.sb, 3 * (size_t)n, (const double*)nullptr) || alloc(&q.hb, 9, (const double*)nullptr) ||
+        alloc(&q.words, 1, (const unsigned long long*)nullptr) ||
+        alloc(&q.stats, 2, (const unsigned long long*)nullptr))
         return ctx->fail(FMD_ERR_CUDA, "device allocation failed");
+    q.n = n;
+    q.stride = arr.in_cap;
+    q.rc = rc_lj;
+    q.delta = kPruneDelta;
+    q.ok = true;
+    if (lj_prune_clear(q, ctx->stream) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "device allocation failed");
+    prune = q;
     arr.prune = &prune;
     arr.prune_sb = prune.sb;
     arr.prune_umax = prune.words;

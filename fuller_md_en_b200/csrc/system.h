@@ -27,7 +27,7 @@ struct System {
     bool initialized = false;
     // one graph per {rebuild, cold/warm phase, judge of the learned REBO term}
     cudaGraphExec_t graphs[2][2][2] = {};
-    std::vector<void*> owned;
+    std::vector<std::pair<void*, size_t>> owned;   // blocks from the context's cache, with their sizes
     std::unique_ptr<SgStep> sg;        // learned REBO term (AIREBO only), nullptr: plain
 
     template <class T> cudaError_t alloc(T** p, size_t count, const T* src);
