@@ -248,7 +248,7 @@ k_mol_rows(const double* __restrict__ pos, const double* __restrict__ hh, int n,
 constexpr int kFlatU = 4;
 constexpr int kFlatWarps = 8;
 
-__global__ void __launch_bounds__(32 * kFlatWarps)
+__global__ void __launch_bounds__(32 * kFlatWarps, 3)
 k_mol_half_flat(const double* __restrict__ pos, const double* __restrict__ hh, int n, const int* __restrict__ off,
                 const int* __restrict__ amol, const int* __restrict__ npart, const int* __restrict__ part, int pmax,
                 int S, const float4* __restrict__ pos32, double rc2, int cap, int* __restrict__ cnt,
