@@ -419,6 +419,17 @@ class System:
         self.ctx.check(self.ctx.lib.fmd_system_lj_rows(self.h, _i(full), _i(pruned)), "fmd_system_lj_rows")
         return full, pruned
 
+    def lj_full_rows(self):
+        """(row lengths, rows as an (n, stride) array) of the LJ gather's full rows of the last build."""
+        stride = ctypes.c_int(0)
+        self.ctx.check(self.ctx.lib.fmd_system_lj_full_rows(self.h, None, None, ctypes.byref(stride)),
+                       "fmd_system_lj_full_rows")
+        cnt = np.zeros(self.n, np.int32)
+        lst = np.zeros(self.n * max(stride.value, 1), np.int32)
+        self.ctx.check(self.ctx.lib.fmd_system_lj_full_rows(self.h, _i(cnt), _i(lst), ctypes.byref(stride)),
+                       "fmd_system_lj_full_rows")
+        return cnt, lst.reshape(self.n, -1)
+
     def lists(self, cap_a: int, cap_b: int = 0):
         n = self.n
         ca, la = np.zeros(n, np.int32), np.zeros(n * cap_a, np.int32)

@@ -120,7 +120,7 @@ __global__ void k_mol_pairs(const double* __restrict__ hh, int M, const double* 
         if (B < M && B != A) {
             double dx = cen[3 * B] - cx, dy = cen[3 * B + 1] - cy, dz = cen[3 * B + 2] - cz;
             mimg(dx, dy, dz, hi, h);
-            const double lim = (rc + ra + rad[B]) * (1.0 + 1e-9) + 1e-6;   // rounding margin
+            const double lim = (rc + (ra + rad[B])) * (1.0 + 1e-9) + 1e-6;   // rounding margin; symmetric in A, B
             ok = dx * dx + dy * dy + dz * dz <= lim * lim;
         }
         const unsigned m = __ballot_sync(kFull, ok);
@@ -252,7 +252,8 @@ __global__ void __launch_bounds__(32 * kFlatWarps, 3)
 k_mol_half_flat(const double* __restrict__ pos, const double* __restrict__ hh, int n, const int* __restrict__ off,
                 const int* __restrict__ amol, const int* __restrict__ npart, const int* __restrict__ part, int pmax,
                 int S, const float4* __restrict__ pos32, double rc2, int cap, int* __restrict__ cnt,
-                int* __restrict__ list, int* __restrict__ dropped, const int* __restrict__ flag) {
+                int* __restrict__ list, int* __restrict__ dropped, const int* __restrict__ flag,
+                unsigned* __restrict__ bm, int W) {
     if (flag[0] == 0) return;
     __shared__ double s_hh[18];
     __shared__ int s_start[kFlatWarps][kMolPartners];
@@ -285,6 +286,9 @@ k_mol_half_flat(const double* __restrict__ pos, const double* __restrict__ hh, i
         const bool screen = sc.on && pi.w != 0.0f;
         int* row = list + (size_t)i * cap;
         int emitted = 0;
+        // candidate bitmap: word w of atom i (bit b = candidate 32 w + b kept
+        // in the row) at bm[(A W + w) S + i - off[A]]
+        unsigned* bmA = bm ? bm + (size_t)A * W * S + (i - off[A]) : nullptr;
         for (int k0 = 0; k0 < ncand; k0 += 32 * kFlatU) {
             int jj[kFlatU];
             float4 q[kFlatU];
@@ -317,6 +321,12 @@ k_mol_half_flat(const double* __restrict__ pos, const double* __restrict__ hh, i
                 const unsigned m = __ballot_sync(kFull, ok);
                 const int kk = emitted + __popc(m & below);
                 if (ok && kk < cap) row[kk] = jj[u];
+                if (bmA) {
+                    // the slice's entries that fit in the row (row position < cap)
+                    const unsigned kept = __ballot_sync(kFull, ok && kk < cap);
+                    const int ks = k0 + 32 * u;
+                    if (lane == 0 && ks < ncand) bmA[(size_t)(ks >> 5) * S] = kept;
+                }
                 emitted += __popc(m);
             }
         }
@@ -325,6 +335,163 @@ k_mol_half_flat(const double* __restrict__ pos, const double* __restrict__ hh, i
             cnt[i] = emitted < cap ? emitted : cap;
             if (emitted > cap && dropped) atomicAdd(dropped, emitted - cap);
         }
+    }
+}
+
+// First index of a partner >= key in an ascending partner list.
+__device__ __forceinline__ int lower_bound_part(const int* pa, int n, int key) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (pa[mid] < key) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+// For each lower partner A = part[B][q] (A < B): rev[B][q] = the position of
+// B among the higher partners of A, i.e. the index of B's atoms (times the
+// molecule size) in the candidate sequence of A's atoms.  One warp per
+// molecule, binary searches per lane.  The lists are ascending, and symmetric
+// (the pair test is odd in the centre difference and symmetric in the radii);
+// should B be missing all the same, the molecule builder is switched off for
+// this build (flag[0] = 0) and the cell-list path builds.
+__global__ void k_mol_rev(int M, const int* __restrict__ npart, const int* __restrict__ part, int pmax,
+                          int* __restrict__ rev, int* __restrict__ flag) {
+    if (flag[0] == 0) return;
+    const int lane = threadIdx.x & 31;
+    const int B = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (B >= M) return;
+    const int nb = npart[B];
+    for (int q = lane; q < nb; q += 32) {
+        const int A = part[(size_t)B * pmax + q];
+        if (A > B) break;                              // ascending: the rest are higher
+        const int* pa = part + (size_t)A * pmax;
+        const int na = npart[A];
+        const int at = lower_bound_part(pa, na, B);
+        rev[(size_t)B * pmax + q] = at - lower_bound_part(pa, na, A);
+        if (at >= na || pa[at] != B) atomicExch(&flag[0], 0);
+    }
+}
+
+// Full LJ rows from the candidate bitmaps of the flat walk, for equal
+// molecules of S atoms (32 <= S <= 64, off[A] = A S): atom j = B S + jb is in
+// the kept row of i = A S + ia (A < B) iff bit rev[B][q] S + jb of i's bitmap
+// is set.  Two blocks per molecule B, one per half of its atoms (jb < 32,
+// jb >= 32): the bitmap words that hold the half's bits (2 words per atom of
+// A) are staged in shared memory for up to kInChunk lower partners at a time,
+// then warp w emits the rows of atoms jb = 32 h + w + 8 t: for each lower
+// partner A (ascending) a ballot over A's atoms gives the entries in
+// ascending order.  Row j thus holds the atoms i < j whose kept row lists j,
+// ascending, then j's own row -- the rows the transpose (nlist_transpose)
+// builds, without atomics or a sort.  The own rows are copied with 8 loads in
+// flight per lane.
+constexpr int kInChunk = 32;
+constexpr int kInWarps = 8;
+constexpr int kInAtoms = 32 / kInWarps;               // atoms per warp
+
+__global__ void __launch_bounds__(32 * kInWarps)
+k_mol_incoming(int M, int S, const int* __restrict__ npart, const int* __restrict__ part, int pmax,
+               const int* __restrict__ rev, int W, const unsigned* __restrict__ bm, int cap,
+               const int* __restrict__ cnt, const int* __restrict__ list, int* __restrict__ in_cnt,
+               int* __restrict__ in_list, int in_cap, DevErr* err, const int* __restrict__ flag) {
+    if (flag[0] == 0) return;
+    __shared__ int s_a[kMolPartners];                 // lower partners, ascending
+    __shared__ int s_b[kMolPartners];                 // first bit of the half's atoms in their bitmaps
+    __shared__ unsigned s_bits[kInChunk][2][64];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned below = (1u << lane) - 1u;
+    const int lim = in_cap - cap;
+    for (int g = blockIdx.x; g < 2 * M; g += gridDim.x) {
+        const int B = g >> 1, h0 = (g & 1) * 32;
+        const int nh = S - h0 < 32 ? S - h0 : 32;    // atoms in this half (0 when S = 32, h0 = 32)
+        if (nh <= 0) continue;
+        int mo[kInAtoms];
+#pragma unroll
+        for (int t = 0; t < kInAtoms; t++) {
+            const int jb = w + kInWarps * t;
+            mo[t] = jb < nh ? cnt[B * S + h0 + jb] : 0;
+        }
+        const int np = npart[B];
+        bool low = false;
+        for (int q = threadIdx.x; q < np; q += blockDim.x) {     // np <= kMolPartners
+            const int A = part[(size_t)B * pmax + q];
+            if (A < B) {
+                low = true;
+                s_a[q] = A;
+                s_b[q] = rev[(size_t)B * pmax + q] * S + h0;
+            }
+        }
+        const int nlow = __syncthreads_count(low);    // ascending: the lower partners come first
+        int em[kInAtoms];
+#pragma unroll
+        for (int t = 0; t < kInAtoms; t++) em[t] = 0;
+        for (int c0 = 0; c0 < nlow; c0 += kInChunk) {
+            const int nc = nlow - c0 < kInChunk ? nlow - c0 : kInChunk;
+            for (int x = threadIdx.x; x < nc * 2 * S; x += blockDim.x) {
+                const int c = x / (2 * S), r = x - c * 2 * S;
+                const int k = r / S, ia = r - k * S;
+                const int b0 = s_b[c0 + c];
+                // words (b0 >> 5) .. ((b0 + nh - 1) >> 5) hold the half's bits
+                if (k <= ((b0 & 31) + nh - 1) >> 5)
+                    s_bits[c][k][ia] = bm[((size_t)s_a[c0 + c] * W + (b0 >> 5) + k) * S + ia];
+            }
+            __syncthreads();
+            for (int c = 0; c < nc; c++) {
+                const int a0 = s_a[c0 + c] * S;
+                const int sb = s_b[c0 + c] & 31;
+#pragma unroll
+                for (int t = 0; t < kInAtoms; t++) {
+                    const int jb = w + kInWarps * t;
+                    if (jb < nh) {
+                        const int pos = sb + jb, k = pos >> 5, b = pos & 31;
+                        const bool ok0 = (s_bits[c][k][lane] >> b) & 1u;
+                        const bool ok1 = lane + 32 < S && ((s_bits[c][k][lane + 32] >> b) & 1u);
+                        const unsigned m0 = __ballot_sync(kFull, ok0), m1 = __ballot_sync(kFull, ok1);
+                        int* row = in_list + (size_t)(B * S + h0 + jb) * in_cap;
+                        const int p0 = em[t] + __popc(m0 & below);
+                        const int p1 = em[t] + __popc(m0) + __popc(m1 & below);
+                        if (ok0 && p0 < lim) row[p0] = a0 + lane;
+                        if (ok1 && p1 < lim) row[p1] = a0 + lane + 32;
+                        em[t] += __popc(m0) + __popc(m1);
+                    }
+                }
+            }
+            __syncthreads();                          // s_bits is restaged
+        }
+        // own rows after the incoming entries
+        int mmax = 0;
+#pragma unroll
+        for (int t = 0; t < kInAtoms; t++) mmax = mo[t] > mmax ? mo[t] : mmax;
+        for (int k0 = lane; k0 < mmax; k0 += 64) {
+            int v[kInAtoms][2];
+#pragma unroll
+            for (int t = 0; t < kInAtoms; t++)
+#pragma unroll
+                for (int u = 0; u < 2; u++) {
+                    const int k = k0 + 32 * u;
+                    v[t][u] = k < mo[t] ? list[(size_t)(B * S + h0 + w + kInWarps * t) * cap + k] : 0;
+                }
+#pragma unroll
+            for (int t = 0; t < kInAtoms; t++) {
+                const int kept = em[t] < lim ? em[t] : lim;
+                int* row = in_list + (size_t)(B * S + h0 + w + kInWarps * t) * in_cap + kept;
+#pragma unroll
+                for (int u = 0; u < 2; u++)
+                    if (k0 + 32 * u < mo[t]) row[k0 + 32 * u] = v[t][u];
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < kInAtoms; t++) {
+            const int jb = w + kInWarps * t;
+            if (lane == 0 && jb < nh) {
+                const int j = B * S + h0 + jb;
+                in_cnt[j] = (em[t] < lim ? em[t] : lim) + mo[t];
+                if (em[t] > lim && atomicCAS(&err->code, FMD_OK, FMD_ERR_CAPACITY) == FMD_OK) {
+                    err->where = K_TRANSPOSE; err->index = j; err->value = em[t];
+                }
+            }
+        }
+        __syncthreads();                              // s_a, s_b are refilled
     }
 }
 
@@ -358,6 +525,8 @@ cudaError_t mol_lists_alloc(MolLists& m, int n, const int* mol_id_host) {
     m.usize = m.max_atoms;
     for (int a = 0; a < M; a++)
         if (off[a + 1] - off[a] != m.usize) m.usize = 0;
+    m.masks = m.usize >= 32 && m.usize <= 64;
+    m.words = (m.pmax * m.usize + 31) / 32;
     cudaError_t e;
     auto A = [&](void** p, size_t bytes) {
         if (e == cudaSuccess) e = cudaMalloc(p, bytes);
@@ -368,6 +537,10 @@ cudaError_t mol_lists_alloc(MolLists& m, int n, const int* mol_id_host) {
     A((void**)&m.cen, sizeof(double) * 3 * M);
     A((void**)&m.rad, sizeof(double) * M);
     A((void**)&m.pos32, sizeof(float4) * n);
+    if (m.masks) {
+        A((void**)&m.bm, sizeof(unsigned) * (size_t)M * m.words * m.usize);
+        A((void**)&m.rev, sizeof(int) * (size_t)M * m.pmax);
+    }
     A((void**)&m.npart, sizeof(int) * M);
     A((void**)&m.part, sizeof(int) * (size_t)M * m.pmax);
     A((void**)&m.flag, sizeof(int) * 2);
@@ -384,7 +557,8 @@ cudaError_t mol_lists_alloc(MolLists& m, int n, const int* mol_id_host) {
 }
 
 void mol_lists_free(MolLists& m) {
-    cudaFree(m.off); cudaFree(m.amol); cudaFree(m.cen); cudaFree(m.rad); cudaFree(m.pos32); cudaFree(m.npart); cudaFree(m.part);
+    cudaFree(m.off); cudaFree(m.amol); cudaFree(m.cen); cudaFree(m.rad); cudaFree(m.pos32); cudaFree(m.bm);
+    cudaFree(m.rev); cudaFree(m.npart); cudaFree(m.part);
     cudaFree(m.flag);
     m = MolLists();
 }
@@ -394,6 +568,7 @@ cudaError_t mol_partners(MolLists& m, const double* pos, const double* hh, doubl
     k_mol_centre<<<wblocks, 256, 0, st>>>(pos, hh, m.off, m.M, m.cen, m.rad, m.pos32, m.flag);
     k_mol_pairs<<<wblocks, 256, 0, st>>>(hh, m.M, m.cen, m.rad, rc, m.pmax, m.npart, m.part, m.flag);
     k_mol_decide<<<1, 32, 0, st>>>(hh, m.flag);
+    if (m.masks) k_mol_rev<<<wblocks, 256, 0, st>>>(m.M, m.npart, m.part, m.pmax, m.rev, m.flag);
     return cudaGetLastError();
 }
 
@@ -409,11 +584,21 @@ cudaError_t mol_rows_half(const MolLists& m, const double* pos, const double* hh
     if (m.usize > 0) {
         k_mol_half_flat<<<kRowBlocksMol, 32 * kFlatWarps, 0, st>>>(pos, hh, m.n, m.off, m.amol, m.npart, m.part,
                                                                    m.pmax, m.usize, m.pos32, rc2, cap, cnt, list,
-                                                                   dropped, m.flag);
+                                                                   dropped, m.flag, m.masks ? m.bm : nullptr,
+                                                                   m.words);
         return cudaGetLastError();
     }
     k_mol_rows<0><<<kRowBlocksMol, 256, 0, st>>>(pos, hh, m.n, m.off, m.amol, m.npart, m.part, m.pmax, m.pos32, rc2,
                                                  cap, cnt, list, dropped, m.flag);
+    return cudaGetLastError();
+}
+
+cudaError_t mol_rows_incoming(const MolLists& m, int cap, const int* cnt, const int* list, int* in_cnt,
+                              int* in_list, int in_cap, DevErr* err, cudaStream_t st) {
+    if (!m.masks) return cudaErrorInvalidValue;
+    const int blocks = 2 * m.M < kRowBlocksMol ? 2 * m.M : kRowBlocksMol;
+    k_mol_incoming<<<blocks, 32 * kInWarps, 0, st>>>(m.M, m.usize, m.npart, m.part, m.pmax, m.rev, m.words, m.bm,
+                                                     cap, cnt, list, in_cnt, in_list, in_cap, err, m.flag);
     return cudaGetLastError();
 }
 

@@ -17,6 +17,10 @@ struct MolLists {
     int n = 0, M = 0, pmax = 0;
     int max_atoms = 0;        // atoms of the largest molecule
     int usize = 0;            // atoms of every molecule when all have the same count, else 0
+    bool masks = false;       // 32 <= usize <= 64: the full LJ rows come from the candidate bitmaps
+    int words = 0;            // bitmap words per atom: ceil(pmax * usize / 32)
+    unsigned* bm = nullptr;   // [M * words * usize] kept-candidate bitmaps of the half-row walk
+    int* rev = nullptr;       // [M * pmax] position of B among the higher partners of its q-th (lower) partner
     int* off = nullptr;       // [M + 1] first atom of each molecule
     int* amol = nullptr;      // [n] molecule of each atom
     double* cen = nullptr;    // [3 M] centres
@@ -39,5 +43,10 @@ cudaError_t mol_rows_intra(const MolLists& m, const double* pos, const double* h
 // Half-list rows (the reference's truncation at cap); no-ops unless flag[0] is set.
 cudaError_t mol_rows_half(const MolLists& m, const double* pos, const double* hh, double rc2, int cap, int* cnt,
                           int* list, int* dropped, cudaStream_t st);
+// The LJ gather's full rows (incoming entries ascending, then the row) from
+// the candidate bitmaps of the last mol_rows_half (m.masks only); no-op
+// unless flag[0] is set.
+cudaError_t mol_rows_incoming(const MolLists& m, int cap, const int* cnt, const int* list, int* in_cnt,
+                              int* in_list, int in_cap, DevErr* err, cudaStream_t st);
 
 }  // namespace fmd

@@ -194,10 +194,21 @@ cudaError_t System::enqueue_rebuild(cudaStream_t st) {
         return e;
     if (mol.ok && (e = mol_rows_half(mol, arr.pos, hh, rc2_a, arr.cap_a, cnt_a, list_a, dropped, st)) != cudaSuccess)
         return e;
-    // the gather's full rows from whichever half list was built
-    if ((e = nlist_transpose(arr.cnt_a, arr.list_a, arr.cap_a, arr.n, const_cast<int*>(arr.in_cnt),
-                             const_cast<int*>(arr.in_list), arr.in_cap, ctx->d_err, st)) != cudaSuccess)
+    // the gather's full rows: from the molecule builder's candidate bitmaps
+    // when it ran (equal molecules of 32-64 atoms), else the transpose of
+    // whichever half list was built (gated the other way; its clear of the
+    // row counts is not gated, so it goes first)
+    if (mol.ok && mol.masks) {
+        if ((e = nlist_transpose(arr.cnt_a, arr.list_a, arr.cap_a, arr.n, const_cast<int*>(arr.in_cnt),
+                                 const_cast<int*>(arr.in_list), arr.in_cap, ctx->d_err, st, gate)) != cudaSuccess)
+            return e;
+        if ((e = mol_rows_incoming(mol, arr.cap_a, arr.cnt_a, arr.list_a, const_cast<int*>(arr.in_cnt),
+                                   const_cast<int*>(arr.in_list), arr.in_cap, ctx->d_err, st)) != cudaSuccess)
+            return e;
+    } else if ((e = nlist_transpose(arr.cnt_a, arr.list_a, arr.cap_a, arr.n, const_cast<int*>(arr.in_cnt),
+                                    const_cast<int*>(arr.in_list), arr.in_cap, ctx->d_err, st)) != cudaSuccess) {
         return e;
+    }
     if (prune.ok) return lj_prune_mark(prune, st);     // new rows: the next evaluation prunes them
     return cudaSuccess;
 }
@@ -675,6 +686,18 @@ extern "C" int fmd_system_lj_rows(fmd_system* s, int* full_cnt, int* pruned_cnt)
     if (full_cnt && y.arr.in_cnt) cudaMemcpyAsync(full_cnt, y.arr.in_cnt, sizeof(int) * n, cudaMemcpyDeviceToHost, st);
     if (pruned_cnt && y.prune.ok) cudaMemcpyAsync(pruned_cnt, y.prune.cnt, sizeof(int) * n, cudaMemcpyDeviceToHost, st);
     return y.ctx->sync_check("system LJ rows");
+}
+
+extern "C" int fmd_system_lj_full_rows(fmd_system* s, int* cnt, int* list, int* stride) {
+    if (!s || !s->sys) return FMD_ERR_ARG;
+    fmd::System& y = *s->sys;
+    if (stride) *stride = y.arr.in_list ? y.arr.in_cap : 0;
+    if (!y.arr.in_list) return FMD_OK;
+    cudaStream_t st = y.ctx->stream;
+    const size_t n = y.arr.n;
+    if (cnt) cudaMemcpyAsync(cnt, y.arr.in_cnt, sizeof(int) * n, cudaMemcpyDeviceToHost, st);
+    if (list) cudaMemcpyAsync(list, y.arr.in_list, sizeof(int) * n * y.arr.in_cap, cudaMemcpyDeviceToHost, st);
+    return y.ctx->sync_check("system LJ full rows");
 }
 
 extern "C" int fmd_system_lists(fmd_system* s, int* cnt_a, int* list_a, int* cnt_b, int* list_b) {

@@ -248,6 +248,11 @@ int fmd_system_lists(fmd_system *s, int *cnt_a, int *list_a, int *cnt_b, int *li
  * the full rows (incoming entries + the reference row) of the last list build
  * and the pruned rows of the last prune (see fmd_system_set_lj_prune). */
 int fmd_system_lj_rows(fmd_system *s, int *full_cnt, int *pruned_cnt);
+/* The full rows themselves: *stride = the row stride (0 for a system without
+ * them, e.g. the rigid model); cnt (n ints) and list (n * stride ints), when
+ * not NULL, receive the row lengths and rows -- row j holds the atoms i < j
+ * whose reference row lists j, ascending, then j's own reference row. */
+int fmd_system_lj_full_rows(fmd_system *s, int *cnt, int *list, int *stride);
 int fmd_system_destroy(fmd_system *s);
 
 /* Measurement helpers (no reference counterpart).  fmd_system_kernel_ms

@@ -33,6 +33,42 @@ def test_airebo_system_lists_match_reference(ctx, oracle, nc, shear, jitter, see
     assert np.array_equal(cb, orc) and same_rows(rows(cb, lb, 12), rows(orc, orl, 12))
     if nc == 5:
         assert (oc == 400).any()                 # truncated rows are part of the check
+    fc, fl = sysd.lj_full_rows()
+    ec, el = full_rows(oc, ol, 400, na)
+    assert np.array_equal(fc, ec)
+    assert all(np.array_equal(fl[j, :fc[j]], el[j]) for j in range(na))
+    sysd.close()
+
+
+def full_rows(cnt, lst, cap, n):
+    """The LJ gather's full rows from the reference's half rows: row j holds
+    the atoms i whose row lists j, ascending, then j's own row."""
+    src = np.repeat(np.arange(n), cnt)
+    dst = np.concatenate([lst[k * cap:k * cap + cnt[k]] for k in range(n)])
+    o = np.lexsort((src, dst))
+    src, dst = src[o], dst[o]
+    start = np.searchsorted(dst, np.arange(n + 1))
+    rws = [np.concatenate([src[start[j]:start[j + 1]], lst[j * cap:j * cap + cnt[j]]]) for j in range(n)]
+    return np.array([len(r) for r in rws], np.int32), rws
+
+
+def test_full_rows_on_a_sequence_of_builds(ctx, oracle):
+    """Full rows after several builds on a moving system (the molecule
+    builder's acceptance masks are rewritten each build) equal those formed
+    from the current half rows."""
+    s = crystal.atomistic(3, jitter=0.02, seed=8, T=600.0)
+    na = s["pos"].size // 3
+    cfg = RunConfig(dt=0.5, T=600.0, Pe=0.0, nsteps=60, nlup=20, nc=3, nmol=s["nmol"])
+    sysd = System.airebo(ctx, cfg, s["pos"], s["vel"], s["mass"], s["mol_id"], s["h"],
+                         crystal.npt_atom(600.0, 0.0, na))
+    sysd.init()
+    for g0 in (1, 21, 41):
+        sysd.run(g0, g0 + 19)                    # 20 steps: one list build
+        ca, la, _, _ = sysd.lists(400)
+        fc, fl = sysd.lj_full_rows()
+        ec, el = full_rows(ca, la, 400, na)
+        assert np.array_equal(fc, ec), g0
+        assert all(np.array_equal(fl[j, :fc[j]], el[j]) for j in range(na)), g0
     sysd.close()
 
 

@@ -145,6 +145,29 @@ def test_mm_pruned_matches_full_rows(ctx):
     f.close()
 
 
+def test_fp32_pair_pruned_matches_full_rows(ctx):
+    """FP32 pair algebra over pruned rows: the same pairs and FP32 pair terms
+    as over the full rows (the cutoff test and the image stay FP64)."""
+    from fuller_md_en_b200._lib import FMD_PREC_FP32_PAIR
+    s = crystal.atomistic(3, jitter=0.02, seed=19)
+    na = s["pos"].size // 3
+    ys = []
+    for delta in (0.5, 0.0):
+        cfg = RunConfig(dt=0.5, T=300.0, Pe=0.0, nsteps=40, nlup=20, nc=3, nmol=s["nmol"],
+                        precision=FMD_PREC_FP32_PAIR)
+        y = System.airebo(ctx, cfg, s["pos"], s["vel"], s["mass"], s["mol_id"], s["h"],
+                          crystal.npt_atom(300.0, 0.0, na))
+        y.set_lj_prune(delta)
+        y.init()
+        ys.append(y)
+    for g in range(1, 41):
+        _agree(ys[0].run(g, g), ys[1].run(g, g), g)
+    st = ys[0].lj_prune()
+    assert st["evaluations"] == 41 and 3 <= st["prunes"] < 41, st
+    for y in ys:
+        y.close()
+
+
 def test_prune_off_and_bad_delta(ctx):
     from fuller_md_en_b200._lib import FmdError
     s = crystal.atomistic(2, jitter=0.01, seed=3)
