@@ -245,15 +245,22 @@ k_mol_rows(const double* __restrict__ pos, const double* __restrict__ hh, int n,
 // and truncation as k_mol_rows<0>.  k div S is (k + 0.5) * fl(1/S) truncated:
 // the quotient's fractional part stays 0.5/S from an integer, and the FP32
 // product's relative error (<= 2^-23) cannot cross that for k < 4e6.
+// PAIRED (32 <= S <= 64): the walk goes by partner instead, two 32-lane
+// slices per partner (atoms 0-31, 32-63; lanes past S idle), kFlatU / 2
+// partners at a time -- no quotient per candidate -- and the ballot of the
+// kept entries of slice h of the p-th higher partner is stored as word 2 p + h
+// of the atom's candidate bitmap, bm[(A * 2 pmax + 2 p + h) * S + i - off[A]],
+// from which k_mol_incoming forms the full rows.
 constexpr int kFlatU = 4;
 constexpr int kFlatWarps = 8;
 
+template <bool PAIRED>
 __global__ void __launch_bounds__(32 * kFlatWarps, 3)
 k_mol_half_flat(const double* __restrict__ pos, const double* __restrict__ hh, int n, const int* __restrict__ off,
                 const int* __restrict__ amol, const int* __restrict__ npart, const int* __restrict__ part, int pmax,
                 int S, const float4* __restrict__ pos32, double rc2, int cap, int* __restrict__ cnt,
                 int* __restrict__ list, int* __restrict__ dropped, const int* __restrict__ flag,
-                unsigned* __restrict__ bm, int W) {
+                unsigned* __restrict__ bm) {
     if (flag[0] == 0) return;
     __shared__ double s_hh[18];
     __shared__ int s_start[kFlatWarps][kMolPartners];
@@ -286,46 +293,53 @@ k_mol_half_flat(const double* __restrict__ pos, const double* __restrict__ hh, i
         const bool screen = sc.on && pi.w != 0.0f;
         int* row = list + (size_t)i * cap;
         int emitted = 0;
-        // candidate bitmap: word w of atom i (bit b = candidate 32 w + b kept
-        // in the row) at bm[(A W + w) S + i - off[A]]
-        unsigned* bmA = bm ? bm + (size_t)A * W * S + (i - off[A]) : nullptr;
-        for (int k0 = 0; k0 < ncand; k0 += 32 * kFlatU) {
+        unsigned* bmA = PAIRED ? bm + (size_t)A * 2 * pmax * S + (i - off[A]) : nullptr;
+        const int nit = PAIRED ? nup : ncand;
+        for (int k0 = 0; k0 < nit; k0 += PAIRED ? kFlatU / 2 : 32 * kFlatU) {
             int jj[kFlatU];
             float4 q[kFlatU];
 #pragma unroll
             for (int u = 0; u < kFlatU; u++) {
-                const int k = k0 + 32 * u + lane;
                 jj[u] = -1;
-                if (k < ncand) {
-                    const int pk = (int)(((float)k + 0.5f) * invS);
-                    jj[u] = st[pk] + (k - pk * S);
+                if (PAIRED) {
+                    const int p = k0 + (u >> 1), a = ((u & 1) << 5) + lane;
+                    if (p < nup && a < S) jj[u] = st[p] + a;
+                } else {
+                    const int k = k0 + 32 * u + lane;
+                    if (k < ncand) {
+                        const int pk = (int)(((float)k + 0.5f) * invS);
+                        jj[u] = st[pk] + (k - pk * S);
+                    }
                 }
             }
 #pragma unroll
             for (int u = 0; u < kFlatU; u++) q[u] = jj[u] >= 0 ? pos32[jj[u]] : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
             for (int u = 0; u < kFlatU; u++) {
-                bool ok = jj[u] >= 0;
-                if (ok) {
-                    if (screen && q[u].w != 0.0f) {
-                        float dx = q[u].x - pi.x, dy = q[u].y - pi.y, dz = q[u].z - pi.z;
-                        dx = fmaf(-sc.L[0], rintf(dx * sc.Li[0]), dx);
-                        dy = fmaf(-sc.L[1], rintf(dy * sc.Li[1]), dy);
-                        dz = fmaf(-sc.L[2], rintf(dz * sc.Li[2]), dz);
-                        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                        ok = r2 < sc.lo2 ? true : (r2 > sc.hi2 ? false : pair_in(pos, i, jj[u], h, hi, diag, rc2));
-                    } else {
-                        ok = pair_in(pos, i, jj[u], h, hi, diag, rc2);
-                    }
+                // FP32 screen on every lane (no divergence); the exact FP64
+                // test runs, warp-uniformly, only in slices where some lane
+                // is in the band, off the screen or without an FP32 copy
+                const bool valid = jj[u] >= 0;
+                float dx = q[u].x - pi.x, dy = q[u].y - pi.y, dz = q[u].z - pi.z;
+                dx = fmaf(-sc.L[0], rintf(dx * sc.Li[0]), dx);
+                dy = fmaf(-sc.L[1], rintf(dy * sc.Li[1]), dy);
+                dz = fmaf(-sc.L[2], rintf(dz * sc.Li[2]), dz);
+                const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                const bool fast = screen && q[u].w != 0.0f;
+                bool ok = valid && fast && r2 < sc.lo2;
+                const bool exact = valid && !(fast && (r2 < sc.lo2 || r2 > sc.hi2));
+                if (__any_sync(kFull, exact)) {
+                    const bool in = pair_in(pos, i, exact ? jj[u] : i, h, hi, diag, rc2);
+                    ok = ok || (exact && in);
                 }
                 const unsigned m = __ballot_sync(kFull, ok);
                 const int kk = emitted + __popc(m & below);
                 if (ok && kk < cap) row[kk] = jj[u];
-                if (bmA) {
+                if (PAIRED) {
                     // the slice's entries that fit in the row (row position < cap)
                     const unsigned kept = __ballot_sync(kFull, ok && kk < cap);
-                    const int ks = k0 + 32 * u;
-                    if (lane == 0 && ks < ncand) bmA[(size_t)(ks >> 5) * S] = kept;
+                    const int p = k0 + (u >> 1);
+                    if (lane == 0 && p < nup) bmA[(size_t)(2 * p + (u & 1)) * S] = kept;
                 }
                 emitted += __popc(m);
             }
@@ -373,18 +387,18 @@ __global__ void k_mol_rev(int M, const int* __restrict__ npart, const int* __res
     }
 }
 
-// Full LJ rows from the candidate bitmaps of the flat walk, for equal
-// molecules of S atoms (32 <= S <= 64, off[A] = A S): atom j = B S + jb is in
-// the kept row of i = A S + ia (A < B) iff bit rev[B][q] S + jb of i's bitmap
-// is set.  Two blocks per molecule B, one per half of its atoms (jb < 32,
-// jb >= 32): the bitmap words that hold the half's bits (2 words per atom of
-// A) are staged in shared memory for up to kInChunk lower partners at a time,
-// then warp w emits the rows of atoms jb = 32 h + w + 8 t: for each lower
-// partner A (ascending) a ballot over A's atoms gives the entries in
-// ascending order.  Row j thus holds the atoms i < j whose kept row lists j,
-// ascending, then j's own row -- the rows the transpose (nlist_transpose)
-// builds, without atomics or a sort.  The own rows are copied with 8 loads in
-// flight per lane.
+// Full LJ rows from the candidate bitmaps of the partner-aligned walk
+// (k_mol_half_flat<true>), for equal molecules of S atoms (32 <= S <= 64,
+// off[A] = A S): atom j = B S + jb is in the kept row of i = A S + ia (A < B)
+// iff bit jb mod 32 of word 2 rev[B][q] + jb div 32 of i's bitmap is set.
+// Two blocks per molecule B, one per half of its atoms (jb < 32, jb >= 32):
+// the half's word of every atom of A is staged in shared memory for up to
+// kInChunk lower partners at a time, then warp w emits the rows of atoms
+// jb = 32 h + w + 8 t: for each lower partner A (ascending) a ballot over A's
+// atoms gives the entries in ascending order.  Row j thus holds the atoms
+// i < j whose kept row lists j, ascending, then j's own row -- the rows the
+// transpose (nlist_transpose) builds, without atomics or a sort.  The own rows
+// are copied with 8 loads in flight per lane.
 constexpr int kInChunk = 32;
 constexpr int kInWarps = 8;
 constexpr int kInAtoms = 32 / kInWarps;               // atoms per warp
@@ -396,8 +410,8 @@ k_mol_incoming(int M, int S, const int* __restrict__ npart, const int* __restric
                int* __restrict__ in_list, int in_cap, DevErr* err, const int* __restrict__ flag) {
     if (flag[0] == 0) return;
     __shared__ int s_a[kMolPartners];                 // lower partners, ascending
-    __shared__ int s_b[kMolPartners];                 // first bit of the half's atoms in their bitmaps
-    __shared__ unsigned s_bits[kInChunk][2][64];
+    __shared__ int s_b[kMolPartners];                 // bitmap word of the half's atoms
+    __shared__ unsigned s_bits[kInChunk][64];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned below = (1u << lane) - 1u;
     const int lim = in_cap - cap;
@@ -418,7 +432,7 @@ k_mol_incoming(int M, int S, const int* __restrict__ npart, const int* __restric
             if (A < B) {
                 low = true;
                 s_a[q] = A;
-                s_b[q] = rev[(size_t)B * pmax + q] * S + h0;
+                s_b[q] = 2 * rev[(size_t)B * pmax + q] + (h0 >> 5);
             }
         }
         const int nlow = __syncthreads_count(low);    // ascending: the lower partners come first
@@ -427,25 +441,20 @@ k_mol_incoming(int M, int S, const int* __restrict__ npart, const int* __restric
         for (int t = 0; t < kInAtoms; t++) em[t] = 0;
         for (int c0 = 0; c0 < nlow; c0 += kInChunk) {
             const int nc = nlow - c0 < kInChunk ? nlow - c0 : kInChunk;
-            for (int x = threadIdx.x; x < nc * 2 * S; x += blockDim.x) {
-                const int c = x / (2 * S), r = x - c * 2 * S;
-                const int k = r / S, ia = r - k * S;
-                const int b0 = s_b[c0 + c];
-                // words (b0 >> 5) .. ((b0 + nh - 1) >> 5) hold the half's bits
-                if (k <= ((b0 & 31) + nh - 1) >> 5)
-                    s_bits[c][k][ia] = bm[((size_t)s_a[c0 + c] * W + (b0 >> 5) + k) * S + ia];
+            for (int x = threadIdx.x; x < nc * S; x += blockDim.x) {
+                const int c = x / S, ia = x - c * S;
+                s_bits[c][ia] = bm[((size_t)s_a[c0 + c] * W + s_b[c0 + c]) * S + ia];
             }
             __syncthreads();
             for (int c = 0; c < nc; c++) {
                 const int a0 = s_a[c0 + c] * S;
-                const int sb = s_b[c0 + c] & 31;
+                const unsigned w0 = s_bits[c][lane], w1 = lane + 32 < S ? s_bits[c][lane + 32] : 0u;
 #pragma unroll
                 for (int t = 0; t < kInAtoms; t++) {
                     const int jb = w + kInWarps * t;
                     if (jb < nh) {
-                        const int pos = sb + jb, k = pos >> 5, b = pos & 31;
-                        const bool ok0 = (s_bits[c][k][lane] >> b) & 1u;
-                        const bool ok1 = lane + 32 < S && ((s_bits[c][k][lane + 32] >> b) & 1u);
+                        const bool ok0 = (w0 >> jb) & 1u;
+                        const bool ok1 = (w1 >> jb) & 1u;
                         const unsigned m0 = __ballot_sync(kFull, ok0), m1 = __ballot_sync(kFull, ok1);
                         int* row = in_list + (size_t)(B * S + h0 + jb) * in_cap;
                         const int p0 = em[t] + __popc(m0 & below);
@@ -526,7 +535,7 @@ cudaError_t mol_lists_alloc(MolLists& m, int n, const int* mol_id_host) {
     for (int a = 0; a < M; a++)
         if (off[a + 1] - off[a] != m.usize) m.usize = 0;
     m.masks = m.usize >= 32 && m.usize <= 64;
-    m.words = (m.pmax * m.usize + 31) / 32;
+    m.words = 2 * m.pmax;
     cudaError_t e;
     auto A = [&](void** p, size_t bytes) {
         if (e == cudaSuccess) e = cudaMalloc(p, bytes);
@@ -581,11 +590,16 @@ cudaError_t mol_rows_intra(const MolLists& m, const double* pos, const double* h
 
 cudaError_t mol_rows_half(const MolLists& m, const double* pos, const double* hh, double rc2, int cap, int* cnt,
                           int* list, int* dropped, cudaStream_t st) {
+    if (m.masks) {
+        k_mol_half_flat<true><<<kRowBlocksMol, 32 * kFlatWarps, 0, st>>>(pos, hh, m.n, m.off, m.amol, m.npart,
+                                                                         m.part, m.pmax, m.usize, m.pos32, rc2, cap,
+                                                                         cnt, list, dropped, m.flag, m.bm);
+        return cudaGetLastError();
+    }
     if (m.usize > 0) {
-        k_mol_half_flat<<<kRowBlocksMol, 32 * kFlatWarps, 0, st>>>(pos, hh, m.n, m.off, m.amol, m.npart, m.part,
-                                                                   m.pmax, m.usize, m.pos32, rc2, cap, cnt, list,
-                                                                   dropped, m.flag, m.masks ? m.bm : nullptr,
-                                                                   m.words);
+        k_mol_half_flat<false><<<kRowBlocksMol, 32 * kFlatWarps, 0, st>>>(pos, hh, m.n, m.off, m.amol, m.npart,
+                                                                          m.part, m.pmax, m.usize, m.pos32, rc2, cap,
+                                                                          cnt, list, dropped, m.flag, nullptr);
         return cudaGetLastError();
     }
     k_mol_rows<0><<<kRowBlocksMol, 256, 0, st>>>(pos, hh, m.n, m.off, m.amol, m.npart, m.part, m.pmax, m.pos32, rc2,

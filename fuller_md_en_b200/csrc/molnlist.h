@@ -18,7 +18,7 @@ struct MolLists {
     int max_atoms = 0;        // atoms of the largest molecule
     int usize = 0;            // atoms of every molecule when all have the same count, else 0
     bool masks = false;       // 32 <= usize <= 64: the full LJ rows come from the candidate bitmaps
-    int words = 0;            // bitmap words per atom: ceil(pmax * usize / 32)
+    int words = 0;            // bitmap words per atom: 2 pmax (two per higher partner)
     unsigned* bm = nullptr;   // [M * words * usize] kept-candidate bitmaps of the half-row walk
     int* rev = nullptr;       // [M * pmax] position of B among the higher partners of its q-th (lower) partner
     int* off = nullptr;       // [M + 1] first atom of each molecule
