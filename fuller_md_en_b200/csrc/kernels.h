@@ -18,6 +18,15 @@ struct GridDev {
     float rc2_hi;    // conservative FP32 rejection threshold
 };
 
+// Device allocation hook: a system passes its own allocator (blocks it owns
+// and releases to the context's cache); the *_free calls then leave such
+// memory to its owner.  Without a hook, cudaMalloc / cudaFree.
+struct DevAlloc {
+    void* user = nullptr;
+    cudaError_t (*fn)(void* user, void** p, size_t bytes) = nullptr;
+    cudaError_t operator()(void** p, size_t bytes) const { return fn ? fn(user, p, bytes) : cudaMalloc(p, bytes); }
+};
+
 struct CellList {
     GridDev* grid = nullptr;    // device
     int* cell_count = nullptr;  // [cap_cells]
@@ -32,12 +41,14 @@ struct CellList {
     int cap_cells = 1;
     int n = 0;
     int K = 1;                  // cells per cutoff length (cell width >= rc / K)
+    bool ext = false;           // arrays from a DevAlloc hook (owned elsewhere)
 };
 
 // Host helper: cells per axis for a cell matrix and list radius.
 void grid_dims_host(const double* h, double rc, int K, int* n);
 // K = 2 halves the candidate volume for large cutoffs; K = 1 suits small ones.
-cudaError_t cells_alloc(CellList& cl, int n, const double* h_host, double rc, int K = 1);
+cudaError_t cells_alloc(CellList& cl, int n, const double* h_host, double rc, int K = 1,
+                        const DevAlloc& da = DevAlloc{});
 void cells_free(CellList& cl);
 // hh = device pointer to {h[9], hi[9]}.  Bins pos[3*n] into cells; mol_id
 // (may be null) is copied into cell order beside the fractional coordinates.

@@ -508,7 +508,7 @@ constexpr int kRowBlocksMol = kSMs * 8;
 
 }  // namespace
 
-cudaError_t mol_lists_alloc(MolLists& m, int n, const int* mol_id_host) {
+cudaError_t mol_lists_alloc(MolLists& m, int n, const int* mol_id_host, const DevAlloc& da) {
     m = MolLists();
     if (n <= 0 || !mol_id_host) return cudaSuccess;
     // contiguous molecules: each id forms one run
@@ -538,9 +538,10 @@ cudaError_t mol_lists_alloc(MolLists& m, int n, const int* mol_id_host) {
     m.words = 2 * m.pmax;
     cudaError_t e;
     auto A = [&](void** p, size_t bytes) {
-        if (e == cudaSuccess) e = cudaMalloc(p, bytes);
+        if (e == cudaSuccess) e = da(p, bytes);
     };
     e = cudaSuccess;
+    m.ext = da.fn != nullptr;
     A((void**)&m.off, sizeof(int) * (M + 1));
     A((void**)&m.amol, sizeof(int) * n);
     A((void**)&m.cen, sizeof(double) * 3 * M);
@@ -556,6 +557,7 @@ cudaError_t mol_lists_alloc(MolLists& m, int n, const int* mol_id_host) {
     if (e == cudaSuccess) e = cudaMemcpy(m.off, off.data(), sizeof(int) * (M + 1), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(m.amol, amol.data(), sizeof(int) * n, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(m.flag, 0, sizeof(int) * 2);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);     // before any other stream reads them
     if (e != cudaSuccess) {
         mol_lists_free(m);
         return e;
@@ -566,6 +568,10 @@ cudaError_t mol_lists_alloc(MolLists& m, int n, const int* mol_id_host) {
 }
 
 void mol_lists_free(MolLists& m) {
+    if (m.ext) {
+        m = MolLists();
+        return;
+    }
     cudaFree(m.off); cudaFree(m.amol); cudaFree(m.cen); cudaFree(m.rad); cudaFree(m.pos32); cudaFree(m.bm);
     cudaFree(m.rev); cudaFree(m.npart); cudaFree(m.part);
     cudaFree(m.flag);

@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "fmd_internal.h"
+#include "kernels.h"
 
 namespace fmd {
 
@@ -17,6 +18,7 @@ struct MolLists {
     int n = 0, M = 0, pmax = 0;
     int max_atoms = 0;        // atoms of the largest molecule
     int usize = 0;            // atoms of every molecule when all have the same count, else 0
+    bool ext = false;         // arrays from a DevAlloc hook (owned elsewhere)
     bool masks = false;       // 32 <= usize <= 64: the full LJ rows come from the candidate bitmaps
     int words = 0;            // bitmap words per atom: 2 pmax (two per higher partner)
     unsigned* bm = nullptr;   // [M * words * usize] kept-candidate bitmaps of the half-row walk
@@ -33,7 +35,7 @@ struct MolLists {
 
 // Host set-up from the atoms' molecule ids; m.ok stays false (the cell-grid
 // builder is used) unless every molecule is one contiguous index range.
-cudaError_t mol_lists_alloc(MolLists& m, int n, const int* mol_id_host);
+cudaError_t mol_lists_alloc(MolLists& m, int n, const int* mol_id_host, const DevAlloc& da = DevAlloc{});
 void mol_lists_free(MolLists& m);
 // Centres, radii and partner molecules for list radius rc; sets flag[0].
 cudaError_t mol_partners(MolLists& m, const double* pos, const double* hh, double rc, cudaStream_t st);

@@ -348,7 +348,7 @@ void grid_dims_host(const double* h, double rc, int K, int* n) {
     grid_dims(h, rc, K, n, &wmin);
 }
 
-cudaError_t cells_alloc(CellList& cl, int n, const double* h_host, double rc, int K) {
+cudaError_t cells_alloc(CellList& cl, int n, const double* h_host, double rc, int K, const DevAlloc& da) {
     int nd[3];
     cl.K = K;
     grid_dims_host(h_host, rc, K, nd);
@@ -359,21 +359,26 @@ cudaError_t cells_alloc(CellList& cl, int n, const double* h_host, double rc, in
         cl.cap_cells *= cl.cap_n[a];
     }
     cl.n = n;
+    cl.ext = da.fn != nullptr;
     cudaError_t e;
-    if ((e = cudaMalloc(&cl.grid, sizeof(GridDev))) != cudaSuccess) return e;
-    if ((e = cudaMalloc(&cl.cell_count, sizeof(int) * cl.cap_cells)) != cudaSuccess) return e;
-    if ((e = cudaMalloc(&cl.cell_start, sizeof(int) * (cl.cap_cells + 1))) != cudaSuccess) return e;
+    if ((e = da((void**)&cl.grid, sizeof(GridDev))) != cudaSuccess) return e;
+    if ((e = da((void**)&cl.cell_count, sizeof(int) * cl.cap_cells)) != cudaSuccess) return e;
+    if ((e = da((void**)&cl.cell_start, sizeof(int) * (cl.cap_cells + 1))) != cudaSuccess) return e;
     size_t nn = n > 0 ? n : 1;
-    if ((e = cudaMalloc(&cl.cell_atoms, sizeof(int) * nn)) != cudaSuccess) return e;
-    if ((e = cudaMalloc(&cl.slot_of, sizeof(int) * nn)) != cudaSuccess) return e;
-    if ((e = cudaMalloc(&cl.cell_of, sizeof(int) * nn)) != cudaSuccess) return e;
-    if ((e = cudaMalloc(&cl.s4, sizeof(float4) * nn)) != cudaSuccess) return e;
-    if ((e = cudaMalloc(&cl.s4s, sizeof(float4) * nn)) != cudaSuccess) return e;
-    if ((e = cudaMalloc(&cl.mols, sizeof(int) * nn)) != cudaSuccess) return e;
+    if ((e = da((void**)&cl.cell_atoms, sizeof(int) * nn)) != cudaSuccess) return e;
+    if ((e = da((void**)&cl.slot_of, sizeof(int) * nn)) != cudaSuccess) return e;
+    if ((e = da((void**)&cl.cell_of, sizeof(int) * nn)) != cudaSuccess) return e;
+    if ((e = da((void**)&cl.s4, sizeof(float4) * nn)) != cudaSuccess) return e;
+    if ((e = da((void**)&cl.s4s, sizeof(float4) * nn)) != cudaSuccess) return e;
+    if ((e = da((void**)&cl.mols, sizeof(int) * nn)) != cudaSuccess) return e;
     return cudaSuccess;
 }
 
 void cells_free(CellList& cl) {
+    if (cl.ext) {
+        cl = CellList();
+        return;
+    }
     cudaFree(cl.grid); cudaFree(cl.cell_count); cudaFree(cl.cell_start); cudaFree(cl.cell_atoms);
     cudaFree(cl.slot_of); cudaFree(cl.cell_of); cudaFree(cl.s4); cudaFree(cl.s4s); cudaFree(cl.mols);
     cl = CellList();

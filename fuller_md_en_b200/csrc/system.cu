@@ -64,6 +64,10 @@ cudaError_t System::alloc(T** p, size_t count, const T* src) {
     return cudaMemcpyAsync(*p, src, sizeof(T) * count, cudaMemcpyHostToDevice, ctx->stream);
 }
 
+cudaError_t System::alloc_raw(void* self, void** p, size_t bytes) {
+    return static_cast<System*>(self)->alloc(reinterpret_cast<char**>(p), bytes, (const char*)nullptr);
+}
+
 int System::alloc_common(const double* pos_h, const double* vel_h, const double* h_h, const fmd_npt* npt_h) {
     cudaStream_t st = ctx->stream;
     const int n = arr.n;
@@ -99,14 +103,14 @@ int System::alloc_lists(double rc_list_a, int cap_a_, double rc_list_b, int cap_
         return ctx->fail(FMD_ERR_CUDA, "list allocation failed");
     cudaMemsetAsync(lst, 0, sizeof(int) * (size_t)n * cap_a_, ctx->stream);
     arr.cnt_a = cnt; arr.list_a = lst;
-    if (cells_alloc(cells_a, n, h0, rc_a, 2) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "cell allocation failed");
+    if (cells_alloc(cells_a, n, h0, rc_a, 2, owned_alloc()) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "cell allocation failed");
     if (cap_b_ > 0) {
         rc_b = rc_list_b; rc2_b = rc_b * rc_b; arr.cap_b = cap_b_;
         if (alloc(&cnt, n, (const int*)nullptr) || alloc(&lst, (size_t)n * cap_b_, (const int*)nullptr))
             return ctx->fail(FMD_ERR_CUDA, "list allocation failed");
         cudaMemsetAsync(lst, 0, sizeof(int) * (size_t)n * cap_b_, ctx->stream);
         arr.cnt_b = cnt; arr.list_b = lst;
-        if (cells_alloc(cells_b, n, h0, rc_b) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "cell allocation failed");
+        if (cells_alloc(cells_b, n, h0, rc_b, 1, owned_alloc()) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "cell allocation failed");
         if (alloc(&arr.rebo_slots, (size_t)n * cap_b_ * kReboSlotDoubles, (const double*)nullptr))
             return ctx->fail(FMD_ERR_CUDA, "list allocation failed");
         int* ids;
@@ -549,7 +553,7 @@ extern "C" int fmd_system_create_airebo(fmd_ctx* ctx, const fmd_run_params* p, i
     const double lj_rcut = 3.0 * 3.40;          // AI:120
     const double rebo_rcut = 2.0 + 0.3;         // AI:116
     if ((rc = s->alloc_lists(lj_rcut + 2.0, 400, rebo_rcut, 12, true)) != FMD_OK) return rc;
-    if (fmd::mol_lists_alloc(s->mol, na, mol_id) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "list allocation failed");
+    if (fmd::mol_lists_alloc(s->mol, na, mol_id, s->owned_alloc()) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "list allocation failed");
     if ((rc = s->alloc_prune(lj_rcut)) != FMD_OK) return rc;
     out[0] = new fmd_system{std::move(s)};
     return FMD_OK;
@@ -585,7 +589,7 @@ extern "C" int fmd_system_create_mm(fmd_ctx* ctx, const fmd_run_params* p, int n
     }
     const double rcut = 3.0 * 3.431;            // MM:114
     if ((rc = s->alloc_lists(rcut + 2.0, 400, 0.0, 0, true)) != FMD_OK) return rc;
-    if (fmd::mol_lists_alloc(s->mol, na, mol_id) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "list allocation failed");
+    if (fmd::mol_lists_alloc(s->mol, na, mol_id, s->owned_alloc()) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "list allocation failed");
     if ((rc = s->alloc_prune(rcut)) != FMD_OK) return rc;
     out[0] = new fmd_system{std::move(s)};
     return FMD_OK;

@@ -31,6 +31,9 @@ struct System {
     std::unique_ptr<SgStep> sg;        // learned REBO term (AIREBO only), nullptr: plain
 
     template <class T> cudaError_t alloc(T** p, size_t count, const T* src);
+    // DevAlloc hook: untyped blocks owned (and released) like alloc's
+    static cudaError_t alloc_raw(void* self, void** p, size_t bytes);
+    DevAlloc owned_alloc() { return DevAlloc{this, &System::alloc_raw}; }
     int alloc_common(const double* pos, const double* vel, const double* h, const fmd_npt* npt);
     int alloc_lists(double rc_list_a, int cap_a, double rc_list_b, int cap_b, bool transpose);
     int alloc_prune(double rc_lj);

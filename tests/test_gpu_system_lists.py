@@ -52,6 +52,30 @@ def full_rows(cnt, lst, cap, n):
     return np.array([len(r) for r in rws], np.int32), rws
 
 
+@pytest.mark.parametrize("natom", [28, 32, 45, 64])
+def test_lists_for_other_molecule_sizes(ctx, oracle, natom):
+    """Molecules of 28 atoms (flat candidate walk, full rows by the
+    transpose), 32 (partner walk with idle upper slices), 45 and 64 (partner
+    walk, full rows from the candidate bitmap; 64 fills both slices): half
+    rows against the reference builder and full rows against the half rows."""
+    c60 = crystal.c60_ih()
+    coords = c60[:natom] if natom <= 60 else np.vstack([c60, 0.45 * c60[:natom - 60]])
+    s = crystal.atomistic(3, coords=coords, jitter=0.02, seed=natom)
+    na = s["pos"].size // 3
+    h, hi = s["h"], crystal.inv9(s["h"])
+    cfg = RunConfig(dt=0.5, T=300.0, Pe=0.0, nsteps=4, nlup=20, nc=3, nmol=s["nmol"])
+    sysd = System.airebo(ctx, cfg, s["pos"], s["vel"], s["mass"], s["mol_id"], h, crystal.npt_atom(300.0, 0.0, na))
+    sysd.init()
+    ca, la, _, _ = sysd.lists(400)
+    oc, ol, _ = oracle.nlist_half(s["pos"], h, hi, na, s["mol_id"], RC_AI)
+    assert np.array_equal(ca, oc) and same_rows(rows(ca, la, 400), rows(oc, ol, 400))
+    fc, fl = sysd.lj_full_rows()
+    ec, el = full_rows(oc, ol, 400, na)
+    assert np.array_equal(fc, ec)
+    assert all(np.array_equal(fl[j, :fc[j]], el[j]) for j in range(na))
+    sysd.close()
+
+
 def test_full_rows_on_a_sequence_of_builds(ctx, oracle):
     """Full rows after several builds on a moving system (the molecule
     builder's acceptance masks are rewritten each build) equal those formed
