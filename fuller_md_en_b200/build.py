@@ -89,7 +89,7 @@ def build_host(verbose: bool = False) -> None:
     cxx = os.environ.get("FMD_CXX", "/usr/bin/g++")
     common = sorted(HOST.glob("fmd_host*.cpp"))
     hdrs = list(HOST.glob("*.hpp")) + [ROOT / "include" / "fullermd.h"]
-    flags = ["-std=c++17", "-O2", "-Wall", "-fPIC", "-I", str(ROOT / "include"), "-I", str(HOST)]
+    flags = ["-std=c++17", "-O2", "-Wall", "-fPIC", "-pthread", "-I", str(ROOT / "include"), "-I", str(HOST)]
     if common and _stale(HOST_LIB, common + hdrs):
         _run([cxx, *flags, "-shared", "-o", str(HOST_LIB), *map(str, common)])
     for d in DRIVERS:

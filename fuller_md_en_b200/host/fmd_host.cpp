@@ -13,6 +13,7 @@
 #include <fstream>
 #include <set>
 #include <sstream>
+#include <thread>
 
 namespace fmdh {
 
@@ -419,20 +420,14 @@ fmd_mm_topology Topology::view() const {
 }
 
 // --------------------------------------------------------------------- OVITO
-namespace {
-void lattice_line(FILE* fp, const double* h, int istep, double dt) {
-    fprintf(fp,
-            "Lattice=\"%.8f %.8f %.8f %.8f %.8f %.8f %.8f %.8f %.8f\" "
-            "Properties=species:S:1:pos:R:3:c_mol:I:1:vx:R:1:vy:R:1:vz:R:1 Time=%.4f Step=%d pbc=\"T T T\"\n",
-            h[0], h[3], h[6], h[1], h[4], h[7], h[2], h[5], h[8], istep * dt, istep);
-}
-}  // namespace
 
-void write_ovito_rigid(FILE* fp, int istep, double dt, const double* pos, const double* vel, const double* qv,
-                       const double* body, const double* h, int n, int natom) {
-    fprintf(fp, "%d\n", n * natom);
-    lattice_line(fp, h, istep, dt);
-    for (int i = 0; i < n; i++) {
+namespace {
+// Lines of molecules [i0, i1) (rigid: natom sites each, lab frame R(q) body +
+// centre) or atoms [i0, i1), in the reference's formats, appended to out.
+void rigid_lines(std::string& out, const double* pos, const double* vel, const double* qv, const double* body,
+                 int i0, int i1, int natom) {
+    char ln[192];
+    for (int i = i0; i < i1; i++) {
         const double* q = qv + 4 * i;
         const double w = q[0], x = q[1], y = q[2], z = q[3];
         const double R[9] = {1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y),
@@ -440,21 +435,156 @@ void write_ovito_rigid(FILE* fp, int istep, double dt, const double* pos, const 
                              2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)};
         for (int a = 0; a < natom; a++) {
             const double bx = body[3 * a], by = body[3 * a + 1], bz = body[3 * a + 2];
-            fprintf(fp, "C %14.8f %14.8f %14.8f %5d %14.8e %14.8e %14.8e\n",
-                    pos[3 * i] + R[0] * bx + R[1] * by + R[2] * bz, pos[3 * i + 1] + R[3] * bx + R[4] * by + R[5] * bz,
-                    pos[3 * i + 2] + R[6] * bx + R[7] * by + R[8] * bz, i + 1, vel[3 * i], vel[3 * i + 1],
-                    vel[3 * i + 2]);
+            const int k = snprintf(ln, sizeof(ln), "C %14.8f %14.8f %14.8f %5d %14.8e %14.8e %14.8e\n",
+                                   pos[3 * i] + R[0] * bx + R[1] * by + R[2] * bz,
+                                   pos[3 * i + 1] + R[3] * bx + R[4] * by + R[5] * bz,
+                                   pos[3 * i + 2] + R[6] * bx + R[7] * by + R[8] * bz, i + 1, vel[3 * i],
+                                   vel[3 * i + 1], vel[3 * i + 2]);
+            out.append(ln, (size_t)std::min(k, (int)sizeof(ln) - 1));
         }
     }
 }
 
+void atom_lines(std::string& out, const double* pos, const double* vel, const int* mol_id, int mol_offset, int i0,
+                int i1) {
+    char ln[192];
+    for (int i = i0; i < i1; i++) {
+        const int k = snprintf(ln, sizeof(ln), "C %14.8f %14.8f %14.8f %5d %14.8e %14.8e %14.8e\n", pos[3 * i],
+                               pos[3 * i + 1], pos[3 * i + 2], mol_id[i] + mol_offset, vel[3 * i], vel[3 * i + 1],
+                               vel[3 * i + 2]);
+        out.append(ln, (size_t)std::min(k, (int)sizeof(ln) - 1));
+    }
+}
+
+std::string frame_head(int lines, const double* h, int istep, double dt) {
+    char buf[512];
+    std::string s = std::to_string(lines) + "\n";
+    snprintf(buf, sizeof(buf),
+             "Lattice=\"%.8f %.8f %.8f %.8f %.8f %.8f %.8f %.8f %.8f\" "
+             "Properties=species:S:1:pos:R:3:c_mol:I:1:vx:R:1:vy:R:1:vz:R:1 Time=%.4f Step=%d pbc=\"T T T\"\n",
+             h[0], h[3], h[6], h[1], h[4], h[7], h[2], h[5], h[8], istep * dt, istep);
+    return s + buf;
+}
+}  // namespace
+
+void write_ovito_rigid(FILE* fp, int istep, double dt, const double* pos, const double* vel, const double* qv,
+                       const double* body, const double* h, int n, int natom) {
+    std::string out = frame_head(n * natom, h, istep, dt);
+    rigid_lines(out, pos, vel, qv, body, 0, n, natom);
+    fwrite(out.data(), 1, out.size(), fp);
+}
+
 void write_ovito_atoms(FILE* fp, int istep, double dt, const double* pos, const double* vel, const int* mol_id,
                        int mol_offset, const double* h, int na) {
-    fprintf(fp, "%d\n", na);
-    lattice_line(fp, h, istep, dt);
-    for (int i = 0; i < na; i++)
-        fprintf(fp, "C %14.8f %14.8f %14.8f %5d %14.8e %14.8e %14.8e\n", pos[3 * i], pos[3 * i + 1], pos[3 * i + 2],
-                mol_id[i] + mol_offset, vel[3 * i], vel[3 * i + 1], vel[3 * i + 2]);
+    std::string out = frame_head(na, h, istep, dt);
+    atom_lines(out, pos, vel, mol_id, mol_offset, 0, na);
+    fwrite(out.data(), 1, out.size(), fp);
+}
+
+struct OvitoWriter::Frame {
+    bool rigid = false;
+    int istep = 0, n = 0, natom = 1, mol_offset = 0;
+    double dt = 0.0, h[9] = {};
+    std::vector<double> pos, vel, qv, body;
+    std::vector<int> mol_id;
+};
+
+OvitoWriter::OvitoWriter(FILE* fp, int threads) : fp_(fp) {
+    const int hw = (int)std::thread::hardware_concurrency();
+    threads_ = threads > 0 ? threads : std::max(1, std::min(hw, 16));
+    th_ = std::thread([this] { loop(); });
+}
+
+OvitoWriter::~OvitoWriter() {
+    finish();
+    {
+        std::lock_guard<std::mutex> g(mu_);
+        stop_ = true;
+    }
+    cv_.notify_all();
+    th_.join();
+}
+
+void OvitoWriter::submit(std::unique_ptr<Frame> f) {
+    std::unique_lock<std::mutex> g(mu_);
+    cv_.wait(g, [this] { return inflight_ < kSlots; });
+    queue_.push_back(std::move(f));
+    inflight_++;
+    cv_.notify_all();
+}
+
+void OvitoWriter::rigid(int istep, double dt, const double* pos, const double* vel, const double* qv,
+                        const double* body, const double* h, int n, int natom) {
+    auto f = std::make_unique<Frame>();
+    f->rigid = true;
+    f->istep = istep; f->dt = dt; f->n = n; f->natom = natom;
+    std::copy(h, h + 9, f->h);
+    f->pos.assign(pos, pos + 3 * (size_t)n);
+    f->vel.assign(vel, vel + 3 * (size_t)n);
+    f->qv.assign(qv, qv + 4 * (size_t)n);
+    f->body.assign(body, body + 3 * (size_t)natom);
+    submit(std::move(f));
+}
+
+void OvitoWriter::atoms(int istep, double dt, const double* pos, const double* vel, const int* mol_id,
+                        int mol_offset, const double* h, int na) {
+    auto f = std::make_unique<Frame>();
+    f->istep = istep; f->dt = dt; f->n = na; f->mol_offset = mol_offset;
+    std::copy(h, h + 9, f->h);
+    f->pos.assign(pos, pos + 3 * (size_t)na);
+    f->vel.assign(vel, vel + 3 * (size_t)na);
+    f->mol_id.assign(mol_id, mol_id + na);
+    submit(std::move(f));
+}
+
+void OvitoWriter::finish() {
+    std::unique_lock<std::mutex> g(mu_);
+    cv_.wait(g, [this] { return inflight_ == 0; });
+}
+
+void OvitoWriter::loop() {
+    for (;;) {
+        std::unique_ptr<Frame> f;
+        {
+            std::unique_lock<std::mutex> g(mu_);
+            cv_.wait(g, [this] { return stop_ || !queue_.empty(); });
+            if (queue_.empty()) return;
+            f = std::move(queue_.front());
+            queue_.pop_front();
+        }
+        write(*f);
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            inflight_--;
+        }
+        cv_.notify_all();
+    }
+}
+
+// Formats the frame in up to threads_ contiguous chunks (at least kChunk
+// lines each) on worker threads, then writes them in order and flushes, so
+// the file only ever grows by whole frames.
+void OvitoWriter::write(const Frame& f) {
+    constexpr int kChunk = 4096;
+    const int per = f.rigid ? f.natom : 1;                       // lines per unit
+    const int units = f.n;
+    int parts = std::min(threads_, std::max(1, (units * per) / kChunk));
+    parts = std::max(1, std::min(parts, units));
+    std::vector<std::string> out((size_t)parts);
+    auto work = [&](int p) {
+        const int i0 = (int)((long long)units * p / parts), i1 = (int)((long long)units * (p + 1) / parts);
+        out[p].reserve((size_t)(i1 - i0) * per * 100);
+        if (f.rigid) rigid_lines(out[p], f.pos.data(), f.vel.data(), f.qv.data(), f.body.data(), i0, i1, f.natom);
+        else atom_lines(out[p], f.pos.data(), f.vel.data(), f.mol_id.data(), f.mol_offset, i0, i1);
+    };
+    std::vector<std::thread> pool;
+    for (int p = 1; p < parts; p++) pool.emplace_back(work, p);
+    work(0);
+    for (auto& t : pool) t.join();
+    const std::string head = frame_head(units * per, f.h, f.istep, f.dt);
+    fwrite(head.data(), 1, head.size(), fp_);
+    for (auto& o : out) fwrite(o.data(), 1, o.size(), fp_);
+    fflush(fp_);
 }
 
 // ------------------------------------------------------------------ restart

@@ -7,9 +7,14 @@
 // MM = fuller_LJ_npt_mmmd_serial_omp_acc.cpp, CORE = ..._core_serial*.cpp).
 // No CUDA here; the drivers call libfullermd_cuda.so for all per-step work.
 #pragma once
+#include <condition_variable>
 #include <cstdio>
+#include <deque>
 #include <map>
+#include <memory>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -73,6 +78,40 @@ void write_ovito_rigid(FILE* fp, int istep, double dt, const double* pos, const 
                        const double* body, const double* h, int n, int natom);
 void write_ovito_atoms(FILE* fp, int istep, double dt, const double* pos, const double* vel, const int* mol_id,
                        int mol_offset, const double* h, int na);
+
+// Asynchronous OVITO output: rigid()/atoms() copy the frame's state and
+// return; a writer thread formats it (the lines split over up to `threads`
+// worker threads, the same text as write_ovito_*) and appends it to fp,
+// flushed frame by frame.  At most two frames are in flight: a third call
+// waits for the oldest to be written.  finish() (and the destructor) wait
+// for every frame; fp stays open (the caller closes it).
+class OvitoWriter {
+public:
+    explicit OvitoWriter(FILE* fp, int threads = 0);
+    ~OvitoWriter();
+    OvitoWriter(const OvitoWriter&) = delete;
+    OvitoWriter& operator=(const OvitoWriter&) = delete;
+    void rigid(int istep, double dt, const double* pos, const double* vel, const double* qv, const double* body,
+               const double* h, int n, int natom);
+    void atoms(int istep, double dt, const double* pos, const double* vel, const int* mol_id, int mol_offset,
+               const double* h, int na);
+    void finish();
+
+private:
+    struct Frame;
+    static constexpr int kSlots = 2;
+    void submit(std::unique_ptr<Frame> f);
+    void loop();
+    void write(const Frame& f);
+    FILE* fp_;
+    int threads_ = 1;
+    std::mutex mu_;
+    std::condition_variable cv_;
+    std::deque<std::unique_ptr<Frame>> queue_;
+    int inflight_ = 0;
+    bool stop_ = false;
+    std::thread th_;
+};
 
 // Restart files (LJ:590-635, AI:629-677, MM:930-976).
 struct RunInfo {

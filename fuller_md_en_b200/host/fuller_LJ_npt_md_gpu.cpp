@@ -193,6 +193,8 @@ int main(int argc, char** argv) {
     const double t0 = now_s();
     FILE* io_o = nrec_o > 0 ? fopen(ovito_file.c_str(), "w") : nullptr;
     sc.ovito = io_o != nullptr;
+    // frames are formatted and written on a writer thread while the steps go on
+    std::unique_ptr<OvitoWriter> ovito(io_o ? new OvitoWriter(io_o) : nullptr);
     printf("  %8s %5s %7s %9s %8s %10s %13s %7s\n", "step", "phase", "T[K]", "P[GPa]", "a[A]", "Ecoh[eV]",
            "Ecoh[kcal/m]", "t[s]");
 
@@ -212,8 +214,7 @@ int main(int argc, char** argv) {
         const double Ec = o.E[0] / N, an = o.a;
         if (sc.ovito_at(e)) {
             check(ctx, fmd_system_download(sys, pos.data(), vel.data(), qv.data(), nullptr, h, nullptr), "download");
-            write_ovito_rigid(io_o, e, dt, pos.data(), vel.data(), qv.data(), mol.coords.data(), h, N, natom);
-            fflush(io_o);
+            ovito->rigid(e, dt, pos.data(), vel.data(), qv.data(), mol.coords.data(), h, N, natom);
         }
         if (sc.restart_at(e)) {
             save(e);
@@ -237,6 +238,7 @@ int main(int argc, char** argv) {
         }
         g = e + 1;
     }
+    ovito.reset();                          // every frame written
     if (io_o) fclose(io_o);
     fmd_avg av;
     check(ctx, fmd_system_averages(sys, &av), "averages");

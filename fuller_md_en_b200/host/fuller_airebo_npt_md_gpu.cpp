@@ -182,6 +182,8 @@ int main(int argc, char** argv) {
     const std::string ovito_file = unique_file("ovito_traj_airebo_gpu", ".xyz");
     FILE* io_o = nrec_o > 0 ? fopen(ovito_file.c_str(), "w") : nullptr;
     sc.ovito = io_o != nullptr;
+    // frames are formatted and written on a writer thread while the steps go on
+    std::unique_ptr<OvitoWriter> ovito(io_o ? new OvitoWriter(io_o) : nullptr);
     printf("  %8s %5s %7s %9s %8s %11s %11s %11s %7s\n", "step", "phase", "T[K]", "P[GPa]", "a[A]", "E_REBO",
            "E_LJ", "E_total", "t[s]");
     const std::string rst_base = nrec_o > 0 ? ovito_file : std::string("restart_airebo_gpu");
@@ -201,8 +203,7 @@ int main(int argc, char** argv) {
         check(ctx, fmd_system_run(sys, gs, e, &o), "MD steps");
         if (sc.ovito_at(e)) {
             check(ctx, fmd_system_download(sys, pos.data(), vel.data(), nullptr, nullptr, h, nullptr), "download");
-            write_ovito_atoms(io_o, e, dt, pos.data(), vel.data(), mol_id.data(), 0, h, Na);
-            fflush(io_o);
+            ovito->atoms(e, dt, pos.data(), vel.data(), mol_id.data(), 0, h, Na);
         }
         if (sc.restart_at(e)) {
             save(e);
@@ -227,6 +228,7 @@ int main(int argc, char** argv) {
         }
         gs = e + 1;
     }
+    ovito.reset();                          // every frame written
     if (io_o) fclose(io_o);
     fmd_avg av;
     check(ctx, fmd_system_averages(sys, &av), "averages");

@@ -1,0 +1,36 @@
+"""The drivers' asynchronous OVITO writer (fmdh::OvitoWriter: frames copied,
+formatted in parallel chunks on a writer thread, appended in order) writes
+exactly the bytes of the synchronous formatter, for atomistic and rigid
+frames, with one and with several formatting threads."""
+from __future__ import annotations
+
+import subprocess
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+LIB = ROOT / "fuller_md_en_b200" / "_lib"
+HOST = ROOT / "fuller_md_en_b200" / "host"
+
+
+@pytest.fixture(scope="module")
+def checker(tmp_path_factory):
+    if not (LIB / "libfullermd_host.so").exists():
+        pytest.fail("libfullermd_host.so is not built (python -m fuller_md_en_b200.build)")
+    exe = tmp_path_factory.mktemp("ovito") / "ovito_writer_check"
+    r = subprocess.run(["g++", "-std=c++17", "-O2", "-pthread", "-I", str(HOST), "-I", str(ROOT / "include"),
+                        "-o", str(exe), str(ROOT / "tests" / "cpp" / "ovito_writer_check.cpp"), f"-L{LIB}",
+                        "-lfullermd_host", f"-Wl,-rpath,{LIB}"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    return exe
+
+
+@pytest.mark.parametrize("threads", [1, 7])
+def test_async_writer_matches_sync_formatter(checker, tmp_path, threads):
+    a, b = tmp_path / "sync.xyz", tmp_path / "async.xyz"
+    r = subprocess.run([str(checker), str(a), str(b), str(threads)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    da, db = a.read_bytes(), b.read_bytes()
+    assert len(da) > 10_000_000 and da == db
+    assert da.count(b"Lattice=") == 11
