@@ -245,7 +245,12 @@ def mm_topology(coords: np.ndarray, bonds: np.ndarray, nmol: int, kb: float = 46
             j, k, l = adj[i]
             im.append((i, j, k, l))
             ig.append(2 * _dihedral0(c, j, i, k, l) + math.pi)
-    rep = lambda a: np.concatenate([np.asarray(a, np.int32) + m * na for m in range(nmol)])
+    shift = (np.arange(nmol, dtype=np.int32) * na)[:, None, None]
+
+    def rep(a):                                      # copy m: indices + m na, copies in order
+        base = np.asarray(a, np.int32).reshape(1, len(a), -1)
+        return (base + shift).reshape(-1, base.shape[2]) if len(a) else np.zeros((0, 2), np.int32)
+
     tile = lambda a: np.tile(np.asarray(a, np.float64), nmol)
     return {"bonds": rep(bl), "kb": np.full(len(bl) * nmol, kb * KCAL2EV), "r0": tile(br0),
             "angles": rep(an), "kth": np.full(len(an) * nmol, kth * KCAL2EV), "th0": tile(ath),
