@@ -17,6 +17,7 @@ _ip = POINTER(c_int)
 
 FMD_OK, FMD_ERR_ARG, FMD_ERR_CUDA, FMD_ERR_CAPACITY, FMD_ERR_NONFINITE, FMD_ERR_STATE = range(6)
 FMD_PREC_FP64, FMD_PREC_FP32_PAIR = 0, 1
+FMD_PHYS_MM_BONDED = 1
 FMD_FF_AIREBO, FMD_FF_MM = 0, 1
 FMD_SYS_RIGID, FMD_SYS_AIREBO, FMD_SYS_MM = 0, 1, 2
 
@@ -129,6 +130,7 @@ _SIGS = {
     "fmd_system_forces": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "fmd_system_lj_rows": (c_int, [c_void_p, c_void_p, c_void_p]),
     "fmd_system_lj_full_rows": (c_int, [c_void_p, c_void_p, c_void_p, POINTER(c_int)]),
+    "fmd_system_set_physics": (c_int, [c_void_p, c_int]),
     "fmd_system_lj_prune": (c_int, [c_void_p, POINTER(c_double), POINTER(c_longlong), POINTER(c_longlong)]),
     "fmd_umma_selftest": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, POINTER(c_float)]),
     "fmd_sg_nparams": (c_int, []),

@@ -475,6 +475,12 @@ class System:
         """Pins the LJ gather's launch shape (feed 0 plain, 1 pipelined, 2 staged rows)."""
         self.ctx.check(self.ctx.lib.fmd_system_set_lj_shape(self.h, threads, unroll, feed), "fmd_system_set_lj_shape")
 
+    def set_physics(self, flags: int) -> None:
+        """Opt-in physics corrections (fmd_physics bits, e.g.
+        _lib.FMD_PHYS_MM_BONDED); before init().  Default 0: the reference's
+        forces."""
+        self.ctx.check(self.ctx.lib.fmd_system_set_physics(self.h, int(flags)), "fmd_system_set_physics")
+
     def set_lj_prune(self, delta: float) -> None:
         """Buffer (A) of the pruned LJ gather rows beyond the cutoff; 0 turns
         pruning off (the full rows every step).  Default 0.5."""

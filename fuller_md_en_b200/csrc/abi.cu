@@ -351,6 +351,7 @@ int upload_topo(fmd_ctx* ctx, const fmd_mm_topology* t, MMTopoDev& d) {
     int *i0, *i1, *i2, *i3, *mu;
     double *x0, *x1, *x2;
     d.nb = t->nb; d.nang = t->nang; d.ndih = t->ndih; d.nimp = t->nimp;
+    d.physical = 0;                                  // the reference's forces
     rc |= up(ctx, s++, t->b_i0, t->nb, &i0); rc |= up(ctx, s++, t->b_i1, t->nb, &i1);
     rc |= up(ctx, s++, t->b_kb, t->nb, &x0); rc |= up(ctx, s++, t->b_r0, t->nb, &x1);
     if (rc) return FMD_ERR_CUDA;

@@ -161,6 +161,7 @@ struct MMTopoDev {
     const int *a_i0, *a_i1, *a_i2; const double *a_kth, *a_th0;
     const int *d_i0, *d_i1, *d_i2, *d_i3; const double *d_vn; const int *d_mult; const double *d_gamma;
     const int *m_i0, *m_i1, *m_i2, *m_i3; const double *m_ki, *m_gamma;
+    int physical;                 // 1: bond and angle forces as -grad E (FMD_PHYS_MM_BONDED)
 };
 constexpr int kMMNV = 7;
 cudaError_t mm_bonded_launch(const MMTopoDev& t, const double* pos, const double* hh, double* Facc,

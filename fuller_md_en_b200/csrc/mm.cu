@@ -5,7 +5,11 @@
 // [bonds | angles | dihedrals | impropers]; forces scattered with FP64
 // atomics into an accumulator that the LJ gather kernel folds into F and
 // clears.  Sign conventions follow the reference exactly, including the bond
-// and angle forces that equal +grad E (MM:389-398, MM:468-491).  Energies and
+// and angle forces that equal +grad E (MM:389-398, MM:468-491), unless the
+// topology is marked physical: then those two are negated, and so are the
+// torsions' projection terms on their middle atoms (torsion()), and every MM
+// force is -grad E (the reference path multiplies by 1.0: its arithmetic is
+// unchanged).  Energies and
 // the bond diagonal virial go to per-block partials.
 //
 // Coulomb: all pairs of different molecules within 3 sigma, gathered per atom
@@ -38,9 +42,14 @@ __device__ __forceinline__ void add3(double* F, int i, double x, double y, doubl
     atomicAdd(&F[3 * i + 2], z);
 }
 
-// Torsion of atoms a1-a2-a3-a4 (MM:503-601); returns the energy.
+// Torsion of atoms a1-a2-a3-a4 (MM:503-601); returns the energy.  The forces
+// on a1 and a4 are -dE/dphi dphi/dr; on the middle atoms the reference adds
+// the projections ci f1 - ck f4 with the opposite sign to the gradient's
+// (b1 = r2 - r1 where the gradient formula's vector is r1 - r2), so they are
+// not -grad E.  sg = -1 (physical forces) negates ci and ck, giving -grad E;
+// sg = 1 is the reference's arithmetic exactly.
 __device__ double torsion(double* F, const double* __restrict__ pos, const double* h, const double* hi,
-                          int a1, int a2, int a3, int a4, int mult, double vn, double gamma) {
+                          int a1, int a2, int a3, int a4, int mult, double vn, double gamma, double sg) {
     double b1x, b1y, b1z, b2x, b2y, b2z, b3x, b3y, b3z;
     vec(pos, a1, a2, h, hi, b1x, b1y, b1z);
     vec(pos, a2, a3, h, hi, b2x, b2y, b2z);
@@ -63,7 +72,7 @@ __device__ double torsion(double* F, const double* __restrict__ pos, const doubl
     const double g1 = dphi * b2len * imm, g4 = -dphi * b2len * inn;
     const double f1x = g1 * mx, f1y = g1 * my, f1z = g1 * mz;
     const double f4x = g4 * nx, f4y = g4 * ny, f4z = g4 * nz;
-    const double ci = b1b2 / (b2len * b2len), ck = b2b3 / (b2len * b2len);
+    const double ci = sg * (b1b2 / (b2len * b2len)), ck = sg * (b2b3 / (b2len * b2len));
     add3(F, a1, f1x, f1y, f1z);
     add3(F, a2, -f1x + ci * f1x - ck * f4x, -f1y + ci * f1y - ck * f4y, -f1z + ci * f1z - ck * f4z);
     add3(F, a3, -f4x - ci * f1x + ck * f4x, -f4y - ci * f1y + ck * f4y, -f4z - ci * f1z + ck * f4z);
@@ -80,6 +89,7 @@ __device__ __forceinline__ void mm_bonded_body(const MMTopoDev& t, const double*
     double acc[kMMNV];   // Eb Ea Ed Ei W00 W11 W22
 #pragma unroll
     for (int k = 0; k < kMMNV; k++) acc[k] = 0.0;
+    const double sg = t.physical ? -1.0 : 1.0;
     const int total = t.nb + t.nang + t.ndih + t.nimp;
     for (int q = blk * blockDim.x + threadIdx.x; q < total; q += nblk * blockDim.x) {
         if (q < t.nb) {                                           // MM:384-447
@@ -90,7 +100,7 @@ __device__ __forceinline__ void mm_bonded_body(const MMTopoDev& t, const double*
             if (r < 1e-10) continue;
             const double dr = r - t.b_r0[b];
             acc[0] += 0.5 * t.b_kb[b] * dr * dr;
-            const double fm = -t.b_kb[b] * dr / r;
+            const double fm = sg * (-t.b_kb[b] * dr / r);
             const double fx = fm * dx, fy = fm * dy, fz = fm * dz;
             add3(F, i, fx, fy, fz);
             add3(F, j, -fx, -fy, -fz);
@@ -107,7 +117,7 @@ __device__ __forceinline__ void mm_bonded_body(const MMTopoDev& t, const double*
             const double th = acos(c), dth = th - t.a_th0[a];
             acc[1] += 0.5 * t.a_kth[a] * dth * dth;
             const double s = sqrt(1.0 - c * c + 1e-30);
-            const double dV = -t.a_kth[a] * dth / s;
+            const double dV = sg * (-t.a_kth[a] * dth / s);
             const double uv = du * dv, uu = du * du, vv = dv * dv;
             const double fi0 = dV * (v0 / uv - c * u0 / uu), fi1 = dV * (v1 / uv - c * u1 / uu),
                          fi2 = dV * (v2 / uv - c * u2 / uu);
@@ -119,11 +129,11 @@ __device__ __forceinline__ void mm_bonded_body(const MMTopoDev& t, const double*
         } else if (q < t.nb + t.nang + t.ndih) {                  // MM:500-602
             const int d = q - t.nb - t.nang;
             acc[2] += torsion(F, pos, h, hi, t.d_i0[d], t.d_i1[d], t.d_i2[d], t.d_i3[d], t.d_mult[d],
-                              t.d_vn[d], t.d_gamma[d]);
+                              t.d_vn[d], t.d_gamma[d], sg);
         } else {                                                  // MM:610-709, order c1,c0,c2,c3
             const int p = q - t.nb - t.nang - t.ndih;
             acc[3] += torsion(F, pos, h, hi, t.m_i1[p], t.m_i0[p], t.m_i2[p], t.m_i3[p], 2, t.m_ki[p],
-                              t.m_gamma[p]);
+                              t.m_gamma[p], sg);
         }
     }
     block_sum_store<kMMNV>(acc, sm, part + (size_t)blk * kMMNV);

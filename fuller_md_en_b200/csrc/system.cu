@@ -692,6 +692,17 @@ extern "C" int fmd_system_lj_rows(fmd_system* s, int* full_cnt, int* pruned_cnt)
     return y.ctx->sync_check("system LJ rows");
 }
 
+extern "C" int fmd_system_set_physics(fmd_system* s, int flags) {
+    if (!s || !s->sys) return FMD_ERR_ARG;
+    fmd::System& y = *s->sys;
+    if (y.initialized) return y.ctx->fail(FMD_ERR_ARG, "fmd_system_set_physics: call before fmd_system_init");
+    if (flags & ~FMD_PHYS_MM_BONDED) return y.ctx->fail(FMD_ERR_ARG, "fmd_system_set_physics: unknown flag");
+    if ((flags & FMD_PHYS_MM_BONDED) && y.arr.kind != FMD_SYS_MM)
+        return y.ctx->fail(FMD_ERR_ARG, "fmd_system_set_physics: FMD_PHYS_MM_BONDED needs an MM system");
+    y.arr.topo.physical = (flags & FMD_PHYS_MM_BONDED) ? 1 : 0;
+    return FMD_OK;
+}
+
 extern "C" int fmd_system_lj_full_rows(fmd_system* s, int* cnt, int* list, int* stride) {
     if (!s || !s->sys) return FMD_ERR_ARG;
     fmd::System& y = *s->sys;

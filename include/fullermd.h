@@ -46,6 +46,14 @@ enum fmd_precision {
                                and force/energy/virial sums in FP64 */
 };
 
+/* Opt-in physics corrections (no reference counterpart; off by default, so a
+ * system computes the reference's forces).  FMD_PHYS_MM_BONDED: every MM
+ * bonded force is -grad E of the MM energy: bond and angle forces negated
+ * (the reference's equal +grad E, MM:389-398, MM:468-491) and the dihedral
+ * and improper forces on the two middle atoms taken from the gradient (the
+ * reference's projection terms have the opposite sign, MM:500-709). */
+enum fmd_physics { FMD_PHYS_MM_BONDED = 1 };
+
 enum fmd_forcefield { FMD_FF_AIREBO = 0, FMD_FF_MM = 1 };
 enum fmd_kind { FMD_SYS_RIGID = 0, FMD_SYS_AIREBO = 1, FMD_SYS_MM = 2 };
 
@@ -253,6 +261,9 @@ int fmd_system_lj_rows(fmd_system *s, int *full_cnt, int *pruned_cnt);
  * not NULL, receive the row lengths and rows -- row j holds the atoms i < j
  * whose reference row lists j, ascending, then j's own reference row. */
 int fmd_system_lj_full_rows(fmd_system *s, int *cnt, int *list, int *stride);
+/* Physics corrections (fmd_physics bits) of a system; before fmd_system_init.
+ * A bit the system's force field lacks is an FMD_ERR_ARG. */
+int fmd_system_set_physics(fmd_system *s, int flags);
 int fmd_system_destroy(fmd_system *s);
 
 /* Measurement helpers (no reference counterpart).  fmd_system_kernel_ms
