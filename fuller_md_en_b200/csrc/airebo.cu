@@ -378,12 +378,18 @@ k_rebo_geo_bo(const double* __restrict__ pos, const double* __restrict__ hh, con
 
 // Three-body forces of centre c for the bond c -> skip with coefficient coeff
 // (AI:368-419) on c's other neighbours k, and the reaction on c.
+// PHYS: the gradient of the bond-order term instead of the reference's
+// three-body forces (which have the opposite sign on the neighbours and lack
+// the term on the bond partner): f_k = -coeff dG/dr_k, and the partner gets
+// -coeff dG/dr_skip = -coeff sum_k fc_k g'(cos) (u_k - cos u_b) / r_b.
+template <bool PHYS>
 __device__ __forceinline__ void three_body_sl(double* __restrict__ F, const Slot* __restrict__ sl,
                                               const int* __restrict__ list, int cap, int c, int m, int skip,
                                               double bx, double by, double bz, double rbinv, double coeff) {
     if (coeff == 0.0) return;
     const double ux = bx * rbinv, uy = by * rbinv, uz = bz * rbinv;
     double fcx = 0.0, fcy = 0.0, fcz = 0.0;
+    double fbx = 0.0, fby = 0.0, fbz = 0.0;
     for (int kn = 0; kn < m; kn++) {
         const size_t o = (size_t)c * cap + kn;
         const int k = list[o];
@@ -394,12 +400,21 @@ __device__ __forceinline__ void three_body_sl(double* __restrict__ F, const Slot
         const double ct = clamp1((bx * q.dx + by * q.dy + bz * q.dz) * (rbinv * q.rinv));
         double gv, dgv;
         ang_g_dg(ct, gv, dgv);
-        const double a1 = coeff * q.dfc * gv, a2 = coeff * q.fc * dgv;
+        const double a1 = PHYS ? -(coeff * q.dfc * gv) : coeff * q.dfc * gv;
+        const double a2 = PHYS ? -(coeff * q.fc * dgv) : coeff * q.fc * dgv;
         const double fx = a1 * rx + a2 * ((ux - ct * rx) * q.rinv);
         const double fy = a1 * ry + a2 * ((uy - ct * ry) * q.rinv);
         const double fz = a1 * rz + a2 * ((uz - ct * rz) * q.rinv);
         atomic_add3(F, k, fx, fy, fz);
         fcx -= fx; fcy -= fy; fcz -= fz;
+        if (PHYS) {
+            const double a3 = a2 * rbinv;
+            fbx += a3 * (rx - ct * ux); fby += a3 * (ry - ct * uy); fbz += a3 * (rz - ct * uz);
+        }
+    }
+    if (PHYS) {
+        atomic_add3(F, skip, fbx, fby, fbz);
+        fcx -= fbx; fcy -= fby; fcz -= fbz;
     }
     atomic_add3(F, c, fcx, fcy, fcz);
 }
@@ -435,6 +450,7 @@ __device__ __forceinline__ void seg_sum3(double& x, double& y, double& z, unsign
 // (seg_sum) and one lane adds it, and the reactions on the centre and its
 // pair-term forces go out as one sum per centre, so a centre with m bonds
 // issues about m + 1 + m/2 atomic triples instead of m^2 + m/2.
+template <bool PHYS>
 __global__ void __launch_bounds__(256)
 k_rebo_force(const Slot* __restrict__ sl, const SlotBO* __restrict__ bo, const int* __restrict__ cnt,
              const int* __restrict__ list, int cap, int na, double* __restrict__ F, double* __restrict__ part,
@@ -487,6 +503,7 @@ k_rebo_force(const Slot* __restrict__ sl, const SlotBO* __restrict__ bo, const i
         const bool tb = ok && o.coeff != 0.0;
         const double ux = q.dx * q.rinv, uy = q.dy * q.rinv, uz = q.dz * q.rinv;
         const int mseg = __reduce_max_sync(kFull, valid ? m : 0);
+        double fbx = 0.0, fby = 0.0, fbz = 0.0;       // PHYS: force on the partner j
         for (int kn = 0; kn < mseg; kn++) {
             double fx = 0.0, fy = 0.0, fz = 0.0;
             int kt = -1;
@@ -500,16 +517,25 @@ k_rebo_force(const Slot* __restrict__ sl, const SlotBO* __restrict__ bo, const i
                         const double ct = clamp1((q.dx * r.dx + q.dy * r.dy + q.dz * r.dz) * (q.rinv * r.rinv));
                         double gv, dgv;
                         ang_g_dg(ct, gv, dgv);
-                        const double a1 = o.coeff * r.dfc * gv, a2 = o.coeff * r.fc * dgv;
+                        const double a1 = PHYS ? -(o.coeff * r.dfc * gv) : o.coeff * r.dfc * gv;
+                        const double a2 = PHYS ? -(o.coeff * r.fc * dgv) : o.coeff * r.fc * dgv;
                         fx = a1 * rx + a2 * ((ux - ct * rx) * r.rinv);
                         fy = a1 * ry + a2 * ((uy - ct * ry) * r.rinv);
                         fz = a1 * rz + a2 * ((uz - ct * rz) * r.rinv);
                         fcx -= fx; fcy -= fy; fcz -= fz;
+                        if (PHYS) {
+                            const double a3 = a2 * q.rinv;
+                            fbx += a3 * (rx - ct * ux); fby += a3 * (ry - ct * uy); fbz += a3 * (rz - ct * uz);
+                        }
                     }
                 }
             }
             seg_sum3(fx, fy, fz, seg, lane, span);
             if (lead && kt >= 0 && (fx != 0.0 || fy != 0.0 || fz != 0.0)) atomic_add3(F, kt, fx, fy, fz);
+        }
+        if (PHYS && tb) {
+            atomic_add3(F, j, fbx, fby, fbz);
+            fcx -= fbx; fcy -= fby; fcz -= fbz;
         }
         if (ok && j > i) {
             double bji;
@@ -518,8 +544,8 @@ k_rebo_force(const Slot* __restrict__ sl, const SlotBO* __restrict__ bo, const i
             } else {
                 const double gji = bo_sum_sl(sl, cap, j, mj, -1, -q.dx, -q.dy, -q.dz, q.rinv);
                 bji = 1.0 / sqrt(1.0 + gji);
-                three_body_sl(F, sl, list, cap, j, mj, i, -q.dx, -q.dy, -q.dz, q.rinv,
-                              three_body_coeff(gji, bji, q.fc, o.va));
+                three_body_sl<PHYS>(F, sl, list, cap, j, mj, i, -q.dx, -q.dy, -q.dz, q.rinv,
+                                    three_body_coeff(gji, bji, q.fc, o.va));
             }
             const double bbar = 0.5 * (o.b + bji);
             acc[0] += q.fc * (o.vr - bbar * o.va);
@@ -897,7 +923,7 @@ cudaError_t rebo_launch_gated(const double* pos, const double* hh, const int* cn
 
 cudaError_t rebo_slots_launch(const double* pos, const double* hh, const int* cnt, const int* list, int cap,
                               int na, double* slots, double* F, double* part, int nblocks, const int* gate,
-                              int want, cudaStream_t st, const int* ids) {
+                              int want, cudaStream_t st, const int* ids, bool phys) {
     Slot* sl = reinterpret_cast<Slot*>(slots);
     SlotBO* bo = reinterpret_cast<SlotBO*>(slots + (size_t)na * cap * 8);
     cudaError_t e;
@@ -913,8 +939,9 @@ cudaError_t rebo_slots_launch(const double* pos, const double* hh, const int* cn
                             gate, want, ids)) != cudaSuccess)
             return e;
     }
-    if ((e = launch_pdl(k_rebo_force, dim3(nblocks), dim3(256), 0, st, (const Slot*)sl, (const SlotBO*)bo, cnt, list,
-                        cap, na, F, part, gate, want, ids)) != cudaSuccess)
+    if ((e = launch_pdl(phys ? k_rebo_force<true> : k_rebo_force<false>, dim3(nblocks), dim3(256), 0, st,
+                        (const Slot*)sl, (const SlotBO*)bo, cnt, list, cap, na, F, part, gate, want, ids)) !=
+        cudaSuccess)
         return e;
     return cudaGetLastError();
 }

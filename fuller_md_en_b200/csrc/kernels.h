@@ -96,9 +96,11 @@ constexpr int kReboSlotDoubles = 16;
 // ids[1 + kIdsLanes * na + t] the partner slot of slot t (i's position in j's
 // row, -1 if absent) (rebo_ids_build); lanes then walk only occupied slots,
 // and the slots of one atom share a warp.
+// phys: the gradient of the bond-order term in place of the reference's
+// three-body forces (FMD_PHYS_REBO).
 cudaError_t rebo_slots_launch(const double* pos, const double* hh, const int* cnt, const int* list, int cap,
                               int na, double* slots, double* F, double* part, int nblocks, const int* gate,
-                              int want, cudaStream_t st, const int* ids = nullptr);
+                              int want, cudaStream_t st, const int* ids = nullptr, bool phys = false);
 // Builds ids (1 + kIdsLanes n + n cap ints) from the list (cap <= 32);
 // scratch: rebo_ids_scratch(n) ints.
 constexpr int kIdsLanes = 32;

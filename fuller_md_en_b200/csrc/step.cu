@@ -520,7 +520,7 @@ cudaError_t enqueue_forces(const StepArrays& a, cudaStream_t st, bool judge) {
         if (a.sg) e = sg_enqueue_rebo(*a.sg, a, judge, st);
         else if (a.rebo_slots)
             e = rebo_slots_launch(a.pos, hh, a.cnt_b, a.list_b, a.cap_b, a.n, a.rebo_slots, a.Facc, a.part_f1,
-                                  kForceBlocks, nullptr, 0, st, a.rebo_ids);
+                                  kForceBlocks, nullptr, 0, st, a.rebo_ids, a.rebo_phys != 0);
         else e = rebo_launch(a.pos, hh, a.cnt_b, a.list_b, a.cap_b, a.n, a.Facc, a.part_f1, st);
         if (e != cudaSuccess) return e;
         e = enqueue_lj(a, FMD_FF_AIREBO, st);

@@ -696,10 +696,14 @@ extern "C" int fmd_system_set_physics(fmd_system* s, int flags) {
     if (!s || !s->sys) return FMD_ERR_ARG;
     fmd::System& y = *s->sys;
     if (y.initialized) return y.ctx->fail(FMD_ERR_ARG, "fmd_system_set_physics: call before fmd_system_init");
-    if (flags & ~FMD_PHYS_MM_BONDED) return y.ctx->fail(FMD_ERR_ARG, "fmd_system_set_physics: unknown flag");
+    if (flags & ~(FMD_PHYS_MM_BONDED | FMD_PHYS_REBO))
+        return y.ctx->fail(FMD_ERR_ARG, "fmd_system_set_physics: unknown flag");
     if ((flags & FMD_PHYS_MM_BONDED) && y.arr.kind != FMD_SYS_MM)
         return y.ctx->fail(FMD_ERR_ARG, "fmd_system_set_physics: FMD_PHYS_MM_BONDED needs an MM system");
+    if ((flags & FMD_PHYS_REBO) && (y.arr.kind != FMD_SYS_AIREBO || !y.arr.rebo_slots))
+        return y.ctx->fail(FMD_ERR_ARG, "fmd_system_set_physics: FMD_PHYS_REBO needs an AIREBO system");
     y.arr.topo.physical = (flags & FMD_PHYS_MM_BONDED) ? 1 : 0;
+    y.arr.rebo_phys = (flags & FMD_PHYS_REBO) ? 1 : 0;
     return FMD_OK;
 }
 
@@ -750,7 +754,7 @@ extern "C" int fmd_system_kernel_ms(fmd_system* s, int stage, int reps, double* 
                     return sg_enqueue_rebo(*a.sg, a, false, st);
                 if (a.kind == FMD_SYS_AIREBO)
                     return rebo_slots_launch(a.pos, hh, a.cnt_b, a.list_b, a.cap_b, a.n, a.rebo_slots, a.Facc,
-                                             a.part_f1, kForceBlocks, nullptr, 0, st, a.rebo_ids);
+                                             a.part_f1, kForceBlocks, nullptr, 0, st, a.rebo_ids, a.rebo_phys != 0);
                 if (a.kind == FMD_SYS_MM) return mm_bonded_launch(a.topo, a.pos, hh, a.Facc, a.part_f1, st);
                 return rigid_launch(a.precision, a.pos, a.qv, a.body, hh, a.cnt_a, a.list_a, a.cap_a, a.n, a.natom,
                                     a.rmcut2, a.F, a.T, a.part_f1, st, a.rigid_lab, a.rigid_shape);

@@ -51,8 +51,12 @@ enum fmd_precision {
  * bonded force is -grad E of the MM energy: bond and angle forces negated
  * (the reference's equal +grad E, MM:389-398, MM:468-491) and the dihedral
  * and improper forces on the two middle atoms taken from the gradient (the
- * reference's projection terms have the opposite sign, MM:500-709). */
-enum fmd_physics { FMD_PHYS_MM_BONDED = 1 };
+ * reference's projection terms have the opposite sign, MM:500-709).
+ * FMD_PHYS_REBO: REBO forces are -grad E of the REBO energy: the bond-order
+ * term's gradient replaces the reference's three-body forces (opposite sign
+ * on the neighbours, no term on the bond partner, AI:361-419).  The learned
+ * REBO term, when attached, is not affected. */
+enum fmd_physics { FMD_PHYS_MM_BONDED = 1, FMD_PHYS_REBO = 2 };
 
 enum fmd_forcefield { FMD_FF_AIREBO = 0, FMD_FF_MM = 1 };
 enum fmd_kind { FMD_SYS_RIGID = 0, FMD_SYS_AIREBO = 1, FMD_SYS_MM = 2 };

@@ -1,16 +1,17 @@
 """Opt-in physics corrections (fmd_system_set_physics).  They have no
 reference counterpart, so they are checked against the mathematics: with
-FMD_PHYS_MM_BONDED every MM force is -grad E of the MM energy, measured by
-central differences of the system's own energy.  Without the flag the system
-keeps the reference's bond and angle forces (+grad E, MM:389-398,
-MM:468-491), which the same check rejects."""
+FMD_PHYS_MM_BONDED every MM force, with FMD_PHYS_REBO every AIREBO force, is
+-grad E of the system's own energy, measured by central differences.  Without
+the flags the systems keep the reference's forces (MM bond and angle forces
++grad E, MM:389-398, MM:468-491; torsion and REBO three-body forces that are
+not gradients), which the same check rejects."""
 from __future__ import annotations
 
 import numpy as np
 import pytest
 
 from fuller_md_en_b200 import RunConfig, System, Topology, crystal
-from fuller_md_en_b200._lib import FMD_PHYS_MM_BONDED, FmdError
+from fuller_md_en_b200._lib import FMD_PHYS_MM_BONDED, FMD_PHYS_REBO, FmdError
 
 pytestmark = pytest.mark.gpu
 
@@ -86,3 +87,43 @@ def test_physics_flag_checks(ctx):
     with pytest.raises(FmdError):
         z.set_physics(FMD_PHYS_MM_BONDED)      # not an MM system
     z.close()
+
+
+def _airebo(ctx, s, pos, physics):
+    na = pos.size // 3
+    cfg = RunConfig(dt=0.5, T=300.0, Pe=0.0, nsteps=4, nlup=20, nc=1, nmol=s["nmol"])
+    y = System.airebo(ctx, cfg, pos, s["vel"], s["mass"], s["mol_id"], s["h"], crystal.npt_atom(300.0, 0.0, na))
+    if physics:
+        y.set_physics(physics)
+    y.init()
+    F, _, E = y.forces()
+    y.close()
+    return F, E[0]
+
+
+def _airebo_fd(ctx, s, physics, comps):
+    F, E = _airebo(ctx, s, s["pos"], physics)
+    err = 0.0
+    for k in comps:
+        p, m = s["pos"].copy(), s["pos"].copy()
+        p[k] += DELTA
+        m[k] -= DELTA
+        g = (_airebo(ctx, s, p, physics)[1] - _airebo(ctx, s, m, physics)[1]) / (2 * DELTA)
+        err = max(err, abs(F[k] + g))
+    return err, float(np.max(np.abs(F))), E
+
+
+@pytest.mark.parametrize("scale,seed", [(1.0, 11), (0.65, 77), (0.7, 5)])
+def test_rebo_physical_forces_are_minus_grad_energy(ctx, scale, seed):
+    """AIREBO (REBO + LJ) with FMD_PHYS_REBO; scales 0.65 and 0.7 crowd the
+    REBO rows past their 12 entries (asymmetric rows: bond orders from a row
+    that lacks the bond's other atom)."""
+    s = crystal.atomistic(1, coords=crystal.c60_ih() * scale, jitter=0.05, seed=seed)
+    comps = np.random.default_rng(seed).choice(s["pos"].size, 12, replace=False)
+    err, fmax, E = _airebo_fd(ctx, s, FMD_PHYS_REBO, comps)
+    assert err <= 1e-6 * fmax + 1e-7, (err, fmax)
+    _, E0 = _airebo(ctx, s, s["pos"], 0)
+    assert abs(E - E0) <= 1e-12 * abs(E0)             # the energy is the reference's
+    if scale == 1.0:
+        err0, fmax0, _ = _airebo_fd(ctx, s, 0, comps)
+        assert err0 > 1e-2 * fmax0, (err0, fmax0)      # the reference's three-body forces are not
