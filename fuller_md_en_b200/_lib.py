@@ -17,7 +17,7 @@ _ip = POINTER(c_int)
 
 FMD_OK, FMD_ERR_ARG, FMD_ERR_CUDA, FMD_ERR_CAPACITY, FMD_ERR_NONFINITE, FMD_ERR_STATE = range(6)
 FMD_PREC_FP64, FMD_PREC_FP32_PAIR = 0, 1
-FMD_PHYS_MM_BONDED, FMD_PHYS_REBO = 1, 2
+FMD_PHYS_MM_BONDED, FMD_PHYS_REBO, FMD_PHYS_QUAT = 1, 2, 4
 FMD_FF_AIREBO, FMD_FF_MM = 0, 1
 FMD_SYS_RIGID, FMD_SYS_AIREBO, FMD_SYS_MM = 0, 1, 2
 

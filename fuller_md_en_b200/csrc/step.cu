@@ -96,17 +96,28 @@ __global__ void k_begin(SysScal* S, int kind, StepParams p) {
     begin_body(S, kind, p);
 }
 
-// LJ:166-174.
+// LJ:166-174.  The reference multiplies q by the rotation increment on the
+// right (q dq), which applies the lab-frame angular velocity as a body-frame
+// one; left (dq q, FMD_PHYS_QUAT) rotates the lab-frame sites about the lab
+// axis w, which is what the lab-frame torque update of w describes.
+template <bool LEFT>
 __device__ __forceinline__ void quat_step(double* q, double wx, double wy, double wz, double dt) {
     double dq[4];
     const double wm = sqrt(wx * wx + wy * wy + wz * wz), th = wm * dt * 0.5;
     if (th < 1e-14) { dq[0] = 1.0; dq[1] = 0.5 * dt * wx; dq[2] = 0.5 * dt * wy; dq[3] = 0.5 * dt * wz; }
     else { const double s = sin(th) / wm; dq[0] = cos(th); dq[1] = s * wx; dq[2] = s * wy; dq[3] = s * wz; }
     double o[4];
-    o[0] = q[0] * dq[0] - q[1] * dq[1] - q[2] * dq[2] - q[3] * dq[3];
-    o[1] = q[0] * dq[1] + q[1] * dq[0] + q[2] * dq[3] - q[3] * dq[2];
-    o[2] = q[0] * dq[2] - q[1] * dq[3] + q[2] * dq[0] + q[3] * dq[1];
-    o[3] = q[0] * dq[3] + q[1] * dq[2] - q[2] * dq[1] + q[3] * dq[0];
+    if (LEFT) {
+        o[0] = dq[0] * q[0] - dq[1] * q[1] - dq[2] * q[2] - dq[3] * q[3];
+        o[1] = dq[0] * q[1] + dq[1] * q[0] + dq[2] * q[3] - dq[3] * q[2];
+        o[2] = dq[0] * q[2] - dq[1] * q[3] + dq[2] * q[0] + dq[3] * q[1];
+        o[3] = dq[0] * q[3] + dq[1] * q[2] - dq[2] * q[1] + dq[3] * q[0];
+    } else {
+        o[0] = q[0] * dq[0] - q[1] * dq[1] - q[2] * dq[2] - q[3] * dq[3];
+        o[1] = q[0] * dq[1] + q[1] * dq[0] + q[2] * dq[3] - q[3] * dq[2];
+        o[2] = q[0] * dq[2] - q[1] * dq[3] + q[2] * dq[0] + q[3] * dq[1];
+        o[3] = q[0] * dq[3] + q[1] * dq[2] - q[2] * dq[1] + q[3] * dq[0];
+    }
     const double nrm = sqrt(o[0] * o[0] + o[1] * o[1] + o[2] * o[2] + o[3] * o[3]), inv = 1.0 / nrm;
     for (int k = 0; k < 4; k++) q[k] = o[k] * inv;
 }
@@ -154,7 +165,8 @@ __device__ void kick_body(const StepArrays& a, double dt, int blk, int nblk) {
                 w[c] = a.omg[3 * i + c] * sc_nh + hdt * a.T[3 * i + c] * cT;
                 a.omg[3 * i + c] = w[c];
             }
-            quat_step(a.qv + 4 * i, w[0], w[1], w[2], dt);               // LJ:503-508
+            if (a.quat_left) quat_step<true>(a.qv + 4 * i, w[0], w[1], w[2], dt);
+            else quat_step<false>(a.qv + 4 * i, w[0], w[1], w[2], dt);     // LJ:503-508
         }
     }
     if (a.prune_sb) {

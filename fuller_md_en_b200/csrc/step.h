@@ -58,6 +58,7 @@ struct StepArrays {
     double* rigid_lab = nullptr;   // [n * natom * kRigidLabDoubles] lab-frame sites (rigid)
     int rigid_shape = 0;           // launch shape of the rigid pair kernel (rigid_launch)
     int precision = FMD_PREC_FP64;
+    int quat_left = 0;              // FMD_PHYS_QUAT: the rotation increment multiplies q on the left
     int rebo_phys = 0;              // FMD_PHYS_REBO: bond-order gradient instead of the reference's three-body forces
     LJShape lj_shape{};            // launch shape of the atomistic LJ gather over the full rows
     LJShape lj_shape_p{};          // ... and over the pruned rows

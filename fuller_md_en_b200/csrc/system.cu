@@ -696,14 +696,17 @@ extern "C" int fmd_system_set_physics(fmd_system* s, int flags) {
     if (!s || !s->sys) return FMD_ERR_ARG;
     fmd::System& y = *s->sys;
     if (y.initialized) return y.ctx->fail(FMD_ERR_ARG, "fmd_system_set_physics: call before fmd_system_init");
-    if (flags & ~(FMD_PHYS_MM_BONDED | FMD_PHYS_REBO))
+    if (flags & ~(FMD_PHYS_MM_BONDED | FMD_PHYS_REBO | FMD_PHYS_QUAT))
         return y.ctx->fail(FMD_ERR_ARG, "fmd_system_set_physics: unknown flag");
+    if ((flags & FMD_PHYS_QUAT) && y.arr.kind != FMD_SYS_RIGID)
+        return y.ctx->fail(FMD_ERR_ARG, "fmd_system_set_physics: FMD_PHYS_QUAT needs a rigid system");
     if ((flags & FMD_PHYS_MM_BONDED) && y.arr.kind != FMD_SYS_MM)
         return y.ctx->fail(FMD_ERR_ARG, "fmd_system_set_physics: FMD_PHYS_MM_BONDED needs an MM system");
     if ((flags & FMD_PHYS_REBO) && (y.arr.kind != FMD_SYS_AIREBO || !y.arr.rebo_slots))
         return y.ctx->fail(FMD_ERR_ARG, "fmd_system_set_physics: FMD_PHYS_REBO needs an AIREBO system");
     y.arr.topo.physical = (flags & FMD_PHYS_MM_BONDED) ? 1 : 0;
     y.arr.rebo_phys = (flags & FMD_PHYS_REBO) ? 1 : 0;
+    y.arr.quat_left = (flags & FMD_PHYS_QUAT) ? 1 : 0;
     return FMD_OK;
 }
 

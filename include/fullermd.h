@@ -55,8 +55,11 @@ enum fmd_precision {
  * FMD_PHYS_REBO: REBO forces are -grad E of the REBO energy: the bond-order
  * term's gradient replaces the reference's three-body forces (opposite sign
  * on the neighbours, no term on the bond partner, AI:361-419).  The learned
- * REBO term, when attached, is not affected. */
-enum fmd_physics { FMD_PHYS_MM_BONDED = 1, FMD_PHYS_REBO = 2 };
+ * REBO term, when attached, is not affected.  FMD_PHYS_QUAT (rigid): the
+ * quaternion's rotation increment from the lab-frame angular velocity
+ * multiplies q on the left (the reference's on the right applies it as a
+ * body-frame one, LJ:166-174, LJ:503-508). */
+enum fmd_physics { FMD_PHYS_MM_BONDED = 1, FMD_PHYS_REBO = 2, FMD_PHYS_QUAT = 4 };
 
 enum fmd_forcefield { FMD_FF_AIREBO = 0, FMD_FF_MM = 1 };
 enum fmd_kind { FMD_SYS_RIGID = 0, FMD_SYS_AIREBO = 1, FMD_SYS_MM = 2 };

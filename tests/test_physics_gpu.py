@@ -127,3 +127,46 @@ def test_rebo_physical_forces_are_minus_grad_energy(ctx, scale, seed):
     if scale == 1.0:
         err0, fmax0, _ = _airebo_fd(ctx, s, 0, comps)
         assert err0 > 1e-2 * fmax0, (err0, fmax0)      # the reference's three-body forces are not
+
+
+def _qmul(a, b):
+    return np.array([a[0] * b[0] - a[1] * b[1] - a[2] * b[2] - a[3] * b[3],
+                     a[0] * b[1] + a[1] * b[0] + a[2] * b[3] - a[3] * b[2],
+                     a[0] * b[2] - a[1] * b[3] + a[2] * b[0] + a[3] * b[1],
+                     a[0] * b[3] + a[1] * b[2] - a[2] * b[1] + a[3] * b[0]])
+
+
+def _free_tops(ctx, physics, steps=100):
+    """Rigid C60s 42 A apart (beyond the site cutoff): no forces or torques,
+    so each is a free spherical top whose lab-frame angular velocity keeps
+    its direction (the thermostat only scales it).  Returns, per molecule,
+    the sine of the angle between the lab-frame rotation axis of
+    q(t) q(0)^-1 and w."""
+    from fuller_md_en_b200._lib import FMD_PHYS_QUAT  # noqa: F401
+    s = crystal.rigid(1, seed=21, a0=60.0)
+    n = s["n"]
+    rmcut = 3.0 * 3.431 + 2 * s["Rmol"] + 1.0
+    cfg = RunConfig(dt=1.0, T=300.0, Pe=0.0, nsteps=steps, nlup=25, nc=1, nmol=n)
+    y = System.rigid(ctx, cfg, 60, s["body"], s["I0"], s["Mmol"], rmcut, s["pos"], s["vel"], s["qv"], s["omg"],
+                     s["h"], crystal.npt_rigid(300.0, 0.0, n))
+    if physics:
+        y.set_physics(physics)
+    y.init()
+    y.run(1, steps)
+    out = y.download()
+    y.close()
+    q0 = s["qv"].reshape(n, 4)
+    q1, w = out["qv"].reshape(n, 4), out["omg"].reshape(n, 3)
+    sines = []
+    for a in range(n):
+        d = _qmul(q1[a], q0[a] * np.array([1.0, -1.0, -1.0, -1.0]))
+        v = d[1:] * np.sign(d[0])
+        assert np.linalg.norm(v) > 1e-3                     # it did rotate
+        sines.append(np.linalg.norm(np.cross(v / np.linalg.norm(v), w[a] / np.linalg.norm(w[a]))))
+    return np.array(sines)
+
+
+def test_quaternion_left_update_rotates_about_the_lab_axis(ctx):
+    from fuller_md_en_b200._lib import FMD_PHYS_QUAT
+    assert np.max(_free_tops(ctx, FMD_PHYS_QUAT)) < 1e-9
+    assert np.min(_free_tops(ctx, 0)) > 1e-2                # the reference's right update does not
