@@ -184,6 +184,10 @@ int main(int argc, char** argv) {
     check(ctx, fmd_system_create_rigid(ctx, &p, N, natom, mol.coords.data(), mol.I0, mol.Mmol, RMCUT, 80, pos.data(),
                                        vel.data(), qv.data(), omg.data(), h, &npt, &sys),
           "system set-up");
+    // --physics=<fmd_physics bits>: opt-in force-field corrections, no
+    // reference counterpart (not in the help text, which is the reference's)
+    const int physics = std::atoi(gopt(opts, "physics", "0").c_str());
+    if (physics) check(ctx, fmd_system_set_physics(sys, physics), "physics corrections");
     check(ctx, fmd_system_init(sys), "initial lists and forces");   // LJ:813-828
 
     Schedule sc;

@@ -174,6 +174,10 @@ int main(int argc, char** argv) {
     check(ctx, fmd_system_create_mm(ctx, &p, Na, pos.data(), vel.data(), ft.mol_id.data(), &tv, charge.data(), h,
                                     &npt, &sys),
           "system set-up");
+    // --physics=<fmd_physics bits>: opt-in force-field corrections, no
+    // reference counterpart (not in the help text, which is the reference's)
+    const int physics = std::atoi(gopt(opts, "physics", "0").c_str());
+    if (physics) check(ctx, fmd_system_set_physics(sys, physics), "physics corrections");
     check(ctx, fmd_system_init(sys), "initial lists and forces");   // MM:1152-1172
 
     Schedule sc;

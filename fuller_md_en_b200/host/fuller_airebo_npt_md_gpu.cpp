@@ -172,6 +172,10 @@ int main(int argc, char** argv) {
     fmd_system* sys = nullptr;
     check(ctx, fmd_system_create_airebo(ctx, &p, Na, pos.data(), vel.data(), mass.data(), mol_id.data(), h, &npt, &sys),
           "system set-up");
+    // --physics=<fmd_physics bits>: opt-in force-field corrections, no
+    // reference counterpart (not in the help text, which is the reference's)
+    const int physics = std::atoi(gopt(opts, "physics", "0").c_str());
+    if (physics) check(ctx, fmd_system_set_physics(sys, physics), "physics corrections");
     check(ctx, fmd_system_init(sys), "initial lists and forces");   // AI:830-853
 
     Schedule sc;
