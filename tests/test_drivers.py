@@ -352,3 +352,23 @@ def test_abort_and_stop_control(prog, work):
     ma = [ln for ln in a.stdout.splitlines() if "***" in ln]
     assert len(mb) == 2 and ma == mb
     assert_rows_match(monitor_rows(a.stdout), monitor_rows(b.stdout))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prog,bits,wrong", [("ai", 2, 1), ("mm", 1, 4), ("lj", 4, 2)])
+def test_physics_option(prog, bits, wrong, work):
+    """--physics=<bits> (no reference counterpart): the run changes, the
+    reference's options and output format do not; a bit the program's force
+    field lacks is refused."""
+    args = ["--cell=1", "--step=40", "--mon=20", f"--libdir={work['lib']}"]
+    a = run(ours(prog), args, work["ours"])
+    (work["ours"] / "p").mkdir()
+    b = run(ours(prog), args + [f"--physics={bits}"], work["ours"] / "p")
+    assert a.returncode == 0 and b.returncode == 0, a.stderr + b.stderr
+    ra, rb = monitor_rows(a.stdout), monitor_rows(b.stdout)
+    assert len(ra) == len(rb) >= 2
+    assert [len(r) for r in ra] == [len(r) for r in rb]
+    assert [r[:-1] for r in ra] != [r[:-1] for r in rb]      # all but the elapsed time
+    (work["ours"] / "w").mkdir()
+    c = run(ours(prog), args + [f"--physics={wrong}"], work["ours"] / "w")
+    assert c.returncode != 0
