@@ -8,8 +8,10 @@
 // atoms of the higher-numbered neighbour molecules in ascending order: the row
 // comes out sorted without a bitmap, its first `cap` entries are the
 // reference's truncation, and the candidates of one molecule are contiguous
-// in memory (coalesced loads).  The LJ gather's full rows are the transpose of
-// these rows (nlist_transpose, nlist.cu), whichever builder made them.
+// in memory (coalesced loads).  The LJ gather's full rows (incoming entries,
+// then the row) come from the walk's candidate bitmap when every molecule has
+// 32-64 atoms (k_mol_incoming), else from the transpose of the half rows
+// (nlist_transpose, nlist.cu), as they do after a cell-grid build.
 // Intramolecular (REBO) rows walk the atom's own molecule.
 //
 // Candidate molecules: a centre c and radius R per molecule, and molecule
@@ -362,9 +364,9 @@ __device__ __forceinline__ int lower_bound_part(const int* pa, int n, int key) {
     return lo;
 }
 
-// For each lower partner A = part[B][q] (A < B): rev[B][q] = the position of
-// B among the higher partners of A, i.e. the index of B's atoms (times the
-// molecule size) in the candidate sequence of A's atoms.  One warp per
+// For each lower partner A = part[B][q] (A < B): rev[B][q] = the position p
+// of B among the higher partners of A, whose kept-entry ballots are words
+// 2 p and 2 p + 1 of each A atom's candidate bitmap.  One warp per
 // molecule, binary searches per lane.  The lists are ascending, and symmetric
 // (the pair test is odd in the centre difference and symmetric in the radii);
 // should B be missing all the same, the molecule builder is switched off for
