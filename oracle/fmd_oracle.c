@@ -7,7 +7,9 @@
  *
  * Parity pin: tests/test_oracle_golden.py checks every function here against
  * fixtures recorded from the unmodified reference (oracle/_ref, built by
- * oracle/Makefile from the reference sources).
+ * oracle/Makefile from the reference sources) -- except fmo_rebo_grad, which
+ * is not the reference's arithmetic (the gradient of its REBO energy, for the
+ * opt-in physics tests) and is checked by finite differences instead.
  *
  * Build: gcc -std=c99 -O2 -ffp-contract=off (no FMA contraction), so that the
  * distance tests round exactly like the reference built by g++ -O3 on x86-64.
@@ -399,6 +401,80 @@ double fmo_rebo(double *F, double *vir9, const double *pos, const double *h, con
                           ux, uy, uz, gij, fcut, va);
             bo_three_body(F, pos, h, hi, cnt, list, max_neigh, j, i, -dx, -dy, -dz, rij,
                           -ux, -uy, -uz, gji, fcut, va);
+        }
+    }
+    return Ep;
+}
+
+/* NOT a restatement of the reference: the gradient of fmo_rebo's energy (the
+ * forces of the FMD_PHYS_REBO option).  The reference's three-body force on a
+ * neighbour k of centre c is +coeff dG/dr_k; the gradient's is -coeff dG/dr_k,
+ * and the bond partner b gets -coeff dG/dr_b = -coeff sum_k fc_k g'(cos)
+ * (u_k - cos u_b) / r_b.  Checked by finite differences of fmo_rebo's energy
+ * (tests/test_force_gradients.py), not against the reference. */
+static void bo_three_body_grad(double *F, const double *pos, const double *h, const double *hi,
+                               const int *cnt, const int *list, int max_neigh, int c, int b,
+                               double bx, double by, double bz, double rb,
+                               double ux, double uy, double uz, double gs, double fcut, double va)
+{
+    if (!(fabs(gs) > 1e-20 && va > 1e-20)) return;
+    double coeff = 0.5 * fcut * va * BO_DELTA * pow(1.0 + gs, -BO_DELTA - 1.0);   /* dE/dG */
+    double fb[3] = {0.0, 0.0, 0.0};
+    for (int kn = 0; kn < cnt[c]; kn++) {
+        int k = list[c * max_neigh + kn];
+        if (k == b) continue;
+        double kx = pos[3 * k] - pos[3 * c], ky = pos[3 * k + 1] - pos[3 * c + 1],
+               kz = pos[3 * k + 2] - pos[3 * c + 2];
+        fmo_mimg(&kx, &ky, &kz, hi, h);
+        double rk = sqrt(kx * kx + ky * ky + kz * kz);
+        if (rk > DMAX_CC) continue;
+        double fck = sw_fc(rk);
+        if (fck < 1e-15) continue;
+        double dfck = sw_dfc(rk), rki = 1.0 / rk;
+        double rkv[3] = {kx * rki, ky * rki, kz * rki}, uv[3] = {ux, uy, uz};
+        double ct = clamp1((bx * kx + by * ky + bz * kz) / (rb * rk));
+        double gv = ang_g(ct), dgv = ang_dg(ct);
+        for (int a = 0; a < 3; a++) {
+            double fk = -coeff * (dfck * gv * rkv[a] + fck * dgv * (uv[a] - ct * rkv[a]) * rki);
+            F[3 * k + a] += fk;
+            F[3 * c + a] -= fk;
+            fb[a] += -coeff * fck * dgv * (rkv[a] - ct * uv[a]) / rb;
+        }
+    }
+    for (int a = 0; a < 3; a++) {
+        F[3 * b + a] += fb[a];
+        F[3 * c + a] -= fb[a];
+    }
+}
+
+double fmo_rebo_grad(double *F, const double *pos, const double *h, const double *hi,
+                     const int *cnt, const int *list, int max_neigh, int na)
+{
+    double Ep = 0;
+    for (int i = 0; i < na; i++) {
+        for (int jn = 0; jn < cnt[i]; jn++) {
+            int j = list[i * max_neigh + jn];
+            if (j <= i) continue;
+            double dx = pos[3 * j] - pos[3 * i], dy = pos[3 * j + 1] - pos[3 * i + 1],
+                   dz = pos[3 * j + 2] - pos[3 * i + 2];
+            fmo_mimg(&dx, &dy, &dz, hi, h);
+            double rij = sqrt(dx * dx + dy * dy + dz * dz);
+            if (rij > DMAX_CC) continue;
+            double fcut = sw_fc(rij), dfcut = sw_dfc(rij);
+            if (fcut < 1e-15 && dfcut == 0) continue;
+            double vr = rep_v(rij), dvr = rep_dv(rij), va = att_v(rij), dva = att_dv(rij);
+            double rinv = 1.0 / rij;
+            double gij = bo_sum(pos, h, hi, cnt, list, max_neigh, i, j, dx, dy, dz, rij);
+            double gji = bo_sum(pos, h, hi, cnt, list, max_neigh, j, i, -dx, -dy, -dz, rij);
+            double bbar = 0.5 * (pow(1.0 + gij, -BO_DELTA) + pow(1.0 + gji, -BO_DELTA));
+            Ep += fcut * (vr - bbar * va);
+            double fpair = (dfcut * (vr - bbar * va) + fcut * (dvr - bbar * dva)) * rinv;
+            F[3 * i] += fpair * dx; F[3 * i + 1] += fpair * dy; F[3 * i + 2] += fpair * dz;
+            F[3 * j] -= fpair * dx; F[3 * j + 1] -= fpair * dy; F[3 * j + 2] -= fpair * dz;
+            bo_three_body_grad(F, pos, h, hi, cnt, list, max_neigh, i, j, dx, dy, dz, rij,
+                               dx * rinv, dy * rinv, dz * rinv, gij, fcut, va);
+            bo_three_body_grad(F, pos, h, hi, cnt, list, max_neigh, j, i, -dx, -dy, -dz, rij,
+                               -dx * rinv, -dy * rinv, -dz * rinv, gji, fcut, va);
         }
     }
     return Ep;

@@ -58,6 +58,10 @@ double fmo_rigid_forces(double *F, double *T, double *W9,
 /* ---- a7-a9: simplified AIREBO (AI:275-495) ---- */
 double fmo_rebo(double *F, double *vir9, const double *pos, const double *h, const double *hi,
                 const int *cnt, const int *list, int max_neigh, int na);
+/* Not the reference: fmo_rebo's energy with forces -grad E (its three-body
+ * forces replaced by the bond-order gradient); adds into F, returns E. */
+double fmo_rebo_grad(double *F, const double *pos, const double *h, const double *hi,
+                     const int *cnt, const int *list, int max_neigh, int na);
 /* Half-list shifted LJ.  full_virial=1: 9 components (AI:465-472);
  * full_virial=0: diagonal only (MM:751-763). */
 typedef struct { double sig2, eps, rc2, vshift; int full_virial; } fmo_lj_params;

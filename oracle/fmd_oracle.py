@@ -119,6 +119,8 @@ class Oracle:
         L.fmo_rigid_forces.argtypes = [_dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _ip, _ip, c_int, c_int, c_int,
                                        c_double, _dp]
         L.fmo_rebo.argtypes = [_dp, _dp, _dp, _dp, _dp, _ip, _ip, c_int, c_int]
+        L.fmo_rebo_grad.argtypes = [_dp, _dp, _dp, _dp, _ip, _ip, c_int, c_int]
+        L.fmo_rebo_grad.restype = c_double
         L.fmo_lj_half.argtypes = [_dp, _dp, _dp, _dp, _dp, _ip, _ip, c_int, c_int, POINTER(LJParams)]
         L.fmo_airebo_forces.argtypes = [_dp, _dp, _dp, _dp, _dp, _ip, _ip, _ip, _ip, c_int, _dp]
         L.fmo_mm_forces.argtypes = [_dp, _dp, _dp, _dp, _dp, POINTER(MMTopo), _ip, _ip, _dp, _ip, c_int, c_int, _dp]
@@ -180,6 +182,13 @@ class Oracle:
         F = np.zeros(3 * na); W = np.zeros(9); E = np.zeros(3)
         self.L.fmo_airebo_forces(d(F), d(W), d(pos), d(h), d(hi), i(cr), i(lr), i(cl), i(ll), na, d(E))
         return E, F, W
+
+    def rebo_grad(self, pos, h, hi, cr, lr, na, max_neigh=12):
+        """Not the reference: the REBO energy with forces -grad E (the
+        FMD_PHYS_REBO option's forces).  Returns (E, F)."""
+        F = np.zeros(3 * na)
+        E = self.L.fmo_rebo_grad(d(F), d(pos), d(h), d(hi), i(cr), i(lr), max_neigh, na)
+        return E, F
 
     def mm_topology_mol(self, coords, bonds):
         coords = np.ascontiguousarray(coords, np.float64).reshape(-1)
