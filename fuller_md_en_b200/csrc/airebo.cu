@@ -221,35 +221,6 @@ __device__ __forceinline__ double bo_sum_sl(const Slot* __restrict__ sl, int cap
     return gs;
 }
 
-// Reference three-body forces on the neighbours of centre c (AI:361-419).
-__device__ __forceinline__ void bo_three_body_sl(double* __restrict__ F, const Slot* __restrict__ sl,
-                                                 const int* __restrict__ list, int cap, int c, int m, int skip,
-                                                 double bx, double by, double bz, double rbinv, double ux,
-                                                 double uy, double uz, double gs, double b, double fcut, double va) {
-    if (!(fabs(gs) > 1e-20 && va > 1e-20)) return;
-    const double dbp = -BO_DELTA * b / (1.0 + gs);
-    const double coeff = -(0.5 * fcut * va) * dbp;
-    double fcx = 0.0, fcy = 0.0, fcz = 0.0;
-    for (int kn = 0; kn < m; kn++) {
-        const size_t o = (size_t)c * cap + kn;
-        const int k = list[o];
-        if (k == skip) continue;
-        const Slot q = sl[o];
-        if (q.fc < 1e-15) continue;
-        const double rx = q.dx * q.rinv, ry = q.dy * q.rinv, rz = q.dz * q.rinv;
-        const double ct = clamp1((bx * q.dx + by * q.dy + bz * q.dz) * (rbinv * q.rinv));
-        double gv, dgv;
-        ang_g_dg(ct, gv, dgv);
-        const double a1 = coeff * q.dfc * gv, a2 = coeff * q.fc * dgv;
-        const double fx = a1 * rx + a2 * ((ux - ct * rx) * q.rinv);
-        const double fy = a1 * ry + a2 * ((uy - ct * ry) * q.rinv);
-        const double fz = a1 * rz + a2 * ((uz - ct * rz) * q.rinv);
-        atomic_add3(F, k, fx, fy, fz);
-        fcx -= fx; fcy -= fy; fcz -= fz;
-    }
-    atomic_add3(F, c, fcx, fcy, fcz);
-}
-
 // Bond order of every directed slot c -> j (AI:301-323 for centre c):
 // g = sum over c's other slots of f_c G(cos), b = (1 + g)^-1/2, the pair
 // functions of r_cj (AI:173-183) and the three-body coefficient
