@@ -132,25 +132,26 @@ int fmd_rebo_forces(fmd_ctx *ctx, const double *pos, const double *h, const doub
                     const int *nlc, const int *nll, int max_neigh, int na,
                     double *F, double *vir9, double *E);
 /* No counterpart in the reference.  The REBO force of fmd_rebo_forces for
- * callers that cannot allocate device memory: code inside a CUDA-graph
- * capture owned by a framework, programs whose memory pool forbids side
- * allocations, drivers that must not touch the allocator after start-up.
- * It needs no fmd_ctx and calls no cudaMalloc/cudaFree or any allocating
- * routine.  All arrays are DEVICE pointers except h and hi (9 doubles each,
- * host): d_pos[3*na], the REBO list d_nlc[na], d_nll[na*max_neigh] (entries
- * must be valid atom indices, as fmd_nlist_rebo produces them); d_F[3*na]
- * and d_vir9[9] are ADDED into like compute_rebo (AI:275-421) does; *d_E
- * receives the REBO energy.  Work is enqueued on `stream` (a cudaStream_t,
- * NULL = default stream) and the call returns without synchronising.
- * Scratch is a fixed file-scope device array (82 KB on every GPU that loads
- * the library, held until exit) for the cell matrix and one partial record
- * per 128 atoms: na is limited to 131,072; larger na returns
- * FMD_ERR_CAPACITY and does nothing.  Every call shares that array and it
- * keeps the last call's contents (each call rewrites all it reads), so calls
- * that overlap on the GPU -- on different streams, or from several host
- * threads -- race and must be serialised by the caller.  The first call on
- * a device looks up the array's device address; make that first call before
- * any stream capture. */
+ * callers that cannot allocate device memory: programs whose memory pool or
+ * allocator owns all device memory and forbids side allocations, and drivers
+ * that must not touch the allocator after start-up.  It needs no fmd_ctx and
+ * calls no cudaMalloc/cudaFree or any allocating routine.  All arrays are
+ * DEVICE pointers except h and hi (9 doubles each, host, read during the
+ * call and passed to the GPU by value): d_pos[3*na], the REBO list
+ * d_nlc[na], d_nll[na*max_neigh] (entries must be valid atom indices, as
+ * fmd_nlist_rebo produces them); d_F[3*na] and d_vir9[9] are ADDED into like
+ * compute_rebo (AI:275-421) does; *d_E receives the REBO energy.  The device
+ * is the one holding d_pos; the caller's current device is unchanged on
+ * return.  Work is enqueued on `stream` (a cudaStream_t, NULL = default
+ * stream) and the call returns without synchronising.  Scratch is a fixed
+ * file-scope device array (82 KB on every GPU that loads the library, held
+ * until exit) for the cell matrix and 1,024 partial {E, W} records: na is
+ * limited to 131,072; larger na returns FMD_ERR_CAPACITY and does nothing.
+ * Every call shares that array and it keeps the last call's contents (each
+ * call rewrites all it reads), so calls that overlap on the GPU -- on
+ * different streams, or from several host threads -- race and must be
+ * serialised by the caller.  The first call on a device looks up the
+ * array's device address; make that first call before any stream capture. */
 int fmd_rebo_forces_noalloc(const double *d_pos, const double *h, const double *hi,
                             const int *d_nlc, const int *d_nll, int max_neigh, int na,
                             double *d_F, double *d_vir9, double *d_E, void *stream);
@@ -289,7 +290,9 @@ int fmd_system_kernel_ms(fmd_system *s, int stage, int reps, double *ms_per_laun
 /* Launch shape of the atomistic LJ gather that fmd_system_init's autotuner
  * chose (threads per block 128/256, list entries in flight per lane 2/4,
  * row feed 0 loads as used / 1 software-pipelined / 2 rows staged in shared
- * memory by bulk asynchronous copies, grid blocks); any pointer may be NULL.
+ * memory by bulk asynchronous copies, plus 4 when each block walks its own
+ * contiguous run of atoms instead of atoms strided over the grid; grid
+ * blocks); any pointer may be NULL.
  * fmd_system_set_lj_shape pins a shape (for reproducible runs; results then
  * do not depend on timing), after fmd_system_init. */
 int fmd_system_lj_shape(fmd_system *s, int *threads, int *unroll, int *pipelined, int *blocks);
