@@ -132,7 +132,6 @@ _SIGS = {
     "fmd_system_lj_full_rows": (c_int, [c_void_p, c_void_p, c_void_p, POINTER(c_int)]),
     "fmd_system_set_physics": (c_int, [c_void_p, c_int]),
     "fmd_system_lj_prune": (c_int, [c_void_p, POINTER(c_double), POINTER(c_longlong), POINTER(c_longlong)]),
-    "fmd_umma_selftest": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, POINTER(c_float)]),
     "fmd_sg_nparams": (c_int, []),
     "fmd_sg_create": (c_int, [c_void_p, _dp, POINTER(c_void_p)]),
     "fmd_sg_set_params": (c_int, [c_void_p, _dp]),

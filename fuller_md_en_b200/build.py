@@ -31,7 +31,7 @@ NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-r
 # Per-file extra flags: the integrator's scalar arithmetic rounds like the
 # reference's host code (no FMA contraction).
 EXTRA = {"step.cu": ["-fmad=false"]}
-CUDA_SOURCES = ["nlist.cu", "airebo.cu", "rigid.cu", "mm.cu", "step.cu", "system.cu", "abi.cu", "noalloc.cu", "umma_selftest.cu", "surrogate.cu",
+CUDA_SOURCES = ["nlist.cu", "airebo.cu", "rigid.cu", "mm.cu", "step.cu", "system.cu", "abi.cu", "noalloc.cu", "surrogate.cu",
                 "sg_train.cu", "sg_abi.cu", "sg_step.cu", "batch.cu", "molnlist.cu", "ljprune.cu"]
 
 DRIVERS = ["fuller_LJ_core_gpu", "fuller_LJ_npt_md_gpu", "fuller_LJ_npt_mmmd_gpu", "fuller_airebo_npt_md_gpu"]
@@ -114,9 +114,25 @@ def build_oracle(verbose: bool = False) -> None:
         print("built oracle")
 
 
+def build_tests(verbose: bool = False) -> None:
+    """Test-only CUDA code (tests/cuda/), into tests/_build/: the tensor-core
+    operand self test, which is not part of the product library."""
+    src = ROOT / "tests" / "cuda" / "umma_selftest.cu"
+    if not src.exists():
+        return
+    out_dir = ROOT / "tests" / "_build"
+    out_dir.mkdir(exist_ok=True)
+    out = out_dir / "libfmd_umma_selftest.so"
+    if _stale(out, [src, CSRC / "umma.cuh"]):
+        _run([nvcc(), *ARCH, *NVCC_FLAGS, "-I", str(CSRC), "-shared", "-cudart", "static", "-o", str(out), str(src)])
+    if verbose:
+        print(f"built {out}")
+
+
 def build_all(verbose: bool = False) -> None:
     build_cuda(verbose)
     build_host(verbose)
+    build_tests(verbose)
     build_oracle(verbose)
 
 

@@ -350,12 +350,6 @@ int fmd_batch_get_tuning(fmd_batch *b, fmd_batch_tuning *t);
 int fmd_batch_step_kernels(fmd_batch *b, int rebuild, int phase, int *nkernels);
 int fmd_batch_destroy(fmd_batch *b);
 
-/* Tensor-core self test (no reference counterpart): D = A * Bt^T for one
- * 128 x N x K BF16 tile through tcgen05.mma, FP32 result.  A is 128 x K and
- * Bt is N x K, row-major bf16 bit patterns; mode bit 0 reads A MN-major and
- * bit 1 reads B MN-major from shared memory (the operand orientations of the
- * learned-potential kernels).  K, N multiples of 16 in [16, 256]. */
-int fmd_umma_selftest(fmd_ctx *ctx, const uint16_t *A, const uint16_t *Bt, int K, int N, int mode, float *D);
 
 /* ------------------------------------------- learned bond-order potential --
  * No counterpart in the reference.  A network stands in for the bond order

@@ -1,11 +1,12 @@
-// umma_selftest.cu -- one 128 x N x K BF16 GEMM through tcgen05.mma with the
-// operands in each major-ness the learned-potential kernels use.  Exposed as
-// fmd_umma_selftest so the tests pin the descriptor conventions of umma.cuh
-// (K-major and MN-major views of the interleaved layout) against a CPU
-// product before any kernel depends on them.
+// umma_selftest.cu -- TEST ONLY (built by fuller_md_en_b200/build.py into
+// tests/_build/, never into the product library): one 128 x N x K BF16 GEMM
+// through tcgen05.mma with the operands in each major-ness the learned-
+// potential kernels use, so tests/test_sg_umma.py pins the descriptor
+// conventions of the package's umma.cuh (K-major and MN-major views of the
+// interleaved layout) against a CPU product.
 #include <cuda_runtime.h>
+#include <stdint.h>
 
-#include "fmd_internal.h"
 #include "umma.cuh"
 
 namespace fmd {
@@ -75,16 +76,19 @@ __global__ void __launch_bounds__(128) k_umma_selftest(const uint16_t* __restric
 }  // namespace
 }  // namespace fmd
 
-extern "C" int fmd_umma_selftest(fmd_ctx* ctx, const uint16_t* A, const uint16_t* Bt, int K, int N, int mode,
-                                 float* D) {
+// D = A * Bt^T on the current device: A is 128 x K and Bt is N x K,
+// row-major bf16 bit patterns; mode bit 0 reads A MN-major and bit 1 reads B
+// MN-major from shared memory.  K, N multiples of 16 in [16, 256].
+// Returns 0 on success, 1 for bad arguments, 2 for a CUDA error, 3 when the
+// kernel's bounded wait for the MMA's completion ran out.
+extern "C" int fmd_umma_selftest(const uint16_t* A, const uint16_t* Bt, int K, int N, int mode, float* D) {
     using namespace fmd;
-    if (!ctx || !A || !Bt || !D) return FMD_ERR_ARG;
-    if (K < 16 || K > 256 || K % 16 || N < 16 || N > 256 || N % 16 || mode < 0 || mode > 3)
-        return ctx->fail(FMD_ERR_ARG, "fmd_umma_selftest: K, N must be multiples of 16 in [16, 256]");
+    if (!A || !Bt || !D || K < 16 || K > 256 || K % 16 || N < 16 || N > 256 || N % 16 || mode < 0 || mode > 3)
+        return 1;
     uint16_t *dA = nullptr, *dB = nullptr;
     float* dD = nullptr;
     int* dErr = nullptr;
-    int rc = FMD_OK, herr = 0;
+    int herr = 0;
     const size_t smem = (size_t)(128 + N) * K * 2;
     auto cleanup = [&]() {
         cudaFree(dA); cudaFree(dB); cudaFree(dD); cudaFree(dErr);
@@ -92,17 +96,17 @@ extern "C" int fmd_umma_selftest(fmd_ctx* ctx, const uint16_t* A, const uint16_t
     if (cudaMalloc(&dA, 128 * (size_t)K * 2) != cudaSuccess || cudaMalloc(&dB, (size_t)N * K * 2) != cudaSuccess ||
         cudaMalloc(&dD, 128 * (size_t)N * 4) != cudaSuccess || cudaMalloc(&dErr, sizeof(int)) != cudaSuccess) {
         cleanup();
-        return ctx->fail(FMD_ERR_CUDA, "fmd_umma_selftest: allocation failed");
+        return 2;
     }
-    cudaMemcpyAsync(dA, A, 128 * (size_t)K * 2, cudaMemcpyHostToDevice, ctx->stream);
-    cudaMemcpyAsync(dB, Bt, (size_t)N * K * 2, cudaMemcpyHostToDevice, ctx->stream);
-    cudaMemsetAsync(dErr, 0, sizeof(int), ctx->stream);
+    cudaMemcpy(dA, A, 128 * (size_t)K * 2, cudaMemcpyHostToDevice);
+    cudaMemcpy(dB, Bt, (size_t)N * K * 2, cudaMemcpyHostToDevice);
+    cudaMemset(dErr, 0, sizeof(int));
     cudaFuncSetAttribute(k_umma_selftest, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_umma_selftest<<<1, 128, smem, ctx->stream>>>(dA, dB, K, N, mode, dD, dErr);
-    cudaMemcpyAsync(D, dD, 128 * (size_t)N * 4, cudaMemcpyDeviceToHost, ctx->stream);
-    cudaMemcpyAsync(&herr, dErr, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
-    rc = ctx->sync_check("fmd_umma_selftest");
+    k_umma_selftest<<<1, 128, smem>>>(dA, dB, K, N, mode, dD, dErr);
+    cudaMemcpy(D, dD, 128 * (size_t)N * 4, cudaMemcpyDeviceToHost);
+    cudaMemcpy(&herr, dErr, sizeof(int), cudaMemcpyDeviceToHost);
+    const cudaError_t e = cudaDeviceSynchronize();
     cleanup();
-    if (rc == FMD_OK && herr) rc = ctx->fail(FMD_ERR_CUDA, "fmd_umma_selftest: MMA completion wait timed out");
-    return rc;
+    if (e != cudaSuccess) return 2;
+    return herr ? 3 : 0;
 }
