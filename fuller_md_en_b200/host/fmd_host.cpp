@@ -588,6 +588,50 @@ void OvitoWriter::write(const Frame& f) {
 }
 
 // ------------------------------------------------------------------ restart
+RestartWriter::RestartWriter() { th_ = std::thread([this] { loop(); }); }
+
+RestartWriter::~RestartWriter() {
+    finish();
+    {
+        std::lock_guard<std::mutex> g(mu_);
+        stop_ = true;
+    }
+    cv_.notify_all();
+    th_.join();
+}
+
+void RestartWriter::submit(std::function<void()> job) {
+    std::unique_lock<std::mutex> g(mu_);
+    cv_.wait(g, [this] { return inflight_ < kSlots; });
+    queue_.push_back(std::move(job));
+    inflight_++;
+    cv_.notify_all();
+}
+
+void RestartWriter::finish() {
+    std::unique_lock<std::mutex> g(mu_);
+    cv_.wait(g, [this] { return inflight_ == 0; });
+}
+
+void RestartWriter::loop() {
+    for (;;) {
+        std::function<void()> job;
+        {
+            std::unique_lock<std::mutex> g(mu_);
+            cv_.wait(g, [this] { return stop_ || !queue_.empty(); });
+            if (queue_.empty()) return;
+            job = std::move(queue_.front());
+            queue_.pop_front();
+        }
+        job();
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            inflight_--;
+        }
+        cv_.notify_all();
+    }
+}
+
 namespace {
 void header(FILE* f, const char* prog, const Opts& o, const RunInfo& r, int istep) {
     fprintf(f, "# RESTART %s\n# OPTIONS:", prog);

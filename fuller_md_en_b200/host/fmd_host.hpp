@@ -10,6 +10,7 @@
 #include <condition_variable>
 #include <cstdio>
 #include <deque>
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -108,6 +109,32 @@ private:
     std::mutex mu_;
     std::condition_variable cv_;
     std::deque<std::unique_ptr<Frame>> queue_;
+    int inflight_ = 0;
+    bool stop_ = false;
+    std::thread th_;
+};
+
+// Background restart saves: submit() hands a write job (a callable that owns
+// copies of the checkpoint's state and calls write_restart_*) to a writer
+// thread and returns, so the step loop goes on while the file is formatted.
+// Jobs run one at a time in submission order; at most two are pending, a
+// third submit() waits for the oldest.  finish() (and the destructor) wait
+// for every job.  The bytes are those of the synchronous call the job makes.
+class RestartWriter {
+public:
+    RestartWriter();
+    ~RestartWriter();
+    RestartWriter(const RestartWriter&) = delete;
+    RestartWriter& operator=(const RestartWriter&) = delete;
+    void submit(std::function<void()> job);
+    void finish();
+
+private:
+    static constexpr int kSlots = 2;
+    void loop();
+    std::mutex mu_;
+    std::condition_variable cv_;
+    std::deque<std::function<void()>> queue_;
     int inflight_ = 0;
     bool stop_ = false;
     std::thread th_;

@@ -205,10 +205,15 @@ int main(int argc, char** argv) {
     RunInfo ri;
     ri.st = st; ri.fspec = fspec; ri.nc = nc; ri.nsteps = nsteps; ri.seed = seed;
     ri.T = T; ri.Pe = Pe; ri.dt = dt; ri.init_scale = init_scale;
+    // checkpoints are formatted and written on a writer thread from copies
+    std::unique_ptr<RestartWriter> rstw(nrec_rst > 0 ? new RestartWriter() : nullptr);
     auto save = [&](int g) {
         check(ctx, fmd_system_download(sys, pos.data(), vel.data(), qv.data(), omg.data(), h, &npt), "download");
-        write_restart_lj(restart_filename(ovito_file, g, total_steps), g, opts, ri, h, npt, pos.data(), qv.data(),
-                         vel.data(), omg.data(), N, natom);
+        // h (a C array) and the vectors are captured by copy
+        rstw->submit([fn = restart_filename(ovito_file, g, total_steps), g, opts, ri, h, npt, p = pos, q = qv, v = vel,
+                      w = omg, N, natom]() {
+            write_restart_lj(fn, g, opts, ri, h, npt, p.data(), q.data(), v.data(), w.data(), N, natom);
+        });
     };
     bool stop_requested = false;
     for (int g = start_step + 1; g <= total_steps;) {
@@ -243,6 +248,7 @@ int main(int argc, char** argv) {
         g = e + 1;
     }
     ovito.reset();                          // every frame written
+    rstw.reset();                           // every checkpoint written
     if (io_o) fclose(io_o);
     fmd_avg av;
     check(ctx, fmd_system_averages(sys, &av), "averages");

@@ -195,10 +195,15 @@ int main(int argc, char** argv) {
     RunInfo ri;
     ri.st = st; ri.fspec = fspec; ri.nc = nc; ri.nsteps = nsteps; ri.seed = seed;
     ri.T = T; ri.Pe = Pe; ri.dt = dt; ri.init_scale = init_scale;
+    // checkpoints are formatted and written on a writer thread from copies
+    std::unique_ptr<RestartWriter> rstw(nrec_rst > 0 ? new RestartWriter() : nullptr);
     auto save = [&](int s) {
         check(ctx, fmd_system_download(sys, pos.data(), vel.data(), nullptr, nullptr, h, &npt), "download");
-        write_restart_airebo(restart_filename(rst_base, s, total_steps), s, opts, ri, h, npt, pos.data(), vel.data(),
-                             mol_id.data(), mass.data(), Na, Nmol, mol.natom);
+        // h (a C array) and the vectors are captured by copy
+        rstw->submit([fn = restart_filename(rst_base, s, total_steps), s, opts, ri, h, npt, p = pos, v = vel,
+                      mid = mol_id, m = mass, Na, Nmol, natom = mol.natom]() {
+            write_restart_airebo(fn, s, opts, ri, h, npt, p.data(), v.data(), mid.data(), m.data(), Na, Nmol, natom);
+        });
     };
     bool stop_requested = false;
     for (int gs = start_step + 1; gs <= total_steps;) {
@@ -233,6 +238,7 @@ int main(int argc, char** argv) {
         gs = e + 1;
     }
     ovito.reset();                          // every frame written
+    rstw.reset();                           // every checkpoint written
     if (io_o) fclose(io_o);
     fmd_avg av;
     check(ctx, fmd_system_averages(sys, &av), "averages");

@@ -1,7 +1,9 @@
-"""The drivers' asynchronous OVITO writer (fmdh::OvitoWriter: frames copied,
-formatted in parallel chunks on a writer thread, appended in order) writes
-exactly the bytes of the synchronous formatter, for atomistic and rigid
-frames, with one and with several formatting threads."""
+"""The drivers' asynchronous output: the OVITO writer (fmdh::OvitoWriter:
+frames copied, formatted in parallel chunks on a writer thread, appended in
+order) writes exactly the bytes of the synchronous formatter, for atomistic
+and rigid frames, with one and with several formatting threads; restart
+saves run as jobs on a writer thread (fmdh::RestartWriter) and write exactly
+the synchronous writers' files for all three programs."""
 from __future__ import annotations
 
 import subprocess
@@ -34,3 +36,21 @@ def test_async_writer_matches_sync_formatter(checker, tmp_path, threads):
     da, db = a.read_bytes(), b.read_bytes()
     assert len(da) > 10_000_000 and da == db
     assert da.count(b"Lattice=") == 11
+
+
+def test_restart_writer_matches_sync_writer(tmp_path):
+    exe = tmp_path / "restart_writer_check"
+    r = subprocess.run(["g++", "-std=c++17", "-O2", "-pthread", "-I", str(HOST), "-I", str(ROOT / "include"),
+                        "-o", str(exe), str(ROOT / "tests" / "cpp" / "restart_writer_check.cpp"), f"-L{LIB}",
+                        "-lfullermd_host", f"-Wl,-rpath,{LIB}"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    a, b = tmp_path / "sync", tmp_path / "async"
+    a.mkdir()
+    b.mkdir()
+    r = subprocess.run([str(exe), str(a), str(b)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    names = sorted(p.name for p in a.iterdir())
+    assert len(names) == 12 and names == sorted(p.name for p in b.iterdir())
+    for nm in names:
+        assert (a / nm).read_bytes() == (b / nm).read_bytes(), nm
+    assert (a / "c40_ai.rst").read_bytes() != (a / "c30_ai.rst").read_bytes()
