@@ -116,23 +116,34 @@ int fmo_nlist_sym(const double *pos, const double *h, const double *hi, int n,
 }
 
 /* AI:263-272, MM:337-346: intermolecular half list, j>i ascending, first
- * max_neigh kept, the rest dropped silently in the reference. */
-int fmo_nlist_half(const double *pos, const double *h, const double *hi, int na,
-                   const int *mol_id, double rc_list, int max_neigh, int *cnt, int *list)
+ * max_neigh kept, the rest dropped silently in the reference.  Row i depends
+ * only on atom i and the atoms after it, so rows [i0, i1) can be built on
+ * their own (the large-system tests split the rows over host threads). */
+int fmo_nlist_half_rows(const double *pos, const double *h, const double *hi, int na,
+                        const int *mol_id, double rc_list, int max_neigh, int i0, int i1,
+                        int *cnt, int *list)
 {
     double rc2 = rc_list * rc_list;
     int dropped = 0;
-    for (int i = 0; i < na; i++) cnt[i] = 0;
-    for (int i = 0; i < na - 1; i++) {
+    if (i1 > na - 1) i1 = na - 1;
+    for (int i = i0; i < i1; i++) {
         int mi = mol_id[i];
+        cnt[i] = 0;
         for (int j = i + 1; j < na; j++) {
             if (mol_id[j] == mi) continue;
             if (pair_r2(pos, i, j, h, hi) < rc2) {
-                if (cnt[i] < max_neigh) list[i * max_neigh + cnt[i]++] = j; else dropped++;
+                if (cnt[i] < max_neigh) list[(size_t)i * max_neigh + cnt[i]++] = j; else dropped++;
             }
         }
     }
     return dropped;
+}
+
+int fmo_nlist_half(const double *pos, const double *h, const double *hi, int na,
+                   const int *mol_id, double rc_list, int max_neigh, int *cnt, int *list)
+{
+    for (int i = 0; i < na; i++) cnt[i] = 0;
+    return fmo_nlist_half_rows(pos, h, hi, na, mol_id, rc_list, max_neigh, 0, na - 1, cnt, list);
 }
 
 /* AI:251-261: intramolecular symmetric list for the bond-order term. */

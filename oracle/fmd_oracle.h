@@ -43,6 +43,9 @@ int fmo_nlist_sym(const double *pos, const double *h, const double *hi, int n,
 int fmo_nlist_half(const double *pos, const double *h, const double *hi, int na,
                    const int *mol_id, double rc_list, int max_neigh,
                    int *cnt, int *list);                                      /* AI:263, MM:337 */
+int fmo_nlist_half_rows(const double *pos, const double *h, const double *hi, int na,
+                        const int *mol_id, double rc_list, int max_neigh, int i0, int i1,
+                        int *cnt, int *list);                                 /* rows [i0, i1) only */
 int fmo_nlist_intra(const double *pos, const double *h, const double *hi, int na,
                     const int *mol_id, double rc, int max_neigh,
                     int *cnt, int *list);                                     /* AI:251 */

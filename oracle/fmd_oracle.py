@@ -116,6 +116,8 @@ class Oracle:
             getattr(L, f).argtypes = [_dp, _dp, _dp, c_int, c_double, c_int, _ip, _ip]
         L.fmo_nlist_half.argtypes = [_dp, _dp, _dp, c_int, _ip, c_double, c_int, _ip, _ip]
         L.fmo_nlist_intra.argtypes = [_dp, _dp, _dp, c_int, _ip, c_double, c_int, _ip, _ip]
+        L.fmo_nlist_half_rows.restype = c_int
+        L.fmo_nlist_half_rows.argtypes = [_dp, _dp, _dp, c_int, _ip, c_double, c_int, c_int, c_int, _ip, _ip]
         L.fmo_rigid_forces.argtypes = [_dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _ip, _ip, c_int, c_int, c_int,
                                        c_double, _dp]
         L.fmo_rebo.argtypes = [_dp, _dp, _dp, _dp, _dp, _ip, _ip, c_int, c_int]
@@ -154,6 +156,22 @@ class Oracle:
         dr = self.L.fmo_nlist_half(d(pos), d(h), d(hi), na, i(np.ascontiguousarray(mol_id, np.int32)), rc, cap,
                                    i(c), i(l))
         return c, l, dr
+
+    def nlist_half_threaded(self, pos, h, hi, na, mol_id, rc, cap=400, threads=None, chunk=2048):
+        """nlist_half with its rows split over host threads (the ctypes
+        calls release the GIL); identical output, for systems where the
+        O(na^2) serial build would take minutes."""
+        import os
+        from concurrent.futures import ThreadPoolExecutor
+        pos = np.ascontiguousarray(pos, np.float64)
+        mol = np.ascontiguousarray(mol_id, np.int32)
+        c = np.zeros(na, np.int32); l = np.zeros(na * cap, np.int32)
+        # rows near the start scan the most partners: interleave chunk sizes
+        spans = [(a, min(a + chunk, na)) for a in range(0, na, chunk)]
+        with ThreadPoolExecutor(max_workers=threads or os.cpu_count() or 1) as ex:
+            drops = list(ex.map(lambda s: self.L.fmo_nlist_half_rows(d(pos), d(h), d(hi), na, i(mol), rc, cap,
+                                                                     s[0], s[1], i(c), i(l)), spans))
+        return c, l, sum(drops)
 
     def nlist_intra(self, pos, h, hi, na, mol_id, rc=2.0 + 0.3, cap=12):
         c = np.zeros(na, np.int32); l = np.zeros(na * cap, np.int32)

@@ -37,6 +37,10 @@ def test_airebo_lists(oracle, golden, nc):
         assert same_rows(rows(cl, ll, 400), csr_rows(g["cnt_lj"], g["csr_lj"]))
     if nc == 2:
         assert dropped > 0 and (cl == 400).any(), "truncation at 400 must be exercised"
+    # the row-split form used for the large-system tests gives the same list
+    tc, tl, tdrop = oracle.nlist_half_threaded(g["pos"], g["h"], g["hi"], na, g["mol_id"], 3.0 * 3.40 + 2.0,
+                                               threads=4, chunk=97)
+    assert np.array_equal(tc, g["cnt_lj"]) and digest(tc, tl, 400) == str(g["digest_lj"]) and tdrop == dropped
 
 
 def _lists(g, na):
