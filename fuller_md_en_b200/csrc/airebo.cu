@@ -621,6 +621,18 @@ __device__ __forceinline__ void lj_atom_done(int i, double fx, double fy, double
     }
 }
 
+// Atoms of warp w of block blk out of nblk blocks of W warps: strided over
+// the system (i = blk W + w, step nblk W), or (contig) block blk's own run of
+// consecutive atoms [blk na / nblk, (blk + 1) na / nblk), warps interleaved.
+struct AtomRange {
+    int first, end, step;
+};
+__device__ __forceinline__ AtomRange atom_range(int blk, int nblk, int W, int w, int na, bool contig) {
+    if (!contig) return AtomRange{blk * W + w, na, nblk * W};
+    const int a0 = (int)((long long)blk * na / nblk), a1 = (int)((long long)(blk + 1) * na / nblk);
+    return AtomRange{a0 + w, a1, W};
+}
+
 // One gather pass over atoms blk, blk + nblk, ... (in warps) of one system;
 // per-block {E, W9} into part[blk].  sm: 32 * kNV doubles, s_hh: 18.
 // Row i of the full list (in_list, stride in_cap, in_cnt[i] entries) is the
@@ -633,7 +645,7 @@ __device__ __forceinline__ void lj_gather_body(const double* __restrict__ pos, c
                                                int in_cap, int na, double* __restrict__ F,
                                                double* __restrict__ Facc, const LJP& p, double* __restrict__ part,
                                                int blk, int nblk, double* sm, double* s_hh,
-                                               const LJPruneOut& po) {
+                                               const LJPruneOut& po, bool contig = false) {
     if (threadIdx.x < 18) s_hh[threadIdx.x] = hh[threadIdx.x];
     __syncthreads();
     const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
@@ -648,7 +660,8 @@ __device__ __forceinline__ void lj_gather_body(const double* __restrict__ pos, c
     double acc[kNV];
 #pragma unroll
     for (int k = 0; k < kNV; k++) acc[k] = 0.0;
-    for (int i = blk * wpb + (threadIdx.x >> 5); i < na; i += nblk * wpb) {
+    const AtomRange ar = atom_range(blk, nblk, wpb, threadIdx.x >> 5, na, contig);
+    for (int i = ar.first; i < ar.end; i += ar.step) {
         const double px = pos[3 * i], py = pos[3 * i + 1], pz = pos[3 * i + 2];
         double fx = 0.0, fy = 0.0, fz = 0.0;
         const int tot = min(in_cnt[i], in_cap);
@@ -699,7 +712,7 @@ template <bool FULL_VIRIAL, bool F32, int U, bool PIPE, int NT>
 __global__ void __launch_bounds__(NT)
 k_lj_gather(const double* __restrict__ pos, const double* __restrict__ hh, const int* __restrict__ in_cnt,
             const int* __restrict__ in_list, int in_cap, int na, double* __restrict__ F,
-            double* __restrict__ Facc, LJP p, double* __restrict__ part, LJPruneOut po, int nrec) {
+            double* __restrict__ Facc, LJP p, double* __restrict__ part, LJPruneOut po, int nrec, int contig) {
     FMD_PDL_WAIT();
     __shared__ double sm[32 * kNV];
     __shared__ double s_hh[18];
@@ -707,7 +720,7 @@ k_lj_gather(const double* __restrict__ pos, const double* __restrict__ hh, const
     const int* rlist = in_list;
     lj_rows_select(hh, rcnt, rlist, po);
     lj_gather_body<FULL_VIRIAL, F32, U, PIPE>(pos, hh, rcnt, rlist, in_cap, na, F, Facc, p, part, blockIdx.x,
-                                              gridDim.x, sm, s_hh, po);
+                                              gridDim.x, sm, s_hh, po, contig != 0);
     lj_zero_records(part, nrec);
 }
 
@@ -734,7 +747,7 @@ __device__ __forceinline__ void lj_gather_staged_body(const double* __restrict__
                                                       double* __restrict__ Facc, const LJP& p,
                                                       double* __restrict__ part, DevErr* err, int blk, int nblk,
                                                       unsigned char* dsm, double* sm, double* s_hh,
-                                                      const LJPruneOut& po) {
+                                                      const LJPruneOut& po, bool contig = false) {
     constexpr int W = NT / 32;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     int* bufs = reinterpret_cast<int*>(dsm) + (size_t)w * 2 * in_cap;
@@ -761,16 +774,17 @@ __device__ __forceinline__ void lj_gather_staged_body(const double* __restrict__
         umma::fence_smem_async();               // earlier reads of this buffer before the async write
         bulk_row(bufs + (size_t)b * in_cap, in_list + (size_t)atom * in_cap, bytes, &mb[b]);
     };
-    const int stride = nblk * W;
-    int i = blk * W + w;
+    const AtomRange ar = atom_range(blk, nblk, W, w, na, contig);
+    const int stride = ar.step, iend = ar.end;
+    int i = ar.first;
     uint32_t ph0 = 0, ph1 = 0;
     int cur = 0;
     bool pending = false;                       // a copy into buffer cur ^ 1 may be in flight
-    if (i < na && lane == 0) issue(i, 0);
-    for (; i < na; i += stride) {
+    if (i < iend && lane == 0) issue(i, 0);
+    for (; i < iend; i += stride) {
         const int inext = i + stride;
-        if (inext < na && lane == 0) issue(inext, cur ^ 1);
-        pending = inext < na;
+        if (inext < iend && lane == 0) issue(inext, cur ^ 1);
+        pending = inext < iend;
         const bool ok = umma::mbar_wait(&mb[cur], cur ? ph1 : ph0);
         if (cur) ph1 ^= 1; else ph0 ^= 1;
         if (!__all_sync(kFull, ok)) {
@@ -815,7 +829,7 @@ __global__ void __launch_bounds__(NT)
 k_lj_gather_staged(const double* __restrict__ pos, const double* __restrict__ hh, const int* __restrict__ in_cnt,
                    const int* __restrict__ in_list, int in_cap, int na, double* __restrict__ F,
                    double* __restrict__ Facc, LJP p, double* __restrict__ part, DevErr* err,
-                   LJPruneOut po, int nrec) {
+                   LJPruneOut po, int nrec, int contig) {
     FMD_PDL_WAIT();
     extern __shared__ __align__(128) unsigned char dsm[];
     __shared__ double sm[32 * kNV];
@@ -824,7 +838,7 @@ k_lj_gather_staged(const double* __restrict__ pos, const double* __restrict__ hh
     const int* rlist = in_list;
     lj_rows_select(hh, rcnt, rlist, po);
     lj_gather_staged_body<FULL_VIRIAL, F32, U, NT>(pos, hh, rcnt, rlist, in_cap, na, F, Facc, p, part, err,
-                                                   blockIdx.x, gridDim.x, dsm, sm, s_hh, po);
+                                                   blockIdx.x, gridDim.x, dsm, sm, s_hh, po, contig != 0);
     lj_zero_records(part, nrec);
 }
 
@@ -1024,11 +1038,11 @@ int lj_occupancy() {
 template <bool FV, bool F32, int U, bool PIPE, int NT>
 int lj_dispatch(bool launch, const double* pos, const double* hh, const int* cnt, const int* list, int cap,
                 const int* in_cnt, const int* in_list, int in_cap, int na, double* F, double* Facc, const LJP& p,
-                double* part, cudaStream_t st, const LJPruneOut& po, int nrec) {
+                double* part, cudaStream_t st, const LJPruneOut& po, int nrec, int contig) {
     const int nb = std::min(kLJMaxBlocks, lj_occupancy<FV, F32, U, PIPE, NT>() * kSMs);
     if (launch)
         launch_pdl(k_lj_gather<FV, F32, U, PIPE, NT>, dim3(nb), dim3(NT), 0, st, pos, hh, in_cnt, in_list, in_cap, na,
-                   F, Facc, p, part, po, nrec);
+                   F, Facc, p, part, po, nrec, contig);
     return nb;
 }
 
@@ -1040,7 +1054,7 @@ size_t staged_smem(int threads, int in_cap) {
 template <bool FV, bool F32, int U, int NT>
 int lj_dispatch_staged(bool launch, const double* pos, const double* hh, const int* in_cnt, const int* in_list,
                        int in_cap, int na, double* F, double* Facc, const LJP& p, double* part, DevErr* err,
-                       cudaStream_t st, const LJPruneOut& po, int nrec) {
+                       cudaStream_t st, const LJPruneOut& po, int nrec, int contig) {
     static std::map<int, int> occ;                 // in_cap -> resident blocks per SM
     const size_t smem = staged_smem(NT, in_cap);
     auto it = occ.find(in_cap);
@@ -1058,7 +1072,7 @@ int lj_dispatch_staged(bool launch, const double* pos, const double* hh, const i
     const int nb = std::min(kLJMaxBlocks, it->second * kSMs);
     if (launch)
         launch_pdl(k_lj_gather_staged<FV, F32, U, NT>, dim3(nb), dim3(NT), smem, st, pos, hh, in_cnt, in_list, in_cap,
-                   na, F, Facc, p, part, err, po, nrec);
+                   na, F, Facc, p, part, err, po, nrec, contig);
     return nb;
 }
 
@@ -1074,7 +1088,7 @@ int lj_select(bool launch, int ff, int precision, const LJShape& sh, const doubl
         if (in_cap % 4 != 0 || (launch && err == nullptr)) return 0;
 #define FMD_LJS(FV, F32, U, NT) \
     return lj_dispatch_staged<FV, F32, U, NT>(launch, pos, hh, in_cnt, in_list, in_cap, na, F, Facc, p, part, err, st, \
-                                              po, nrec)
+                                              po, nrec, sh.contig)
 #define FMD_LJS_NT(FV, F32, U) if (sh.threads == 128) { FMD_LJS(FV, F32, U, 128); } else { FMD_LJS(FV, F32, U, 256); }
 #define FMD_LJS_U(FV, F32) if (sh.unroll == 2) { FMD_LJS_NT(FV, F32, 2) } else { FMD_LJS_NT(FV, F32, 4) }
         if (fv) { if (f32) { FMD_LJS_U(true, true) } else { FMD_LJS_U(true, false) } }
@@ -1085,7 +1099,7 @@ int lj_select(bool launch, int ff, int precision, const LJShape& sh, const doubl
     }
 #define FMD_LJ_CALL(FV, F32, U, PIPE, NT) \
     return lj_dispatch<FV, F32, U, PIPE, NT>(launch, pos, hh, cnt, list, cap, in_cnt, in_list, in_cap, na, F, Facc, p, \
-                                             part, st, po, nrec)
+                                             part, st, po, nrec, sh.contig)
 #define FMD_LJ_NT(FV, F32, U, PIPE) \
     if (sh.threads == 128) { FMD_LJ_CALL(FV, F32, U, PIPE, 128); } else { FMD_LJ_CALL(FV, F32, U, PIPE, 256); }
 #define FMD_LJ_PIPE(FV, F32, U) if (sh.pipe) { FMD_LJ_NT(FV, F32, U, true) } else { FMD_LJ_NT(FV, F32, U, false) }

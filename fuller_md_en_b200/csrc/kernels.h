@@ -126,7 +126,14 @@ int rebo_ids_scratch(int n);
 // written as zeros.
 struct LJShape {
     int threads = 256, unroll = 4, pipe = 0;
+    // contig = 1: block b walks the atoms [b na / nblk, (b+1) na / nblk) in
+    // order (the warps of a block share partner molecules, so their partner
+    // positions stay in L1); 0: atoms strided over the whole grid.
+    int contig = 0;
 };
+// The feed value of the shape entry points: bits 0-1 the row feed (0..2),
+// bit 2 contig.
+inline bool lj_feed_valid(int feed) { return feed >= 0 && feed <= 6 && (feed & 3) <= 2; }
 struct LJPruneOut {
     int* cnt = nullptr;
     int* list = nullptr;

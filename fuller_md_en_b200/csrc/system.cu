@@ -240,10 +240,11 @@ LJShape System::pick_lj_shape(const int* rcnt, const int* rlist, int& rc) {
     cudaEventCreate(&e1);
     float best = 1e30f;
     LJShape pick;
+    for (int contig : {0, 1})
     for (int nt : {128, 256})
         for (int u : {2, 4})
             for (int pipe : {0, 1, 2}) {
-                const LJShape sh{nt, u, pipe};
+                const LJShape sh{nt, u, pipe, contig};
                 if (lj_gather_blocks(ff, arr.precision, sh, arr.in_cap) < 1) continue;
                 auto go = [&]() {
                     return lj_gather_launch(ff, arr.pos, arr.S->h, arr.cnt_a, arr.list_a, arr.cap_a, rcnt, rlist,
@@ -290,19 +291,25 @@ int System::tune_lj() {
     static std::map<std::tuple<int, int, int, int, int>, LJShape> cache;
     const int ff = arr.kind == FMD_SYS_AIREBO ? FMD_FF_AIREBO : FMD_FF_MM;
     // FMD_LJ_SHAPE="threads,unroll,feed" pins the shape of both gathers (no
-    // trial launches), for reproducible runs and profiler captures.
+    // trial launches), for reproducible runs and profiler captures; feed is
+    // 0..2, plus 4 for contiguous atom runs per block.
     if (const char* env = std::getenv("FMD_LJ_SHAPE")) {
         LJShape sh;
-        if (std::sscanf(env, "%d,%d,%d", &sh.threads, &sh.unroll, &sh.pipe) == 3 &&
-            (sh.threads == 128 || sh.threads == 256) && (sh.unroll == 2 || sh.unroll == 4) && sh.pipe >= 0 &&
-            sh.pipe <= 2 && lj_gather_blocks(ff, arr.precision, sh, arr.in_cap) > 0) {
-            arr.lj_shape = sh;
-            arr.lj_shape_p = sh;
-            set_lj_blocks();
-            return FMD_OK;
+        int feed = -1;
+        if (std::sscanf(env, "%d,%d,%d", &sh.threads, &sh.unroll, &feed) == 3 &&
+            (sh.threads == 128 || sh.threads == 256) && (sh.unroll == 2 || sh.unroll == 4) &&
+            lj_feed_valid(feed)) {
+            sh.pipe = feed & 3;
+            sh.contig = feed >> 2;
+            if (lj_gather_blocks(ff, arr.precision, sh, arr.in_cap) > 0) {
+                arr.lj_shape = sh;
+                arr.lj_shape_p = sh;
+                set_lj_blocks();
+                return FMD_OK;
+            }
         }
         return ctx->fail(FMD_ERR_ARG, "FMD_LJ_SHAPE: expected threads,unroll,feed with threads 128|256, "
-                                      "unroll 2|4, feed 0..2");
+                                      "unroll 2|4, feed 0..2 or 4..6");
     }
     const auto key = std::make_tuple(ctx->device, arr.kind, arr.n, arr.cap_a, arr.precision);
     auto it = cache.find(key);
@@ -815,9 +822,9 @@ extern "C" int fmd_system_set_lj_shape(fmd_system* s, int threads, int unroll, i
     if (!s || !s->sys) return FMD_ERR_ARG;
     fmd::System& y = *s->sys;
     if (y.arr.kind == FMD_SYS_RIGID || (threads != 128 && threads != 256) || (unroll != 2 && unroll != 4) ||
-        feed < 0 || feed > 2)
+        !lj_feed_valid(feed))
         return y.ctx->fail(FMD_ERR_ARG, "fmd_system_set_lj_shape: bad shape");
-    const LJShape sh{threads, unroll, feed};
+    const LJShape sh{threads, unroll, feed & 3, feed >> 2};
     const int ff = y.arr.kind == FMD_SYS_AIREBO ? FMD_FF_AIREBO : FMD_FF_MM;
     const int nb = lj_gather_blocks(ff, y.arr.precision, sh, y.arr.in_cap);
     if (nb < 1) return y.ctx->fail(FMD_ERR_ARG, "fmd_system_set_lj_shape: shape cannot run with this list");
@@ -882,7 +889,7 @@ extern "C" int fmd_system_lj_shape_pruned(fmd_system* s, int* threads, int* unro
     const StepArrays& a = s->sys->arr;
     if (threads) *threads = a.lj_shape_p.threads;
     if (unroll) *unroll = a.lj_shape_p.unroll;
-    if (feed) *feed = a.lj_shape_p.pipe;
+    if (feed) *feed = a.lj_shape_p.pipe | (a.lj_shape_p.contig << 2);
     return FMD_OK;
 }
 
@@ -891,7 +898,7 @@ extern "C" int fmd_system_lj_shape(fmd_system* s, int* threads, int* unroll, int
     const StepArrays& a = s->sys->arr;
     if (threads) *threads = a.lj_shape.threads;
     if (unroll) *unroll = a.lj_shape.unroll;
-    if (pipelined) *pipelined = a.lj_shape.pipe;
+    if (pipelined) *pipelined = a.lj_shape.pipe | (a.lj_shape.contig << 2);
     if (blocks) *blocks = a.lj_blocks;
     return FMD_OK;
 }
