@@ -211,7 +211,20 @@ struct fmd_batch {
         e = cudaGraphInstantiate(&ge, graph, 0);
         cudaGraphDestroy(graph);
         if (e != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, cudaGetErrorString(e));
+        // upload now, so the first launch of this variant does no set-up work
+        if ((e = cudaGraphUpload(ge, st)) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, cudaGetErrorString(e));
         return FMD_OK;
+    }
+
+    // All four step variants, captured and uploaded at creation (as a system
+    // does in its init), so no host-side capture sits between two steps.
+    int capture_all() {
+        for (int r = 0; r < 2; r++)
+            for (int ph = 0; ph < 2; ph++) {
+                const int rc = capture(r != 0, ph != 0);
+                if (rc != FMD_OK) return rc;
+            }
+        return ctx->sync_check("batch graph capture");
     }
 
     int enqueue(int first, int last) {
@@ -298,6 +311,7 @@ extern "C" int fmd_batch_create(fmd_ctx* ctx, int R, fmd_system* const* systems,
     b->bd.ff = FMD_FF_MM;
     b->bd.precision = b->sys[0]->arr.precision;
     int rc = autotune ? b->autotune() : b->set_offsets(b->tune);
+    if (!rc) rc = b->capture_all();
     if (rc) { b->release(); delete b; return rc; }
     *out = b;
     return FMD_OK;
