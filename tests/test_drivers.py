@@ -70,6 +70,31 @@ def write_library(root: Path) -> Path:
     return root / "FullereneLib"
 
 
+REF_MOLECULES = Path(__file__).resolve().parent / "golden" / "fullerenes.npz"
+
+
+def cc1_text(xyz, flag, nbr) -> str:
+    """A molecule in the .cc1 layout of the reference's FullereneLib, byte
+    for byte as the library writes it (count line; "C", index, x y z with six
+    decimals, flag, 1-based neighbours)."""
+    lines = [f" {len(xyz)}"]
+    for i, (p, f, b) in enumerate(zip(xyz, flag, nbr)):
+        lines.append(f"  C{i + 1:5d}{p[0]:12.6f}{p[1]:12.6f}{p[2]:12.6f}{f:5d}" + "".join(f"{v:4d}" for v in b if v >= 0))
+    return "\n".join(lines) + "\n"
+
+
+def write_reference_library(root: Path) -> Path:
+    """FullereneLib holding the reference library's own molecules recorded in
+    tests/golden/fullerenes.npz (C60-Ih, C70-D5h, C72-D6d, C84 No.01-D2 and
+    No.24-D6h; tests/golden/gen_fullerenes.py)."""
+    z = np.load(REF_MOLECULES)
+    for key in sorted({k.split("/")[0] for k in z.files}):
+        d = root / "FullereneLib" / str(z[f"{key}/dir"])
+        d.mkdir(parents=True, exist_ok=True)
+        (d / f"{key}.cc1").write_text(cc1_text(z[f"{key}/xyz"], z[f"{key}/flag"], z[f"{key}/nbr"]))
+    return root / "FullereneLib"
+
+
 def run(exe: Path, args: list[str], cwd: Path, timeout: int = 600, env: dict | None = None):
     e = dict(os.environ)
     e.setdefault("OMP_NUM_THREADS", str(min(16, os.cpu_count() or 1)))
@@ -172,6 +197,21 @@ def test_restart_reader_reads_reference_file(prog, tag, unit, work):
     lc = [ln for ln in c.stdout.splitlines() if "Restart" in ln]
     assert len(lc) == 2 and lc[0].endswith(f"{unit})")
     assert la == lc
+
+
+def test_recorded_molecules_are_the_reference_library():
+    """The recorded molecules, written back by cc1_text, are the reference
+    library's files byte for byte (checked where the reference checkout is
+    present: REF, or "reference" beside this repository)."""
+    root = Path(os.environ.get("REF", ROOT.parent / "reference")) / "FullereneLib"
+    if not root.exists():
+        pytest.skip("reference checkout not present")
+    z = np.load(REF_MOLECULES)
+    keys = sorted({k.split("/")[0] for k in z.files})
+    assert len(keys) == 5
+    for key in keys:
+        want = (root / str(z[f"{key}/dir"]) / f"{key}.cc1").read_text()
+        assert cc1_text(z[f"{key}/xyz"], z[f"{key}/flag"], z[f"{key}/nbr"]) == want, key
 
 
 # ---------------------------------------------------------------- GPU tests
@@ -372,3 +412,54 @@ def test_physics_option(prog, bits, wrong, work):
     (work["ours"] / "w").mkdir()
     c = run(ours(prog), args + [f"--physics={wrong}"], work["ours"] / "w")
     assert c.returncode != 0
+
+
+@pytest.fixture()
+def reflib(tmp_path):
+    lib = write_reference_library(tmp_path)
+    a = tmp_path / "ours"
+    b = tmp_path / "ref"
+    a.mkdir()
+    b.mkdir()
+    return {"lib": str(lib), "ours": a, "ref": b, "root": tmp_path}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prog,species,args", [
+    ("lj", "C70", ["--cell=2", "--step=60", "--mon=20"]),
+    ("lj", "C84:1", ["--cell=2", "--step=60", "--mon=20"]),
+    ("ai", "C60", ["--cell=2", "--step=20", "--mon=5"]),
+    ("ai", "C70", ["--cell=2", "--step=20", "--mon=5"]),
+    ("ai", "C84:24:D6h", ["--cell=2", "--step=20", "--mon=5"]),
+    ("mm", "C72", ["--cell=2", "--step=30", "--mon=10"]),
+    ("mm", "C84:1", ["--cell=2", "--step=30", "--mon=10"]),
+])
+def test_reference_molecules_match_reference(prog, species, args, reflib):
+    """Whole runs on the reference library's own molecules (resolve_fullerene,
+    LJ:210-226; load_cc1, LJ:178-207): the 70-84 atom molecules take the
+    cell-grid list path of the atomistic programs (the molecule-wise builder
+    covers 32-64 atoms).  Monitor and average lines against the serial
+    reference."""
+    args = args + [f"--fullerene={species}", f"--libdir={reflib['lib']}"]
+    a = run(ours(prog), args, reflib["ours"])
+    assert a.returncode == 0, a.stdout + a.stderr
+    b = run(ref(prog), args, reflib["ref"])
+    assert b.returncode == 0, b.stderr
+    assert banner(a.stdout) == banner(b.stdout)
+    assert_rows_match(monitor_rows(a.stdout), monitor_rows(b.stdout))
+    assert_avg_match(averages(a.stdout), averages(b.stdout))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prog,args", [("core", []), ("lj", ["--step=200", "--mon=100"]),
+                                       ("mm", ["--step=200", "--mon=100"]), ("ai", ["--step=200", "--mon=100"])])
+def test_reference_test_script_gpu_rows(prog, args, reflib):
+    """The *_gpu rows of the reference's own validation script
+    (Test_fuller.sh:211-272; pass rule run_test, :159-183): each program
+    with the script's arguments, run from a directory holding FullereneLib
+    (the script cd's to the checkout's root), passes when it exits 0 and its
+    output contains "Done".  The script itself does not travel with this
+    repository; these are its invocations and its pass rule."""
+    r = run(ours(prog), args, reflib["root"], timeout=900)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr
+    assert "Done" in r.stdout
