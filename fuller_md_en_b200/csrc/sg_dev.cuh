@@ -32,7 +32,10 @@ __device__ __forceinline__ bool bond_kept(double r) {
     return !(sw_fc(r) < 1e-15 && sw_dfc(r) == 0.0);
 }
 
-__device__ __forceinline__ float sigm(float z) { return 1.f / (1.f + __expf(-z)); }
+// Logistic sigmoid by the fast exponential and fast reciprocal (a few ulp;
+// every use rounds to BF16 or enters an FP32 sum): 1 / (1 + e^-z).  For
+// z < ~-88, e^-z is infinite and the quotient 0.
+__device__ __forceinline__ float sigm(float z) { return __fdividef(1.f, 1.f + __expf(-z)); }
 
 
 // SiLU'(z) and SiLU''(z) from s = sigmoid(z).
@@ -71,6 +74,14 @@ __device__ __forceinline__ void to_mma() {
     umma::fence_before();
     __syncthreads();
     umma::fence_after();
+}
+// The same hand-off, also returning whether `ok` holds in every thread.
+__device__ __forceinline__ bool to_mma_and(bool ok) {
+    umma::fence_smem_async();
+    umma::fence_before();
+    const bool all = __syncthreads_and(ok) != 0;
+    umma::fence_after();
+    return all;
 }
 
 __device__ __forceinline__ void issue(uint32_t d, uint32_t a_base, int a_cols, bool a_mn, uint32_t b_base,

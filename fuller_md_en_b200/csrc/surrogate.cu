@@ -203,29 +203,48 @@ constexpr int SM_W1 = 0, SM_W2 = SM_W1 + H * D * 2, SM_W3 = SM_W2 + H * H * 2, S
 // TMEM columns
 constexpr uint32_t TM_Z1 = 0, TM_Z2 = 128, TM_Z3 = 256, TM_T = 384;
 
-// Epilogue writing one 128 x 128 BF16 operand tile from TMEM: each thread
-// owns row q and kColsPerThread columns from c0.  kind 0: h = SiLU(z), column 127
-// held at 1.  kind 1: g = t * SiLU'(z) (z from a second TMEM region),
-// column 127 held at 0.
-template <int KIND>
-__device__ __forceinline__ void epi_tile(uint32_t ta, uint32_t tz, unsigned char* act, int q, int c0) {
+// Forward epilogue of one hidden layer: each thread owns row q and
+// kColsPerThread columns from c0 of z (TMEM at ta).  Writes h = SiLU(z) as
+// the next BF16 operand tile (column 127 held at 1) and puts SiLU'(z) back
+// into z's TMEM columns, where the gradient epilogue of this layer reads it,
+// so the sigmoid is evaluated once per element.
+__device__ __forceinline__ void epi_fwd(uint32_t ta, unsigned char* act, int q, int c0) {
 #pragma unroll 1
     for (int cc = 0; cc < kColsPerThread; cc += 16) {
-        float v[16];
-        umma::tmem_ld16(ta + c0 + cc, v);
-        if (KIND == 1) {
-            float z[16];
-            umma::tmem_ld16(tz + c0 + cc, z);
+        float z[16], v[16], d[16];
+        umma::tmem_ld16(ta + c0 + cc, z);
 #pragma unroll
-            for (int e = 0; e < 16; e++) {
-                const float s = sigm(z[e]);
-                v[e] = v[e] * s * (1.f + z[e] * (1.f - s));
-            }
-        } else {
-#pragma unroll
-            for (int e = 0; e < 16; e++) v[e] = v[e] * sigm(v[e]);
+        for (int e = 0; e < 16; e++) {
+            const float s = sigm(z[e]);
+            v[e] = z[e] * s;
+            d[e] = dsilu(z[e], s);
         }
-        if (c0 + cc + 16 == H) v[15] = KIND == 0 ? 1.f : 0.f;
+        if (c0 + cc + 16 == H) v[15] = 1.f;
+        umma::tmem_st16(ta + c0 + cc, d);
+#pragma unroll
+        for (int h8 = 0; h8 < 2; h8++) {
+            uint4 o;
+            o.x = umma::pack_bf16(v[8 * h8 + 0], v[8 * h8 + 1]);
+            o.y = umma::pack_bf16(v[8 * h8 + 2], v[8 * h8 + 3]);
+            o.z = umma::pack_bf16(v[8 * h8 + 4], v[8 * h8 + 5]);
+            o.w = umma::pack_bf16(v[8 * h8 + 6], v[8 * h8 + 7]);
+            *reinterpret_cast<uint4*>(act + umma::il_off(q, c0 + cc + 8 * h8, H)) = o;
+        }
+    }
+    umma::tmem_wait_st();
+}
+
+// Gradient epilogue: g = t * SiLU'(z) from the t accumulator (ta) and the
+// SiLU'(z) the forward epilogue left at td; column 127 held at 0.
+__device__ __forceinline__ void epi_bwd(uint32_t ta, uint32_t td, unsigned char* act, int q, int c0) {
+#pragma unroll 1
+    for (int cc = 0; cc < kColsPerThread; cc += 16) {
+        float v[16], d[16];
+        umma::tmem_ld16(ta + c0 + cc, v);
+        umma::tmem_ld16(td + c0 + cc, d);
+#pragma unroll
+        for (int e = 0; e < 16; e++) v[e] *= d[e];
+        if (c0 + cc + 16 == H) v[15] = 0.f;
 #pragma unroll
         for (int h8 = 0; h8 < 2; h8++) {
             uint4 o;
@@ -277,29 +296,40 @@ k_sg_mlp(const uint16_t* __restrict__ img, const float* __restrict__ vec, const 
     uint32_t ph = 0;
     bool ok = true;
 
+    // The descriptor tile of the next 128 rows: 8 KB, one 16-byte piece per
+    // thread, loaded into a register while the current tile is computed.
+    static_assert(TILE * D * 2 / 16 == kMlpThreads, "one 16-byte piece of the descriptor tile per thread");
+    uint4 xnext = reinterpret_cast<const uint4*>(X + (size_t)blockIdx.x * TILE * D)[t];
+
+    // Wait for the MMAs of this step, then (after the epilogue) hand the new
+    // operand tile to the issuing thread; a wait that ran out ends every
+    // thread at the next hand-off.
 #define SG_WAIT()                                                     \
     do {                                                              \
-        const bool _w = umma::mbar_wait(&mbar, ph);                   \
-        ph ^= 1u;                                                     \
+        if (ok) {                                                     \
+            ok = umma::mbar_wait(&mbar, ph);                          \
+            if (ok) ph ^= 1u;                                         \
+        }                                                             \
         umma::fence_after();                                          \
-        if (!__syncthreads_and(_w)) { ok = false; goto done; }        \
+    } while (0)
+#define SG_HANDOFF()                                                  \
+    do {                                                              \
+        if (!to_mma_and(ok)) { ok = false; goto done; }               \
     } while (0)
 
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        {   // descriptor tile: 8 KB, already in the operand layout
-            const uint4* src = reinterpret_cast<const uint4*>(X + (size_t)tile * TILE * D);
-            uint4* dst = reinterpret_cast<uint4*>(sm + SM_X);
-            for (int e = t; e < TILE * D * 2 / 16; e += kMlpThreads) dst[e] = src[e];
-        }
-        to_mma();
+        reinterpret_cast<uint4*>(sm + SM_X)[t] = xnext;                // operand layout already
+        SG_HANDOFF();
         if (t == 0) issue(tm + TM_Z1, sX, D, false, sW1, D, false, H, D / 16, &mbar);
         SG_WAIT();
-        epi_tile<0>(tl + TM_Z1, 0, act, q, c0);                       // h1
-        to_mma();
+        if (tile + (int)gridDim.x < ntiles)                           // X is free once z1 is done
+            xnext = reinterpret_cast<const uint4*>(X + (size_t)(tile + gridDim.x) * TILE * D)[t];
+        epi_fwd(tl + TM_Z1, act, q, c0);                              // h1, SiLU'(z1) -> TM_Z1
+        SG_HANDOFF();
         if (t == 0) issue(tm + TM_Z2, sA, H, false, sW2, H, false, H, H / 16, &mbar);
         SG_WAIT();
-        epi_tile<0>(tl + TM_Z2, 0, act, q, c0);                       // h2
-        to_mma();
+        epi_fwd(tl + TM_Z2, act, q, c0);                              // h2, SiLU'(z2) -> TM_Z2
+        SG_HANDOFF();
         if (t == 0) issue(tm + TM_Z3, sA, H, false, sW3, H, false, H, H / 16, &mbar);
         SG_WAIT();
         {   // output layer and g3 = bs * w4 * SiLU'(z3)
@@ -315,7 +345,7 @@ k_sg_mlp(const uint16_t* __restrict__ img, const float* __restrict__ vec, const 
                     const float s = sigm(z[e]);
                     const float hv = col == H - 1 ? 1.f : z[e] * s;
                     y += hv * w4[col];
-                    g[e] = col == H - 1 ? 0.f : bs * w4[col] * s * (1.f + z[e] * (1.f - s));
+                    g[e] = col == H - 1 ? 0.f : bs * w4[col] * dsilu(z[e], s);
                 }
 #pragma unroll
                 for (int h8 = 0; h8 < 2; h8++) {
@@ -329,7 +359,7 @@ k_sg_mlp(const uint16_t* __restrict__ img, const float* __restrict__ vec, const 
             }
             red[(w >> 2) * TILE + q] = y;
         }
-        to_mma();
+        SG_HANDOFF();
         {
             const int row = tile * TILE + q;
             if (c0 == 0 && row < R) {
@@ -341,12 +371,12 @@ k_sg_mlp(const uint16_t* __restrict__ img, const float* __restrict__ vec, const 
         }
         if (t == 0) issue(tm + TM_T, sA, H, false, sW3, H, true, H, H / 16, &mbar);   // t2 = g3 W3^T
         SG_WAIT();
-        epi_tile<1>(tl + TM_T, tl + TM_Z2, act, q, c0);               // g2
-        to_mma();
+        epi_bwd(tl + TM_T, tl + TM_Z2, act, q, c0);                   // g2
+        SG_HANDOFF();
         if (t == 0) issue(tm + TM_T, sA, H, false, sW2, H, true, H, H / 16, &mbar);   // t1 = g2 W2^T
         SG_WAIT();
-        epi_tile<1>(tl + TM_T, tl + TM_Z1, act, q, c0);               // g1
-        to_mma();
+        epi_bwd(tl + TM_T, tl + TM_Z1, act, q, c0);                   // g1
+        SG_HANDOFF();
         if (t == 0) issue(tm + TM_T, sA, H, false, sW1, D, true, D, H / 16, &mbar);   // gx = g1 W1^T
         SG_WAIT();
         if ((w >> 2) < D / 16) {                // gx has D = 32 columns: two groups of 16
@@ -361,18 +391,20 @@ k_sg_mlp(const uint16_t* __restrict__ img, const float* __restrict__ vec, const 
             }
         }
         umma::fence_before();
-        __syncthreads();
-        umma::fence_after();
+        // the next tile's first hand-off orders these TMEM reads before its MMAs
     }
 done:
     if (!ok) {
         if (t == 0) atomicCAS(err + 1, 0, 1);
-        umma::mbar_wait(&mbar, ph);   // give an in-flight MMA a bounded chance to land
+        // a thread whose own wait ran out still holds that phase: give the
+        // MMA in flight a bounded chance to land before TMEM is released
+        umma::mbar_wait(&mbar, ph);
     }
     umma::fence_before();
     __syncthreads();
     if (w == 0) umma::tmem_dealloc(tm, 512);
 #undef SG_WAIT
+#undef SG_HANDOFF
 }
 
 // ------------------------------------------------------------------ forces
