@@ -259,6 +259,22 @@ k_rigid_w(const double* __restrict__ pos, const Site<P>* __restrict__ lab, const
     const int a0 = lane, a1 = lane + 32;
     const bool v0 = a0 < natom, v1 = a1 < natom;
     const Site<P> r0 = lab_i[v0 ? a0 : 0], r1 = lab_i[v1 ? a1 : 0];
+    // Site screen: a pair within the cutoff has |m + r_b| <= |d| + |r_a| <
+    // rcut + R, with m the COM image, d the pair vector and R the largest site
+    // radius (all molecules share one body, so i's own sites give it).  Only
+    // j's sites within rcut + R (+ a margin far above the rounding of either
+    // precision) of i's centre enter the pair loop, in ascending order, so
+    // the pairs that count and the order of their sums are unchanged.
+    double rmax2 = 0.0;
+    {
+        const double q0 = v0 ? (double)r0.x * r0.x + (double)r0.y * r0.y + (double)r0.z * r0.z : 0.0;
+        const double q1 = v1 ? (double)r1.x * r1.x + (double)r1.y * r1.y + (double)r1.z * r1.z : 0.0;
+        rmax2 = fmax(q0, q1);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) rmax2 = fmax(rmax2, __shfl_xor_sync(kFull, rmax2, o));
+    }
+    const double screen = sqrt(rc.rcut2) + sqrt(rmax2) + 1e-2, screen2 = screen * screen;
+    const unsigned lt = (1u << lane) - 1u;
     double acc[16];   // F(3) T(3) W(9) E
 #pragma unroll
     for (int k = 0; k < 16; k++) acc[k] = 0.0;
@@ -272,29 +288,37 @@ k_rigid_w(const double* __restrict__ pos, const Site<P>* __restrict__ lab, const
         mimg(mx, my, mz, hi, h);
         if (norm2_rn(mx, my, mz) > rmcut2) continue;             // warp-uniform (LJ:320)
         __syncwarp();
-        if constexpr (sizeof(P) == 8) {
-            if (v0) sj[a0] = lab[(size_t)j * natom + a0];
-            if (v1) sj[a1] = lab[(size_t)j * natom + a1];
-        } else {
-            // FP32 pairs: j's sites moved by the COM image m in FP64 and rounded
-            // once, so each pair distance is one subtraction; the rounding error
-            // is independent per site (not shared by the whole molecule pair).
+        // j's sites a0, a1 of this lane, kept by the screen, stored compacted
+        int nb;
+        {
+            Site<P> q[2];
+            bool keep[2];
 #pragma unroll
             for (int s = 0; s < 2; s++) {
                 const int b = s ? a1 : a0;
-                if (!(s ? v1 : v0)) continue;
-                const Site<P> q = lab[(size_t)j * natom + b];
-                Site<P> t;
-                t.x = (float)((double)q.x + mx); t.y = (float)((double)q.y + my); t.z = (float)((double)q.z + mz);
-                t.pad = 0.f;
-                sj[b] = t;
+                keep[s] = s ? v1 : v0;
+                if (!keep[s]) continue;
+                q[s] = lab[(size_t)j * natom + b];
+                const double ux = (double)q[s].x + mx, uy = (double)q[s].y + my, uz = (double)q[s].z + mz;
+                keep[s] = ux * ux + uy * uy + uz * uz < screen2;
+                if constexpr (sizeof(P) == 4) {
+                    // FP32 pairs: j's sites moved by the COM image m in FP64 and
+                    // rounded once, so each pair distance is one subtraction; the
+                    // rounding error is independent per site.
+                    q[s].x = (float)ux; q[s].y = (float)uy; q[s].z = (float)uz; q[s].pad = 0.f;
+                }
             }
+            const unsigned m0 = __ballot_sync(kFull, keep[0]), m1 = __ballot_sync(kFull, keep[1]);
+            if (keep[0]) sj[__popc(m0 & lt)] = q[0];
+            if (keep[1]) sj[__popc(m0) + __popc(m1 & lt)] = q[1];
+            nb = __popc(m0) + __popc(m1);
         }
         __syncwarp();
+        if (nb == 0) continue;                                   // warp-uniform
         // per-neighbour partial sums for sites a0 and a1
         P f[2][3] = {{0, 0, 0}, {0, 0, 0}}, wv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, e = 0;
         if constexpr (sizeof(P) == 8) {
-            for (int b = 0; b < natom; b++) {
+            for (int b = 0; b < nb; b++) {
                 const Site<P> rb = sj[b];
 #pragma unroll
                 for (int s = 0; s < 2; s++) {
@@ -322,7 +346,7 @@ k_rigid_w(const double* __restrict__ pos, const Site<P>* __restrict__ lab, const
             float eterm = 0.f;
             float wxx = 0.f, wyy = 0.f, wzz = 0.f, wxy = 0.f, wxz = 0.f, wyz = 0.f;
             int npair = 0;
-            for (int b = 0; b < natom; b++) {
+            for (int b = 0; b < nb; b++) {
                 const Site<P> rb = sj[b];
 #pragma unroll
                 for (int s = 0; s < 2; s++) {
