@@ -113,6 +113,8 @@ _SIGS = {
                                          POINTER(NPT), POINTER(c_void_p)]),
     "fmd_system_create_mm": (c_int, [c_void_p, POINTER(RunParams), c_int, _dp, _dp, _ip,
                                      POINTER(MMTopology), _dp, _dp, POINTER(NPT), POINTER(c_void_p)]),
+    "fmd_system_create_mm_replicated": (c_int, [c_void_p, POINTER(RunParams), c_int, c_int, _dp, _dp,
+                                                POINTER(MMTopology), _dp, POINTER(NPT), POINTER(c_void_p)]),
     "fmd_system_init": (c_int, [c_void_p]),
     "fmd_system_run": (c_int, [c_void_p, c_int, c_int, POINTER(Obs)]),
     "fmd_system_enqueue": (c_int, [c_void_p, c_int, c_int]),
@@ -158,6 +160,7 @@ _SIGS = {
     "fmd_batch_observables": (c_int, [c_void_p, POINTER(Obs)]),
     "fmd_batch_get_tuning": (c_int, [c_void_p, POINTER(BatchTuning)]),
     "fmd_batch_step_kernels": (c_int, [c_void_p, c_int, c_int, POINTER(c_int)]),
+    "fmd_batch_step_kernels_conditional": (c_int, [c_void_p, c_int, c_int, POINTER(c_int)]),
     "fmd_batch_destroy": (c_int, [c_void_p]),
     "fmd_system_surrogate_status": (c_int, [c_void_p, POINTER(SgStatus)]),
 }

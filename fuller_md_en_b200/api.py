@@ -375,6 +375,23 @@ class System:
         sysm._topo = topo
         return sysm
 
+    @classmethod
+    def mm_replicated(cls, ctx: Context, cfg: RunConfig, nmol: int, natom_mol: int, pos, vel, mol_topo: Topology,
+                      h, npt) -> "System":
+        """An MM system of nmol contiguous molecules of natom_mol atoms (no
+        charges) from ONE molecule's topology, replicated on the device
+        (fmd_system_create_mm_replicated): the same system as System.mm with
+        the full flat topology of the copies."""
+        out = ctypes.c_void_p()
+        s = npt_from_array(npt)
+        ctx.check(ctx.lib.fmd_system_create_mm_replicated(ctx.h, ctypes.byref(cfg.c()), nmol, natom_mol,
+                                                          _d(_f64(pos)), _d(_f64(vel)), ctypes.byref(mol_topo.c),
+                                                          _d(_f64(h)), ctypes.byref(s), ctypes.byref(out)),
+                  "fmd_system_create_mm_replicated")
+        sysm = cls(ctx, out, nmol * natom_mol, _lib.FMD_SYS_MM)
+        sysm._topo = mol_topo
+        return sysm
+
     def init(self) -> None:
         self.ctx.check(self.ctx.lib.fmd_system_init(self.h), "fmd_system_init")
 
@@ -392,12 +409,22 @@ class System:
         self.ctx.check(self.ctx.lib.fmd_system_averages(self.h, ctypes.byref(a)), "fmd_system_averages")
         return a
 
-    def download(self):
+    def download(self, out: dict | None = None):
+        """State of the system: pos, vel (and qv, omg for rigid systems), h and
+        the NPT state.  `out` may hold caller-owned float64 arrays of the
+        right sizes (e.g. in pinned memory) for pos, vel, qv, omg and h, which
+        are filled in place instead of fresh arrays."""
         n = self.n
-        pos, vel = np.zeros(3 * n), np.zeros(3 * n)
-        qv = np.zeros(4 * n) if self.kind == _lib.FMD_SYS_RIGID else None
-        omg = np.zeros(3 * n) if self.kind == _lib.FMD_SYS_RIGID else None
-        h = np.zeros(9)
+        out = out or {}
+        pos = out.get("pos") if out.get("pos") is not None else np.zeros(3 * n)
+        vel = out.get("vel") if out.get("vel") is not None else np.zeros(3 * n)
+        rigid = self.kind == _lib.FMD_SYS_RIGID
+        qv = (out.get("qv") if out.get("qv") is not None else np.zeros(4 * n)) if rigid else None
+        omg = (out.get("omg") if out.get("omg") is not None else np.zeros(3 * n)) if rigid else None
+        h = out.get("h") if out.get("h") is not None else np.zeros(9)
+        for a, m in ((pos, 3 * n), (vel, 3 * n), (qv, 4 * n), (omg, 3 * n), (h, 9)):
+            if a is not None and (a.dtype != np.float64 or a.size != m or not a.flags.c_contiguous):
+                raise ValueError("download: out arrays must be contiguous float64 of the state's sizes")
         npt = NPT()
         self.ctx.check(self.ctx.lib.fmd_system_download(self.h, _d(pos), _d(vel), _d(qv) if qv is not None else None,
                                                         _d(omg) if omg is not None else None, _d(h),
@@ -556,10 +583,12 @@ class Batch:
         self.ctx.check(self.ctx.lib.fmd_batch_get_tuning(self.h, ctypes.byref(t)), "fmd_batch_get_tuning")
         return {k: getattr(t, k) for k, _ in t._fields_}
 
-    def step_kernels(self, rebuild: bool, phase: bool = False) -> int:
+    def step_kernels(self, rebuild: bool, phase: bool = False, conditional: bool = False) -> int:
+        """Kernels launched on every replay of a step's graph; with
+        conditional=True, those of its conditional fallback body instead."""
         k = ctypes.c_int(0)
-        self.ctx.check(self.ctx.lib.fmd_batch_step_kernels(self.h, int(rebuild), int(phase), ctypes.byref(k)),
-                       "fmd_batch_step_kernels")
+        f = self.ctx.lib.fmd_batch_step_kernels_conditional if conditional else self.ctx.lib.fmd_batch_step_kernels
+        self.ctx.check(f(self.h, int(rebuild), int(phase), ctypes.byref(k)), "fmd_batch_step_kernels")
         return k.value
 
     def close(self) -> None:
@@ -579,13 +608,27 @@ def mm_replica(ctx: Context, nc: int, T: float, P: float, dt: float = 0.1, seed:
     """An MM system of C60 FCC nc x nc x nc (Ih C60 geometry, reference force
     constants) at temperature T (K) and pressure P (GPa), not yet initialised."""
     from . import crystal
-    coords = crystal.c60_ih()
-    bonds = crystal.bonds_from_geometry(coords)
+    coords, topo = _c60_molecule_topology()
     s = crystal.atomistic(nc, coords=coords, jitter=jitter, seed=seed, T=T, mol_base=0)
     na, nmol = s["pos"].size // 3, s["nmol"]
-    t = crystal.mm_topology(coords, bonds, nmol)
-    topo = Topology(t["bonds"], t["kb"], t["r0"], t["angles"], t["kth"], t["th0"], t["dihedrals"], t["vn"],
-                    t["mult"], t["gamma"], t["impropers"], t["ki"], t["igamma"])
     cfg = RunConfig(dt=dt, T=T, Pe=P, nsteps=nsteps, nlup=nlup, gavg_from=1, gavg_to=nsteps, nc=nc, nmol=nmol,
                     precision=precision)
-    return System.mm(ctx, cfg, s["pos"], s["vel"], s["mol_id"], topo, s["h"], crystal.npt_atom(T, P, na))
+    # one molecule's topology, replicated over the crystal on the device
+    return System.mm_replicated(ctx, cfg, nmol, na // nmol, s["pos"], s["vel"], topo, s["h"],
+                                crystal.npt_atom(T, P, na))
+
+
+_MOL_TOPO = {}
+
+
+def _c60_molecule_topology():
+    """The Ih C60 geometry and its one-molecule MM topology (reference force
+    constants), built once per process."""
+    if "c60" not in _MOL_TOPO:
+        from . import crystal
+        coords = crystal.c60_ih()
+        t = crystal.mm_topology(coords, crystal.bonds_from_geometry(coords), 1)
+        topo = Topology(t["bonds"], t["kb"], t["r0"], t["angles"], t["kth"], t["th0"], t["dihedrals"], t["vn"],
+                        t["mult"], t["gamma"], t["impropers"], t["ki"], t["igamma"])
+        _MOL_TOPO["c60"] = (coords, topo)
+    return _MOL_TOPO["c60"]

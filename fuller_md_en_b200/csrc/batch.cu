@@ -24,6 +24,7 @@
 #include <tuple>
 #include <vector>
 
+#include "molnlist.h"
 #include "step.h"
 #include "system.h"
 
@@ -66,6 +67,133 @@ struct fmd_batch {
     cudaGraphExec_t graphs[2][2] = {};
     cudaStream_t side[kSideStreams] = {};
     cudaEvent_t ev_fork = nullptr, ev_join[kSideStreams] = {};
+    // Batched list rebuild (every replica on the candidate-bitmap molecule
+    // path): replica table and block offsets on the device.
+    bool molb = false;
+    MolRep* dReps = nullptr;
+    int* dMolOff = nullptr;
+    MolBatch mb;
+
+    // Replica table and block offsets of the batched rebuild; leaves molb
+    // false (per-replica rebuild branches) unless every replica has equal
+    // molecules of 32-64 atoms, the path the batched kernels implement.
+    int setup_mol_batch() {
+        for (System* s : sys)
+            if (!(s->mol.ok && s->mol.masks) || s->arr.kind != FMD_SYS_MM) return FMD_OK;
+        std::vector<MolRep> reps(R);
+        std::vector<int> off(3 * (R + 1), 0);
+        long long ntot = 0;
+        for (System* s : sys) ntot += s->arr.n;
+        constexpr int kRowBlocks = kSMs * 8;     // the single-system row kernels' grid
+        for (int r = 0; r < R; r++) {
+            System* s = sys[r];
+            MolRep& q = reps[r];
+            q.m = s->mol;
+            q.pos = s->arr.pos;
+            q.hh = s->arr.S->h;
+            q.rc = s->rc_a;
+            q.rc2 = s->rc2_a;
+            q.cap = s->arr.cap_a;
+            q.in_cap = s->arr.in_cap;
+            q.cnt = const_cast<int*>(s->arr.cnt_a);
+            q.list = const_cast<int*>(s->arr.list_a);
+            q.dropped = s->dropped;
+            q.in_cnt = const_cast<int*>(s->arr.in_cnt);
+            q.in_list = const_cast<int*>(s->arr.in_list);
+            q.err = ctx->d_err;
+            q.prune_words = s->prune.ok ? s->prune.words : nullptr;
+            const int M = s->mol.M;
+            const int share = (int)std::max(1LL, (kRowBlocks * (long long)s->arr.n + ntot / 2) / ntot);
+            off[r + 1] = off[r] + (M * 32 + 255) / 256;
+            off[(R + 1) + r + 1] = off[(R + 1) + r] + share;
+            off[2 * (R + 1) + r + 1] = off[2 * (R + 1) + r] + std::min(2 * M, share);
+        }
+        if (cudaMalloc(&dReps, sizeof(MolRep) * R) != cudaSuccess ||
+            cudaMalloc(&dMolOff, sizeof(int) * off.size()) != cudaSuccess)
+            return ctx->fail(FMD_ERR_CUDA, "batch: allocation failed");
+        if (cudaMemcpyAsync(dReps, reps.data(), sizeof(MolRep) * R, cudaMemcpyHostToDevice, ctx->stream) !=
+                cudaSuccess ||
+            cudaMemcpyAsync(dMolOff, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice, ctx->stream) !=
+                cudaSuccess)
+            return ctx->fail(FMD_ERR_CUDA, "batch: upload failed");
+        mb.reps = dReps;
+        mb.R = R;
+        mb.off_w = dMolOff;
+        mb.off_rows = dMolOff + (R + 1);
+        mb.off_in = dMolOff + 2 * (R + 1);
+        mb.nblk_w = off[R];
+        mb.nblk_rows = off[(R + 1) + R];
+        mb.nblk_in = off[2 * (R + 1) + R];
+        molb = true;
+        int rc = ctx->sync_check("batch rebuild tables");
+        if (rc) return rc;
+        // kernels of the conditional fallback body: the same launches captured
+        // once into a graph of their own and counted
+        cudaGraph_t fb = nullptr;
+        if (cudaStreamBeginCapture(side[0], cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+            return ctx->fail(FMD_ERR_CUDA, "batch: fallback capture failed to start");
+        cudaError_t ef = cudaSuccess;
+        for (System* s : sys)
+            if ((ef = s->enqueue_rebuild_fallback(side[0])) != cudaSuccess) break;
+        const cudaError_t e2 = cudaStreamEndCapture(side[0], &fb);
+        if (ef != cudaSuccess || e2 != cudaSuccess) {
+            cudaGetLastError();
+            return ctx->fail(FMD_ERR_CUDA, "batch: fallback capture failed");
+        }
+        body_kernels = count_kernel_nodes(fb, nullptr);
+        cudaGraphDestroy(fb);
+        return pending("after counting the fallback's kernels");
+    }
+
+    // The batched rebuild, inside a stream capture: one launch per phase for
+    // all replicas, and between the path decision and the half rows a
+    // conditional node whose body -- every replica's cell-grid fallback,
+    // gated per replica on the device -- runs only when some replica's
+    // molecule path was rejected for this build.
+    cudaError_t enqueue_rebuild_batched(cudaStream_t st) {
+        cudaStreamCaptureStatus cs;
+        cudaGraph_t g = nullptr;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t nd = 0;
+        cudaError_t e;
+        where = "an error pending before the rebuild";
+        if ((e = cudaPeekAtLastError()) != cudaSuccess) return e;
+        where = "capture info";
+        if ((e = cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd)) != cudaSuccess) return e;
+        if (cs != cudaStreamCaptureStatusActive) return cudaErrorStreamCaptureUnsupported;
+        where = "conditional handle";
+        cudaGraphConditionalHandle cond;
+        if ((e = cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault)) != cudaSuccess) return e;
+        where = "batched partner tables";
+        if ((e = mol_rebuild_batch_pre(mb, cond, st, &where)) != cudaSuccess) return e;
+        where = "capture info";
+        if ((e = cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd)) != cudaSuccess) return e;
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = cond;
+        cp.conditional.type = cudaGraphCondTypeIf;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        where = "conditional node";
+        if ((e = cudaGraphAddNode(&node, g, deps, nd, &cp)) != cudaSuccess) return e;
+        where = "capture dependencies";
+        if ((e = cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies)) != cudaSuccess)
+            return e;
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        where = "fallback capture";
+        if ((e = cudaStreamBeginCaptureToGraph(side[0], body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed)) !=
+            cudaSuccess)
+            return e;
+        cudaError_t ef = cudaSuccess;
+        for (System* s : sys)
+            if ((ef = s->enqueue_rebuild_fallback(side[0])) != cudaSuccess) break;
+        cudaGraph_t got = nullptr;
+        if ((e = cudaStreamEndCapture(side[0], &got)) != cudaSuccess) return e;
+        if (ef != cudaSuccess) return ef;
+        where = "batched rows";
+        return mol_rebuild_batch_rows(mb, st);
+    }
+    const char* where = "";
 
     int set_offsets(const Tune& t) {
         std::vector<int> off(3 * (R + 1), 0);
@@ -181,7 +309,9 @@ struct fmd_batch {
 
     cudaError_t enqueue_variant(bool rebuild, bool phase, cudaStream_t st) {
         cudaError_t e;
-        if (rebuild) {
+        if (rebuild && molb) {
+            if ((e = enqueue_rebuild_batched(st)) != cudaSuccess) return e;
+        } else if (rebuild) {
             // per-replica rebuilds as parallel branches
             if ((e = cudaEventRecord(ev_fork, st)) != cudaSuccess) return e;
             for (int k = 0; k < kSideStreams; k++)
@@ -205,15 +335,74 @@ struct fmd_batch {
             return ctx->fail(FMD_ERR_CUDA, "batch: graph capture failed to start");
         cudaError_t e = enqueue_variant(rebuild, phase, st);
         cudaError_t e2 = cudaStreamEndCapture(st, &graph);
-        if (e != cudaSuccess || e2 != cudaSuccess)
-            return ctx->fail(FMD_ERR_CUDA, std::string("batch: graph capture failed: ") +
-                                               cudaGetErrorString(e != cudaSuccess ? e : e2));
+        if (e != cudaSuccess || e2 != cudaSuccess) {
+            cudaGetLastError();
+            if (e2 == cudaSuccess && graph) cudaGraphDestroy(graph);
+            return ctx->fail(FMD_ERR_CUDA, std::string("batch: graph capture failed: ") + where + ": " +
+                                               cudaGetErrorName(e != cudaSuccess ? e : e2) + " (" +
+                                               cudaGetErrorString(e != cudaSuccess ? e : e2) + ")");
+        }
+        if (int rc = pending("after the capture")) return rc;
+        count_kernels(graph, rebuild, nkern[rebuild ? 1 : 0][phase ? 1 : 0], nkern_cond[rebuild ? 1 : 0][phase ? 1 : 0]);
+        if (int rc = pending("after counting the graph's kernels")) return rc;
         e = cudaGraphInstantiate(&ge, graph, 0);
         cudaGraphDestroy(graph);
         if (e != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, cudaGetErrorString(e));
+        if (int rc = pending("after instantiation")) return rc;
         // upload now, so the first launch of this variant does no set-up work
         if ((e = cudaGraphUpload(ge, st)) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, cudaGetErrorString(e));
+        if (int rc = pending("after the upload")) return rc;
         return FMD_OK;
+    }
+
+    // Kernel nodes of a captured step graph: launched every replay (top
+    // level), and inside conditional bodies (launched only when the body runs).
+    int nkern[2][2] = {}, nkern_cond[2][2] = {};
+    int body_kernels = 0;               // kernel nodes of the conditional fallback body
+    std::string count_note;             // a graph query that failed while counting (diagnostic)
+    int count_kernel_nodes(cudaGraph_t g, int* conditionals) {
+        size_t n = 0;
+        cudaError_t e;
+        if ((e = cudaGraphGetNodes(g, nullptr, &n)) != cudaSuccess) {
+            count_note = std::string("cudaGraphGetNodes(count): ") + cudaGetErrorName(e);
+            cudaGetLastError();
+            return 0;
+        }
+        std::vector<cudaGraphNode_t> nodes(n);
+        if (n && (e = cudaGraphGetNodes(g, nodes.data(), &n)) != cudaSuccess) {
+            count_note = std::string("cudaGraphGetNodes: ") + cudaGetErrorName(e);
+            cudaGetLastError();
+            return 0;
+        }
+        int k = 0, c = 0;
+        for (size_t q = 0; q < n; q++) {
+            cudaGraphNodeType t = cudaGraphNodeTypeEmpty;
+            if ((e = cudaGraphNodeGetType(nodes[q], &t)) != cudaSuccess) {
+                count_note = std::string("cudaGraphNodeGetType: ") + cudaGetErrorName(e);
+                cudaGetLastError();
+                continue;
+            }
+            k += t == cudaGraphNodeTypeKernel;
+            c += t == cudaGraphNodeTypeConditional;
+        }
+        if (conditionals) *conditionals = c;
+        return k;
+    }
+    // (A conditional node's type query fails on this runtime, so the rebuild
+    // variant's one conditional body is counted from the fallback's own
+    // capture at set-up.)
+    void count_kernels(cudaGraph_t g, bool rebuild, int& top, int& cond) {
+        top = count_kernel_nodes(g, nullptr);
+        cond = rebuild && molb ? body_kernels : 0;
+    }
+
+    // Fails when a CUDA error is pending (left by an earlier runtime call).
+    int pending(const char* stage) {
+        const cudaError_t e = cudaPeekAtLastError();
+        if (e == cudaSuccess) return FMD_OK;
+        cudaGetLastError();
+        return ctx->fail(FMD_ERR_CUDA, std::string("batch: ") + cudaGetErrorName(e) + " pending " + stage +
+                                           (count_note.empty() ? std::string() : " [" + count_note + "]"));
     }
 
     // All four step variants, captured and uploaded at creation (as a system
@@ -251,8 +440,8 @@ struct fmd_batch {
         if (ev_fork) cudaEventDestroy(ev_fork);
         for (auto& e : ev_join)
             if (e) cudaEventDestroy(e);
-        cudaFree(dA); cudaFree(dP); cudaFree(dOff);
-        dA = nullptr; dP = nullptr; dOff = nullptr;
+        cudaFree(dA); cudaFree(dP); cudaFree(dOff); cudaFree(dReps); cudaFree(dMolOff);
+        dA = nullptr; dP = nullptr; dOff = nullptr; dReps = nullptr; dMolOff = nullptr;
     }
 };
 
@@ -310,7 +499,11 @@ extern "C" int fmd_batch_create(fmd_ctx* ctx, int R, fmd_system* const* systems,
     b->bd.kind = FMD_SYS_MM;
     b->bd.ff = FMD_FF_MM;
     b->bd.precision = b->sys[0]->arr.precision;
-    int rc = autotune ? b->autotune() : b->set_offsets(b->tune);
+    int rc = b->pending("before the batch set-up");
+    if (!rc) rc = autotune ? b->autotune() : b->set_offsets(b->tune);
+    if (!rc) rc = b->pending("after the launch-shape set-up");
+    if (!rc) rc = b->setup_mol_batch();
+    if (!rc) rc = b->pending("after the rebuild tables");
     if (!rc) rc = b->capture_all();
     if (rc) { b->release(); delete b; return rc; }
     *out = b;
@@ -356,26 +549,13 @@ extern "C" int fmd_batch_get_tuning(fmd_batch* b, fmd_batch_tuning* t) {
 
 extern "C" int fmd_batch_step_kernels(fmd_batch* b, int rebuild, int phase, int* nk) {
     if (!b || !nk) return FMD_ERR_ARG;
-    fmd_ctx* ctx = b->ctx;
-    cudaStream_t st = ctx->stream;
-    cudaGraph_t graph;
-    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
-        return ctx->fail(FMD_ERR_CUDA, "capture failed");
-    cudaError_t e = b->enqueue_variant(rebuild != 0, phase != 0, st);
-    cudaError_t e2 = cudaStreamEndCapture(st, &graph);
-    if (e != cudaSuccess || e2 != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "capture failed");
-    size_t n = 0;
-    cudaGraphGetNodes(graph, nullptr, &n);
-    std::vector<cudaGraphNode_t> nodes(n);
-    cudaGraphGetNodes(graph, nodes.data(), &n);
-    int k = 0;
-    for (auto& nd : nodes) {
-        cudaGraphNodeType t;
-        cudaGraphNodeGetType(nd, &t);
-        if (t == cudaGraphNodeTypeKernel) k++;
-    }
-    cudaGraphDestroy(graph);
-    *nk = k;
+    *nk = b->nkern[rebuild ? 1 : 0][phase ? 1 : 0];
+    return FMD_OK;
+}
+
+extern "C" int fmd_batch_step_kernels_conditional(fmd_batch* b, int rebuild, int phase, int* nk) {
+    if (!b || !nk) return FMD_ERR_ARG;
+    *nk = b->nkern_cond[rebuild ? 1 : 0][phase ? 1 : 0];
     return FMD_OK;
 }
 

@@ -173,6 +173,18 @@ struct MMTopoDev {
     int physical;                 // 1: bond and angle forces as -grad E (FMD_PHYS_MM_BONDED)
 };
 constexpr int kMMNV = 7;
+// Writable view of a system's topology arrays (the replication's output).
+struct MMTopoOut {
+    int *b_i0, *b_i1; double *b_kb, *b_r0;
+    int *a_i0, *a_i1, *a_i2; double *a_kth, *a_th0;
+    int *d_i0, *d_i1, *d_i2, *d_i3; double* d_vn; int* d_mult; double* d_gamma;
+    int *m_i0, *m_i1, *m_i2, *m_i3; double *m_ki, *m_gamma;
+};
+// The flat topology of nmol copies of one molecule of `natom` atoms (the
+// replication of build_flat_topology, MM:254-334): term k of copy m is the
+// molecule's term k with every index offset by m natom, copies in order,
+// each term kind molecule-major.  `mol` holds one molecule's terms.
+cudaError_t mm_replicate_launch(const MMTopoDev& mol, int nmol, int natom, const MMTopoOut& out, cudaStream_t st);
 cudaError_t mm_bonded_launch(const MMTopoDev& t, const double* pos, const double* hh, double* Facc,
                              double* part, cudaStream_t st);
 // Cut Coulomb (a15), all pairs of different molecules: adds into Facc; {Ecoul} partials.

@@ -28,8 +28,6 @@
 namespace fmd {
 namespace {
 
-constexpr unsigned long long kPruneMark = 0x7F7F7F7F7F7F7F7Full;   // ~1.4e306 A: forces a prune
-
 __global__ void k_prune_mark(unsigned long long* words) { *words = kPruneMark; }
 
 }  // namespace

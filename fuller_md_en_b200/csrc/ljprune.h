@@ -24,6 +24,9 @@ struct LJPrune {
     unsigned long long* stats = nullptr;  // [2] {force evaluations, prune evaluations}
 };
 
+// Displacement bound that forces the next evaluation to prune (~1.4e306 A).
+constexpr unsigned long long kPruneMark = 0x7F7F7F7F7F7F7F7Full;
+
 // Clears the counters, snapshot and cell on st and marks the first
 // evaluation as a prune (the arrays are owned by the system; the row buffer
 // is written by that prune before any read).

@@ -15,6 +15,7 @@
 // Coulomb: all pairs of different molecules within 3 sigma, gathered per atom
 // through shared-memory tiles (no atomics); energy counted for j>i only.  The
 // reference runs it serially only when some charge is nonzero (MM:1110-1111).
+#include <algorithm>
 #include <cmath>
 #include "kernels.h"
 #include "geom.cuh"
@@ -205,7 +206,53 @@ k_coulomb(const double* __restrict__ pos, const double* __restrict__ hh, const d
     if (threadIdx.x == 0) part[blockIdx.x] = tot[0];
 }
 
+// One thread per output term, over [bonds | angles | dihedrals | impropers]
+// of all copies.
+__global__ void k_mm_replicate(MMTopoDev t, int nmol, int natom, MMTopoOut o) {
+    const long long nb = (long long)nmol * t.nb, na = (long long)nmol * t.nang, nd = (long long)nmol * t.ndih,
+                    ni = (long long)nmol * t.nimp;
+    const long long tot = nb + na + nd + ni;
+    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < tot;
+         x += (long long)gridDim.x * blockDim.x) {
+        long long y = x;
+        if (y < nb) {
+            const int m = (int)(y / t.nb), k = (int)(y - (long long)m * t.nb), off = m * natom;
+            o.b_i0[y] = t.b_i0[k] + off; o.b_i1[y] = t.b_i1[k] + off;
+            o.b_kb[y] = t.b_kb[k]; o.b_r0[y] = t.b_r0[k];
+            continue;
+        }
+        y -= nb;
+        if (y < na) {
+            const int m = (int)(y / t.nang), k = (int)(y - (long long)m * t.nang), off = m * natom;
+            o.a_i0[y] = t.a_i0[k] + off; o.a_i1[y] = t.a_i1[k] + off; o.a_i2[y] = t.a_i2[k] + off;
+            o.a_kth[y] = t.a_kth[k]; o.a_th0[y] = t.a_th0[k];
+            continue;
+        }
+        y -= na;
+        if (y < nd) {
+            const int m = (int)(y / t.ndih), k = (int)(y - (long long)m * t.ndih), off = m * natom;
+            o.d_i0[y] = t.d_i0[k] + off; o.d_i1[y] = t.d_i1[k] + off;
+            o.d_i2[y] = t.d_i2[k] + off; o.d_i3[y] = t.d_i3[k] + off;
+            o.d_vn[y] = t.d_vn[k]; o.d_mult[y] = t.d_mult[k]; o.d_gamma[y] = t.d_gamma[k];
+            continue;
+        }
+        y -= nd;
+        const int m = (int)(y / t.nimp), k = (int)(y - (long long)m * t.nimp), off = m * natom;
+        o.m_i0[y] = t.m_i0[k] + off; o.m_i1[y] = t.m_i1[k] + off;
+        o.m_i2[y] = t.m_i2[k] + off; o.m_i3[y] = t.m_i3[k] + off;
+        o.m_ki[y] = t.m_ki[k]; o.m_gamma[y] = t.m_gamma[k];
+    }
+}
+
 }  // namespace
+
+cudaError_t mm_replicate_launch(const MMTopoDev& mol, int nmol, int natom, const MMTopoOut& out, cudaStream_t st) {
+    const long long tot = (long long)nmol * ((long long)mol.nb + mol.nang + mol.ndih + mol.nimp);
+    if (tot <= 0) return cudaSuccess;
+    const int blocks = (int)std::min<long long>((tot + 255) / 256, kSMs * 16);
+    k_mm_replicate<<<blocks, 256, 0, st>>>(mol, nmol, natom, out);
+    return cudaGetLastError();
+}
 
 cudaError_t mm_bonded_launch(const MMTopoDev& t, const double* pos, const double* hh, double* Facc,
                              double* part, cudaStream_t st) {

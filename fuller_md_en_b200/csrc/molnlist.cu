@@ -26,6 +26,7 @@
 
 #include "geom.cuh"
 #include "kernels.h"
+#include "ljprune.h"
 #include "molnlist.h"
 
 namespace fmd {
@@ -67,14 +68,15 @@ __device__ __forceinline__ bool pair_in(const double* __restrict__ pos, int i, i
 // (largest minimum-image distance of an atom from the centre) per molecule,
 // and the FP32 copy of the positions; one warp per molecule.  Resets the
 // partner-overflow flag.
-__global__ void k_mol_centre(const double* __restrict__ pos, const double* __restrict__ hh,
-                             const int* __restrict__ off, int M, double* __restrict__ cen, double* __restrict__ rad,
-                             float4* __restrict__ pos32, int* __restrict__ flag) {
+__device__ __forceinline__ void mol_centre_body(const double* __restrict__ pos, const double* __restrict__ hh,
+                                                const int* __restrict__ off, int M, double* __restrict__ cen,
+                                                double* __restrict__ rad, float4* __restrict__ pos32,
+                                                int* __restrict__ flag, int blk) {
     const double* h = hh;
     const double* hi = hh + 9;
     const int lane = threadIdx.x & 31;
-    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (blockIdx.x == 0 && threadIdx.x == 0) flag[1] = 0;
+    const int w = (blk * blockDim.x + threadIdx.x) >> 5;
+    if (blk == 0 && threadIdx.x == 0) flag[1] = 0;
     if (w >= M) return;
     const int a0 = off[w], a1 = off[w + 1];
     double sx = 0.0, sy = 0.0, sz = 0.0;
@@ -103,16 +105,23 @@ __global__ void k_mol_centre(const double* __restrict__ pos, const double* __res
     }
 }
 
+__global__ void k_mol_centre(const double* __restrict__ pos, const double* __restrict__ hh,
+                             const int* __restrict__ off, int M, double* __restrict__ cen, double* __restrict__ rad,
+                             float4* __restrict__ pos32, int* __restrict__ flag) {
+    mol_centre_body(pos, hh, off, M, cen, rad, pos32, flag, blockIdx.x);
+}
+
 // Partner molecules of each molecule (both directions, ascending); one warp
 // per molecule.  flag[0] = 1 when the molecule path is valid for this
 // rebuild (diagonal cell, no table overflow), else 0.
-__global__ void k_mol_pairs(const double* __restrict__ hh, int M, const double* __restrict__ cen,
-                            const double* __restrict__ rad, double rc, int pmax, int* __restrict__ npart,
-                            int* __restrict__ part, int* __restrict__ flag) {
+__device__ __forceinline__ void mol_pairs_body(const double* __restrict__ hh, int M, const double* __restrict__ cen,
+                                               const double* __restrict__ rad, double rc, int pmax,
+                                               int* __restrict__ npart, int* __restrict__ part,
+                                               int* __restrict__ flag, int blk) {
     const double* h = hh;
     const double* hi = hh + 9;
     const int lane = threadIdx.x & 31;
-    const int A = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int A = (blk * blockDim.x + threadIdx.x) >> 5;
     if (A >= M) return;
     const double cx = cen[3 * A], cy = cen[3 * A + 1], cz = cen[3 * A + 2], ra = rad[A];
     int n = 0;
@@ -134,6 +143,12 @@ __global__ void k_mol_pairs(const double* __restrict__ hh, int M, const double* 
         npart[A] = n < pmax ? n : pmax;
         if (n > pmax) atomicOr(&flag[1], 1);
     }
+}
+
+__global__ void k_mol_pairs(const double* __restrict__ hh, int M, const double* __restrict__ cen,
+                            const double* __restrict__ rad, double rc, int pmax, int* __restrict__ npart,
+                            int* __restrict__ part, int* __restrict__ flag) {
+    mol_pairs_body(hh, M, cen, rad, rc, pmax, npart, part, flag, blockIdx.x);
 }
 
 __global__ void k_mol_decide(const double* __restrict__ hh, int* __restrict__ flag) {
@@ -257,12 +272,13 @@ constexpr int kFlatU = 4;
 constexpr int kFlatWarps = 8;
 
 template <bool PAIRED>
-__global__ void __launch_bounds__(32 * kFlatWarps, 3)
-k_mol_half_flat(const double* __restrict__ pos, const double* __restrict__ hh, int n, const int* __restrict__ off,
-                const int* __restrict__ amol, const int* __restrict__ npart, const int* __restrict__ part, int pmax,
-                int S, const float4* __restrict__ pos32, double rc2, int cap, int* __restrict__ cnt,
-                int* __restrict__ list, int* __restrict__ dropped, const int* __restrict__ flag,
-                unsigned* __restrict__ bm) {
+__device__ __forceinline__ void mol_half_flat_body(const double* __restrict__ pos, const double* __restrict__ hh,
+                                                   int n, const int* __restrict__ off, const int* __restrict__ amol,
+                                                   const int* __restrict__ npart, const int* __restrict__ part,
+                                                   int pmax, int S, const float4* __restrict__ pos32, double rc2,
+                                                   int cap, int* __restrict__ cnt, int* __restrict__ list,
+                                                   int* __restrict__ dropped, const int* __restrict__ flag,
+                                                   unsigned* __restrict__ bm, int blk, int nblk) {
     if (flag[0] == 0) return;
     __shared__ double s_hh[18];
     __shared__ int s_start[kFlatWarps][kMolPartners];
@@ -276,7 +292,7 @@ k_mol_half_flat(const double* __restrict__ pos, const double* __restrict__ hh, i
     const unsigned below = (1u << lane) - 1u;
     int* st = s_start[w];
     const float invS = 1.0f / (float)S;
-    for (int i = blockIdx.x * kFlatWarps + w; i < n; i += gridDim.x * kFlatWarps) {
+    for (int i = blk * kFlatWarps + w; i < n; i += nblk * kFlatWarps) {
         const int A = amol[i];
         const int np = npart[A];
         const int* pa = part + (size_t)A * pmax;
@@ -354,6 +370,17 @@ k_mol_half_flat(const double* __restrict__ pos, const double* __restrict__ hh, i
     }
 }
 
+template <bool PAIRED>
+__global__ void __launch_bounds__(32 * kFlatWarps, 3)
+k_mol_half_flat(const double* __restrict__ pos, const double* __restrict__ hh, int n, const int* __restrict__ off,
+                const int* __restrict__ amol, const int* __restrict__ npart, const int* __restrict__ part, int pmax,
+                int S, const float4* __restrict__ pos32, double rc2, int cap, int* __restrict__ cnt,
+                int* __restrict__ list, int* __restrict__ dropped, const int* __restrict__ flag,
+                unsigned* __restrict__ bm) {
+    mol_half_flat_body<PAIRED>(pos, hh, n, off, amol, npart, part, pmax, S, pos32, rc2, cap, cnt, list, dropped, flag,
+                               bm, blockIdx.x, gridDim.x);
+}
+
 // First index of a partner >= key in an ascending partner list.
 __device__ __forceinline__ int lower_bound_part(const int* pa, int n, int key) {
     int lo = 0, hi = n;
@@ -371,11 +398,11 @@ __device__ __forceinline__ int lower_bound_part(const int* pa, int n, int key) {
 // (the pair test is odd in the centre difference and symmetric in the radii);
 // should B be missing all the same, the molecule builder is switched off for
 // this build (flag[0] = 0) and the cell-list path builds.
-__global__ void k_mol_rev(int M, const int* __restrict__ npart, const int* __restrict__ part, int pmax,
-                          int* __restrict__ rev, int* __restrict__ flag) {
+__device__ __forceinline__ void mol_rev_body(int M, const int* __restrict__ npart, const int* __restrict__ part,
+                                             int pmax, int* __restrict__ rev, int* __restrict__ flag, int blk) {
     if (flag[0] == 0) return;
     const int lane = threadIdx.x & 31;
-    const int B = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int B = (blk * blockDim.x + threadIdx.x) >> 5;
     if (B >= M) return;
     const int nb = npart[B];
     for (int q = lane; q < nb; q += 32) {
@@ -387,6 +414,11 @@ __global__ void k_mol_rev(int M, const int* __restrict__ npart, const int* __res
         rev[(size_t)B * pmax + q] = at - lower_bound_part(pa, na, A);
         if (at >= na || pa[at] != B) atomicExch(&flag[0], 0);
     }
+}
+
+__global__ void k_mol_rev(int M, const int* __restrict__ npart, const int* __restrict__ part, int pmax,
+                          int* __restrict__ rev, int* __restrict__ flag) {
+    mol_rev_body(M, npart, part, pmax, rev, flag, blockIdx.x);
 }
 
 // Full LJ rows from the candidate bitmaps of the partner-aligned walk
@@ -405,11 +437,12 @@ constexpr int kInChunk = 32;
 constexpr int kInWarps = 8;
 constexpr int kInAtoms = 32 / kInWarps;               // atoms per warp
 
-__global__ void __launch_bounds__(32 * kInWarps)
-k_mol_incoming(int M, int S, const int* __restrict__ npart, const int* __restrict__ part, int pmax,
-               const int* __restrict__ rev, int W, const unsigned* __restrict__ bm, int cap,
-               const int* __restrict__ cnt, const int* __restrict__ list, int* __restrict__ in_cnt,
-               int* __restrict__ in_list, int in_cap, DevErr* err, const int* __restrict__ flag) {
+__device__ __forceinline__ void mol_incoming_body(int M, int S, const int* __restrict__ npart,
+                                                  const int* __restrict__ part, int pmax, const int* __restrict__ rev,
+                                                  int W, const unsigned* __restrict__ bm, int cap,
+                                                  const int* __restrict__ cnt, const int* __restrict__ list,
+                                                  int* __restrict__ in_cnt, int* __restrict__ in_list, int in_cap,
+                                                  DevErr* err, const int* __restrict__ flag, int blk, int nblk) {
     if (flag[0] == 0) return;
     __shared__ int s_a[kMolPartners];                 // lower partners, ascending
     __shared__ int s_b[kMolPartners];                 // bitmap word of the half's atoms
@@ -417,7 +450,7 @@ k_mol_incoming(int M, int S, const int* __restrict__ npart, const int* __restric
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned below = (1u << lane) - 1u;
     const int lim = in_cap - cap;
-    for (int g = blockIdx.x; g < 2 * M; g += gridDim.x) {
+    for (int g = blk; g < 2 * M; g += nblk) {
         const int B = g >> 1, h0 = (g & 1) * 32;
         const int nh = S - h0 < 32 ? S - h0 : 32;    // atoms in this half (0 when S = 32, h0 = 32)
         if (nh <= 0) continue;
@@ -506,8 +539,120 @@ k_mol_incoming(int M, int S, const int* __restrict__ npart, const int* __restric
     }
 }
 
+__global__ void __launch_bounds__(32 * kInWarps)
+k_mol_incoming(int M, int S, const int* __restrict__ npart, const int* __restrict__ part, int pmax,
+               const int* __restrict__ rev, int W, const unsigned* __restrict__ bm, int cap,
+               const int* __restrict__ cnt, const int* __restrict__ list, int* __restrict__ in_cnt,
+               int* __restrict__ in_list, int in_cap, DevErr* err, const int* __restrict__ flag) {
+    mol_incoming_body(M, S, npart, part, pmax, rev, W, bm, cap, cnt, list, in_cnt, in_list, in_cap, err, flag,
+                      blockIdx.x, gridDim.x);
+}
+
 constexpr int kRowBlocksMol = kSMs * 8;
 
+// ------------------------------------------------------- replica batches --
+// Block b of a batched launch serves replica r (off[r] <= b < off[r + 1]) as
+// its local block b - off[r] of off[r + 1] - off[r].
+__device__ __forceinline__ int rep_of(const int* __restrict__ off, int R, int b) {
+    int lo = 0, hi = R - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= b) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Per replica: h^-1 (as inv9_launch) and the pruned rows marked stale (as
+// lj_prune_mark after a build).
+__global__ void k_b_inv9(const MolRep* __restrict__ reps, int R) {
+    for (int r = threadIdx.x; r < R; r += blockDim.x) {
+        inv9(reps[r].hh, reps[r].hh + 9);
+        if (reps[r].prune_words) *reps[r].prune_words = kPruneMark;
+    }
+}
+
+__global__ void k_b_mol_centre(const MolRep* __restrict__ reps, const int* __restrict__ off, int R) {
+    const int r = rep_of(off, R, blockIdx.x);
+    const MolRep& q = reps[r];
+    mol_centre_body(q.pos, q.hh, q.m.off, q.m.M, q.m.cen, q.m.rad, q.m.pos32, q.m.flag, blockIdx.x - off[r]);
+}
+
+__global__ void k_b_mol_pairs(const MolRep* __restrict__ reps, const int* __restrict__ off, int R) {
+    const int r = rep_of(off, R, blockIdx.x);
+    const MolRep& q = reps[r];
+    mol_pairs_body(q.hh, q.m.M, q.m.cen, q.m.rad, q.rc, q.m.pmax, q.m.npart, q.m.part, q.m.flag, blockIdx.x - off[r]);
+}
+
+__global__ void k_b_mol_decide(const MolRep* __restrict__ reps, int R) {
+    for (int r = threadIdx.x; r < R; r += blockDim.x) {
+        const double* hh = reps[r].hh;
+        int* flag = reps[r].m.flag;
+        flag[0] = (diag_cell(hh, hh + 9) && flag[1] == 0) ? 1 : 0;
+    }
+}
+
+__global__ void k_b_mol_rev(const MolRep* __restrict__ reps, const int* __restrict__ off, int R) {
+    const int r = rep_of(off, R, blockIdx.x);
+    const MolRep& q = reps[r];
+    mol_rev_body(q.m.M, q.m.npart, q.m.part, q.m.pmax, q.m.rev, q.m.flag, blockIdx.x - off[r]);
+}
+
+// Sets the fallback's conditional when some replica's molecule path was
+// rejected (by the decision or the partner-symmetry check).
+__global__ void k_b_mol_cond(const MolRep* __restrict__ reps, int R, cudaGraphConditionalHandle cond) {
+    int need = 0;
+    for (int r = threadIdx.x; r < R; r += blockDim.x) need |= reps[r].m.flag[0] == 0;
+    if (__syncthreads_or(need) && threadIdx.x == 0) cudaGraphSetConditional(cond, 1u);
+}
+
+__global__ void __launch_bounds__(32 * kFlatWarps, 3)
+k_b_mol_half_flat(const MolRep* __restrict__ reps, const int* __restrict__ off, int R) {
+    const int r = rep_of(off, R, blockIdx.x);
+    const MolRep& q = reps[r];
+    mol_half_flat_body<true>(q.pos, q.hh, q.m.n, q.m.off, q.m.amol, q.m.npart, q.m.part, q.m.pmax, q.m.usize,
+                             q.m.pos32, q.rc2, q.cap, q.cnt, q.list, q.dropped, q.m.flag, q.m.bm,
+                             blockIdx.x - off[r], off[r + 1] - off[r]);
+}
+
+__global__ void __launch_bounds__(32 * kInWarps)
+k_b_mol_incoming(const MolRep* __restrict__ reps, const int* __restrict__ off, int R) {
+    const int r = rep_of(off, R, blockIdx.x);
+    const MolRep& q = reps[r];
+    mol_incoming_body(q.m.M, q.m.usize, q.m.npart, q.m.part, q.m.pmax, q.m.rev, q.m.words, q.m.bm, q.cap, q.cnt,
+                      q.list, q.in_cnt, q.in_list, q.in_cap, q.err, q.m.flag, blockIdx.x - off[r],
+                      off[r + 1] - off[r]);
+}
+
+}  // namespace
+
+cudaError_t mol_rebuild_batch_pre(const MolBatch& b, cudaGraphConditionalHandle cond, cudaStream_t st,
+                                  const char** stage) {
+    if (b.R < 1) return cudaSuccess;
+    cudaError_t e;
+#define FMD_MB_STEP(NAME, LAUNCH)                              \
+    do {                                                       \
+        if (stage) *stage = NAME;                              \
+        LAUNCH;                                                \
+        if ((e = cudaGetLastError()) != cudaSuccess) return e; \
+    } while (0)
+    FMD_MB_STEP("k_b_inv9", (k_b_inv9<<<1, 256, 0, st>>>(b.reps, b.R)));
+    FMD_MB_STEP("k_b_mol_centre", (k_b_mol_centre<<<b.nblk_w, 256, 0, st>>>(b.reps, b.off_w, b.R)));
+    FMD_MB_STEP("k_b_mol_pairs", (k_b_mol_pairs<<<b.nblk_w, 256, 0, st>>>(b.reps, b.off_w, b.R)));
+    FMD_MB_STEP("k_b_mol_decide", (k_b_mol_decide<<<1, 256, 0, st>>>(b.reps, b.R)));
+    FMD_MB_STEP("k_b_mol_rev", (k_b_mol_rev<<<b.nblk_w, 256, 0, st>>>(b.reps, b.off_w, b.R)));
+    FMD_MB_STEP("k_b_mol_cond", (k_b_mol_cond<<<1, 256, 0, st>>>(b.reps, b.R, cond)));
+#undef FMD_MB_STEP
+    return cudaSuccess;
+}
+
+cudaError_t mol_rebuild_batch_rows(const MolBatch& b, cudaStream_t st) {
+    if (b.R < 1) return cudaSuccess;
+    k_b_mol_half_flat<<<b.nblk_rows, 32 * kFlatWarps, 0, st>>>(b.reps, b.off_rows, b.R);
+    k_b_mol_incoming<<<b.nblk_in, 32 * kInWarps, 0, st>>>(b.reps, b.off_in, b.R);
+    return cudaGetLastError();
+}
+
+namespace {
 }  // namespace
 
 cudaError_t mol_lists_alloc(MolLists& m, int n, const int* mol_id_host, const DevAlloc& da) {

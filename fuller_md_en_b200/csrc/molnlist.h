@@ -51,4 +51,41 @@ cudaError_t mol_rows_half(const MolLists& m, const double* pos, const double* hh
 cudaError_t mol_rows_incoming(const MolLists& m, int cap, const int* cnt, const int* list, int* in_cnt,
                               int* in_list, int in_cap, DevErr* err, cudaStream_t st);
 
+// One replica of a batched molecule-path rebuild (replica batches of MM
+// systems, batch.cu): its molecule tables and the lists it builds.
+struct MolRep {
+    MolLists m;
+    const double* pos = nullptr;
+    double* hh = nullptr;                 // h then h^-1 (h^-1 recomputed first)
+    double rc = 0.0, rc2 = 0.0;           // list radius, squared
+    int cap = 0, in_cap = 0;
+    int* cnt = nullptr;
+    int* list = nullptr;
+    int* dropped = nullptr;
+    int* in_cnt = nullptr;
+    int* in_list = nullptr;
+    DevErr* err = nullptr;
+    unsigned long long* prune_words = nullptr;   // the replica's pruned-row bound (marked stale), or null
+};
+// Device table of the replicas and the block offsets (R + 1 each) of the
+// batched launches: warp-per-molecule kernels, half rows, full rows.
+struct MolBatch {
+    const MolRep* reps = nullptr;
+    int R = 0;
+    const int* off_w = nullptr;
+    const int* off_rows = nullptr;
+    const int* off_in = nullptr;
+    int nblk_w = 0, nblk_rows = 0, nblk_in = 0;
+};
+// The molecule-path rebuild of every replica of a batch, one launch per
+// phase, for equal molecules of 32-64 atoms (the candidate-bitmap path).
+// First part: h^-1, centres and radii, partner tables and the path decision
+// of each replica; `cond` (a conditional node's handle in the graph being
+// captured) is set to 1 when some replica's molecule path is rejected for
+// this build, whose cell-grid fallback the caller places next.  Second part:
+// the half rows and the gather's full rows of every accepted replica.
+cudaError_t mol_rebuild_batch_pre(const MolBatch& b, cudaGraphConditionalHandle cond, cudaStream_t st,
+                                  const char** stage = nullptr);
+cudaError_t mol_rebuild_batch_rows(const MolBatch& b, cudaStream_t st);
+
 }  // namespace fmd

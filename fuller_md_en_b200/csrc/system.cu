@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstddef>
 #include <cstring>
+#include <vector>
 #include <cstdio>
 #include <cstdlib>
 #include <map>
@@ -215,6 +216,21 @@ cudaError_t System::enqueue_rebuild(cudaStream_t st) {
     }
     if (prune.ok) return lj_prune_mark(prune, st);     // new rows: the next evaluation prunes them
     return cudaSuccess;
+}
+
+cudaError_t System::enqueue_rebuild_fallback(cudaStream_t st) {
+    if (!(mol.ok && mol.masks) || arr.kind == FMD_SYS_RIGID) return cudaErrorInvalidValue;
+    double* hh = arr.S->h;
+    int* cnt_a = const_cast<int*>(arr.cnt_a);
+    int* list_a = const_cast<int*>(arr.list_a);
+    const int* gate = mol.flag;
+    cudaError_t e;
+    if ((e = cells_build(cells_a, arr.pos, arr.n, hh, rc_a, ctx->d_err, st, arr.mol_id, gate)) != cudaSuccess) return e;
+    if ((e = nlist_build(cells_a, LIST_HALF, arr.pos, arr.mol_id, arr.n, hh, rc2_a, arr.cap_a, cnt_a, list_a,
+                         dropped, ctx->d_err, st, gate)) != cudaSuccess)
+        return e;
+    return nlist_transpose(arr.cnt_a, arr.list_a, arr.cap_a, arr.n, const_cast<int*>(arr.in_cnt),
+                           const_cast<int*>(arr.in_list), arr.in_cap, ctx->d_err, st, gate);
 }
 
 // Launch shape of the atomistic LJ gather: every candidate (threads per
@@ -566,12 +582,13 @@ extern "C" int fmd_system_create_airebo(fmd_ctx* ctx, const fmd_run_params* p, i
     return FMD_OK;
 }
 
-extern "C" int fmd_system_create_mm(fmd_ctx* ctx, const fmd_run_params* p, int na, const double* pos,
-                                    const double* vel, const int* mol_id, const fmd_mm_topology* t,
-                                    const double* charge, const double* h, const fmd_npt* npt,
-                                    fmd_system** out) {
-    if (!ctx || !p || !out || !pos || !vel || !mol_id || !t || !h || !npt || na < 2)
-        return ctx ? ctx->fail(FMD_ERR_ARG, "fmd_system_create_mm: bad argument") : FMD_ERR_ARG;
+namespace {
+// An MM system; its topology comes from the full flat topology t, or when t
+// is null from one molecule's topology t1 replicated over nmol molecules of
+// natom_mol atoms on the device.
+int create_mm(fmd_ctx* ctx, const fmd_run_params* p, int na, const double* pos, const double* vel,
+              const int* mol_id, const fmd_mm_topology* t, const fmd_mm_topology* t1, int nmol, int natom_mol,
+              const double* charge, const double* h, const fmd_npt* npt, fmd_system** out) {
     auto s = std::make_unique<fmd::System>();
     s->ctx = ctx;
     if (make_params(p, *s) != FMD_OK) return ctx->fail(FMD_ERR_ARG, "bad run parameters");
@@ -584,7 +601,7 @@ extern "C" int fmd_system_create_mm(fmd_ctx* ctx, const fmd_run_params* p, int n
     int* mid;
     if (s->alloc(&mid, na, mol_id)) return ctx->fail(FMD_ERR_CUDA, "device allocation failed");
     s->arr.mol_id = mid;
-    if ((rc = s->upload_topology(t)) != FMD_OK) return rc;
+    if ((rc = t ? s->upload_topology(t) : s->replicate_topology(t1, nmol, natom_mol)) != FMD_OK) return rc;
     bool has_charge = false;
     if (charge)
         for (int i = 0; i < na && !has_charge; i++) has_charge = std::fabs(charge[i]) > 1e-10;   // MM:1110
@@ -601,6 +618,71 @@ extern "C" int fmd_system_create_mm(fmd_ctx* ctx, const fmd_run_params* p, int n
     out[0] = new fmd_system{std::move(s)};
     return FMD_OK;
 }
+}  // namespace
+
+extern "C" int fmd_system_create_mm(fmd_ctx* ctx, const fmd_run_params* p, int na, const double* pos,
+                                    const double* vel, const int* mol_id, const fmd_mm_topology* t,
+                                    const double* charge, const double* h, const fmd_npt* npt,
+                                    fmd_system** out) {
+    if (!ctx || !p || !out || !pos || !vel || !mol_id || !t || !h || !npt || na < 2)
+        return ctx ? ctx->fail(FMD_ERR_ARG, "fmd_system_create_mm: bad argument") : FMD_ERR_ARG;
+    return create_mm(ctx, p, na, pos, vel, mol_id, t, nullptr, 0, 0, charge, h, npt, out);
+}
+
+extern "C" int fmd_system_create_mm_replicated(fmd_ctx* ctx, const fmd_run_params* p, int nmol, int natom_mol,
+                                               const double* pos, const double* vel, const fmd_mm_topology* t1,
+                                               const double* h, const fmd_npt* npt, fmd_system** out) {
+    if (!ctx || !p || !out || !pos || !vel || !t1 || !h || !npt || nmol < 1 || natom_mol < 1 ||
+        (long long)nmol * natom_mol < 2 || (long long)nmol * natom_mol > (1LL << 30))
+        return ctx ? ctx->fail(FMD_ERR_ARG, "fmd_system_create_mm_replicated: bad argument") : FMD_ERR_ARG;
+    const int na = nmol * natom_mol;
+    std::vector<int> mol_id((size_t)na);
+    for (int i = 0; i < na; i++) mol_id[i] = i / natom_mol;     // contiguous molecules, 0-based
+    return create_mm(ctx, p, na, pos, vel, mol_id.data(), nullptr, t1, nmol, natom_mol, nullptr, h, npt, out);
+}
+
+int fmd::System::replicate_topology(const fmd_mm_topology* t, int nmol, int natom) {
+    // One molecule's indices address its own atoms: check them on the host.
+    auto ok = [&](const int* a, int m) {
+        if (m > 0 && !a) return false;
+        for (int k = 0; k < m; k++)
+            if (a[k] < 0 || a[k] >= natom) return false;
+        return true;
+    };
+    if (t->nb < 0 || t->nang < 0 || t->ndih < 0 || t->nimp < 0 || !ok(t->b_i0, t->nb) || !ok(t->b_i1, t->nb) ||
+        !ok(t->ang_i0, t->nang) || !ok(t->ang_i1, t->nang) || !ok(t->ang_i2, t->nang) ||
+        !ok(t->dih_i0, t->ndih) || !ok(t->dih_i1, t->ndih) || !ok(t->dih_i2, t->ndih) || !ok(t->dih_i3, t->ndih) ||
+        !ok(t->imp_i0, t->nimp) || !ok(t->imp_i1, t->nimp) || !ok(t->imp_i2, t->nimp) || !ok(t->imp_i3, t->nimp))
+        return ctx->fail(FMD_ERR_ARG, "MM molecule topology: index out of range");
+    if (upload_topology_arrays(t) != FMD_OK) return FMD_ERR_CUDA;   // the molecule's terms
+    const MMTopoDev mol = arr.topo;
+    MMTopoOut o{};
+    const size_t nb = (size_t)nmol * t->nb, na = (size_t)nmol * t->nang, nd = (size_t)nmol * t->ndih,
+                 ni = (size_t)nmol * t->nimp;
+    if (alloc(&o.b_i0, nb, (const int*)nullptr) || alloc(&o.b_i1, nb, (const int*)nullptr) ||
+        alloc(&o.b_kb, nb, (const double*)nullptr) || alloc(&o.b_r0, nb, (const double*)nullptr) ||
+        alloc(&o.a_i0, na, (const int*)nullptr) || alloc(&o.a_i1, na, (const int*)nullptr) ||
+        alloc(&o.a_i2, na, (const int*)nullptr) || alloc(&o.a_kth, na, (const double*)nullptr) ||
+        alloc(&o.a_th0, na, (const double*)nullptr) || alloc(&o.d_i0, nd, (const int*)nullptr) ||
+        alloc(&o.d_i1, nd, (const int*)nullptr) || alloc(&o.d_i2, nd, (const int*)nullptr) ||
+        alloc(&o.d_i3, nd, (const int*)nullptr) || alloc(&o.d_vn, nd, (const double*)nullptr) ||
+        alloc(&o.d_mult, nd, (const int*)nullptr) || alloc(&o.d_gamma, nd, (const double*)nullptr) ||
+        alloc(&o.m_i0, ni, (const int*)nullptr) || alloc(&o.m_i1, ni, (const int*)nullptr) ||
+        alloc(&o.m_i2, ni, (const int*)nullptr) || alloc(&o.m_i3, ni, (const int*)nullptr) ||
+        alloc(&o.m_ki, ni, (const double*)nullptr) || alloc(&o.m_gamma, ni, (const double*)nullptr))
+        return ctx->fail(FMD_ERR_CUDA, "topology allocation failed");
+    if (mm_replicate_launch(mol, nmol, natom, o, ctx->stream) != cudaSuccess)
+        return ctx->fail(FMD_ERR_CUDA, "topology replication failed");
+    MMTopoDev d{};
+    d.nb = (int)nb; d.nang = (int)na; d.ndih = (int)nd; d.nimp = (int)ni;
+    d.b_i0 = o.b_i0; d.b_i1 = o.b_i1; d.b_kb = o.b_kb; d.b_r0 = o.b_r0;
+    d.a_i0 = o.a_i0; d.a_i1 = o.a_i1; d.a_i2 = o.a_i2; d.a_kth = o.a_kth; d.a_th0 = o.a_th0;
+    d.d_i0 = o.d_i0; d.d_i1 = o.d_i1; d.d_i2 = o.d_i2; d.d_i3 = o.d_i3; d.d_vn = o.d_vn; d.d_mult = o.d_mult;
+    d.d_gamma = o.d_gamma;
+    d.m_i0 = o.m_i0; d.m_i1 = o.m_i1; d.m_i2 = o.m_i2; d.m_i3 = o.m_i3; d.m_ki = o.m_ki; d.m_gamma = o.m_gamma;
+    arr.topo = d;
+    return ctx->sync_check("topology replication");
+}
 
 int fmd::System::upload_topology(const fmd_mm_topology* t) {
     // Topology indices address device arrays: check them before any launch.
@@ -615,6 +697,12 @@ int fmd::System::upload_topology(const fmd_mm_topology* t) {
         !ok(t->dih_i0, t->ndih) || !ok(t->dih_i1, t->ndih) || !ok(t->dih_i2, t->ndih) || !ok(t->dih_i3, t->ndih) ||
         !ok(t->imp_i0, t->nimp) || !ok(t->imp_i1, t->nimp) || !ok(t->imp_i2, t->nimp) || !ok(t->imp_i3, t->nimp))
         return ctx->fail(FMD_ERR_ARG, "MM topology: index out of range");
+    return upload_topology_arrays(t);
+}
+
+// Copies the topology arrays of t to the device as the system's topology
+// (indices already checked).
+int fmd::System::upload_topology_arrays(const fmd_mm_topology* t) {
     MMTopoDev d{};
     d.nb = t->nb; d.nang = t->nang; d.ndih = t->ndih; d.nimp = t->nimp;
     int *i0, *i1, *i2, *i3, *mult;
@@ -914,16 +1002,17 @@ extern "C" int fmd_system_step_kernels(fmd_system* s, int rebuild, int phase, in
     cudaError_t e2 = cudaStreamEndCapture(st, &graph);
     if (e != cudaSuccess || e2 != cudaSuccess) return y.ctx->fail(FMD_ERR_CUDA, "capture failed");
     size_t n = 0;
-    cudaGraphGetNodes(graph, nullptr, &n);
-    std::vector<cudaGraphNode_t> nodes(n);
-    cudaGraphGetNodes(graph, nodes.data(), &n);
     int k = 0;
-    for (auto& nd : nodes) {
-        cudaGraphNodeType t;
-        cudaGraphNodeGetType(nd, &t);
-        if (t == cudaGraphNodeTypeKernel) k++;
+    if (cudaGraphGetNodes(graph, nullptr, &n) == cudaSuccess) {
+        std::vector<cudaGraphNode_t> nodes(n);
+        if (n && cudaGraphGetNodes(graph, nodes.data(), &n) != cudaSuccess) n = 0;
+        for (size_t q = 0; q < n; q++) {
+            cudaGraphNodeType t = cudaGraphNodeTypeEmpty;
+            if (cudaGraphNodeGetType(nodes[q], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) k++;
+        }
     }
     cudaGraphDestroy(graph);
+    cudaGetLastError();          // a failed graph query leaves no error for the next launch check
     *nk = k;
     return FMD_OK;
 }

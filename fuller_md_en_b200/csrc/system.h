@@ -38,7 +38,16 @@ struct System {
     int alloc_lists(double rc_list_a, int cap_a, double rc_list_b, int cap_b, bool transpose);
     int alloc_prune(double rc_lj);
     int upload_topology(const fmd_mm_topology* t);
+    int upload_topology_arrays(const fmd_mm_topology* t);
+    // One molecule's topology t (indices within the molecule) replicated on
+    // the device over nmol contiguous molecules of natom atoms.
+    int replicate_topology(const fmd_mm_topology* t, int nmol, int natom);
     cudaError_t enqueue_rebuild(cudaStream_t st);
+    // The cell-grid half rows and their transpose, gated off on the device
+    // when the molecule path built this rebuild (the fallback part of
+    // enqueue_rebuild for systems whose full rows come from the candidate
+    // bitmaps; replica batches run it inside a conditional graph node).
+    cudaError_t enqueue_rebuild_fallback(cudaStream_t st);
     cudaError_t enqueue_variant(bool rebuild, bool phase, cudaStream_t st, bool judge = false);
     cudaError_t enqueue_one(int g, cudaStream_t st);
     bool judge_step(int g) const { return arr.sg && arr.sg->judge_every > 0 && g % arr.sg->judge_every == 0; }

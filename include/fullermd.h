@@ -234,6 +234,16 @@ int fmd_system_create_mm(fmd_ctx *ctx, const fmd_run_params *p, int na, const do
                          const double *vel, const int *mol_id, const fmd_mm_topology *t,
                          const double *charge, const double *h, const fmd_npt *npt,
                          fmd_system **out);
+/* MM system of nmol molecules of natom_mol atoms each (atoms of molecule m
+ * at m*natom_mol .. (m+1)*natom_mol-1), no charges (the reference's are all
+ * zero, MM:1098-1111), built from ONE molecule's topology t1 (indices
+ * 0..natom_mol-1): the copies of build_flat_topology's replication
+ * (MM:254-334) are made on the device, term k of molecule m being t1's term
+ * k with every index offset by m*natom_mol, each term kind molecule-major --
+ * the arrays fmd_system_create_mm receives from a full flat topology. */
+int fmd_system_create_mm_replicated(fmd_ctx *ctx, const fmd_run_params *p, int nmol, int natom_mol,
+                                    const double *pos, const double *vel, const fmd_mm_topology *t1,
+                                    const double *h, const fmd_npt *npt, fmd_system **out);
 /* The reference's pre-loop work: apply_pbc, neighbour lists, first forces
  * (LJ:813-828, AI:830-853, MM:1152-1172). */
 int fmd_system_init(fmd_system *s);
@@ -346,8 +356,14 @@ int fmd_batch_enqueue(fmd_batch *b, int first, int last);
 /* Observables of the last step of each replica: obs[nrep]. */
 int fmd_batch_observables(fmd_batch *b, fmd_obs *obs);
 int fmd_batch_get_tuning(fmd_batch *b, fmd_batch_tuning *t);
-/* Kernel launches of one batch step (rebuild or not, cold/warm phase or not). */
+/* Kernel launches of one batch step (rebuild or not, cold/warm phase or not):
+ * the kernels of the step's graph that run on every replay.  A rebuild step
+ * of a batch whose replicas all use the molecule-wise list builder also
+ * holds a conditional node whose kernels (every replica's cell-grid
+ * fallback, counted by fmd_batch_step_kernels_conditional) run only when
+ * some replica's molecule path is rejected for that build. */
 int fmd_batch_step_kernels(fmd_batch *b, int rebuild, int phase, int *nkernels);
+int fmd_batch_step_kernels_conditional(fmd_batch *b, int rebuild, int phase, int *nkernels);
 int fmd_batch_destroy(fmd_batch *b);
 
 

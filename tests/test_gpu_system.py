@@ -151,3 +151,44 @@ def test_run_before_init_is_an_error(ctx):
     with pytest.raises(FmdError):
         sysd.run(1, 1)
     sysd.close()
+
+
+@pytest.mark.parametrize("nc", [1, 3])
+def test_mm_replicated_topology_is_the_full_topology(ctx, nc):
+    """An MM system built from one molecule's topology replicated on the
+    device (fmd_system_create_mm_replicated) is the system built from the
+    full flat topology (build_flat_topology, MM:254-334): the same forces
+    and energies at set-up and the same observables over steps that include
+    a list rebuild (to 1e-9: the bonded forces are scattered with FP64
+    atomics, whose order varies from run to run at the 1e-16 level)."""
+    from fuller_md_en_b200 import RunConfig, System, Topology, crystal
+    coords = crystal.c60_ih()
+    bonds = crystal.bonds_from_geometry(coords)
+    s = crystal.atomistic(nc, coords=coords, jitter=0.02, seed=17, T=400.0, mol_base=0)
+    na, nmol = s["pos"].size // 3, s["nmol"]
+
+    def topo(t):
+        return Topology(t["bonds"], t["kb"], t["r0"], t["angles"], t["kth"], t["th0"], t["dihedrals"], t["vn"],
+                        t["mult"], t["gamma"], t["impropers"], t["ki"], t["igamma"])
+
+    cfg = RunConfig(dt=0.1, T=400.0, Pe=0.5, nsteps=100, nlup=20, nc=nc, nmol=nmol)
+    npt = crystal.npt_atom(400.0, 0.5, na)
+    full = System.mm(ctx, cfg, s["pos"], s["vel"], s["mol_id"], topo(crystal.mm_topology(coords, bonds, nmol)),
+                     s["h"], npt)
+    rep = System.mm_replicated(ctx, cfg, nmol, na // nmol, s["pos"], s["vel"],
+                               topo(crystal.mm_topology(coords, bonds, 1)), s["h"], npt)
+    full.init()
+    rep.init()
+    Fa, _, Ea = full.forces()
+    Fb, _, Eb = rep.forces()
+    assert np.max(np.abs(Fa - Fb)) <= 1e-12 * np.max(np.abs(Fa))
+    assert np.max(np.abs(Ea - Eb)) <= 1e-12 * np.max(np.abs(Ea))
+    for g in range(1, 23):
+        a, b = full.run(g, g), rep.run(g, g)
+        assert abs(a.T - b.T) <= 1e-9 * abs(a.T) and abs(a.P - b.P) <= 1e-9 * max(1.0, abs(a.P)), g
+        for k in range(7):
+            assert abs(a.E[k] - b.E[k]) <= 1e-9 * max(1e-6, abs(a.E[k])), (g, k)
+    da, db = full.download(), rep.download()
+    assert np.max(np.abs(da["pos"] - db["pos"])) < 1e-9
+    full.close()
+    rep.close()
