@@ -443,13 +443,20 @@ def run_rigid(args, ctx, stream, flush, ws, rank, local):
     if not math.isfinite(obs.E[0]):
         raise RuntimeError("non-finite energy in the rigid benchmark run")
     pair_ms = sysd.kernel_ms(0, 10)
+    pairs = sysd.site_pairs()
     sysd.close()
     ms = max_over_ranks(float(sum(step_ms)), device=f"cuda:{local}")
     sites = n * 60
+    fp32_peak = 148 * 128 * 2 * 1965.0e6 / 1e12          # TFLOP/s, nominal
+    achieved = 72.0 * pairs / (pair_ms * 1e-3) / 1e12
     out = {"value": job_throughput(sites, K, ms, ws), "unit": "site-steps/s", "ms_per_step": ms / K,
            "workload": "rigid-body LJ, C60 FCC nc=10: 4,000 molecules / 240,000 sites, 300 K, 1 GPa, dt 1 fs, "
                        "molecule lists every 25 steps, FP32 site pairs with FP64 sums and integrator",
-           "site_pair_kernel_ms": pair_ms}
+           "site_pair_kernel_ms": pair_ms,
+           "roofline": {"bound": "fp32 simt", "kernel": "k_rigid_w (site pairs)", "achieved": achieved,
+                        "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+                        "peak_source": "nominal (148 SMs x 128 FP32 lanes x 2 x 1965 MHz)",
+                        "site_pairs_in_cutoff": pairs, "flop_per_pair": 72}}
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = rigid_reference_sample(s, n, rmcut)
     return out

@@ -125,6 +125,7 @@ _SIGS = {
     "fmd_system_destroy": (c_int, [c_void_p]),
     "fmd_system_kernel_ms": (c_int, [c_void_p, c_int, c_int, POINTER(c_double)]),
     "fmd_system_step_kernels": (c_int, [c_void_p, c_int, c_int, POINTER(c_int)]),
+    "fmd_system_site_pairs": (c_int, [c_void_p, POINTER(c_longlong)]),
     "fmd_system_lj_shape": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int), POINTER(c_int), POINTER(c_int)]),
     "fmd_system_set_lj_shape": (c_int, [c_void_p, c_int, c_int, c_int]),
     "fmd_system_lj_shape_pruned": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int), POINTER(c_int)]),

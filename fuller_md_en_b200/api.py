@@ -479,6 +479,13 @@ class System:
         self.ctx.check(self.ctx.lib.fmd_system_kernel_ms(self.h, stage, reps, ctypes.byref(ms)), "kernel_ms")
         return ms.value
 
+    def site_pairs(self) -> int:
+        """Rigid systems: site pairs within the LJ cutoff in the current state
+        (each molecule pair once), the site-pair kernel's work count."""
+        k = ctypes.c_longlong(0)
+        self.ctx.check(self.ctx.lib.fmd_system_site_pairs(self.h, ctypes.byref(k)), "fmd_system_site_pairs")
+        return k.value
+
     def step_kernels(self, rebuild: bool, phase: bool = False, judge: bool = False) -> int:
         k = ctypes.c_int(0)
         self.ctx.check(self.ctx.lib.fmd_system_step_kernels(self.h, int(rebuild), int(phase) | (2 * int(judge)),

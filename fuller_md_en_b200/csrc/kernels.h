@@ -157,6 +157,11 @@ cudaError_t lj_gather_launch(int ff, const double* pos, const double* hh, const 
 // shape 0 (4 warps per molecule), 1 (4 warps, registers capped for 4 blocks
 // per SM) or 2 (8 warps, capped for 2 blocks per SM).
 constexpr int kRigidLabDoubles = 4;   // per site
+// Site pairs within the cutoff (each molecule pair once) into *total
+// (device), by the FP64 test; rebuilds the lab-frame sites in FP64 into lab.
+cudaError_t rigid_count_pairs(const double* pos, const double* qv, const double* body, const double* hh,
+                              const int* cnt, const int* list, int cap, int n, int natom, double rmcut2, double* lab,
+                              unsigned long long* total, cudaStream_t st);
 cudaError_t rigid_launch(int precision, const double* pos, const double* qv, const double* body,
                          const double* hh, const int* cnt, const int* list, int cap, int n,
                          int natom, double rmcut2, double* F, double* T, double* part,

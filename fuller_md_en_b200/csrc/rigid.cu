@@ -61,6 +61,7 @@ template <> struct Site<double> { double x, y, z, pad; };
 template <> struct __align__(16) Site<float> { float x, y, z, pad; };
 
 constexpr int kMaxSites = 96;   // up to C84 (natom <= 84), padded to warps
+constexpr int kRigidMaxNeigh = 128;   // list width the warp kernel accepts (the reference's is 80)
 
 template <class P>
 __global__ void __launch_bounds__(2 * kMaxSites)
@@ -248,6 +249,8 @@ k_rigid_w(const double* __restrict__ pos, const Site<P>* __restrict__ lab, const
     __shared__ Site<P> lab_j[kRigidWarps][2 * 32];
     __shared__ double sm[32 * 16];
     __shared__ double s_hh[18];
+    __shared__ float s_cost[kRigidMaxNeigh];
+    __shared__ int s_order[kRigidMaxNeigh];
     const int i = blockIdx.x;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     if (threadIdx.x < 18) s_hh[threadIdx.x] = hh[threadIdx.x];
@@ -275,15 +278,54 @@ k_rigid_w(const double* __restrict__ pos, const Site<P>* __restrict__ lab, const
     }
     const double screen = sqrt(rc.rcut2) + sqrt(rmax2) + 1e-2, screen2 = screen * screen;
     const unsigned lt = (1u << lane) - 1u;
+    // Neighbour order: a neighbour's cost is about the number of its sites
+    // inside the screen radius -- the fraction of a sphere of radius R at
+    // distance d inside a sphere of radius S about i's centre, (S^2 - (d -
+    // R)^2) / (4 d R) -- plus its staging.  Ranked by cost (ties by list
+    // position) and dealt to the warps in snake order, the same assignment
+    // on every run, so the summation order stays fixed.
+    const int nn = cnt[i];
+    if (nn > kRigidMaxNeigh) return;                  // the lists are built with cap <= kRigidMaxNeigh
+    {
+        const double R = sqrt(rmax2);
+        for (int k = threadIdx.x; k < nn; k += blockDim.x) {
+            const int j = list[(size_t)i * cap + k];
+            double mx = __dsub_rn(pos[3 * j], pix), my = __dsub_rn(pos[3 * j + 1], piy),
+                   mz = __dsub_rn(pos[3 * j + 2], piz);
+            mimg(mx, my, mz, hi, h);
+            const double d2 = norm2_rn(mx, my, mz);
+            float cost = 0.f;
+            if (!(d2 > rmcut2)) {
+                const double d = sqrt(d2);
+                const double f = d + R <= screen ? 1.0 : (d - R >= screen ? 0.0
+                                 : (screen2 - (d - R) * (d - R)) / (4.0 * d * R));
+                cost = 8.f + (float)(natom * fmin(1.0, fmax(0.0, f)));
+            }
+            s_cost[k] = cost;
+        }
+        __syncthreads();
+        for (int k = threadIdx.x; k < nn; k += blockDim.x) {
+            const float ck = s_cost[k];
+            int rank = 0;
+            for (int u = 0; u < nn; u++) {
+                const float cu = s_cost[u];
+                rank += cu > ck || (cu == ck && u < k);
+            }
+            s_order[rank] = k;
+        }
+        __syncthreads();
+    }
     double acc[16];   // F(3) T(3) W(9) E
 #pragma unroll
     for (int k = 0; k < 16; k++) acc[k] = 0.0;
     const float sig2 = (float)rc.sig2, sig2_lo = (float)(rc.sig2 - (double)(float)rc.sig2);
     const float rcut2f = (float)rc.rcut2, c24f = (float)rc.c24, c4f = (float)rc.c4;
-    const int nn = cnt[i];
     Site<P>* sj = lab_j[w];
-    for (int k = w; k < nn; k += kRigidWarps) {
-        const int j = list[(size_t)i * cap + k];
+    for (int p0 = 0; p0 < nn; p0 += kRigidWarps) {
+        // snake: warp w takes position p0 + w on even rounds, p0 + W-1-w on odd ones
+        const int p = p0 + (((p0 / kRigidWarps) & 1) ? kRigidWarps - 1 - w : w);
+        if (p >= nn) continue;
+        const int j = list[(size_t)i * cap + s_order[p]];
         double mx = __dsub_rn(pos[3 * j], pix), my = __dsub_rn(pos[3 * j + 1], piy), mz = __dsub_rn(pos[3 * j + 2], piz);
         mimg(mx, my, mz, hi, h);
         if (norm2_rn(mx, my, mz) > rmcut2) continue;             // warp-uniform (LJ:320)
@@ -406,9 +448,58 @@ k_rigid_w(const double* __restrict__ pos, const Site<P>* __restrict__ lab, const
     }
 }
 
+// Site pairs within the cutoff, each molecule pair once (j > i), by the
+// reference's FP64 test on the lab-frame sites (LJ:320-336): the algorithmic
+// work count of the site-pair kernel (72 FLOP per counted pair).  One CTA
+// per molecule, one warp per listed neighbour.
+__global__ void __launch_bounds__(128)
+k_rigid_count(const double* __restrict__ pos, const Site<double>* __restrict__ lab, const double* __restrict__ hh,
+              const int* __restrict__ cnt, const int* __restrict__ list, int cap, int natom, double rmcut2,
+              double rcut2, unsigned long long* __restrict__ total) {
+    const int i = blockIdx.x;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, W = blockDim.x >> 5;
+    const double* h = hh;
+    const double* hi = hh + 9;
+    const double pix = pos[3 * i], piy = pos[3 * i + 1], piz = pos[3 * i + 2];
+    unsigned long long c = 0;
+    for (int k = w; k < cnt[i]; k += W) {
+        const int j = list[(size_t)i * cap + k];
+        if (j <= i) continue;
+        double mx = __dsub_rn(pos[3 * j], pix), my = __dsub_rn(pos[3 * j + 1], piy), mz = __dsub_rn(pos[3 * j + 2], piz);
+        mimg(mx, my, mz, hi, h);
+        if (norm2_rn(mx, my, mz) > rmcut2) continue;
+        for (int a = 0; a < natom; a++) {
+            const Site<double> ra = lab[(size_t)i * natom + a];
+            for (int b = lane; b < natom; b += 32) {
+                const Site<double> rb = lab[(size_t)j * natom + b];
+                const double dx = __dsub_rn(__dadd_rn(mx, rb.x), ra.x);
+                const double dy = __dsub_rn(__dadd_rn(my, rb.y), ra.y);
+                const double dz = __dsub_rn(__dadd_rn(mz, rb.z), ra.z);
+                c += norm2_rn(dx, dy, dz) < rcut2;
+            }
+        }
+    }
+    c = __reduce_add_sync(kFull, (unsigned)c);
+    if (lane == 0 && c) atomicAdd(total, c);
+}
+
 }  // namespace
 
 int rigid_grid(int n) { return n; }
+
+cudaError_t rigid_count_pairs(const double* pos, const double* qv, const double* body, const double* hh,
+                              const int* cnt, const int* list, int cap, int n, int natom, double rmcut2, double* lab,
+                              unsigned long long* total, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    if (natom < 1 || natom > kMaxSites || !lab) return cudaErrorInvalidValue;
+    const RigidConst rc = rigid_const();
+    const int lb = (int)std::min<long long>(((long long)n * natom + 255) / 256, kSMs * 16);
+    Site<double>* sl = reinterpret_cast<Site<double>*>(lab);
+    k_rigid_lab<double><<<lb, 256, 0, st>>>(qv, body, n, natom, sl);
+    cudaMemsetAsync(total, 0, sizeof(unsigned long long), st);
+    k_rigid_count<<<n, 128, 0, st>>>(pos, sl, hh, cnt, list, cap, natom, rmcut2, rc.rcut2, total);
+    return cudaGetLastError();
+}
 
 cudaError_t rigid_launch(int precision, const double* pos, const double* qv, const double* body,
                          const double* hh, const int* cnt, const int* list, int cap, int n, int natom,
@@ -417,7 +508,7 @@ cudaError_t rigid_launch(int precision, const double* pos, const double* qv, con
     if (n <= 0) return cudaSuccess;
     if (natom < 1 || natom > kMaxSites) return cudaErrorInvalidValue;
     const RigidConst rc = rigid_const();
-    if (lab != nullptr && natom <= 64) {
+    if (lab != nullptr && natom <= 64 && cap <= kRigidMaxNeigh) {
         const int lb = (int)std::min<long long>(((long long)n * natom + 255) / 256, kSMs * 16);
 #define FMD_RW(P, W, MB) \
     k_rigid_w<P, W, MB><<<n, 32 * W, 0, st>>>(pos, reinterpret_cast<const Site<P>*>(lab), hh, cnt, list, cap, n, natom, \

@@ -991,6 +991,27 @@ extern "C" int fmd_system_lj_shape(fmd_system* s, int* threads, int* unroll, int
     return FMD_OK;
 }
 
+extern "C" int fmd_system_site_pairs(fmd_system* s, long long* pairs) {
+    if (!s || !s->sys || !pairs) return FMD_ERR_ARG;
+    fmd::System& y = *s->sys;
+    const StepArrays& a = y.arr;
+    if (a.kind != FMD_SYS_RIGID) return y.ctx->fail(FMD_ERR_ARG, "fmd_system_site_pairs: not a rigid system");
+    if (!y.initialized) return y.ctx->fail(FMD_ERR_STATE, "fmd_system_site_pairs before init");
+    unsigned long long* d = nullptr;
+    unsigned long long h = 0;
+    if (cudaMalloc(&d, sizeof(unsigned long long)) != cudaSuccess)
+        return y.ctx->fail(FMD_ERR_CUDA, "fmd_system_site_pairs: allocation failed");
+    cudaStream_t st = y.ctx->stream;
+    cudaError_t e = rigid_count_pairs(a.pos, a.qv, a.body, a.S->h, a.cnt_a, a.list_a, a.cap_a, a.n, a.natom,
+                                      a.rmcut2, a.rigid_lab, d, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(d);
+    if (e != cudaSuccess) return y.ctx->fail(FMD_ERR_CUDA, cudaGetErrorString(e));
+    *pairs = (long long)h;
+    return FMD_OK;
+}
+
 extern "C" int fmd_system_step_kernels(fmd_system* s, int rebuild, int phase, int* nk) {
     if (!s || !nk) return FMD_ERR_ARG;
     fmd::System& y = *s->sys;

@@ -323,6 +323,11 @@ int fmd_system_set_lj_prune(fmd_system *s, double delta);
 int fmd_system_lj_prune(fmd_system *s, double *delta, long long *evaluations, long long *prunes);
 int fmd_system_set_lj_shape(fmd_system *s, int threads, int unroll, int feed);
 int fmd_system_step_kernels(fmd_system *s, int rebuild, int phase, int *nkernels);
+/* Rigid systems: the number of site pairs within the LJ cutoff in the
+ * current state (the reference's FP64 test, LJ:320-336; each molecule pair
+ * once): the work count of the site-pair kernel.  Overwrites the system's
+ * lab-frame site scratch (the next force evaluation rebuilds it). */
+int fmd_system_site_pairs(fmd_system *s, long long *pairs);
 
 /* ------------------------------------------------------- replica batches --
  * No counterpart in the reference (its programs run one system each).  A

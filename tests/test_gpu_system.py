@@ -192,3 +192,43 @@ def test_mm_replicated_topology_is_the_full_topology(ctx, nc):
     assert np.max(np.abs(da["pos"] - db["pos"])) < 1e-9
     full.close()
     rep.close()
+
+
+def test_rigid_site_pair_count(ctx):
+    """fmd_system_site_pairs: the site pairs within the cutoff (each molecule
+    pair once) of a rigid system, against a count from the state on the host."""
+    s = crystal.rigid(2, seed=3)
+    n = s["n"]
+    rmcut = 3.0 * 3.431 + 2 * s["Rmol"] + 1.0
+    cfg = RunConfig(dt=1.0, T=300.0, Pe=0.0, nsteps=100, nlup=25, nc=2, nmol=n)
+    sysd = System.rigid(ctx, cfg, 60, s["body"], s["I0"], s["Mmol"], rmcut, s["pos"], s["vel"], s["qv"], s["omg"],
+                        s["h"], crystal.npt_rigid(300.0, 0.0, n))
+    sysd.init()
+    got = sysd.site_pairs()
+    st = sysd.download()
+    c, l, _, _ = sysd.lists(80)
+    pos, qv, h = st["pos"].reshape(-1, 3), st["qv"].reshape(-1, 4), st["h"].reshape(3, 3)
+    L = np.diag(h)
+    body = np.asarray(s["body"]).reshape(-1, 3)
+
+    def rot(q):
+        w, x, y, z = q
+        return np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y)],
+                         [2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x)],
+                         [2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)]])
+
+    lab = np.stack([body @ rot(q).T for q in qv])
+    rc2 = (3.0 * 3.431) ** 2
+    want = 0
+    for i in range(n):
+        for j in l[i * 80:i * 80 + c[i]]:
+            if j <= i:
+                continue
+            m = pos[j] - pos[i]
+            m -= L * np.round(m / L)
+            if m @ m > rmcut * rmcut:
+                continue
+            d = m[None, None, :] + lab[j][None, :, :] - lab[i][:, None, :]
+            want += int(np.count_nonzero((d * d).sum(axis=2) < rc2))
+    assert got == want and got > 0
+    sysd.close()
