@@ -668,7 +668,24 @@ def cpu_baseline():
                       f"(step_npt {ts / K * 1e3:.0f} ms/step, list build {tr:.2f} s)"}
 
 
-STAGES = {"lj_full": 0, "rebo": 1, "rebuild": 2, "forces": 3, "lj_pruned": 4, "rigid": 0, "sg": 1}
+STAGES = {"lj_full": 0, "rebo": 1, "rebuild": 2, "forces": 3, "lj_pruned": 4, "rigid": 0, "sg": 1, "rebo2": 1,
+          "lj_switch": 5}
+
+
+def synthetic_rebo2_knots(seed: int = 0):
+    """Spline knots of the tables' scale for timing the REBO-II kernels (the
+    published tables are not in this repository; the kernels' cost does not
+    depend on the knot values)."""
+    from fuller_md_en_b200 import Rebo2Knots
+    rng = np.random.default_rng(seed)
+    pcc = np.column_stack([rng.uniform(-0.05, 0.05, 5), rng.uniform(-0.03, 0.03, 5)])
+
+    def tri(shift, amp):
+        t = rng.uniform(-0.3 * amp, 0.3 * amp, (5, 5, 10, 8))
+        t[..., 0] = rng.uniform(-amp, amp, (5, 5, 10)) + shift
+        return t
+
+    return Rebo2Knots(pcc, tri(-0.05, 0.03), tri(0.0, 0.01))
 
 
 def run_stage(args):
@@ -688,7 +705,9 @@ def run_stage(args):
     timed launch of the stage, then the recomputation's, so a profiler
     capturing the gather's launch 3 sees the timed, warm launch on the bench
     state.  The REBO kernels launch twice per force evaluation (geometry +
-    bond order, forces).  Prints one JSON line."""
+    bond order, forces).  "rebo2" / "lj_switch": the REBO-II term (coordination
+    and bond kernels) / the switched-LJ correction of the same workload with
+    both extensions on and synthetic spline knots.  Prints one JSON line."""
     from fuller_md_en_b200 import Context, RunConfig, System, crystal
     from fuller_md_en_b200._lib import FMD_PREC_FP32_PAIR
     ctx = Context(0)
@@ -715,6 +734,9 @@ def run_stage(args):
         y = System.airebo(ctx, cfg, s["pos"], s["vel"], s["mass"], s["mol_id"], s["h"],
                           crystal.npt_atom(T_K, P_GPA, na))
         y.set_lj_prune(args.delta)
+        if args.stage in ("rebo2", "lj_switch"):
+            from fuller_md_en_b200._lib import FMD_REBO2_BOND_ORDER, FMD_REBO2_LJ_SWITCH
+            y.set_rebo2(synthetic_rebo2_knots(), FMD_REBO2_BOND_ORDER | FMD_REBO2_LJ_SWITCH)
         y.init()
         model = None
         if args.stage == "sg":

@@ -5,5 +5,7 @@ C-ABI (include/fullermd.h, libfullermd_cuda.so), with C++ drop-in drivers
 """
 from ._lib import FmdError, load, LIB_PATH  # noqa: F401
 from .api import Batch, Context, System, Topology, RunConfig, mm_replica  # noqa: F401
+from .rebo2 import Rebo2Knots  # noqa: F401
 
-__all__ = ["Batch", "Context", "System", "Topology", "RunConfig", "mm_replica", "FmdError", "load", "LIB_PATH"]
+__all__ = ["Batch", "Context", "System", "Topology", "RunConfig", "mm_replica", "Rebo2Knots", "FmdError", "load",
+           "LIB_PATH"]

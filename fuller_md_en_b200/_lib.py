@@ -18,6 +18,7 @@ _ip = POINTER(c_int)
 FMD_OK, FMD_ERR_ARG, FMD_ERR_CUDA, FMD_ERR_CAPACITY, FMD_ERR_NONFINITE, FMD_ERR_STATE = range(6)
 FMD_PREC_FP64, FMD_PREC_FP32_PAIR = 0, 1
 FMD_PHYS_MM_BONDED, FMD_PHYS_REBO, FMD_PHYS_QUAT = 1, 2, 4
+FMD_REBO2_BOND_ORDER, FMD_REBO2_LJ_SWITCH = 1, 2
 FMD_FF_AIREBO, FMD_FF_MM = 0, 1
 FMD_SYS_RIGID, FMD_SYS_AIREBO, FMD_SYS_MM = 0, 1, 2
 
@@ -26,6 +27,13 @@ class NPT(ctypes.Structure):
     """fmd_npt: NPTState of the reference (LJ:425, AI:511, MM:804)."""
     _fields_ = [("xi", c_double), ("Q", c_double), ("Vg", c_double * 9), ("W", c_double),
                 ("Pe", c_double), ("Tt", c_double), ("Nf", c_int)]
+
+
+class Rebo2Knots(ctypes.Structure):
+    """fmd_rebo2_knots: spline knots of the REBO-II extension -- P_CC(N, 0)
+    at N = 0..4 {P, dP/dN}; pi^rc_CC and T_CC at N_ij, N_ji = 0..4,
+    N_conj = 0..9 {f, f_x, f_y, f_z, f_xy, f_xz, f_yz, f_xyz}."""
+    _fields_ = [("pcc", c_double * 10), ("pirc", c_double * 2000), ("tcc", c_double * 2000)]
 
 
 class MMTopology(ctypes.Structure):
@@ -94,6 +102,11 @@ _SIGS = {
                                     c_double, c_int, _dp, _dp, _dp, _dp]),
     "fmd_rebo_forces": (c_int, [c_void_p, _dp, _dp, _dp, _ip, _ip, c_int, c_int, _dp, _dp, _dp]),
     "fmd_lj_half_forces": (c_int, [c_void_p, c_int, _dp, _dp, _dp, _ip, _ip, c_int, c_int, _dp, _dp, _dp]),
+    "fmd_rebo2_coeffs": (c_int, [POINTER(Rebo2Knots), _dp]),
+    "fmd_rebo2_forces": (c_int, [c_void_p, _dp, _dp, _dp, _ip, _ip, c_int, c_int, POINTER(Rebo2Knots), _dp, _dp,
+                                 _dp]),
+    "fmd_lj_switch_forces": (c_int, [c_void_p, _dp, _dp, _dp, _ip, _ip, c_int, _ip, _ip, c_int, c_int,
+                                     POINTER(Rebo2Knots), _dp, _dp, _dp]),
     "fmd_rebo_forces_noalloc": (c_int, [c_void_p, _dp, _dp, c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p,
                                         c_void_p, c_void_p]),
     "fmd_airebo_forces": (c_int, [c_void_p, _dp, _dp, _dp, _ip, _ip, _ip, _ip, c_int, _dp, _dp, _dp]),
@@ -134,6 +147,7 @@ _SIGS = {
     "fmd_system_lj_rows": (c_int, [c_void_p, c_void_p, c_void_p]),
     "fmd_system_lj_full_rows": (c_int, [c_void_p, c_void_p, c_void_p, POINTER(c_int)]),
     "fmd_system_set_physics": (c_int, [c_void_p, c_int]),
+    "fmd_system_set_rebo2": (c_int, [c_void_p, POINTER(Rebo2Knots), c_int]),
     "fmd_system_lj_prune": (c_int, [c_void_p, POINTER(c_double), POINTER(c_longlong), POINTER(c_longlong)]),
     "fmd_sg_nparams": (c_int, []),
     "fmd_sg_create": (c_int, [c_void_p, _dp, POINTER(c_void_p)]),

@@ -189,6 +189,28 @@ class Context:
                                                ctypes.byref(E)), "compute_lj")
         return E.value
 
+    def rebo2_forces(self, F: np.ndarray, vir9: np.ndarray, pos, h, hi, nlc, nll, na: int, knots: "Rebo2Knots",
+                     max_neigh: int = MAX_REBO_NEIGH) -> float:
+        """REBO-II energy (fmd_rebo2_forces; no reference counterpart): adds
+        -grad E into F and the full virial into vir9; returns E."""
+        E = ctypes.c_double(0)
+        self.check(self.lib.fmd_rebo2_forces(self.h, _d(_f64(pos)), _d(_f64(h)), _d(_f64(hi)), _i(_i32(nlc)),
+                                             _i(_i32(nll)), max_neigh, na, ctypes.byref(knots.raw()), _d(F),
+                                             _d(vir9), ctypes.byref(E)), "fmd_rebo2_forces")
+        return E.value
+
+    def lj_switch_forces(self, F: np.ndarray, vir9: np.ndarray, pos, h, hi, nlc_r, nll_r, nlc_l, nll_l, na: int,
+                         knots: "Rebo2Knots", max_neigh_r: int = MAX_REBO_NEIGH,
+                         max_neigh_l: int = MAX_LJ_NEIGH) -> float:
+        """The switched-LJ correction (fmd_lj_switch_forces): adds into F and
+        vir9; returns its energy (the switched LJ is compute_lj plus this)."""
+        E = ctypes.c_double(0)
+        self.check(self.lib.fmd_lj_switch_forces(self.h, _d(_f64(pos)), _d(_f64(h)), _d(_f64(hi)), _i(_i32(nlc_r)),
+                                                 _i(_i32(nll_r)), max_neigh_r, _i(_i32(nlc_l)), _i(_i32(nll_l)),
+                                                 max_neigh_l, na, ctypes.byref(knots.raw()), _d(F), _d(vir9),
+                                                 ctypes.byref(E)), "fmd_lj_switch_forces")
+        return E.value
+
     def compute_forces_airebo(self, pos, h, hi, nlc_r, nll_r, nlc_l, nll_l, na: int):
         """compute_forces (AI:477-495) -> (E3, F, vir9), E3 = (Ep, Ep_rebo, Ep_lj)."""
         F = np.zeros(3 * na)
@@ -514,6 +536,12 @@ class System:
         _lib.FMD_PHYS_MM_BONDED); before init().  Default 0: the reference's
         forces."""
         self.ctx.check(self.ctx.lib.fmd_system_set_physics(self.h, int(flags)), "fmd_system_set_physics")
+
+    def set_rebo2(self, knots: "Rebo2Knots", flags: int) -> None:
+        """REBO-II extension (fmd_system_set_rebo2): _lib.FMD_REBO2_BOND_ORDER
+        and/or _lib.FMD_REBO2_LJ_SWITCH with the spline knots; before init()."""
+        self.ctx.check(self.ctx.lib.fmd_system_set_rebo2(self.h, ctypes.byref(knots.raw()), int(flags)),
+                       "fmd_system_set_rebo2")
 
     def set_lj_prune(self, delta: float) -> None:
         """Buffer (A) of the pruned LJ gather rows beyond the cutoff; 0 turns

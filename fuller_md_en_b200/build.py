@@ -32,7 +32,7 @@ NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-r
 # reference's host code (no FMA contraction).
 EXTRA = {"step.cu": ["-fmad=false"]}
 CUDA_SOURCES = ["nlist.cu", "airebo.cu", "rigid.cu", "mm.cu", "step.cu", "system.cu", "abi.cu", "noalloc.cu", "surrogate.cu",
-                "sg_train.cu", "sg_abi.cu", "sg_step.cu", "batch.cu", "molnlist.cu", "ljprune.cu"]
+                "sg_train.cu", "sg_abi.cu", "sg_step.cu", "batch.cu", "molnlist.cu", "ljprune.cu", "rebo2.cu"]
 
 DRIVERS = ["fuller_LJ_core_gpu", "fuller_LJ_npt_md_gpu", "fuller_LJ_npt_mmmd_gpu", "fuller_airebo_npt_md_gpu"]
 

@@ -130,7 +130,7 @@ namespace {
 enum Slot {
     S_POS = 0, S_HH, S_MOL, S_CNT, S_LIST, S_CNT2, S_LIST2, S_INCNT, S_INLIST, S_DROP,
     S_F, S_FACC, S_T, S_QV, S_BODY, S_VEL, S_OMG, S_MASS, S_PART1, S_PART2, S_PART3, S_PARTKE,
-    S_SCAL, S_CHARGE, S_RSLOT, S_RLAB, S_TOPO0
+    S_SCAL, S_CHARGE, S_RSLOT, S_RLAB, S_R2TAB, S_R2NC, S_TOPO0
 };
 
 template <class T>
@@ -492,6 +492,106 @@ extern "C" int fmd_lj_half_forces(fmd_ctx* ctx, int ff, const double* pos, const
     if (ff != FMD_FF_AIREBO && ff != FMD_FF_MM)
         return ctx ? ctx->fail(FMD_ERR_ARG, "fmd_lj_half_forces: unknown force field") : FMD_ERR_ARG;
     return atom_term(ctx, 1, ff, pos, h, hi, nlc, nll, max_neigh, na, F, vir9, E);
+}
+
+namespace {
+
+// REBO-II tables of one host call: the knots expanded into per-cell
+// coefficients and uploaded, and the coordination scratch.
+int rebo2_tables(fmd_ctx* ctx, const fmd_rebo2_knots* kn, int na, Rebo2Dev& t) {
+    static_assert(sizeof(fmd_rebo2_knots) == sizeof(double) * kRebo2Knots, "knot layout");
+    std::vector<double> c(kRebo2PccCoef + 2 * (size_t)kRebo2TriCoef);
+    rebo2_coeffs(&kn->pcc[0][0], c.data(), c.data() + kRebo2PccCoef, c.data() + kRebo2PccCoef + kRebo2TriCoef);
+    double *tab, *nc;
+    int rc = up(ctx, S_R2TAB, c.data(), c.size(), &tab);
+    if (!rc) rc = up<double>(ctx, S_R2NC, nullptr, (size_t)na, &nc);
+    if (rc) return rc;
+    t.pcc = tab;
+    t.pirc = tab + kRebo2PccCoef;
+    t.tcc = tab + kRebo2PccCoef + kRebo2TriCoef;
+    t.ncoord = nc;
+    // the staging vector dies at return: finish the copy first
+    return cudaStreamSynchronize(ctx->stream) == cudaSuccess ? FMD_OK
+                                                             : ctx->fail(FMD_ERR_CUDA, "table upload failed");
+}
+
+// Reduces nblk {E, W9} partial records, adds the virial into vir9 and copies
+// the forces back.
+int finish_term(fmd_ctx* ctx, const double* part, int nblk, const double* dF, double* F, int na, double* vir9,
+                double* E, const char* what) {
+    double* red;
+    int rc = up<double>(ctx, S_PART3, nullptr, 16, &red);
+    if (rc) return rc;
+    if (reduce_partials(part, nblk, kNV, red, ctx->stream) != cudaSuccess)
+        return ctx->fail(FMD_ERR_CUDA, "reduce launch failed");
+    double r[kNV];
+    down(ctx, F, dF, 3 * (size_t)na);
+    down(ctx, r, red, kNV);
+    if ((rc = ctx->sync_check(what))) return rc;
+    *E = r[0];
+    for (int q = 0; q < 9; q++) vir9[q] += r[1 + q];
+    return FMD_OK;
+}
+
+}  // namespace
+
+extern "C" int fmd_rebo2_coeffs(const fmd_rebo2_knots* kn, double* out) {
+    if (!kn || !out) return FMD_ERR_ARG;
+    rebo2_coeffs(&kn->pcc[0][0], out, out + kRebo2PccCoef, out + kRebo2PccCoef + kRebo2TriCoef);
+    return FMD_OK;
+}
+
+extern "C" int fmd_rebo2_forces(fmd_ctx* ctx, const double* pos, const double* h, const double* hi, const int* nlc,
+                                const int* nll, int max_neigh, int na, const fmd_rebo2_knots* kn, double* F,
+                                double* vir9, double* E) {
+    if (!ctx) return FMD_ERR_ARG;
+    if (!pos || !h || !hi || !nlc || !nll || !kn || !F || !vir9 || !E || na < 1 || max_neigh < 1)
+        return ctx->fail(FMD_ERR_ARG, "fmd_rebo2_forces: bad argument");
+    if (!list_ok(ctx, nlc, nll, max_neigh, na, "REBO list")) return FMD_ERR_ARG;
+    double *dpos, *hh, *dF, *part;
+    int *dc, *dl;
+    Rebo2Dev t;
+    int rc = up(ctx, S_POS, pos, 3 * (size_t)na, &dpos);
+    if (!rc) rc = upload_cell(ctx, h, hi, &hh);
+    if (!rc) rc = up(ctx, S_F, F, 3 * (size_t)na, &dF);
+    if (!rc) rc = up(ctx, S_CNT2, nlc, na, &dc);
+    if (!rc) rc = up(ctx, S_LIST2, nll, (size_t)na * max_neigh, &dl);
+    if (!rc) rc = up<double>(ctx, S_PART1, nullptr, (size_t)kForceBlocks * kNV, &part);
+    if (!rc) rc = rebo2_tables(ctx, kn, na, t);
+    if (rc) return rc;
+    if (rebo2_launch(t, dpos, hh, dc, dl, max_neigh, na, dF, part, kForceBlocks, ctx->stream) != cudaSuccess)
+        return ctx->fail(FMD_ERR_CUDA, "rebo2 launch failed");
+    return finish_term(ctx, part, kForceBlocks, dF, F, na, vir9, E, "rebo2 forces");
+}
+
+extern "C" int fmd_lj_switch_forces(fmd_ctx* ctx, const double* pos, const double* h, const double* hi,
+                                    const int* nlc_r, const int* nll_r, int max_neigh_r, const int* nlc_l,
+                                    const int* nll_l, int max_neigh_l, int na, const fmd_rebo2_knots* kn, double* F,
+                                    double* vir9, double* E) {
+    if (!ctx) return FMD_ERR_ARG;
+    if (!pos || !h || !hi || !nlc_r || !nll_r || !nlc_l || !nll_l || !kn || !F || !vir9 || !E || na < 1 ||
+        max_neigh_r < 1 || max_neigh_l < 1)
+        return ctx->fail(FMD_ERR_ARG, "fmd_lj_switch_forces: bad argument");
+    if (!list_ok(ctx, nlc_r, nll_r, max_neigh_r, na, "REBO list") ||
+        !list_ok(ctx, nlc_l, nll_l, max_neigh_l, na, "LJ list"))
+        return FMD_ERR_ARG;
+    double *dpos, *hh, *dF, *part;
+    int *dcr, *dlr, *dcl, *dll;
+    Rebo2Dev t;
+    int rc = up(ctx, S_POS, pos, 3 * (size_t)na, &dpos);
+    if (!rc) rc = upload_cell(ctx, h, hi, &hh);
+    if (!rc) rc = up(ctx, S_F, F, 3 * (size_t)na, &dF);
+    if (!rc) rc = up(ctx, S_CNT2, nlc_r, na, &dcr);
+    if (!rc) rc = up(ctx, S_LIST2, nll_r, (size_t)na * max_neigh_r, &dlr);
+    if (!rc) rc = up(ctx, S_CNT, nlc_l, na, &dcl);
+    if (!rc) rc = up(ctx, S_LIST, nll_l, (size_t)na * max_neigh_l, &dll);
+    if (!rc) rc = up<double>(ctx, S_PART1, nullptr, (size_t)kForceBlocks * kNV, &part);
+    if (!rc) rc = rebo2_tables(ctx, kn, na, t);
+    if (rc) return rc;
+    if (lj_switch_launch(t, dpos, hh, dcr, dlr, max_neigh_r, dcl, dll, max_neigh_l, na, dF, part, kForceBlocks,
+                         false, ctx->stream) != cudaSuccess)
+        return ctx->fail(FMD_ERR_CUDA, "lj switch launch failed");
+    return finish_term(ctx, part, kForceBlocks, dF, F, na, vir9, E, "lj switch forces");
 }
 
 namespace {

@@ -101,6 +101,42 @@ constexpr int kReboSlotDoubles = 16;
 cudaError_t rebo_slots_launch(const double* pos, const double* hh, const int* cnt, const int* list, int cap,
                               int na, double* slots, double* F, double* part, int nblocks, const int* gate,
                               int want, cudaStream_t st, const int* ids = nullptr, bool phys = false);
+// REBO-II extension (rebo2.cu; no reference counterpart): bond order with
+// P_CC(N, 0), pi^rc_CC(N_ij, N_ji, N_conj) and the dihedral term
+// T_CC(...) sum (1 - cos^2 w) f_c f_c, and AIREBO's switched LJ.  Splines on
+// integer knots N in [0, kRebo2Nx] x [0, kRebo2Ny] x [0, kRebo2Nz] (P_CC on
+// [0, kRebo2Nx]); tables are per-cell polynomial coefficients: pcc[4 * cell
+// + a] of u^a, pirc/tcc[cell * 64 + a + 4 b + 16 c] of u^a v^b w^c.
+constexpr int kRebo2Nx = 4, kRebo2Ny = 4, kRebo2Nz = 9;
+constexpr int kRebo2PccCoef = 4 * kRebo2Nx;
+constexpr int kRebo2TriCoef = kRebo2Nx * kRebo2Ny * kRebo2Nz * 64;
+// knots as fmd_rebo2_knots: P_CC {P, dP/dN} x (Nx+1), then pi^rc and T_CC,
+// each (Nx+1)(Ny+1)(Nz+1) x {f, fx, fy, fz, fxy, fxz, fyz, fxyz}
+constexpr int kRebo2Knots = 2 * (kRebo2Nx + 1) + 2 * (kRebo2Nx + 1) * (kRebo2Ny + 1) * (kRebo2Nz + 1) * 8;
+struct Rebo2Dev {
+    const double* pcc = nullptr;
+    const double* pirc = nullptr;
+    const double* tcc = nullptr;
+    double* ncoord = nullptr;      // [n] scratch: sum of f_c over each atom's REBO row
+};
+// Host: the per-cell coefficients of the cubic Hermite splines through the
+// knots (kRebo2Knots doubles) into pcc, pirc, tcc.
+void rebo2_coeffs(const double* knots, double* pcc, double* pirc, double* tcc);
+// N_k into t.ncoord.
+cudaError_t rebo2_coord_launch(const Rebo2Dev& t, const double* pos, const double* hh, const int* cnt,
+                               const int* list, int cap, int na, cudaStream_t st);
+// REBO-II energy over the bonds i < j of the REBO rows: forces -grad E ADDED
+// into F, {E, W9} partials in part[nblk * kNV] (full virial).  Computes
+// t.ncoord first.
+cudaError_t rebo2_launch(const Rebo2Dev& t, const double* pos, const double* hh, const int* cnt, const int* list,
+                         int cap, int na, double* F, double* part, int nblk, cudaStream_t st);
+// Switched-LJ correction over the LJ half rows (cnt_a, list_a): energy
+// -V S(t_r) (1 - S(t_b(b*))) per pair, forces ADDED into F, {E, W9} partials.
+// coord_ready: t.ncoord already holds this configuration's N_k.
+cudaError_t lj_switch_launch(const Rebo2Dev& t, const double* pos, const double* hh, const int* cnt_b,
+                             const int* list_b, int cap_b, const int* cnt_a, const int* list_a, int cap_a, int na,
+                             double* F, double* part, int nblk, bool coord_ready, cudaStream_t st);
+
 // Builds ids (1 + kIdsLanes n + n cap ints) from the list (cap <= 32);
 // scratch: rebo_ids_scratch(n) ints.
 constexpr int kIdsLanes = 32;

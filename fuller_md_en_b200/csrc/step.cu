@@ -13,13 +13,15 @@
 //   k_kick      first half-kick, drift in fractional coordinates, wrap,
 //               back to Cartesian with the new cell (+ quaternion update)
 //   forces      (airebo.cu / rigid.cu / mm.cu)
-//   k_kick2     second half-kick, per-block kinetic partials
-//   k_end       force/kinetic reductions (fixed order), thermostat/barostat
-//               second half, observables, rescale decision, averages
+//   k_kick2_end second half-kick with per-block kinetic partials; the last
+//               block to finish: force/kinetic reductions (fixed order),
+//               thermostat/barostat second half, observables, rescale
+//               decision, averages
 //   k_rescale / k_rescale_end   cold/warm phases only
 //
 // Scalar arithmetic follows the reference expressions; this file is built
 // with -fmad=false so they round like the reference's host code.
+#include <algorithm>
 #include <cmath>
 #include "step.h"
 #include "ljprune.h"
@@ -216,12 +218,6 @@ __global__ void __launch_bounds__(kPB) k_kick(StepArrays a, double dt) {
     kick_body(a, dt, blockIdx.x, gridDim.x);
 }
 
-__global__ void __launch_bounds__(kPB) k_kick2(StepArrays a, double dt) {
-    FMD_PDL_WAIT();
-    __shared__ double sm[32 * 2];
-    kick2_body(a, dt, blockIdx.x, gridDim.x, sm);
-}
-
 __global__ void __launch_bounds__(kPB) k_ke_partial(StepArrays a) {
     __shared__ double sm[32 * 2];
     const bool rigid = a.kind == FMD_SYS_RIGID;
@@ -284,29 +280,37 @@ __device__ void reduce_all(const StepArrays& a, int nblk_f1, int nblk_ke, bool f
     double acc[kRedFields];
 #pragma unroll
     for (int k = 0; k < kRedFields; k++) acc[k] = 0.0;
+    // L2 loads (__ldcg): the fused second kick reduces records that other
+    // blocks of the same launch have just written.
     if (forces) {
         // record widths as compile-time constants so each thread's loads issue together
         if (a.kind == FMD_SYS_MM) {
             for (int b = threadIdx.x; b < nblk_f1; b += blockDim.x)
 #pragma unroll
-                for (int k = 0; k < kMMNV; k++) acc[k] += a.part_f1[(size_t)b * kMMNV + k];
+                for (int k = 0; k < kMMNV; k++) acc[k] += __ldcg(a.part_f1 + (size_t)b * kMMNV + k);
         } else {
             for (int b = threadIdx.x; b < nblk_f1; b += blockDim.x)
 #pragma unroll
-                for (int k = 0; k < kNV; k++) acc[k] += a.part_f1[(size_t)b * kNV + k];
+                for (int k = 0; k < kNV; k++) acc[k] += __ldcg(a.part_f1 + (size_t)b * kNV + k);
         }
         if (a.kind != FMD_SYS_RIGID)
             for (int b = threadIdx.x; b < nblk_f2; b += blockDim.x) {
 #pragma unroll
-                for (int k = 0; k < kNV; k++) acc[10 + k] += a.part_f2[(size_t)b * kNV + k];
+                for (int k = 0; k < kNV; k++) acc[10 + k] += __ldcg(a.part_f2 + (size_t)b * kNV + k);
             }
         if (a.kind == FMD_SYS_MM && a.has_charge)
-            for (int b = threadIdx.x; b < kForceBlocks; b += blockDim.x) acc[20] += a.part_f3[b];
+            for (int b = threadIdx.x; b < kForceBlocks; b += blockDim.x) acc[20] += __ldcg(a.part_f3 + b);
+        // the switched-LJ correction belongs to the LJ term
+        if (a.kind == FMD_SYS_AIREBO && (a.rebo2_flags & FMD_REBO2_LJ_SWITCH))
+            for (int b = threadIdx.x; b < kForceBlocks; b += blockDim.x) {
+#pragma unroll
+                for (int k = 0; k < kNV; k++) acc[10 + k] += __ldcg(a.part_sw + (size_t)b * kNV + k);
+            }
     }
     if (kinetic)
         for (int b = threadIdx.x; b < nblk_ke; b += blockDim.x) {
-            acc[21] += a.part_ke[2 * b];
-            acc[22] += a.part_ke[2 * b + 1];
+            acc[21] += __ldcg(a.part_ke + 2 * b);
+            acc[22] += __ldcg(a.part_ke + 2 * b + 1);
         }
     block_sum_store<kRedFields>(acc, sm, t);   // result valid in thread 0
 }
@@ -434,10 +438,22 @@ __device__ void rescale_end_body(const StepArrays& a, const StepParams& p, int n
 
 namespace {
 
-__global__ void __launch_bounds__(kRedThreads) k_end(StepArrays a, StepParams p, int nblk_f1, int nblk_ke) {
+// The second half-kick and the end of the step in one launch: every block
+// writes its kinetic partial and takes a ticket; the last block to finish
+// runs end_body (the same fixed-order reduction of all partial records, so
+// the result does not depend on which block is last) and resets the ticket.
+__global__ void __launch_bounds__(kPB) k_kick2_end(StepArrays a, StepParams p, int nblk_f1) {
     FMD_PDL_WAIT();
     __shared__ double sm[32 * kRedFields];
-    end_body(a, p, nblk_f1, nblk_ke, a.lj_blocks, sm);
+    __shared__ bool last;
+    kick2_body(a, p.dt, blockIdx.x, gridDim.x, sm);
+    __threadfence();                      // this block's partial before its ticket
+    if (threadIdx.x == 0) last = atomicAdd(&a.S->kick2_done, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    end_body(a, p, nblk_f1, gridDim.x, a.lj_blocks, sm);
+    if (threadIdx.x == 0) a.S->kick2_done = 0u;
 }
 
 __global__ void __launch_bounds__(kRedThreads) k_rescale_end(StepArrays a, StepParams p, int nblk_ke) {
@@ -529,13 +545,20 @@ cudaError_t enqueue_forces(const StepArrays& a, cudaStream_t st, bool judge) {
         e = rigid_launch(a.precision, a.pos, a.qv, a.body, hh, a.cnt_a, a.list_a, a.cap_a, a.n, a.natom,
                          a.rmcut2, a.F, a.T, a.part_f1, st, a.rigid_lab, a.rigid_shape);
     } else if (a.kind == FMD_SYS_AIREBO) {
-        if (a.sg) e = sg_enqueue_rebo(*a.sg, a, judge, st);
+        if (a.rebo2_flags & FMD_REBO2_BOND_ORDER)
+            e = rebo2_launch(a.rebo2, a.pos, hh, a.cnt_b, a.list_b, a.cap_b, a.n, a.Facc, a.part_f1, a.rebo_blocks,
+                             st);
+        else if (a.sg) e = sg_enqueue_rebo(*a.sg, a, judge, st);
         else if (a.rebo_slots)
             e = rebo_slots_launch(a.pos, hh, a.cnt_b, a.list_b, a.cap_b, a.n, a.rebo_slots, a.Facc, a.part_f1,
                                   kForceBlocks, nullptr, 0, st, a.rebo_ids, a.rebo_phys != 0);
         else e = rebo_launch(a.pos, hh, a.cnt_b, a.list_b, a.cap_b, a.n, a.Facc, a.part_f1, st);
         if (e != cudaSuccess) return e;
         e = enqueue_lj(a, FMD_FF_AIREBO, st);
+        // the switched LJ: its correction adds into the finished F
+        if (e == cudaSuccess && (a.rebo2_flags & FMD_REBO2_LJ_SWITCH))
+            e = lj_switch_launch(a.rebo2, a.pos, hh, a.cnt_b, a.list_b, a.cap_b, a.cnt_a, a.list_a, a.cap_a, a.n,
+                                 a.F, a.part_sw, kForceBlocks, (a.rebo2_flags & FMD_REBO2_BOND_ORDER) != 0, st);
     } else {
         if ((e = mm_bonded_launch(a.topo, a.pos, hh, a.Facc, a.part_f1, st)) != cudaSuccess) return e;
         if (a.has_charge)
@@ -561,12 +584,12 @@ cudaError_t enqueue_step(const StepArrays& a, const StepParams& p, bool rescale_
     cudaError_t e;
     // programmatic dependent launches: each kernel's launch overlaps the
     // previous one's tail (pdl.cuh)
+    // per-particle kernels: one thread per particle (grid-stride beyond kForceBlocks)
+    const int pblocks = std::max(1, std::min(kForceBlocks, (a.n + kPB - 1) / kPB));
     if ((e = launch_pdl(k_begin, dim3(1), dim3(32), 0, st, a.S, a.kind, p)) != cudaSuccess) return e;
-    if ((e = launch_pdl(k_kick, dim3(kForceBlocks), dim3(kPB), 0, st, a, p.dt)) != cudaSuccess) return e;
+    if ((e = launch_pdl(k_kick, dim3(pblocks), dim3(kPB), 0, st, a, p.dt)) != cudaSuccess) return e;
     if ((e = enqueue_forces(a, st, judge)) != cudaSuccess) return e;
-    if ((e = launch_pdl(k_kick2, dim3(kForceBlocks), dim3(kPB), 0, st, a, p.dt)) != cudaSuccess) return e;
-    if ((e = launch_pdl(k_end, dim3(1), dim3(kRedThreads), 0, st, a, p, force_partial_blocks(a), kForceBlocks)) !=
-        cudaSuccess)
+    if ((e = launch_pdl(k_kick2_end, dim3(pblocks), dim3(kPB), 0, st, a, p, force_partial_blocks(a))) != cudaSuccess)
         return e;
     if (rescale_phase && p.schedule) {
         if ((e = launch_pdl(k_rescale, dim3(kForceBlocks), dim3(kPB), 0, st, a)) != cudaSuccess) return e;

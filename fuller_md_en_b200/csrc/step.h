@@ -26,6 +26,7 @@ struct SysScal {
     int sg_judged;           // judge evaluations so far
     int sg_takeover;         // global step of the takeover (0: none)
     double sg_rmse_last, sg_rmse_max;
+    unsigned int kick2_done; // blocks of the fused second kick done this step (the last one reduces)
 };
 
 struct SgStep;   // learned REBO term of a system (sg_host.h)
@@ -66,6 +67,11 @@ struct StepArrays {
     int lj_blocks = 0;             // partial records in part_f2: the larger grid of the two gathers
     SgStep* sg = nullptr;          // AIREBO: learned REBO term instead of the plain kernel
     int rebo_blocks = kForceBlocks;  // partial records the REBO term writes into part_f1
+    // REBO-II extension (fmd_system_set_rebo2): FMD_REBO2_* flags, the device
+    // tables, and the switched-LJ correction's partials (kForceBlocks records)
+    int rebo2_flags = 0;
+    Rebo2Dev rebo2{};
+    double* part_sw = nullptr;
     // Pruned LJ rows (AIREBO, MM): host descriptor (nullptr: full rows every
     // step), and the fractional positions of the last prune and the
     // displacement word the drift raises.

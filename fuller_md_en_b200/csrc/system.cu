@@ -240,8 +240,10 @@ cudaError_t System::enqueue_rebuild_fallback(cudaStream_t st) {
 // Times every launch shape of the atomistic LJ gather over the rows
 // (rcnt, rlist; stride in_cap) and returns the fastest.  Each candidate is
 // timed right after a write larger than L2, as the gather runs inside a step
-// whose other kernels have evicted its rows; the runs accumulate into the
-// scratch accumulator, which is cleared afterwards.
+// whose other kernels have evicted its rows, behind the short-range term it
+// follows in the step; the runs accumulate into the scratch accumulator,
+// which is cleared afterwards (the force partials are rewritten by the next
+// evaluation).
 LJShape System::pick_lj_shape(const int* rcnt, const int* rlist, int& rc) {
     const int ff = arr.kind == FMD_SYS_AIREBO ? FMD_FF_AIREBO : FMD_FF_MM;
     cudaStream_t st = ctx->stream;
@@ -254,6 +256,18 @@ LJShape System::pick_lj_shape(const int* rcnt, const int* rlist, int& rc) {
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
+    // The gather follows the short-range term inside a step (programmatic
+    // launch edge, REBO's tail overlapping the gather's first blocks), so each
+    // candidate is timed together with that term: a shape that is fastest
+    // alone can lose the overlap.
+    auto short_range = [&]() -> cudaError_t {
+        const double* hh = arr.S->h;
+        if (arr.kind == FMD_SYS_MM) return mm_bonded_launch(arr.topo, arr.pos, hh, arr.Facc, arr.part_f1, st);
+        if (arr.rebo_slots)
+            return rebo_slots_launch(arr.pos, hh, arr.cnt_b, arr.list_b, arr.cap_b, arr.n, arr.rebo_slots, arr.Facc,
+                                     arr.part_f1, kForceBlocks, nullptr, 0, st, arr.rebo_ids, arr.rebo_phys != 0);
+        return rebo_launch(arr.pos, hh, arr.cnt_b, arr.list_b, arr.cap_b, arr.n, arr.Facc, arr.part_f1, st);
+    };
     float best = 1e30f;
     LJShape pick;
     for (int contig : {0, 1})
@@ -272,6 +286,7 @@ LJShape System::pick_lj_shape(const int* rcnt, const int* rlist, int& rc) {
                 for (int r = 0; r < 3; r++) {
                     if (flush) cudaMemsetAsync(flush, r, flush_bytes, st);
                     cudaEventRecord(e0, st);
+                    short_range();
                     go();
                     cudaEventRecord(e1, st);
                     cudaEventSynchronize(e1);
@@ -308,24 +323,29 @@ int System::tune_lj() {
     const int ff = arr.kind == FMD_SYS_AIREBO ? FMD_FF_AIREBO : FMD_FF_MM;
     // FMD_LJ_SHAPE="threads,unroll,feed" pins the shape of both gathers (no
     // trial launches), for reproducible runs and profiler captures; feed is
-    // 0..2, plus 4 for contiguous atom runs per block.
+    // 0..2, plus 4 for contiguous atom runs per block.  A second triple after
+    // ';' pins the gather over the pruned rows separately.
     if (const char* env = std::getenv("FMD_LJ_SHAPE")) {
-        LJShape sh;
-        int feed = -1;
-        if (std::sscanf(env, "%d,%d,%d", &sh.threads, &sh.unroll, &feed) == 3 &&
-            (sh.threads == 128 || sh.threads == 256) && (sh.unroll == 2 || sh.unroll == 4) &&
-            lj_feed_valid(feed)) {
+        auto parse = [&](const char* t, LJShape& sh) {
+            int feed = -1;
+            if (std::sscanf(t, "%d,%d,%d", &sh.threads, &sh.unroll, &feed) != 3 ||
+                !(sh.threads == 128 || sh.threads == 256) || !(sh.unroll == 2 || sh.unroll == 4) ||
+                !lj_feed_valid(feed))
+                return false;
             sh.pipe = feed & 3;
             sh.contig = feed >> 2;
-            if (lj_gather_blocks(ff, arr.precision, sh, arr.in_cap) > 0) {
-                arr.lj_shape = sh;
-                arr.lj_shape_p = sh;
-                set_lj_blocks();
-                return FMD_OK;
-            }
+            return lj_gather_blocks(ff, arr.precision, sh, arr.in_cap) > 0;
+        };
+        LJShape sh, shp;
+        const char* second = std::strchr(env, ';');
+        if (parse(env, sh) && (second ? parse(second + 1, shp) : (shp = sh, true))) {
+            arr.lj_shape = sh;
+            arr.lj_shape_p = shp;
+            set_lj_blocks();
+            return FMD_OK;
         }
-        return ctx->fail(FMD_ERR_ARG, "FMD_LJ_SHAPE: expected threads,unroll,feed with threads 128|256, "
-                                      "unroll 2|4, feed 0..2 or 4..6");
+        return ctx->fail(FMD_ERR_ARG, "FMD_LJ_SHAPE: expected threads,unroll,feed[;threads,unroll,feed] with "
+                                      "threads 128|256, unroll 2|4, feed 0..2 or 4..6");
     }
     const auto key = std::make_tuple(ctx->device, arr.kind, arr.n, arr.cap_a, arr.precision);
     auto it = cache.find(key);
@@ -805,6 +825,41 @@ extern "C" int fmd_system_set_physics(fmd_system* s, int flags) {
     return FMD_OK;
 }
 
+extern "C" int fmd_system_set_rebo2(fmd_system* s, const fmd_rebo2_knots* kn, int flags) {
+    if (!s || !s->sys) return FMD_ERR_ARG;
+    fmd::System& y = *s->sys;
+    if (y.initialized) return y.ctx->fail(FMD_ERR_ARG, "fmd_system_set_rebo2: call before fmd_system_init");
+    if (flags & ~(FMD_REBO2_BOND_ORDER | FMD_REBO2_LJ_SWITCH))
+        return y.ctx->fail(FMD_ERR_ARG, "fmd_system_set_rebo2: unknown flag");
+    if (flags && y.arr.kind != FMD_SYS_AIREBO)
+        return y.ctx->fail(FMD_ERR_ARG, "fmd_system_set_rebo2: needs an AIREBO system");
+    if (flags && !kn) return y.ctx->fail(FMD_ERR_ARG, "fmd_system_set_rebo2: no knots");
+    if ((flags & FMD_REBO2_BOND_ORDER) && y.arr.sg)
+        return y.ctx->fail(FMD_ERR_ARG, "fmd_system_set_rebo2: the system uses a learned REBO term");
+    if (flags) {
+        static_assert(sizeof(fmd_rebo2_knots) == sizeof(double) * fmd::kRebo2Knots, "knot layout");
+        std::vector<double> c(fmd::kRebo2PccCoef + 2 * (size_t)fmd::kRebo2TriCoef);
+        fmd::rebo2_coeffs(&kn->pcc[0][0], c.data(), c.data() + fmd::kRebo2PccCoef,
+                          c.data() + fmd::kRebo2PccCoef + fmd::kRebo2TriCoef);
+        if (!y.arr.rebo2.pcc) {
+            double *tab, *nc, *sw;
+            if (y.alloc(&tab, c.size(), (const double*)nullptr) || y.alloc(&nc, (size_t)y.arr.n, (const double*)nullptr) ||
+                y.alloc(&sw, (size_t)fmd::kForceBlocks * fmd::kNV, (const double*)nullptr))
+                return y.ctx->fail(FMD_ERR_CUDA, "fmd_system_set_rebo2: allocation failed");
+            y.arr.rebo2.pcc = tab;
+            y.arr.rebo2.pirc = tab + fmd::kRebo2PccCoef;
+            y.arr.rebo2.tcc = tab + fmd::kRebo2PccCoef + fmd::kRebo2TriCoef;
+            y.arr.rebo2.ncoord = nc;
+            y.arr.part_sw = sw;
+        }
+        if (cudaMemcpyAsync(const_cast<double*>(y.arr.rebo2.pcc), c.data(), sizeof(double) * c.size(),
+                            cudaMemcpyHostToDevice, y.ctx->stream) != cudaSuccess)
+            return y.ctx->fail(FMD_ERR_CUDA, "fmd_system_set_rebo2: copy failed");
+    }
+    y.arr.rebo2_flags = flags;
+    return y.ctx->sync_check("fmd_system_set_rebo2");
+}
+
 extern "C" int fmd_system_lj_full_rows(fmd_system* s, int* cnt, int* list, int* stride) {
     if (!s || !s->sys) return FMD_ERR_ARG;
     fmd::System& y = *s->sys;
@@ -831,7 +886,7 @@ extern "C" int fmd_system_lists(fmd_system* s, int* cnt_a, int* list_a, int* cnt
 }
 
 extern "C" int fmd_system_kernel_ms(fmd_system* s, int stage, int reps, double* ms) {
-    if (!s || !ms || reps < 1 || stage < 0 || stage > 4) return FMD_ERR_ARG;
+    if (!s || !ms || reps < 1 || stage < 0 || stage > 5) return FMD_ERR_ARG;
     fmd::System& y = *s->sys;
     if (!y.initialized) return y.ctx->fail(FMD_ERR_STATE, "kernel timing before init");
     cudaStream_t st = y.ctx->stream;
@@ -848,7 +903,10 @@ extern "C" int fmd_system_kernel_ms(fmd_system* s, int stage, int reps, double* 
                                         a.list_a, a.cap_a, a.in_cnt, a.in_list, a.in_cap, a.n, a.Facc, a.Facc,
                                         a.part_f2, st, a.precision, a.lj_shape, a.err);
             case 1:
-                if (a.kind == FMD_SYS_AIREBO && a.sg)   // the REBO term the step uses
+                if (a.kind == FMD_SYS_AIREBO && (a.rebo2_flags & FMD_REBO2_BOND_ORDER))   // the REBO term the step uses
+                    return rebo2_launch(a.rebo2, a.pos, hh, a.cnt_b, a.list_b, a.cap_b, a.n, a.Facc, a.part_f1,
+                                        a.rebo_blocks, st);
+                if (a.kind == FMD_SYS_AIREBO && a.sg)
                     return sg_enqueue_rebo(*a.sg, a, false, st);
                 if (a.kind == FMD_SYS_AIREBO)
                     return rebo_slots_launch(a.pos, hh, a.cnt_b, a.list_b, a.cap_b, a.n, a.rebo_slots, a.Facc,
@@ -864,6 +922,11 @@ extern "C" int fmd_system_kernel_ms(fmd_system* s, int stage, int reps, double* 
                 return lj_gather_launch(a.kind == FMD_SYS_AIREBO ? FMD_FF_AIREBO : FMD_FF_MM, a.pos, hh, a.cnt_a,
                                         a.list_a, a.cap_a, a.prune->cnt, a.prune->list, a.in_cap, a.n, a.Facc,
                                         a.Facc, a.part_f2, st, a.precision, a.lj_shape_p, a.err);
+            case 5:
+                // the switched-LJ correction, into the scratch accumulator
+                if (!(a.rebo2_flags & FMD_REBO2_LJ_SWITCH)) return cudaErrorInvalidValue;
+                return lj_switch_launch(a.rebo2, a.pos, hh, a.cnt_b, a.list_b, a.cap_b, a.cnt_a, a.list_a, a.cap_a,
+                                        a.n, a.Facc, a.part_sw, kForceBlocks, false, st);
             default:
                 return enqueue_forces(a, st);
         }
@@ -1057,6 +1120,8 @@ int fmd::System::use_surrogate(fmd_sg* model, int judge_every, double rmse_max) 
         arr.sg = nullptr;
         arr.rebo_blocks = kForceBlocks;
     } else {
+        if (arr.rebo2_flags & FMD_REBO2_BOND_ORDER)
+            return ctx->fail(FMD_ERR_ARG, "fmd_system_use_surrogate: the system uses the REBO-II bond order");
         if (!sg) {
             auto g = std::make_unique<SgStep>();
             if (sg::work_alloc(g->work, arr.n, arr.cap_b) != cudaSuccess)

@@ -165,6 +165,52 @@ int fmd_lj_half_forces(fmd_ctx *ctx, int ff, const double *pos, const double *h,
 int fmd_airebo_forces(fmd_ctx *ctx, const double *pos, const double *h, const double *hi,
                       const int *nlc_r, const int *nll_r, const int *nlc_l, const int *nll_l,
                       int na, double *F, double *vir9, double *E3);
+/* ---- REBO-II extension (no counterpart in the reference) ----
+ * The reference's REBO bond order is b = (1 + sum f_c G)^-1/2 (AI:301-323).
+ * The extension adds, for carbon-only systems, the terms of Brenner et al.,
+ * J. Phys.: Condens. Matter 14 (2002) 783:
+ *   bbar = (p_ij + p_ji)/2 + pi^rc + pi^dh,
+ *   p_ij = (1 + sum_k f_c G + P_CC(N_ij))^-1/2,  pi^rc = F_CC(N_ij, N_ji, N_conj),
+ *   pi^dh = T_CC(N_ij, N_ji, N_conj) sum_kl (1 - cos^2 w_kijl) f_c(r_ik) f_c(r_jl)
+ *           tau(cos theta_jik) tau(cos theta_ijl)
+ * (N_ij = sum_{k != j} f_c(r_ik); N_conj = 1 + A_ij^2 + A_ji^2 with
+ * A_ij = sum_{k != j} f_c(r_ik) F(N_k - f_c(r_ik)); tau = 1 for |cos| <= 0.995,
+ * cubic switch to 0 at |cos| = 1), and AIREBO's switched LJ (Stuart, Tutein,
+ * Harrison, J. Chem. Phys. 112 (2000) 6472) over the reference's LJ pairs:
+ * V(r) [1 - S(t_r) (1 - S(t_b(b*)))], t_r = (r - sigma)/(2^(1/6) sigma - sigma),
+ * t_b = (b* - 0.77)/0.04, b* the bond order of the pair's own direction.
+ * f_c, V_R, V_A, G and the LJ V are the reference's (AI:119-124, 164-191).
+ * Forces are -grad E and the virial is the full virial of every term.  The
+ * spline tables are the caller's: cubic Hermite in each variable through
+ * values and derivatives given at integer knots (with every knot zero the
+ * bond order is the reference's). */
+typedef struct fmd_rebo2_knots {
+    double pcc[5][2];           /* P_CC(N, N_H = 0) at N = 0..4: {P, dP/dN} */
+    double pirc[5][5][10][8];   /* pi^rc_CC at N_ij, N_ji = 0..4, N_conj = 0..9:
+                                   {f, f_x, f_y, f_z, f_xy, f_xz, f_yz, f_xyz} */
+    double tcc[5][5][10][8];    /* T_CC, same layout */
+} fmd_rebo2_knots;
+enum fmd_rebo2_flags { FMD_REBO2_BOND_ORDER = 1, FMD_REBO2_LJ_SWITCH = 2 };
+/* Host only (no GPU needed): the splines' per-cell polynomial coefficients
+ * that the kernels evaluate, out[16 + 2 * 9216]: P_CC as out[4 n + a] (u^a on
+ * cell [n, n+1)), then pi^rc_CC and T_CC as [((x * 4 + y) * 9 + z) * 64 +
+ * a + 4 b + 16 c] (u^a v^b w^c on the cell at (x, y, z)), u, v, w the
+ * offsets from the cell's lower knots.  Arguments beyond the knots are
+ * clamped to them. */
+int fmd_rebo2_coeffs(const fmd_rebo2_knots *kn, double *out);
+/* REBO-II energy over the bonds i < j of the REBO rows (the enumeration of
+ * AI:286-290): ADDS -grad E into F and the virial into vir9; *E = energy. */
+int fmd_rebo2_forces(fmd_ctx *ctx, const double *pos, const double *h, const double *hi,
+                     const int *nlc, const int *nll, int max_neigh, int na, const fmd_rebo2_knots *kn,
+                     double *F, double *vir9, double *E);
+/* The switched-LJ correction over the LJ half rows (nlc_l, nll_l): *E = sum of
+ * -V S(t_r) (1 - S(t_b(b*))); ADDS its -grad into F and its virial into vir9.
+ * The switched LJ term is fmd_lj_half_forces (FMD_FF_AIREBO) plus this. */
+int fmd_lj_switch_forces(fmd_ctx *ctx, const double *pos, const double *h, const double *hi,
+                         const int *nlc_r, const int *nll_r, int max_neigh_r,
+                         const int *nlc_l, const int *nll_l, int max_neigh_l, int na,
+                         const fmd_rebo2_knots *kn, double *F, double *vir9, double *E);
+
 /* compute_forces (MM:351-788): zeroes F, vir9;
  * E7 = {Eb, Ea, Ed, Ei, Elj, Ecoul, Etot}.  LJ list width 400. */
 int fmd_mm_forces(fmd_ctx *ctx, const fmd_mm_topology *t, const double *pos, const double *h,
@@ -282,16 +328,24 @@ int fmd_system_lj_full_rows(fmd_system *s, int *cnt, int *list, int *stride);
 /* Physics corrections (fmd_physics bits) of a system; before fmd_system_init.
  * A bit the system's force field lacks is an FMD_ERR_ARG. */
 int fmd_system_set_physics(fmd_system *s, int flags);
+/* REBO-II extension in an AIREBO system (see fmd_rebo2_knots): flags
+ * FMD_REBO2_BOND_ORDER replaces the REBO term, FMD_REBO2_LJ_SWITCH switches the
+ * LJ term; 0 turns both off.  Call before fmd_system_init; not with a learned
+ * REBO term.  The system's energies and virial then hold the extended terms
+ * (E[1] REBO-II, E[2] the switched LJ). */
+int fmd_system_set_rebo2(fmd_system *s, const fmd_rebo2_knots *kn, int flags);
 int fmd_system_destroy(fmd_system *s);
 
 /* Measurement helpers (no reference counterpart).  fmd_system_kernel_ms
  * launches one stage `reps` times on the context stream between CUDA events
  * and returns the mean duration per launch in milliseconds; stages:
  *   0 the pair kernel (rigid site-site LJ, or the atomistic LJ gather),
- *   1 the second force kernel (REBO, or MM bonded), 2 a full list rebuild,
+ *   1 the second force kernel (REBO -- REBO-II when the system uses it --,
+ *     or MM bonded), 2 a full list rebuild,
  *   3 the whole force evaluation of a step (eager launches),
  *   4 the atomistic LJ gather over the pruned rows of the last prune (see
- *     fmd_system_set_lj_prune).
+ *     fmd_system_set_lj_prune),
+ *   5 the switched-LJ correction (systems with FMD_REBO2_LJ_SWITCH).
  * The force stages leave F in place (they recompute the current forces).
  * fmd_system_step_kernels returns the number of kernel launches of one step
  * of each variant (list rebuild or not; phase bit 0: cold/warm phase, bit 1:

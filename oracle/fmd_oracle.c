@@ -316,6 +316,15 @@ static double clamp1(double c)
     return c;
 }
 
+/* The C-C pair pieces above for other files of the oracle (rebo2_oracle.c). */
+void fmo_rebo_pair_fns(double r, double *fc, double *dfc, double *vr, double *dvr, double *va, double *dva)
+{
+    *fc = sw_fc(r); *dfc = sw_dfc(r);
+    *vr = rep_v(r); *dvr = rep_dv(r);
+    *va = att_v(r); *dva = att_dv(r);
+}
+double fmo_rebo_ang_g(double c) { return ang_g(c); }
+
 /* Bond-order sum of the centre atom c around its bond to `skip`, whose bond
  * vector from c is (bx,by,bz) with length rb (AI:301-309, 313-322). */
 static double bo_sum(const double *pos, const double *h, const double *hi, const int *cnt,

@@ -78,6 +78,33 @@ void fmo_airebo_forces(double *F, double *vir9, const double *pos, const double 
                        const int *cnt_r, const int *list_r, const int *cnt_l, const int *list_l,
                        int na, double *E);
 
+/* ---- f4: REBO-II extension (rebo2_oracle.c; no reference counterpart) ----
+ * Spline knots of the carbon-only terms, field for field as fmd_rebo2_knots
+ * in include/fullermd.h: P_CC(N, 0) at N = 0..4 (value, dP/dN); pi^rc_CC and
+ * T_CC on the integer knots N_ij, N_ji in 0..4, N_conj in 0..9 with
+ * f, f_x, f_y, f_z, f_xy, f_xz, f_yz, f_xyz per knot. */
+typedef struct {
+    double pcc[5][2];
+    double pirc[5][5][10][8];
+    double tcc[5][5][10][8];
+} fmo_rebo2_knots;
+/* N_k = sum of f_c over k's REBO row. */
+void fmo_rebo2_coordination(const double *pos, const double *h, const double *hi, const int *cnt,
+                            const int *list, int max_neigh, int na, double *ncoord);
+/* bbar_ij = (p_ij + p_ji)/2 + pi^rc + T sum(1 - cos^2) ... for bond vector dij = r_j - r_i. */
+double fmo_rebo2_bond_order(const double *pos, const double *h, const double *hi, const int *cnt,
+                            const int *list, int max_neigh, const fmo_rebo2_knots *kn, const double *ncoord,
+                            int i, int j, const double *dij);
+/* REBO-II energy over the bonds i < j of the REBO rows. */
+double fmo_rebo2_energy(const double *pos, const double *h, const double *hi, const int *cnt, const int *list,
+                        int max_neigh, int na, const fmo_rebo2_knots *kn);
+/* Switched-LJ correction over the LJ half rows: sum of -V S(t_r) (1 - S(t_b(b*))). */
+double fmo_lj_switch_energy(const double *pos, const double *h, const double *hi, const int *cnt_r,
+                            const int *list_r, int max_neigh_r, const int *cnt_l, const int *list_l,
+                            int max_neigh_l, int na, const fmo_rebo2_knots *kn);
+double fmo_rebo2_spline3(const fmo_rebo2_knots *kn, int which, double x, double y, double z);
+double fmo_rebo2_spline_p(const fmo_rebo2_knots *kn, double x);
+
 /* ---- a10-a16: molecular mechanics (MM:226-788) ---- */
 typedef struct {
     int nb;   const int *b_i0, *b_i1; const double *b_kb, *b_r0;

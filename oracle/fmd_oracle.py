@@ -3,7 +3,8 @@
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
 cpu_baseline / reference legs of bench.py, never by the product package.
 
-* ``Oracle``: the CPU restatement (fmd_oracle.c, _build/libfmd_oracle.so).
+* ``Oracle``: the CPU restatement (fmd_oracle.c and the REBO-II extension's
+  rebo2_oracle.c, _build/libfmd_oracle.so).
 * ``Ref``: the unmodified reference translation units behind extern "C"
   shims (_ref/libref_*.so), when they have been built.
 """
@@ -60,6 +61,21 @@ class MMTopo(ctypes.Structure):
                 ("d_mult", _ip), ("d_gamma", _dp),
                 ("nimp", c_int), ("m_i0", _ip), ("m_i1", _ip), ("m_i2", _ip), ("m_i3", _ip), ("m_ki", _dp),
                 ("m_gamma", _dp)]
+
+
+class Rebo2Knots(ctypes.Structure):
+    """fmo_rebo2_knots (the layout of fmd_rebo2_knots): P_CC(N, 0) knots
+    [5][2], pi^rc_CC and T_CC knots [5][5][10][8]."""
+    _fields_ = [("pcc", c_double * 10), ("pirc", c_double * 2000), ("tcc", c_double * 2000)]
+
+    @classmethod
+    def of(cls, pcc, pirc, tcc):
+        s = cls()
+        for name, a, n in (("pcc", pcc, 10), ("pirc", pirc, 2000), ("tcc", tcc, 2000)):
+            a = np.ascontiguousarray(a, np.float64).reshape(-1)
+            assert a.size == n, (name, a.size)
+            ctypes.memmove(getattr(s, name), a.ctypes.data, 8 * n)
+        return s
 
 
 def make_topo(t: dict):
@@ -133,6 +149,18 @@ class Oracle:
                                       _ip, _ip, _dp]
         L.fmo_mm_step.argtypes = [_dp, _dp, _dp, _dp, _dp, _dp, c_int, c_double, POINTER(FmoNpt), POINTER(MMTopo),
                                   _ip, _ip, _dp, _ip, c_int, _dp]
+        K = POINTER(Rebo2Knots)
+        L.fmo_rebo2_energy.restype = c_double
+        L.fmo_rebo2_energy.argtypes = [_dp, _dp, _dp, _ip, _ip, c_int, c_int, K]
+        L.fmo_lj_switch_energy.restype = c_double
+        L.fmo_lj_switch_energy.argtypes = [_dp, _dp, _dp, _ip, _ip, c_int, _ip, _ip, c_int, c_int, K]
+        L.fmo_rebo2_coordination.argtypes = [_dp, _dp, _dp, _ip, _ip, c_int, c_int, _dp]
+        L.fmo_rebo2_bond_order.restype = c_double
+        L.fmo_rebo2_bond_order.argtypes = [_dp, _dp, _dp, _ip, _ip, c_int, K, _dp, c_int, c_int, _dp]
+        L.fmo_rebo2_spline3.restype = c_double
+        L.fmo_rebo2_spline3.argtypes = [K, c_int, c_double, c_double, c_double]
+        L.fmo_rebo2_spline_p.restype = c_double
+        L.fmo_rebo2_spline_p.argtypes = [K, c_double]
         L.fmo_mat_inv9.argtypes = [_dp, _dp]
         L.fmo_apply_pbc.argtypes = [_dp, _dp, _dp, c_int]
 
@@ -207,6 +235,30 @@ class Oracle:
         F = np.zeros(3 * na)
         E = self.L.fmo_rebo_grad(d(F), d(pos), d(h), d(hi), i(cr), i(lr), max_neigh, na)
         return E, F
+
+    # REBO-II extension (no reference counterpart; rebo2_oracle.c)
+    def rebo2_energy(self, pos, h, hi, cr, lr, na, knots: Rebo2Knots, max_neigh=12):
+        return self.L.fmo_rebo2_energy(d(pos), d(h), d(hi), i(cr), i(lr), max_neigh, na, ctypes.byref(knots))
+
+    def lj_switch_energy(self, pos, h, hi, cr, lr, cl, ll, na, knots: Rebo2Knots, max_neigh_r=12, max_neigh_l=400):
+        return self.L.fmo_lj_switch_energy(d(pos), d(h), d(hi), i(cr), i(lr), max_neigh_r, i(cl), i(ll),
+                                           max_neigh_l, na, ctypes.byref(knots))
+
+    def rebo2_coordination(self, pos, h, hi, cr, lr, na, max_neigh=12):
+        nc = np.zeros(na)
+        self.L.fmo_rebo2_coordination(d(pos), d(h), d(hi), i(cr), i(lr), max_neigh, na, d(nc))
+        return nc
+
+    def rebo2_bond_order(self, pos, h, hi, cr, lr, knots: Rebo2Knots, ncoord, a, b, dab, max_neigh=12):
+        dv = np.ascontiguousarray(dab, np.float64)
+        return self.L.fmo_rebo2_bond_order(d(pos), d(h), d(hi), i(cr), i(lr), max_neigh, ctypes.byref(knots),
+                                           d(ncoord), int(a), int(b), d(dv))
+
+    def rebo2_spline3(self, knots: Rebo2Knots, which, x, y, z):
+        return self.L.fmo_rebo2_spline3(ctypes.byref(knots), int(which), float(x), float(y), float(z))
+
+    def rebo2_spline_p(self, knots: Rebo2Knots, x):
+        return self.L.fmo_rebo2_spline_p(ctypes.byref(knots), float(x))
 
     def mm_topology_mol(self, coords, bonds):
         coords = np.ascontiguousarray(coords, np.float64).reshape(-1)
