@@ -130,7 +130,7 @@ namespace {
 enum Slot {
     S_POS = 0, S_HH, S_MOL, S_CNT, S_LIST, S_CNT2, S_LIST2, S_INCNT, S_INLIST, S_DROP,
     S_F, S_FACC, S_T, S_QV, S_BODY, S_VEL, S_OMG, S_MASS, S_PART1, S_PART2, S_PART3, S_PARTKE,
-    S_SCAL, S_CHARGE, S_RSLOT, S_RLAB, S_R2TAB, S_R2NC, S_TOPO0
+    S_SCAL, S_CHARGE, S_RSLOT, S_RLAB, S_R2TAB, S_R2NC, S_R2BOND, S_R2PAIR, S_R2CNT, S_TOPO0
 };
 
 template <class T>
@@ -498,18 +498,28 @@ namespace {
 
 // REBO-II tables of one host call: the knots expanded into per-cell
 // coefficients and uploaded, and the coordination scratch.
-int rebo2_tables(fmd_ctx* ctx, const fmd_rebo2_knots* kn, int na, Rebo2Dev& t) {
+int rebo2_tables(fmd_ctx* ctx, const fmd_rebo2_knots* kn, int na, int cap_b, Rebo2Dev& t) {
     static_assert(sizeof(fmd_rebo2_knots) == sizeof(double) * kRebo2Knots, "knot layout");
     std::vector<double> c(kRebo2PccCoef + 2 * (size_t)kRebo2TriCoef);
     rebo2_coeffs(&kn->pcc[0][0], c.data(), c.data() + kRebo2PccCoef, c.data() + kRebo2PccCoef + kRebo2TriCoef);
     double *tab, *nc;
+    int2 *bonds, *pairs;
+    int* counts;
     int rc = up(ctx, S_R2TAB, c.data(), c.size(), &tab);
     if (!rc) rc = up<double>(ctx, S_R2NC, nullptr, (size_t)na, &nc);
+    if (!rc) rc = up<int2>(ctx, S_R2BOND, nullptr, (size_t)na * cap_b, &bonds);
+    if (!rc) rc = up<int2>(ctx, S_R2PAIR, nullptr, (size_t)na * kRebo2SwitchPerAtom, &pairs);
+    if (!rc) rc = up<int>(ctx, S_R2CNT, nullptr, 2, &counts);
     if (rc) return rc;
     t.pcc = tab;
     t.pirc = tab + kRebo2PccCoef;
     t.tcc = tab + kRebo2PccCoef + kRebo2TriCoef;
     t.ncoord = nc;
+    t.bonds = bonds;
+    t.sw_pairs = pairs;
+    t.counts = counts;
+    t.sw_cap = na * kRebo2SwitchPerAtom;
+    t.err = ctx->d_err;
     // the staging vector dies at return: finish the copy first
     return cudaStreamSynchronize(ctx->stream) == cudaSuccess ? FMD_OK
                                                              : ctx->fail(FMD_ERR_CUDA, "table upload failed");
@@ -557,7 +567,7 @@ extern "C" int fmd_rebo2_forces(fmd_ctx* ctx, const double* pos, const double* h
     if (!rc) rc = up(ctx, S_CNT2, nlc, na, &dc);
     if (!rc) rc = up(ctx, S_LIST2, nll, (size_t)na * max_neigh, &dl);
     if (!rc) rc = up<double>(ctx, S_PART1, nullptr, (size_t)kForceBlocks * kNV, &part);
-    if (!rc) rc = rebo2_tables(ctx, kn, na, t);
+    if (!rc) rc = rebo2_tables(ctx, kn, na, max_neigh, t);
     if (rc) return rc;
     if (rebo2_launch(t, dpos, hh, dc, dl, max_neigh, na, dF, part, kForceBlocks, ctx->stream) != cudaSuccess)
         return ctx->fail(FMD_ERR_CUDA, "rebo2 launch failed");
@@ -586,7 +596,7 @@ extern "C" int fmd_lj_switch_forces(fmd_ctx* ctx, const double* pos, const doubl
     if (!rc) rc = up(ctx, S_CNT, nlc_l, na, &dcl);
     if (!rc) rc = up(ctx, S_LIST, nll_l, (size_t)na * max_neigh_l, &dll);
     if (!rc) rc = up<double>(ctx, S_PART1, nullptr, (size_t)kForceBlocks * kNV, &part);
-    if (!rc) rc = rebo2_tables(ctx, kn, na, t);
+    if (!rc) rc = rebo2_tables(ctx, kn, na, max_neigh_r, t);
     if (rc) return rc;
     if (lj_switch_launch(t, dpos, hh, dcr, dlr, max_neigh_r, dcl, dll, max_neigh_l, na, dF, part, kForceBlocks,
                          false, ctx->stream) != cudaSuccess)

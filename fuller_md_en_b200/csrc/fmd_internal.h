@@ -47,7 +47,7 @@ struct DevErr {
 
 enum KernelId {
     K_NLIST = 1, K_TRANSPOSE = 2, K_REBO = 3, K_LJ = 4, K_RIGID = 5, K_MM = 6, K_INTEGRATE = 7,
-    K_CELLS = 8,
+    K_CELLS = 8, K_REBO2 = 9,
 };
 
 }  // namespace fmd

@@ -113,11 +113,20 @@ constexpr int kRebo2TriCoef = kRebo2Nx * kRebo2Ny * kRebo2Nz * 64;
 // knots as fmd_rebo2_knots: P_CC {P, dP/dN} x (Nx+1), then pi^rc and T_CC,
 // each (Nx+1)(Ny+1)(Nz+1) x {f, fx, fy, fz, fxy, fxz, fyz, fxyz}
 constexpr int kRebo2Knots = 2 * (kRebo2Nx + 1) + 2 * (kRebo2Nx + 1) * (kRebo2Ny + 1) * (kRebo2Nz + 1) * 8;
+// Close LJ pairs per atom the switched-LJ work list holds (more is an
+// FMD_ERR_CAPACITY): far above the ~40 atoms dense carbon places within
+// 2^(1/6) sigma of an atom.
+constexpr int kRebo2SwitchPerAtom = 64;
 struct Rebo2Dev {
     const double* pcc = nullptr;
     const double* pirc = nullptr;
     const double* tcc = nullptr;
     double* ncoord = nullptr;      // [n] scratch: sum of f_c over each atom's REBO row
+    int2* bonds = nullptr;         // [n * cap_b] scratch: compacted bonds (i, j)
+    int2* sw_pairs = nullptr;      // [sw_cap] scratch: compacted close LJ pairs
+    int* counts = nullptr;         // [2] lengths of the two lists
+    int sw_cap = 0;                // n * kRebo2SwitchPerAtom
+    DevErr* err = nullptr;
 };
 // Host: the per-cell coefficients of the cubic Hermite splines through the
 // knots (kRebo2Knots doubles) into pcc, pirc, tcc.

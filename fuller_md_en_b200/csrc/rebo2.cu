@@ -35,8 +35,9 @@
 // every term depends on bond vectors only, and each gradient g with respect to
 // a bond vector e = r_b - r_a adds F_a += g, F_b -= g and W -= e (x) g (the
 // reference's pair virial convention, AI:339-349, extended to every term).
-// One thread per bond (REBO) or per LJ half-row entry, FP64 throughout,
-// forces by atomics, energy and virial as per-block partial records.
+// A scan compacts the work (the bonds of the REBO rows; the LJ pairs closer
+// than 2^(1/6) sigma), then one thread per item, FP64 throughout, forces by
+// atomics, energy and virial as per-block partial records.
 #include <cmath>
 #include <cstring>
 
@@ -52,6 +53,7 @@ using namespace rebo;
 
 constexpr double kBswMin = 0.77, kBswMax = 0.81;   // bond-order switch of the LJ term
 constexpr double kTauC0 = 0.995;                   // dihedral angle weight starts to fall
+constexpr double kSwitchRmaxOverSigma2 = 1.2599210498948732;   // (2^(1/6))^2: the switch ends at 2^(1/6) sigma
 
 struct V3 {
     double x, y, z;
@@ -404,12 +406,60 @@ k_rebo2_coord(const double* __restrict__ pos, const double* __restrict__ hh, con
     }
 }
 
-// One thread per REBO row slot i -> j with j > i (the bond enumeration of
-// AI:286-290): the bond's energy, and forces and virial of its gradient.
+// Appends (i, j) to a compacted work list from every lane of the warp that
+// takes its entry (one atomic per warp); entries beyond cap are dropped and
+// reported in err.  The whole warp calls it.
+__device__ __forceinline__ void warp_append(bool take, int i, int j, int2* __restrict__ out, int* __restrict__ count,
+                                            int cap, DevErr* err) {
+    const unsigned m = __ballot_sync(kFull, take);
+    if (!m) return;
+    const int lane = threadIdx.x & 31, lead = __ffs(m) - 1;
+    int base = 0;
+    if (lane == lead) base = atomicAdd(count, __popc(m));
+    base = __shfl_sync(kFull, base, lead);
+    if (!take) return;
+    const int k = base + __popc(m & ((1u << lane) - 1u));
+    if (k < cap) out[k] = make_int2(i, j);
+    else if (err && atomicCAS(&err->code, FMD_OK, FMD_ERR_CAPACITY) == FMD_OK) {
+        err->where = K_REBO2; err->index = i; err->value = k + 1;
+    }
+}
+
+// The bonds of the REBO rows: slot i -> j with j > i (the enumeration of
+// AI:286-290) and r < D_max, compacted (the rows are 12 wide and hold ~3).
 __global__ void __launch_bounds__(256)
+k_rebo2_scan(const double* __restrict__ pos, const double* __restrict__ hh, const int* __restrict__ cnt,
+             const int* __restrict__ list, int cap, int na, Rebo2Dev t) {
+    FMD_PDL_WAIT();
+    __shared__ double s_hh[18];
+    if (threadIdx.x < 18) s_hh[threadIdx.x] = hh[threadIdx.x];
+    __syncthreads();
+    const long long tot = (long long)na * cap, stride = (long long)gridDim.x * blockDim.x;
+    for (long long b = blockIdx.x * (long long)blockDim.x + (threadIdx.x & ~31); b < tot; b += stride) {
+        const long long s = b + (threadIdx.x & 31);
+        bool take = false;
+        int i = 0, j = 0;
+        if (s < tot) {
+            i = (int)(s / cap);
+            const int jn = (int)(s - (long long)i * cap);
+            if (jn < cnt[i]) {
+                j = list[s];
+                if (j > i) {
+                    double x, y, z;
+                    bond_vec(pos, i, j, s_hh, s_hh + 9, x, y, z);
+                    take = sqrt(x * x + y * y + z * z) < DMAX_CC;
+                }
+            }
+        }
+        warp_append(take, i, j, t.bonds, &t.counts[0], na * cap, nullptr);
+    }
+}
+
+// One thread per bond of the compacted list: the bond's energy, and forces
+// and virial of its gradient.
+__global__ void __launch_bounds__(128)
 k_rebo2_bonds(const double* __restrict__ pos, const double* __restrict__ hh, const int* __restrict__ cnt,
-              const int* __restrict__ list, int cap, int na, Rebo2Dev t, double* __restrict__ F,
-              double* __restrict__ part) {
+              const int* __restrict__ list, int cap, Rebo2Dev t, double* __restrict__ F, double* __restrict__ part) {
     FMD_PDL_WAIT();
     __shared__ double sm[32 * kNV];
     __shared__ double s_hh[18];
@@ -420,15 +470,12 @@ k_rebo2_bonds(const double* __restrict__ pos, const double* __restrict__ hh, con
 #pragma unroll
     for (int k = 0; k < kNV; k++) acc[k] = 0.0;
     double w[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    const long long tot = (long long)na * cap;
-    for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < tot; s += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(s / cap), jn = (int)(s - (long long)i * cap);
-        if (jn >= cnt[i]) continue;
-        const int j = list[s];
-        if (j <= i) continue;
+    const int nb = t.counts[0];
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nb; k += gridDim.x * blockDim.x) {
+        const int2 ij = t.bonds[k];
+        const int i = ij.x, j = ij.y;
         const V3 d = bvec(g, i, j);
         const double r = len(d);
-        if (r >= DMAX_CC) continue;
         double fc, dfc, vr, dvr, va, dva;
         cut_fns(r, fc, dfc);
         pair_fns(r, vr, dvr, va, dva);
@@ -444,13 +491,41 @@ k_rebo2_bonds(const double* __restrict__ pos, const double* __restrict__ hh, con
     block_sum_store<kNV>(acc, sm, part + (size_t)blockIdx.x * kNV);
 }
 
-// One thread per LJ half-row entry; only pairs closer than 2^(1/6) sigma do
-// work: the correction -V S(t_r) (1 - S(t_b(b*))) that turns the plain LJ
-// term into the switched one.
+// The LJ pairs closer than 2^(1/6) sigma (where the switch acts), compacted
+// from the half rows.
 __global__ void __launch_bounds__(256)
+k_lj_switch_scan(const double* __restrict__ pos, const double* __restrict__ hh, const int* __restrict__ cnt_a,
+                 const int* __restrict__ list_a, int cap_a, int na, Rebo2Dev t) {
+    FMD_PDL_WAIT();
+    __shared__ double s_hh[18];
+    if (threadIdx.x < 18) s_hh[threadIdx.x] = hh[threadIdx.x];
+    __syncthreads();
+    const LJP lp = lj_params_dev(FMD_FF_AIREBO);
+    const double rmax2 = kSwitchRmaxOverSigma2 * lp.sig2;
+    const long long tot = (long long)na * cap_a, stride = (long long)gridDim.x * blockDim.x;
+    for (long long b = blockIdx.x * (long long)blockDim.x + (threadIdx.x & ~31); b < tot; b += stride) {
+        const long long s = b + (threadIdx.x & 31);
+        bool take = false;
+        int i = 0, j = 0;
+        if (s < tot) {
+            i = (int)(s / cap_a);
+            const int jn = (int)(s - (long long)i * cap_a);
+            if (jn < cnt_a[i]) {
+                j = list_a[s];
+                double x, y, z;
+                bond_vec(pos, i, j, s_hh, s_hh + 9, x, y, z);
+                take = x * x + y * y + z * z < rmax2;
+            }
+        }
+        warp_append(take, i, j, t.sw_pairs, &t.counts[1], t.sw_cap, t.err);
+    }
+}
+
+// One thread per compacted close LJ pair: the correction
+// -V S(t_r) (1 - S(t_b(b*))) that turns the plain LJ term into the switched one.
+__global__ void __launch_bounds__(128)
 k_lj_switch(const double* __restrict__ pos, const double* __restrict__ hh, const int* __restrict__ cnt_b,
-            const int* __restrict__ list_b, int cap_b, const int* __restrict__ cnt_a, const int* __restrict__ list_a,
-            int cap_a, int na, Rebo2Dev t, double* __restrict__ F, double* __restrict__ part) {
+            const int* __restrict__ list_b, int cap_b, Rebo2Dev t, double* __restrict__ F, double* __restrict__ part) {
     FMD_PDL_WAIT();
     __shared__ double sm[32 * kNV];
     __shared__ double s_hh[18];
@@ -458,20 +533,17 @@ k_lj_switch(const double* __restrict__ pos, const double* __restrict__ hh, const
     __syncthreads();
     const Geo g{pos, cnt_b, list_b, cap_b, s_hh, s_hh + 9, t.ncoord, t};
     const LJP lp = lj_params_dev(FMD_FF_AIREBO);
-    const double sig = sqrt(lp.sig2), rmax = 1.122462048309373 * sig;   // 2^(1/6) sigma
+    const double sig = sqrt(lp.sig2), rmax = sqrt(kSwitchRmaxOverSigma2) * sig;
     double acc[kNV];
 #pragma unroll
     for (int k = 0; k < kNV; k++) acc[k] = 0.0;
     double w[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    const long long tot = (long long)na * cap_a;
-    for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < tot; s += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(s / cap_a), jn = (int)(s - (long long)i * cap_a);
-        if (jn >= cnt_a[i]) continue;
-        const int j = list_a[s];
+    const int np = min(t.counts[1], t.sw_cap);
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < np; k += gridDim.x * blockDim.x) {
+        const int2 ij = t.sw_pairs[k];
+        const int i = ij.x, j = ij.y;
         const V3 d = bvec(g, i, j);
-        const double r2 = dot(d, d);
-        if (r2 >= rmax * rmax) continue;
-        const double r = sqrt(r2);
+        const double r2 = dot(d, d), r = sqrt(r2);
         double sr, dsr;
         sw_cubic((r - sig) / (rmax - sig), sr, dsr);
         if (sr == 0.0) continue;
@@ -511,20 +583,26 @@ cudaError_t rebo2_coord_launch(const Rebo2Dev& t, const double* pos, const doubl
 
 cudaError_t rebo2_launch(const Rebo2Dev& t, const double* pos, const double* hh, const int* cnt, const int* list,
                          int cap, int na, double* F, double* part, int nblk, cudaStream_t st) {
-    cudaError_t e = rebo2_coord_launch(t, pos, hh, cnt, list, cap, na, st);
-    if (e != cudaSuccess) return e;
-    return launch_pdl(k_rebo2_bonds, dim3(nblk), dim3(256), 0, st, pos, hh, cnt, list, cap, na, t, F, part);
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(t.counts, 0, 2 * sizeof(int), st)) != cudaSuccess) return e;
+    if ((e = rebo2_coord_launch(t, pos, hh, cnt, list, cap, na, st)) != cudaSuccess) return e;
+    const int ns = std::max(1, std::min((int)(((long long)na * cap + 255) / 256), kForceBlocks));
+    if ((e = launch_pdl(k_rebo2_scan, dim3(ns), dim3(256), 0, st, pos, hh, cnt, list, cap, na, t)) != cudaSuccess)
+        return e;
+    return launch_pdl(k_rebo2_bonds, dim3(nblk), dim3(128), 0, st, pos, hh, cnt, list, cap, t, F, part);
 }
 
 cudaError_t lj_switch_launch(const Rebo2Dev& t, const double* pos, const double* hh, const int* cnt_b,
                              const int* list_b, int cap_b, const int* cnt_a, const int* list_a, int cap_a, int na,
                              double* F, double* part, int nblk, bool coord_ready, cudaStream_t st) {
-    if (!coord_ready) {
-        const cudaError_t e = rebo2_coord_launch(t, pos, hh, cnt_b, list_b, cap_b, na, st);
-        if (e != cudaSuccess) return e;
-    }
-    return launch_pdl(k_lj_switch, dim3(nblk), dim3(256), 0, st, pos, hh, cnt_b, list_b, cap_b, cnt_a, list_a,
-                      cap_a, na, t, F, part);
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(t.counts + 1, 0, sizeof(int), st)) != cudaSuccess) return e;
+    if (!coord_ready && (e = rebo2_coord_launch(t, pos, hh, cnt_b, list_b, cap_b, na, st)) != cudaSuccess) return e;
+    const int ns = std::max(1, std::min((int)(((long long)na * cap_a + 255) / 256), 4 * kForceBlocks));
+    if ((e = launch_pdl(k_lj_switch_scan, dim3(ns), dim3(256), 0, st, pos, hh, cnt_a, list_a, cap_a, na, t)) !=
+        cudaSuccess)
+        return e;
+    return launch_pdl(k_lj_switch, dim3(nblk), dim3(128), 0, st, pos, hh, cnt_b, list_b, cap_b, t, F, part);
 }
 
 void rebo2_coeffs(const double* knots, double* pcc, double* pirc, double* tcc) {

@@ -233,18 +233,20 @@ cudaError_t System::enqueue_rebuild_fallback(cudaStream_t st) {
                            const_cast<int*>(arr.in_list), arr.in_cap, ctx->d_err, st, gate);
 }
 
-// Launch shape of the atomistic LJ gather: every candidate (threads per
-// block, list entries in flight per lane, software pipelining) is timed on
-// this system's own lists at set-up and the fastest kept; the choice is
-// cached per (device, kind, atoms, list width, precision) for the process.
-// Times every launch shape of the atomistic LJ gather over the rows
-// (rcnt, rlist; stride in_cap) and returns the fastest.  Each candidate is
-// timed right after a write larger than L2, as the gather runs inside a step
-// whose other kernels have evicted its rows, behind the short-range term it
-// follows in the step; the runs accumulate into the scratch accumulator,
-// which is cleared afterwards (the force partials are rewritten by the next
-// evaluation).
-LJShape System::pick_lj_shape(const int* rcnt, const int* rlist, int& rc) {
+// Times every launch shape of the atomistic LJ gather and returns the
+// fastest.  Each candidate is timed as the step runs it: right after a write
+// larger than L2 (the step's other kernels have evicted the rows), behind the
+// short-range term it follows (programmatic launch edge), writing F from the
+// accumulator.  pruned: the gather of a system with pruned rows, which walks
+// the pruned rows on most evaluations and the full rows (writing new pruned
+// rows) on the rest; its cost is the walk plus one prune evaluation per
+// kPruneEvery walks (the prune rate of the bench workload).  Otherwise the
+// gather over the full rows alone.  The timed launches leave the accumulator
+// zero and F holding the plain short-range term plus LJ (the caller
+// recomputes F when it must hold the system's forces); a forced prune
+// evaluation rewrites the pruned rows as they are (same positions).
+LJShape System::pick_lj_shape(bool pruned, int& rc) {
+    constexpr int kPruneEvery = 8;
     const int ff = arr.kind == FMD_SYS_AIREBO ? FMD_FF_AIREBO : FMD_FF_MM;
     cudaStream_t st = ctx->stream;
     void* flush = nullptr;
@@ -256,10 +258,6 @@ LJShape System::pick_lj_shape(const int* rcnt, const int* rlist, int& rc) {
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    // The gather follows the short-range term inside a step (programmatic
-    // launch edge, REBO's tail overlapping the gather's first blocks), so each
-    // candidate is timed together with that term: a shape that is fastest
-    // alone can lose the overlap.
     auto short_range = [&]() -> cudaError_t {
         const double* hh = arr.S->h;
         if (arr.kind == FMD_SYS_MM) return mm_bonded_launch(arr.topo, arr.pos, hh, arr.Facc, arr.part_f1, st);
@@ -267,6 +265,21 @@ LJShape System::pick_lj_shape(const int* rcnt, const int* rlist, int& rc) {
             return rebo_slots_launch(arr.pos, hh, arr.cnt_b, arr.list_b, arr.cap_b, arr.n, arr.rebo_slots, arr.Facc,
                                      arr.part_f1, kForceBlocks, nullptr, 0, st, arr.rebo_ids, arr.rebo_phys != 0);
         return rebo_launch(arr.pos, hh, arr.cnt_b, arr.list_b, arr.cap_b, arr.n, arr.Facc, arr.part_f1, st);
+    };
+    const LJPruneOut walk = pruned ? lj_prune_out(prune) : LJPruneOut{};
+    LJPruneOut full = walk;
+    full.words = nullptr;                // no decision: the full rows, pruned rows written
+    auto time_one = [&](const LJShape& sh, const LJPruneOut& po, int r) {
+        if (flush) cudaMemsetAsync(flush, r, flush_bytes, st);
+        cudaEventRecord(e0, st);
+        short_range();
+        lj_gather_launch(ff, arr.pos, arr.S->h, arr.cnt_a, arr.list_a, arr.cap_a, arr.in_cnt, arr.in_list, arr.in_cap,
+                         arr.n, arr.F, arr.Facc, arr.part_f2, st, arr.precision, sh, ctx->d_err, po);
+        cudaEventRecord(e1, st);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        return ms;
     };
     float best = 1e30f;
     LJShape pick;
@@ -276,23 +289,13 @@ LJShape System::pick_lj_shape(const int* rcnt, const int* rlist, int& rc) {
             for (int pipe : {0, 1, 2}) {
                 const LJShape sh{nt, u, pipe, contig};
                 if (lj_gather_blocks(ff, arr.precision, sh, arr.in_cap) < 1) continue;
-                auto go = [&]() {
-                    return lj_gather_launch(ff, arr.pos, arr.S->h, arr.cnt_a, arr.list_a, arr.cap_a, rcnt, rlist,
-                                            arr.in_cap, arr.n, arr.Facc, arr.Facc, arr.part_f2, st, arr.precision,
-                                            sh, ctx->d_err);
-                };
-                go();
+                time_one(sh, walk, 0);           // untimed: first launch of this shape
                 float tot = 0.f;
-                for (int r = 0; r < 3; r++) {
-                    if (flush) cudaMemsetAsync(flush, r, flush_bytes, st);
-                    cudaEventRecord(e0, st);
-                    short_range();
-                    go();
-                    cudaEventRecord(e1, st);
-                    cudaEventSynchronize(e1);
-                    float ms = 0.f;
-                    cudaEventElapsedTime(&ms, e0, e1);
-                    tot += ms;
+                for (int r = 0; r < 3; r++) tot += time_one(sh, walk, r);
+                if (pruned) {
+                    float tp = 0.f;
+                    for (int r = 0; r < 2; r++) tp += time_one(sh, full, r);
+                    tot += 3.f * tp / (2.f * kPruneEvery);
                 }
                 if (tot < best) { best = tot; pick = sh; }
             }
@@ -353,7 +356,7 @@ int System::tune_lj() {
         arr.lj_shape = it->second;
     } else {
         int rc = FMD_OK;
-        const LJShape pick = pick_lj_shape(arr.in_cnt, arr.in_list, rc);
+        const LJShape pick = pick_lj_shape(false, rc);
         if (rc != FMD_OK) return rc;
         cache[key] = pick;
         arr.lj_shape = pick;
@@ -372,10 +375,14 @@ int System::tune_lj_pruned() {
         arr.lj_shape_p = it->second;
     } else {
         int rc = FMD_OK;
-        const LJShape pick = pick_lj_shape(prune.cnt, prune.list, rc);
+        const LJShape pick = pick_lj_shape(true, rc);
         if (rc != FMD_OK) return rc;
         cache[key] = pick;
         arr.lj_shape_p = pick;
+        // the trials timed the plain short-range term: F again from the
+        // system's own terms (REBO-II, the learned term, the LJ switch)
+        if (enqueue_forces(arr, ctx->stream) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "force launch failed");
+        if ((rc = ctx->sync_check("LJ launch-shape tuning")) != FMD_OK) return rc;
     }
     set_lj_blocks();
     return FMD_OK;
@@ -842,14 +849,26 @@ extern "C" int fmd_system_set_rebo2(fmd_system* s, const fmd_rebo2_knots* kn, in
         fmd::rebo2_coeffs(&kn->pcc[0][0], c.data(), c.data() + fmd::kRebo2PccCoef,
                           c.data() + fmd::kRebo2PccCoef + fmd::kRebo2TriCoef);
         if (!y.arr.rebo2.pcc) {
+            const size_t n = (size_t)y.arr.n;
             double *tab, *nc, *sw;
-            if (y.alloc(&tab, c.size(), (const double*)nullptr) || y.alloc(&nc, (size_t)y.arr.n, (const double*)nullptr) ||
-                y.alloc(&sw, (size_t)fmd::kForceBlocks * fmd::kNV, (const double*)nullptr))
+            int2 *bonds, *pairs;
+            int* counts;
+            if (y.alloc(&tab, c.size(), (const double*)nullptr) || y.alloc(&nc, n, (const double*)nullptr) ||
+                y.alloc(&sw, (size_t)fmd::kForceBlocks * fmd::kNV, (const double*)nullptr) ||
+                y.alloc(&bonds, n * y.arr.cap_b, (const int2*)nullptr) ||
+                y.alloc(&pairs, n * fmd::kRebo2SwitchPerAtom, (const int2*)nullptr) ||
+                y.alloc(&counts, 2, (const int*)nullptr))
                 return y.ctx->fail(FMD_ERR_CUDA, "fmd_system_set_rebo2: allocation failed");
-            y.arr.rebo2.pcc = tab;
-            y.arr.rebo2.pirc = tab + fmd::kRebo2PccCoef;
-            y.arr.rebo2.tcc = tab + fmd::kRebo2PccCoef + fmd::kRebo2TriCoef;
-            y.arr.rebo2.ncoord = nc;
+            fmd::Rebo2Dev& t = y.arr.rebo2;
+            t.pcc = tab;
+            t.pirc = tab + fmd::kRebo2PccCoef;
+            t.tcc = tab + fmd::kRebo2PccCoef + fmd::kRebo2TriCoef;
+            t.ncoord = nc;
+            t.bonds = bonds;
+            t.sw_pairs = pairs;
+            t.counts = counts;
+            t.sw_cap = (int)(n * fmd::kRebo2SwitchPerAtom);
+            t.err = y.ctx->d_err;
             y.arr.part_sw = sw;
         }
         if (cudaMemcpyAsync(const_cast<double*>(y.arr.rebo2.pcc), c.data(), sizeof(double) * c.size(),

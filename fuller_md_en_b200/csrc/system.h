@@ -54,7 +54,7 @@ struct System {
     int init();
     int tune_lj();
     int tune_lj_pruned();
-    LJShape pick_lj_shape(const int* rcnt, const int* rlist, int& rc);
+    LJShape pick_lj_shape(bool pruned, int& rc);
     void set_lj_blocks();
     int tune_rigid();
     int capture(bool rebuild, bool phase, bool judge = false);
