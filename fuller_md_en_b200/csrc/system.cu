@@ -366,13 +366,20 @@ int System::tune_lj() {
     return FMD_OK;
 }
 
-int System::tune_lj_pruned() {
+// run_tuner false: only a shape cached by an earlier system of the same size
+// is applied, and *pending tells whether the tuner still has to run (after
+// the first evaluation has written the pruned rows).
+int System::tune_lj_pruned(bool run_tuner, bool* pending) {
     static std::map<std::tuple<int, int, int, int, int>, LJShape> cache;
+    if (pending) *pending = false;
     if (!prune.ok || prune.delta <= 0.0 || std::getenv("FMD_LJ_SHAPE")) return FMD_OK;
     const auto key = std::make_tuple(ctx->device, arr.kind, arr.n, arr.cap_a, arr.precision);
     auto it = cache.find(key);
     if (it != cache.end()) {
         arr.lj_shape_p = it->second;
+    } else if (!run_tuner) {
+        if (pending) *pending = true;
+        return FMD_OK;
     } else {
         int rc = FMD_OK;
         const LJShape pick = pick_lj_shape(true, rc);
@@ -445,17 +452,31 @@ int System::init() {
     if (enqueue_forces(arr, st) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "force launch failed");
     if (enqueue_force_reduce(arr, st) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "reduce launch failed");
     if (enqueue_ke(arr, st) != cudaSuccess) return ctx->fail(FMD_ERR_CUDA, "kinetic launch failed");
-    int rc = ctx->sync_check("system init");
-    if (rc != FMD_OK) return rc;
-    // the first evaluation pruned the LJ rows: tune the gather over them
-    if (arr.kind != FMD_SYS_RIGID && (rc = tune_lj_pruned()) != FMD_OK) return rc;
-    initialized = true;
+    // The gather shape over the pruned rows, when an earlier system of this
+    // size has tuned it; else the tuner runs once the first evaluation has
+    // pruned the rows.
+    int rc = FMD_OK;
+    bool pending = false;
+    if (arr.kind != FMD_SYS_RIGID && (rc = tune_lj_pruned(false, &pending)) != FMD_OK) return rc;
     // Capture the four step variants now, so no host-side capture ever sits
-    // between two steps of a run.
-    if (p.use_graphs)
-        for (int r = 0; r < 2; r++)
-            for (int ph = 0; ph < 2; ph++)
-                if ((rc = capture(r != 0, ph != 0)) != FMD_OK) return rc;
+    // between two steps of a run; the host captures while the device runs
+    // the set-up work enqueued above.
+    auto capture_all = [&]() -> int {
+        if (p.use_graphs)
+            for (int r = 0; r < 2; r++)
+                for (int ph = 0; ph < 2; ph++)
+                    if ((rc = capture(r != 0, ph != 0)) != FMD_OK) return rc;
+        return FMD_OK;
+    };
+    if ((rc = capture_all()) != FMD_OK) return rc;
+    if ((rc = ctx->sync_check("system init")) != FMD_OK) return rc;
+    if (pending) {
+        // the graphs hold the launch shapes: capture again with the tuned one
+        if ((rc = tune_lj_pruned(true, nullptr)) != FMD_OK) return rc;
+        drop_graphs();
+        if ((rc = capture_all()) != FMD_OK) return rc;
+    }
+    initialized = true;
     return FMD_OK;
 }
 

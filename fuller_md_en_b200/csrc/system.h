@@ -53,7 +53,7 @@ struct System {
     bool judge_step(int g) const { return arr.sg && arr.sg->judge_every > 0 && g % arr.sg->judge_every == 0; }
     int init();
     int tune_lj();
-    int tune_lj_pruned();
+    int tune_lj_pruned(bool run_tuner, bool* pending);
     LJShape pick_lj_shape(bool pruned, int& rc);
     void set_lj_blocks();
     int tune_rigid();
