@@ -934,13 +934,15 @@ cudaError_t rebo_slots_launch(const double* pos, const double* hh, const int* cn
 namespace {
 
 // Occupied slots of a REBO list in atom-major order, packed into 32-lane
-// bins so that no atom's slots straddle a warp: per 1024-atom block one thread
+// bins so that no atom's slots straddle a warp: per 256-atom block one thread
 // places the atoms one after another, starting a new bin when an atom's slots
 // would cross one (cap <= 32), and the block's length is rounded up to whole
 // bins; a scan of the block lengths then places the blocks.  Unused lanes hold
 // -1.  Layout: ids[0] = padded length P, ids[1 .. P] slot ids or -1, then at
-// ids[1 + 32 n + t] the partner slot of slot t.
-constexpr int kIdsBlock = 1024;
+// ids[1 + 32 n + t] the partner slot of slot t.  The block size trades the
+// serial placement (one thread, 256 steps) against the padding at block ends
+// (at most 31 lanes per block, ~2 % of the lanes at 3 slots per atom).
+constexpr int kIdsBlock = 256;
 
 __global__ void __launch_bounds__(kIdsBlock) k_ids_count(const int* __restrict__ cnt, int cap, int n,
                                                           int* __restrict__ bsum, int* __restrict__ istart) {

@@ -25,6 +25,12 @@ template <class T>
 size_t dbytes(size_t count) {
     return sizeof(T) * (count > 0 ? count : 1);
 }
+
+// Runs the rebuild's cell-grid fallback (a conditional graph node) only when
+// the molecule path was rejected for this rebuild (flag[0] == 0).
+__global__ void k_fallback_cond(const int* __restrict__ flag, cudaGraphConditionalHandle cond) {
+    if (threadIdx.x == 0) cudaGraphSetConditional(cond, flag[0] == 0 ? 1u : 0u);
+}
 }  // namespace
 
 void System::drop_graphs() {
@@ -36,6 +42,10 @@ void System::drop_graphs() {
 
 void System::release() {
     drop_graphs();
+    if (side) {
+        cudaStreamDestroy(side);
+        side = nullptr;
+    }
     if (sg) sg::work_free(sg->work);
     sg.reset();
     arr.sg = nullptr;
@@ -188,10 +198,25 @@ cudaError_t System::enqueue_rebuild(cudaStream_t st) {
     }
     // Half list: the molecule path when valid for this rebuild (decided on
     // the device), else the cell-grid path; both are in the graph, gated.
+    // In a captured graph the cell-grid path sits in a conditional node that
+    // the decision switches on, so a rebuild by the molecule path launches
+    // none of its kernels.
     const int* gate = nullptr;
     if (mol.ok) {
         if ((e = mol_partners(mol, arr.pos, hh, rc_a, st)) != cudaSuccess) return e;
         gate = mol.flag;
+    }
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (mol.ok && mol.masks && (e = cudaStreamIsCapturing(st, &cs)) != cudaSuccess) return e;
+    if (cs == cudaStreamCaptureStatusActive) {
+        if ((e = enqueue_fallback_conditional(st)) != cudaSuccess) return e;
+        if ((e = mol_rows_half(mol, arr.pos, hh, rc2_a, arr.cap_a, cnt_a, list_a, dropped, st)) != cudaSuccess)
+            return e;
+        if ((e = mol_rows_incoming(mol, arr.cap_a, arr.cnt_a, arr.list_a, const_cast<int*>(arr.in_cnt),
+                                   const_cast<int*>(arr.in_list), arr.in_cap, ctx->d_err, st)) != cudaSuccess)
+            return e;
+        if (prune.ok) return lj_prune_mark(prune, st);
+        return cudaSuccess;
     }
     if ((e = cells_build(cells_a, arr.pos, arr.n, hh, rc_a, ctx->d_err, st, arr.mol_id, gate)) != cudaSuccess) return e;
     if ((e = nlist_build(cells_a, LIST_HALF, arr.pos, arr.mol_id, arr.n, hh, rc2_a, arr.cap_a, cnt_a, list_a,
@@ -216,6 +241,39 @@ cudaError_t System::enqueue_rebuild(cudaStream_t st) {
     }
     if (prune.ok) return lj_prune_mark(prune, st);     // new rows: the next evaluation prunes them
     return cudaSuccess;
+}
+
+cudaError_t System::enqueue_fallback_conditional(cudaStream_t st) {
+    cudaError_t e;
+    if (!side && (e = cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking)) != cudaSuccess) return e;
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    if ((e = cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd)) != cudaSuccess) return e;
+    if (cs != cudaStreamCaptureStatusActive) return cudaErrorStreamCaptureUnsupported;
+    cudaGraphConditionalHandle cond;
+    if ((e = cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault)) != cudaSuccess) return e;
+    k_fallback_cond<<<1, 32, 0, st>>>(mol.flag, cond);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd)) != cudaSuccess) return e;
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = cond;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    if ((e = cudaGraphAddNode(&node, g, deps, nd, &cp)) != cudaSuccess) return e;
+    if ((e = cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies)) != cudaSuccess)
+        return e;
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    if ((e = cudaStreamBeginCaptureToGraph(side, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed)) !=
+        cudaSuccess)
+        return e;
+    const cudaError_t ef = enqueue_rebuild_fallback(side);
+    cudaGraph_t got = nullptr;
+    if ((e = cudaStreamEndCapture(side, &got)) != cudaSuccess) return e;
+    return ef;
 }
 
 cudaError_t System::enqueue_rebuild_fallback(cudaStream_t st) {

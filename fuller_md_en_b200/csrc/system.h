@@ -24,6 +24,7 @@ struct System {
     double h0[9] = {0};
     int* dropped = nullptr;            // device: {list a, list b} overflow counts
     int* rebo_bsum = nullptr;          // device scratch of the REBO slot index build
+    cudaStream_t side = nullptr;       // captures the rebuild fallback's conditional body
     bool initialized = false;
     // one graph per {rebuild, cold/warm phase, judge of the learned REBO term}
     cudaGraphExec_t graphs[2][2][2] = {};
@@ -48,6 +49,9 @@ struct System {
     // enqueue_rebuild for systems whose full rows come from the candidate
     // bitmaps; replica batches run it inside a conditional graph node).
     cudaError_t enqueue_rebuild_fallback(cudaStream_t st);
+    // While st is being captured: the fallback as a conditional node that the
+    // molecule path's decision switches on only when it rejected this rebuild.
+    cudaError_t enqueue_fallback_conditional(cudaStream_t st);
     cudaError_t enqueue_variant(bool rebuild, bool phase, cudaStream_t st, bool judge = false);
     cudaError_t enqueue_one(int g, cudaStream_t st);
     bool judge_step(int g) const { return arr.sg && arr.sg->judge_every > 0 && g % arr.sg->judge_every == 0; }
