@@ -456,8 +456,10 @@ k_rebo2_scan(const double* __restrict__ pos, const double* __restrict__ hh, cons
 }
 
 // One thread per bond of the compacted list: the bond's energy, and forces
-// and virial of its gradient.
-__global__ void __launch_bounds__(128)
+// and virial of its gradient.  Capped at 128 registers (4 blocks per SM; some
+// spill to L1): the uncapped kernel held 254 registers at 7 warps per SM and
+// took 123 us at nc = 5, the capped one 97 us.
+__global__ void __launch_bounds__(128, 4)
 k_rebo2_bonds(const double* __restrict__ pos, const double* __restrict__ hh, const int* __restrict__ cnt,
               const int* __restrict__ list, int cap, Rebo2Dev t, double* __restrict__ F, double* __restrict__ part) {
     FMD_PDL_WAIT();
