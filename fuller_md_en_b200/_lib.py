@@ -131,6 +131,8 @@ _SIGS = {
     "fmd_system_init": (c_int, [c_void_p]),
     "fmd_system_run": (c_int, [c_void_p, c_int, c_int, POINTER(Obs)]),
     "fmd_system_enqueue": (c_int, [c_void_p, c_int, c_int]),
+    "fmd_system_enqueue_obs": (c_int, [c_void_p, c_int, c_int, c_void_p]),
+    "fmd_system_wait_obs": (c_int, [c_void_p, c_int]),
     "fmd_system_averages": (c_int, [c_void_p, POINTER(Avg)]),
     "fmd_system_download": (c_int, [c_void_p, _dp, _dp, _dp, _dp, _dp, POINTER(NPT)]),
     "fmd_system_lists": (c_int, [c_void_p, _ip, _ip, _ip, _ip]),

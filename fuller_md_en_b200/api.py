@@ -426,6 +426,16 @@ class System:
         """Enqueues steps first..last without synchronising."""
         self.ctx.check(self.ctx.lib.fmd_system_enqueue(self.h, first, last), "fmd_system_enqueue")
 
+    def enqueue_obs(self, first: int, last: int, addr: int) -> None:
+        """Enqueues steps first..last and an asynchronous copy of step `last`'s
+        observables (an Obs) to host address `addr` (page-locked memory lets
+        the copy overlap the next steps); wait_obs(last) completes it."""
+        self.ctx.check(self.ctx.lib.fmd_system_enqueue_obs(self.h, first, last, ctypes.c_void_p(addr)),
+                       "fmd_system_enqueue_obs")
+
+    def wait_obs(self, step: int) -> None:
+        self.ctx.check(self.ctx.lib.fmd_system_wait_obs(self.h, step), "fmd_system_wait_obs")
+
     def averages(self) -> Avg:
         a = Avg()
         self.ctx.check(self.ctx.lib.fmd_system_averages(self.h, ctypes.byref(a)), "fmd_system_averages")

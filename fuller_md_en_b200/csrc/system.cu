@@ -42,6 +42,8 @@ void System::drop_graphs() {
 
 void System::release() {
     drop_graphs();
+    for (auto& ev : obs_ev)
+        if (ev) { cudaEventDestroy(ev); ev = nullptr; }
     if (side) {
         cudaStreamDestroy(side);
         side = nullptr;
@@ -847,6 +849,30 @@ extern "C" int fmd_system_run(fmd_system* s, int first, int last, fmd_obs* obs) 
 extern "C" int fmd_system_enqueue(fmd_system* s, int first, int last) {
     if (!s) return FMD_ERR_ARG;
     return s->sys->enqueue(first, last);
+}
+
+extern "C" int fmd_system_enqueue_obs(fmd_system* s, int first, int last, fmd_obs* obs) {
+    if (!s || !s->sys || !obs) return FMD_ERR_ARG;
+    fmd::System& y = *s->sys;
+    int rc = y.enqueue(first, last);
+    if (rc != FMD_OK) return rc;
+    cudaEvent_t& ev = y.obs_ev[last & 1];
+    if (!ev && cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess)
+        return y.ctx->fail(FMD_ERR_CUDA, "fmd_system_enqueue_obs: event creation failed");
+    if (cudaMemcpyAsync(obs, &y.arr.S->obs, sizeof(fmd_obs), cudaMemcpyDeviceToHost, y.ctx->stream) != cudaSuccess ||
+        cudaEventRecord(ev, y.ctx->stream) != cudaSuccess)
+        return y.ctx->fail(FMD_ERR_CUDA, "fmd_system_enqueue_obs: copy failed");
+    return FMD_OK;
+}
+
+extern "C" int fmd_system_wait_obs(fmd_system* s, int step) {
+    if (!s || !s->sys) return FMD_ERR_ARG;
+    fmd::System& y = *s->sys;
+    cudaEvent_t ev = y.obs_ev[step & 1];
+    if (!ev) return y.ctx->fail(FMD_ERR_STATE, "fmd_system_wait_obs: no copy enqueued for this step");
+    const cudaError_t e = cudaEventSynchronize(ev);
+    if (e != cudaSuccess) return y.ctx->fail(FMD_ERR_CUDA, std::string("fmd_system_wait_obs: ") + cudaGetErrorString(e));
+    return FMD_OK;
 }
 
 extern "C" int fmd_system_averages(fmd_system* s, fmd_avg* avg) {

@@ -25,6 +25,7 @@ struct System {
     int* dropped = nullptr;            // device: {list a, list b} overflow counts
     int* rebo_bsum = nullptr;          // device scratch of the REBO slot index build
     cudaStream_t side = nullptr;       // captures the rebuild fallback's conditional body
+    cudaEvent_t obs_ev[2] = {};        // fmd_system_enqueue_obs: copies of odd / even last steps
     bool initialized = false;
     // one graph per {rebuild, cold/warm phase, judge of the learned REBO term}
     cudaGraphExec_t graphs[2][2][2] = {};

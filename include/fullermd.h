@@ -302,6 +302,14 @@ int fmd_system_run(fmd_system *s, int first, int last, fmd_obs *obs);
  * returns without synchronising (errors surface at the next synchronising
  * call). */
 int fmd_system_enqueue(fmd_system *s, int first, int last);
+/* As fmd_system_enqueue, then an asynchronous copy of the observables of
+ * step `last` into *obs (host memory; page-locked for the copy to run without
+ * a host round trip), so a caller can enqueue the next steps before it reads
+ * these: the copy is complete once fmd_system_wait_obs(s, last) returns.  The
+ * completion marks alternate by the parity of `last`: at most two copies may
+ * be waited for at once.  Errors surface at the next synchronising call. */
+int fmd_system_enqueue_obs(fmd_system *s, int first, int last, fmd_obs *obs);
+int fmd_system_wait_obs(fmd_system *s, int step);
 int fmd_system_averages(fmd_system *s, fmd_avg *avg);
 /* Copies the state to host arrays (any may be NULL). */
 int fmd_system_download(fmd_system *s, double *pos, double *vel, double *qv, double *omg,

@@ -8,6 +8,8 @@ pressures to 1e-6 GPa absolute (pressure is a small difference of large
 terms near 0 GPa), and the neighbour lists at the last rebuild bit for bit."""
 from __future__ import annotations
 
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -232,3 +234,42 @@ def test_rigid_site_pair_count(ctx):
             want += int(np.count_nonzero((d * d).sum(axis=2) < rc2))
     assert got == want and got > 0
     sysd.close()
+
+
+def test_pipelined_observables_match_synchronous_runs(ctx):
+    """fmd_system_enqueue_obs / _wait_obs: each step's observables copied
+    behind its step and read while the next step runs are those that
+    fmd_system_run returns step by step."""
+    from fuller_md_en_b200._lib import Obs
+    s = crystal.atomistic(2, jitter=0.02, seed=5, T=300.0)
+    na = s["pos"].size // 3
+
+    def make():
+        cfg = RunConfig(dt=0.5, T=300.0, Pe=0.0, nsteps=100, nlup=5, nc=2, nmol=s["nmol"], use_graphs=1)
+        y = System.airebo(ctx, cfg, s["pos"], s["vel"], s["mass"], s["mol_id"], s["h"],
+                          crystal.npt_atom(300.0, 0.0, na))
+        y.init()
+        return y
+
+    a, b = make(), make()
+    try:
+        ref = [a.run(g, g) for g in range(1, 13)]
+        bufs = [Obs(), Obs()]
+        got, prev = [], None
+        for g in range(1, 13):
+            b.enqueue_obs(g, g, ctypes.addressof(bufs[g & 1]))
+            if prev is not None:
+                b.wait_obs(prev)
+                o = bufs[prev & 1]
+                got.append((o.step, o.T, o.P, o.KE))
+            prev = g
+        b.wait_obs(prev)
+        o = bufs[prev & 1]
+        got.append((o.step, o.T, o.P, o.KE))
+        for r, (st, T, P, KE) in zip(ref, got):
+            assert st == r.step
+            for x, y in ((T, r.T), (P, r.P), (KE, r.KE)):
+                assert abs(x - y) <= 1e-9 * max(1.0, abs(y)), (st, x, y)
+    finally:
+        a.close()
+        b.close()
