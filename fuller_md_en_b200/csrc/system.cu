@@ -518,14 +518,16 @@ int System::init() {
     int rc = FMD_OK;
     bool pending = false;
     if (arr.kind != FMD_SYS_RIGID && (rc = tune_lj_pruned(false, &pending)) != FMD_OK) return rc;
-    // Capture the four step variants now, so no host-side capture ever sits
-    // between two steps of a run; the host captures while the device runs
-    // the set-up work enqueued above.
+    // Capture the step variants the schedule can reach (the cold/warm phase
+    // ones only with coldstart + warmup > 0) now, so no host-side capture
+    // ever sits between two steps of a run; the host captures while the
+    // device runs the set-up work enqueued above.
     auto capture_all = [&]() -> int {
         if (p.use_graphs)
             for (int r = 0; r < 2; r++)
                 for (int ph = 0; ph < 2; ph++)
-                    if ((rc = capture(r != 0, ph != 0)) != FMD_OK) return rc;
+                    if ((ph == 0 || p.coldstart + p.warmup > 0) && (rc = capture(r != 0, ph != 0)) != FMD_OK)
+                        return rc;
         return FMD_OK;
     };
     if ((rc = capture_all()) != FMD_OK) return rc;
