@@ -153,3 +153,14 @@ def test_switch_vanishes_beyond_its_range(oracle):
     cr, lr, cl, ll = lists(oracle, s)
     K = oracle_knots(random_knots(2))
     assert oracle.lj_switch_energy(s["pos"], s["h"], s["hi"], cr, lr, cl, ll, s["na"], K) == 0.0
+
+
+def test_coefficient_builder_rejects_null_arguments():
+    from fuller_md_en_b200 import _lib
+    lib = _lib.load()
+    out = np.zeros(16 + 2 * 9216)
+    raw = Rebo2Knots().raw()
+    assert lib.fmd_rebo2_coeffs(None, out.ctypes.data_as(_lib._dp)) == _lib.FMD_ERR_ARG
+    assert lib.fmd_rebo2_coeffs(ctypes.byref(raw), None) == _lib.FMD_ERR_ARG
+    assert lib.fmd_rebo2_coeffs(ctypes.byref(raw), out.ctypes.data_as(_lib._dp)) == _lib.FMD_OK
+    assert not np.any(out), "zero knots give zero coefficients"
