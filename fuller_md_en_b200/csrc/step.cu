@@ -3,15 +3,16 @@
 // (a19: LJ:847-897, AI:871-912, MM:1192-1236).
 //
 // The reference keeps xi, Vg and h on the host and synchronises several
-// times per step.  Here they live in a device struct (SysScal) updated by
-// single-thread "scalar" kernels, so a whole step -- and a list rebuild -- is
+// times per step.  Here they live in a device struct (SysScal) updated on the
+// device, so a whole step -- and a list rebuild -- is
 // a fixed sequence of launches with no host round trip, which is what lets
 // the step be replayed as a CUDA graph:
 //
-//   k_begin     schedule (Tt ramp, cold resets), thermostat/barostat first
-//               half, scaling factors, cell update and its inverse
-//   k_kick      first half-kick, drift in fractional coordinates, wrap,
-//               back to Cartesian with the new cell (+ quaternion update)
+//   k_begin_kick  schedule (Tt ramp, cold resets), thermostat/barostat
+//               first half, scaling factors, cell update and its inverse
+//               (every block on its own copy of the scalars), then the first
+//               half-kick, drift in fractional coordinates, wrap, back to
+//               Cartesian with the new cell (+ quaternion update)
 //   forces      (airebo.cu / rigid.cu / mm.cu)
 //   k_kick2_end second half-kick with per-block kinetic partials; the last
 //               block to finish: force/kinetic reductions (fixed order),
@@ -92,12 +93,6 @@ __device__ void begin_body(SysScal* S, int kind, const StepParams& p) {
 
 namespace {
 
-__global__ void k_begin(SysScal* S, int kind, StepParams p) {
-    FMD_PDL_WAIT();
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    begin_body(S, kind, p);
-}
-
 // LJ:166-174.  The reference multiplies q by the rotation increment on the
 // right (q dq), which applies the lab-frame angular velocity as a body-frame
 // one; left (dq q, FMD_PHYS_QUAT) rotates the lab-frame sites about the lab
@@ -126,8 +121,8 @@ __device__ __forceinline__ void quat_step(double* q, double wx, double wy, doubl
 
 }  // namespace
 
-__device__ void kick_body(const StepArrays& a, double dt, int blk, int nblk) {
-    const SysScal* S = a.S;
+__device__ void kick_body(const StepArrays& a, double dt, int blk, int nblk, const SysScal* sc = nullptr) {
+    const SysScal* S = sc ? sc : a.S;
     const double hdt = 0.5 * dt, sc_v = S->sc_v, sc_nh = S->sc_nh;
     const double* hi = S->hi_old;
     const double* h = S->h;
@@ -213,9 +208,31 @@ __device__ void kick2_body(const StepArrays& a, double dt, int blk, int nblk, do
 
 namespace {
 
-__global__ void __launch_bounds__(kPB) k_kick(StepArrays a, double dt) {
+// The start of a step and the first half-kick with drift in one launch: every
+// block copies the step scalars into shared memory and runs the thermostat,
+// barostat and cell update on its copy (the same arithmetic on the same
+// inputs, so every copy is the same), kicks and drifts its particles with
+// them and takes a ticket; the last block, once every block has read the old
+// scalars, writes its copy back and so resets the ticket.
+__global__ void __launch_bounds__(kPB) k_begin_kick(StepArrays a, StepParams p) {
     FMD_PDL_WAIT();
-    kick_body(a, dt, blockIdx.x, gridDim.x);
+    __shared__ SysScal sS;
+    __shared__ bool last;
+    static_assert(sizeof(SysScal) % sizeof(int) == 0, "SysScal copied as words");
+    constexpr int kWords = sizeof(SysScal) / sizeof(int);
+    const int* src = reinterpret_cast<const int*>(a.S);
+    int* dst = reinterpret_cast<int*>(&sS);
+    for (int k = threadIdx.x; k < kWords; k += blockDim.x) dst[k] = src[k];
+    __syncthreads();
+    if (threadIdx.x == 0) begin_body(&sS, a.kind, p);
+    __syncthreads();
+    kick_body(a, p.dt, blockIdx.x, gridDim.x, &sS);
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(&a.S->kick_done, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    int* out = reinterpret_cast<int*>(a.S);
+    for (int k = threadIdx.x; k < kWords; k += blockDim.x) out[k] = dst[k];   // kick_done: 0 again
 }
 
 __global__ void __launch_bounds__(kPB) k_ke_partial(StepArrays a) {
@@ -586,8 +603,7 @@ cudaError_t enqueue_step(const StepArrays& a, const StepParams& p, bool rescale_
     // previous one's tail (pdl.cuh)
     // per-particle kernels: one thread per particle (grid-stride beyond kForceBlocks)
     const int pblocks = std::max(1, std::min(kForceBlocks, (a.n + kPB - 1) / kPB));
-    if ((e = launch_pdl(k_begin, dim3(1), dim3(32), 0, st, a.S, a.kind, p)) != cudaSuccess) return e;
-    if ((e = launch_pdl(k_kick, dim3(pblocks), dim3(kPB), 0, st, a, p.dt)) != cudaSuccess) return e;
+    if ((e = launch_pdl(k_begin_kick, dim3(pblocks), dim3(kPB), 0, st, a, p)) != cudaSuccess) return e;
     if ((e = enqueue_forces(a, st, judge)) != cudaSuccess) return e;
     if ((e = launch_pdl(k_kick2_end, dim3(pblocks), dim3(kPB), 0, st, a, p, force_partial_blocks(a))) != cudaSuccess)
         return e;

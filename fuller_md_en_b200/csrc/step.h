@@ -27,6 +27,7 @@ struct SysScal {
     int sg_takeover;         // global step of the takeover (0: none)
     double sg_rmse_last, sg_rmse_max;
     unsigned int kick2_done; // blocks of the fused second kick done this step (the last one reduces)
+    unsigned int kick_done;  // blocks of the fused first kick done this step (the last one writes back)
 };
 
 struct SgStep;   // learned REBO term of a system (sg_host.h)
