@@ -332,9 +332,8 @@ __device__ void reduce_all(const StepArrays& a, int nblk_f1, int nblk_ke, bool f
     block_sum_store<kRedFields>(acc, sm, t);   // result valid in thread 0
 }
 
-// Thread 0: kinetic energies from the reduced sums.
-__device__ void kinetic_from_sums(const StepArrays& a, const double (&t)[kRedFields]) {
-    SysScal* S = a.S;
+// Thread 0: kinetic energies from the reduced sums into S (a.S or a copy).
+__device__ void kinetic_from_sums(SysScal* S, const StepArrays& a, const double (&t)[kRedFields]) {
     if (a.kind == FMD_SYS_RIGID) {
         S->kt = 0.5 * a.Mmol * t[21] / kConv;     // LJ:411
         S->kr = 0.5 * a.I0 * t[22] / kConv;       // LJ:420
@@ -344,9 +343,9 @@ __device__ void kinetic_from_sums(const StepArrays& a, const double (&t)[kRedFie
     }
 }
 
-// Thread 0: virial and energies (program grouping) from the reduced sums.
-__device__ void forces_from_sums(const StepArrays& a, const double (&t)[kRedFields]) {
-    SysScal* S = a.S;
+// Thread 0: virial and energies (program grouping) from the reduced sums
+// into S (a.S or a copy).
+__device__ void forces_from_sums(SysScal* S, const StepArrays& a, const double (&t)[kRedFields]) {
     double e[8] = {0, 0, 0, 0, 0, 0, 0, 0}, w[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     if (a.kind == FMD_SYS_RIGID) {
         e[0] = t[0];
@@ -394,11 +393,10 @@ __device__ void record(SysScal* S, int kind, const StepParams& p) {
 
 // After the LJ gather of a force evaluation (thread 0 of its reduction): when
 // that gather pruned (the same decision on the same inputs), the displacement
-// bound restarts from this step's positions and cell; counts evaluations and
-// prunes.
-__device__ void lj_prune_commit(const StepArrays& a) {
+// bound restarts from this step's positions and cell hh; counts evaluations
+// and prunes.
+__device__ void lj_prune_commit(const StepArrays& a, const double* hh) {
     if (!a.prune_hb || !(a.prune_delta > 0.0)) return;
-    const double* hh = a.S->h;
     if (lj_prune_needed(a.prune_umax, hh, a.prune_hb, a.prune_delta, a.prune_rc)) {
         *a.prune_umax = 0ull;
         for (int q = 0; q < 9; q++) a.prune_hb[q] = hh[q];
@@ -407,15 +405,13 @@ __device__ void lj_prune_commit(const StepArrays& a) {
     a.prune_stats[0] += 1ull;
 }
 
-__device__ void end_body(const StepArrays& a, const StepParams& p, int nblk_f1, int nblk_ke, int nblk_f2,
-                         double* sm) {
-    double t[kRedFields];
-    reduce_all(a, nblk_f1, nblk_ke, true, true, sm, t, nblk_f2);
-    if (threadIdx.x != 0) return;
-    lj_prune_commit(a);
-    forces_from_sums(a, t);
-    kinetic_from_sums(a, t);
-    SysScal* S = a.S;
+// Thread 0 of the step end: prune commit, energies, virial and kinetic
+// energy from the reduced sums, the thermostat/barostat second half and the
+// driver's observables, on the scalars S.
+__device__ void end_scalars(const StepArrays& a, const StepParams& p, const double (&t)[kRedFields], SysScal* S) {
+    lj_prune_commit(a, S->h);
+    forces_from_sums(S, a, t);
+    kinetic_from_sums(S, a, t);
     const double hdt = 0.5 * p.dt;
     const bool rigid = a.kind == FMD_SYS_RIGID;
     const double V2 = fabs(det9(S->h));
@@ -437,6 +433,29 @@ __device__ void end_body(const StepArrays& a, const StepParams& p, int nblk_f1, 
     if (!phase) record(S, a.kind, p);
 }
 
+// The end of a step in one block: the step scalars are copied into shared
+// memory (sS) while the partial records are reduced, thread 0 runs the
+// scalar end on that copy (shared-memory latency on its serial chain instead
+// of global), and the block writes the copy back with the block ticket
+// kick2_done reset.  No other block reads the scalars meanwhile.
+__device__ void end_body(const StepArrays& a, const StepParams& p, int nblk_f1, int nblk_ke, int nblk_f2,
+                         double* sm, SysScal* sS) {
+    static_assert(sizeof(SysScal) % sizeof(int) == 0, "SysScal copied as words");
+    constexpr int kWords = sizeof(SysScal) / sizeof(int);
+    int* gS = reinterpret_cast<int*>(a.S);
+    int* cS = reinterpret_cast<int*>(sS);
+    for (int k = threadIdx.x; k < kWords; k += blockDim.x) cS[k] = __ldcg(gS + k);
+    __syncthreads();
+    double t[kRedFields];
+    reduce_all(a, nblk_f1, nblk_ke, true, true, sm, t, nblk_f2);
+    if (threadIdx.x == 0) {
+        end_scalars(a, p, t, sS);
+        sS->kick2_done = 0u;
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < kWords; k += blockDim.x) gS[k] = cS[k];
+}
+
 __device__ void rescale_end_body(const StepArrays& a, const StepParams& p, int nblk_ke, double* sm) {
     SysScal* S = a.S;
     const bool doit = S->do_rescale != 0;
@@ -444,7 +463,7 @@ __device__ void rescale_end_body(const StepArrays& a, const StepParams& p, int n
     if (doit) reduce_all(a, 0, nblk_ke, false, true, sm, t, 0);
     if (threadIdx.x != 0) return;
     if (doit) {
-        kinetic_from_sums(a, t);
+        kinetic_from_sums(S, a, t);
         S->Tn = inst_T(S->KE, S->npt.Nf);
         S->npt.xi = 0;
         if (S->gstep <= p.coldstart)
@@ -462,6 +481,7 @@ namespace {
 __global__ void __launch_bounds__(kPB) k_kick2_end(StepArrays a, StepParams p, int nblk_f1) {
     FMD_PDL_WAIT();
     __shared__ double sm[32 * kRedFields];
+    __shared__ SysScal sS;
     __shared__ bool last;
     kick2_body(a, p.dt, blockIdx.x, gridDim.x, sm);
     __threadfence();                      // this block's partial before its ticket
@@ -469,8 +489,7 @@ __global__ void __launch_bounds__(kPB) k_kick2_end(StepArrays a, StepParams p, i
     __syncthreads();
     if (!last) return;
     __threadfence();
-    end_body(a, p, nblk_f1, gridDim.x, a.lj_blocks, sm);
-    if (threadIdx.x == 0) a.S->kick2_done = 0u;
+    end_body(a, p, nblk_f1, gridDim.x, a.lj_blocks, sm, &sS);   // resets kick2_done
 }
 
 __global__ void __launch_bounds__(kRedThreads) k_rescale_end(StepArrays a, StepParams p, int nblk_ke) {
@@ -483,7 +502,7 @@ __global__ void __launch_bounds__(kRedThreads) k_ke_final(StepArrays a, int nblk
     __shared__ double sm[32 * kRedFields];
     double t[kRedFields];
     reduce_all(a, 0, nblk_ke, false, true, sm, t, 0);
-    if (threadIdx.x == 0) kinetic_from_sums(a, t);
+    if (threadIdx.x == 0) kinetic_from_sums(a.S, a, t);
 }
 
 // ---- replica batch: each single-system kernel once over all replicas ----
@@ -512,9 +531,10 @@ __global__ void __launch_bounds__(kPB) k_b_rescale(BatchDev b) {
 
 __global__ void __launch_bounds__(256) k_b_end(BatchDev b) {
     __shared__ double sm[32 * kRedFields];
+    __shared__ SysScal sS;
     const int r = blockIdx.x;
     end_body(b.A[r], b.P[r], b.off_f1[r + 1] - b.off_f1[r], b.off_atom[r + 1] - b.off_atom[r],
-             b.off_lj[r + 1] - b.off_lj[r], sm);
+             b.off_lj[r + 1] - b.off_lj[r], sm, &sS);
 }
 
 __global__ void __launch_bounds__(256) k_b_rescale_end(BatchDev b) {
@@ -528,8 +548,8 @@ __global__ void __launch_bounds__(kRedThreads) k_force_final(StepArrays a, int n
     double t[kRedFields];
     reduce_all(a, nblk_f1, 0, true, false, sm, t, a.lj_blocks);
     if (threadIdx.x == 0) {
-        forces_from_sums(a, t);
-        lj_prune_commit(a);
+        forces_from_sums(a.S, a, t);
+        lj_prune_commit(a, a.S->h);
     }
 }
 
