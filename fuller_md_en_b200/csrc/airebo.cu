@@ -601,16 +601,29 @@ __device__ __forceinline__ void lj_chunk(const int (&jc)[U], const double (&cx)[
     }
 }
 
-// End of atom i's row: F[i] = Facc[i] + the warp's sum (Facc cleared), and for
-// a pruning gather the pruned row's length and i's fractional position.
+// Facc[i] for lj_atom_done, read by lane 0 when the atom's row starts so the
+// load is not on the row's tail.
+struct LJAcc {
+    double x = 0.0, y = 0.0, z = 0.0;
+};
+__device__ __forceinline__ LJAcc lj_acc_load(const double* __restrict__ Facc, int i, int lane) {
+    LJAcc a;
+    if (lane == 0) { a.x = Facc[3 * i]; a.y = Facc[3 * i + 1]; a.z = Facc[3 * i + 2]; }
+    return a;
+}
+
+// End of atom i's row: F[i] = Facc[i] (fa, read at the row's start) + the
+// warp's sum (Facc cleared), and for a pruning gather the pruned row's length
+// and i's fractional position.
 __device__ __forceinline__ void lj_atom_done(int i, double fx, double fy, double fz, double px, double py,
                                              double pz, const double* hi, double* __restrict__ F,
-                                             double* __restrict__ Facc, const LJPruneOut& po, int pc, int lane) {
+                                             double* __restrict__ Facc, const LJPruneOut& po, int pc, int lane,
+                                             const LJAcc& fa) {
     fx = warp_sum(fx); fy = warp_sum(fy); fz = warp_sum(fz);
     if (lane == 0) {
-        F[3 * i] = Facc[3 * i] + fx;
-        F[3 * i + 1] = Facc[3 * i + 1] + fy;
-        F[3 * i + 2] = Facc[3 * i + 2] + fz;
+        F[3 * i] = fa.x + fx;
+        F[3 * i + 1] = fa.y + fy;
+        F[3 * i + 2] = fa.z + fz;
         if (Facc != F) { Facc[3 * i] = 0.0; Facc[3 * i + 1] = 0.0; Facc[3 * i + 2] = 0.0; }
         if (po.cnt) {
             po.cnt[i] = pc;
@@ -663,6 +676,7 @@ __device__ __forceinline__ void lj_gather_body(const double* __restrict__ pos, c
     const AtomRange ar = atom_range(blk, nblk, wpb, threadIdx.x >> 5, na, contig);
     for (int i = ar.first; i < ar.end; i += ar.step) {
         const double px = pos[3 * i], py = pos[3 * i + 1], pz = pos[3 * i + 2];
+        const LJAcc fa = lj_acc_load(Facc, i, lane);
         double fx = 0.0, fy = 0.0, fz = 0.0;
         const int tot = min(in_cnt[i], in_cap);
         const int* row = in_list + (size_t)i * in_cap;
@@ -684,7 +698,7 @@ __device__ __forceinline__ void lj_gather_body(const double* __restrict__ pos, c
             lj_chunk<FULL_VIRIAL, F32, U>(jc, cx, cy, cz, i, px, py, pz, h, hi, diag, wide, p, pf, fx, fy, fz, acc, po,
                                           prow, pc, lane);
         }
-        lj_atom_done(i, fx, fy, fz, px, py, pz, hi, F, Facc, po, pc, lane);
+        lj_atom_done(i, fx, fy, fz, px, py, pz, hi, F, Facc, po, pc, lane, fa);
     }
     lj_virial_mirror<FULL_VIRIAL>(acc);
     block_sum_store<kNV>(acc, sm, part + (size_t)blk * kNV);
@@ -796,6 +810,7 @@ __device__ __forceinline__ void lj_gather_staged_body(const double* __restrict__
         const int* row = bufs + (size_t)cur * in_cap;
         const int tot = min(in_cnt[i], in_cap);
         const double px = pos[3 * i], py = pos[3 * i + 1], pz = pos[3 * i + 2];
+        const LJAcc fa = lj_acc_load(Facc, i, lane);
         double fx = 0.0, fy = 0.0, fz = 0.0;
         int* prow = po.cnt ? po.list + (size_t)i * in_cap : nullptr;
         int pc = 0;
@@ -813,7 +828,7 @@ __device__ __forceinline__ void lj_gather_staged_body(const double* __restrict__
             lj_chunk<FULL_VIRIAL, F32, U>(jc, cx, cy, cz, i, px, py, pz, h, hi, diag, wide, p, pf, fx, fy, fz, acc, po,
                                           prow, pc, lane);
         }
-        lj_atom_done(i, fx, fy, fz, px, py, pz, hi, F, Facc, po, pc, lane);
+        lj_atom_done(i, fx, fy, fz, px, py, pz, hi, F, Facc, po, pc, lane, fa);
         __syncwarp();                           // buffer cur is reused two atoms on
         cur ^= 1;
         pending = false;
