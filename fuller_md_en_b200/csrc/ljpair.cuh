@@ -79,7 +79,8 @@ struct LJF {
 // One listed pair seen from atom i: d = r_j - r_i after the minimum image.
 // The cutoff test is the reference's FP64 one in both precisions, so both
 // modes interact through exactly the reference's pair set.  FP64: the
-// reference's arithmetic (AI:447-466).  FP32: the pair algebra (1/r^2, s^6,
+// reference's pair terms (AI:443-466) in the factored form below, equal to a
+// few ulp.  FP32: the pair algebra (1/r^2, s^6,
 // s^12, fm) in FP32; the minimum image, r^2, the force, energy and virial
 // accumulation stay FP64.  COUNT: this side counts energy and virial.
 // FULL_VIRIAL (AIREBO's vir9, AI:455-466): the pair tensor d fm d^T is
