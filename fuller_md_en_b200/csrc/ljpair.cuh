@@ -1,7 +1,7 @@
 // ljpair.cuh -- the shifted 12-6 LJ pair of the AIREBO and MM programs
-// (AI:119-124, 441-446; MM:113-116), the exact diagonal-cell minimum image
-// and the FP64 reciprocal shared by the list gather (airebo.cu) and the
-// molecule-tile kernel (ljtile.cu).
+// (AI:119-124, 441-446; MM:113-116) and the exact diagonal-cell minimum
+// image, used by the list gathers (airebo.cu); the switched-LJ correction
+// (rebo2.cu) takes the pair constants from here.
 #pragma once
 #include <cmath>
 #include "geom.cuh"
@@ -56,18 +56,6 @@ __device__ __forceinline__ double mimg1_rint(double d, double hii, double hii_in
     return __dmul_rn(hii, __dsub_rn(s, rint(s)));
 }
 
-// 1/x for x in the FP32 normal range: the hardware's FP64 reciprocal
-// approximation refined by one third-order step y + y (e + e^2),
-// e = 1 - x y (the series of 1/(1 - e) to second order), which cubes its
-// error: 2.2e-16 relative at most over the LJ gather's r^2 in [0.25, 110]
-// (measured on B200), in place of a full IEEE division.
-__device__ __forceinline__ double rcp_nr(double x) {
-    double y;
-    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-    const double e = fma(-x, y, 1.0);
-    return fma(y, fma(e, e, e), y);
-}
-
 // FP32 copies of the pair constants (FP32-pair precision).  sigma^2 is kept
 // as a head + tail pair: its FP32 rounding would scale every s^6 by the same
 // factor, a bias that the near-cancelling repulsive and attractive virial
@@ -80,9 +68,9 @@ struct LJF {
 // The cutoff test is the reference's FP64 one in both precisions, so both
 // modes interact through exactly the reference's pair set.  FP64: the
 // reference's pair terms (AI:443-466) in the factored form below, equal to a
-// few ulp.  FP32: the pair algebra (1/r^2, s^6,
-// s^12, fm) in FP32; the minimum image, r^2, the force, energy and virial
-// accumulation stay FP64.  COUNT: this side counts energy and virial.
+// few ulp.  FP32: the pair algebra (1/r^2, s^6, s^12, fm) in FP32; the
+// minimum image, r^2, the force, energy and virial accumulation stay FP64.
+// COUNT: this side counts energy and virial.
 // FULL_VIRIAL (AIREBO's vir9, AI:455-466): the pair tensor d fm d^T is
 // symmetric, so only its six distinct entries are accumulated, in acc[1],
 // acc[2], acc[3], acc[5], acc[6], acc[9] (row-major W at acc[1..9]);
@@ -105,6 +93,10 @@ __device__ __forceinline__ void lj_pair(double dx, double dy, double dz, const L
         // with s^2 = sigma^2 / r^2 formed from the reciprocal approximation y
         // and its refinement c directly (sigma^2 y (1 + c)): the same values
         // to a few ulp, by a dependency chain four operations shorter.
+        // 1/r^2 = y (1 + c), c = e + e^2, e = 1 - r^2 y: one third-order step
+        // (the series of 1/(1 - e) to second order) cubes the approximation's
+        // error, 2.2e-16 relative at most over r^2 in [0.25, 110] (measured on
+        // B200), in place of a full IEEE division.
         double y;
         asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(r2));
         const double e0 = fma(-r2, y, 1.0), c = fma(e0, e0, e0);
