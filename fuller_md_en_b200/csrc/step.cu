@@ -433,8 +433,8 @@ __device__ void end_scalars(const StepArrays& a, const StepParams& p, const doub
     if (!phase) record(S, a.kind, p);
 }
 
-// The end of a step in one block: the step scalars are copied into shared
-// memory (sS) while the partial records are reduced, thread 0 runs the
+// The end of a step in one block: the block copies the step scalars into
+// shared memory (sS) and reduces the partial records, thread 0 runs the
 // scalar end on that copy (shared-memory latency on its serial chain instead
 // of global), and the block writes the copy back with the block ticket
 // kick2_done reset.  No other block reads the scalars meanwhile.
